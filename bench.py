@@ -1,0 +1,391 @@
+#!/usr/bin/env python
+"""Throughput of mfa's per-timestep force and integration loop on B200.
+
+Metric: bead-steps/s (beads x time steps / second), mixed precision (FP32 pair
+and bond forces, FP64 positions / velocity Verlet / reductions), with the plain
+FP64 GPU path reported beside it.
+
+Workload (default): polymer brush with explicit solvent -- 32 x 32 chains of 64
+beads end-grafted on a square lattice at 0.3 sigma^-2 (Lx = Ly = 58.42), 9-3
+walls at z = 0 and 60 (cutoff 2.5), FENE k = 30 R0 = 1.5, bending k_b = 2,
+WCA everywhere, solvent to total density 0.85 (174,080 beads), DPD gamma = 4.5
+kT = 1, dt = 0.005, skin 0.3.  Synthetic seeded configuration; one replica per
+GPU (weak scaling, no data exchange between ranks).
+
+Timing: W untimed warm-up steps; K timed steps, each bracketed by CUDA events on
+the context's stream, with L2 flushed (a 256 MiB write on the same stream)
+between timed steps; barrier + synchronize around the loop; max over ranks.
+`e2e` is the same metric through the public API with host buffers: the initial
+state uploaded from pinned host memory, every step followed by a device->host
+read of the step's energies, the final state downloaded.
+
+--impl reference runs the CPU restatement of the reference's loop (serial, one
+core, like the Fortran program) on the same workload.
+"""
+import argparse
+import json
+import os
+import platform
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "bead-steps/s"
+
+
+def args_():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="brush", choices=["brush", "melt", "charged"])
+    ap.add_argument("--equil", type=int, default=2000, help="untimed relaxation steps of the fresh configuration")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--seed", type=int, default=2024)
+    return ap.parse_args()
+
+
+def make_config(name, seed):
+    from mfa_b200 import configs
+    if name == "brush":
+        return configs.brush(seed=seed), {
+            "workload": "brush_explicit_solvent_32x32x64", "chains": "32x32", "n_mon": 64,
+            "grafting_density": 0.3, "wall_gap": 60.0, "solvent_density": 0.85}
+    if name == "melt":
+        return configs.melt(seed=seed), {"workload": "melt_100x32", "chains": 100, "n_mon": 32}
+    return configs.charged(seed=seed), {"workload": "polyelectrolyte_200x50_ewald", "chains": 200,
+                                         "n_mon": 50, "n_kmax": 10}
+
+
+def cpu_info():
+    model = platform.processor()
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return model, os.cpu_count()
+
+
+def run_oracle(cfg, seconds, max_steps, warm=2):
+    """The CPU restatement (serial, like the reference) on the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle
+    o = Oracle(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, list_cap=512, rng_mode=1)
+    o.init_forces()
+    for _ in range(warm):
+        o.md_step()
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < max_steps and (time.perf_counter() - t0) < seconds:
+        o.md_step()
+        steps += 1
+    dt = time.perf_counter() - t0
+    return cfg.n * steps / dt, steps, dt
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the loop runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu_id), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for nm, flag in zip(names, parts[4:8]):
+                if flag.lower().startswith("active"):
+                    reasons.add(nm)
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def pair_work(g, cfg):
+    """Counts behind the algorithmic figures of one pair-kernel launch: listed
+    half-pairs, in-cutoff half-pairs and the sum of list rows."""
+    import numpy as np
+    from mfa_b200 import _abi
+    p = cfg.params
+    st = g.download(_abi.R0)
+    cell, cnt, nbr = g.debug_lists(int(g.scalars()["max_neigh"]) + 1)
+    r = st["r0"]
+    t = cfg.a_type
+    ii = np.repeat(np.arange(cfg.n), cnt)
+    jj = nbr[np.arange(nbr.shape[1])[None, :] < cnt[:, None]] - 1
+    d = r[ii] - r[jj]
+    for k in range(3):
+        if k < 2 or p.symmetry == 1:
+            L = p.boundary[k]
+            d[:, k] -= L * np.trunc(2.0 * d[:, k] / L)
+    r2 = (d * d).sum(1)
+    rc2 = np.array(p.range_2[:]).reshape(8, 8)[t[ii] - 1, t[jj] - 1]
+    inside = int((r2 < rc2).sum())
+    return {"listed_half_pairs": int(cnt.sum()) // 2, "incut_half_pairs": inside // 2,
+            "list_entries": int(cnt.sum())}
+
+
+def main():
+    a = args_()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if a.impl == "reference":
+        if rank != 0:
+            return 0
+        cfg, meta = make_config(a.workload, a.seed)
+        # each step is one full time step of the workload; the run is capped at
+        # about two minutes of CPU time (the step count reported is what ran)
+        rate, steps, dt = run_oracle(cfg, seconds=120.0, max_steps=a.steps, warm=min(a.warmup, 3))
+        model, ncpu = cpu_info()
+        line = {
+            "impl": "reference", "metric": METRIC, "value": rate, "unit": METRIC, "n_gpus": a.gpus,
+            "steps": steps, "warmup": a.warmup, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(meta, beads=cfg.n, dt=cfg.params.dt, skin=cfg.params.skin),
+            "cpu_baseline": {"value": rate, "unit": METRIC, "cores": 1, "kind": "port",
+                             "sample": f"{steps} full time steps of the {cfg.n}-bead workload, serial C restatement "
+                                       f"of the Fortran loop on 1 core ({model}, {ncpu} host threads)"},
+            "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return 0
+
+    import numpy as np
+    import torch
+    from mfa_b200 import _abi
+    from mfa_b200.api import System
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    dev = local
+    torch.cuda.set_device(dev)
+    cfg, meta = make_config(a.workload, a.seed + rank)
+    n = cfg.n
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
+
+    def timed_run(prec, steps, warmup, flush_l2=True):
+        g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=prec, device=dev)
+        if cfg.params.charged:
+            g.ewald_k(0)
+        g.init_forces()
+        if a.equil:
+            g.step(a.equil)
+        ext = torch.cuda.ExternalStream(g.stream_ptr(), device=f"cuda:{dev}")
+        for k in range(warmup):
+            with torch.cuda.stream(ext):
+                flush.fill_(k & 0xff)
+            g.step(1)
+        g.sync()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        launches0 = g.scalars()["kernel_launches"]
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        sampler = ClockSampler(dev)
+        sampler.start()
+        for k in range(steps):
+            if flush_l2:
+                with torch.cuda.stream(ext):
+                    flush.fill_(k & 0xff)
+            ev[k][0].record(ext)
+            g.step(1)
+            ev[k][1].record(ext)
+        g.sync()
+        torch.cuda.synchronize(dev)
+        clocks = sampler.stop()
+        if dist is not None:
+            dist.barrier()
+        ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
+        s = g.scalars()
+        return g, ms, s["kernel_launches"] - launches0, clocks, s
+
+    # headline: mixed precision
+    g, ms_mixed, launches, clocks, s_mixed = timed_run(_abi.MIXED, a.steps, a.warmup)
+    ms_max = ms_mixed
+    if dist is not None:
+        t = torch.tensor([ms_mixed], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = world * n * a.steps / (ms_max * 1e-3)
+
+    # steady state without flushes: captured 10-step graphs, L2-resident state
+    g.sync()
+    ext = torch.cuda.ExternalStream(g.stream_ptr(), device=f"cuda:{dev}")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    g.step(a.steps)
+    e1.record(ext)
+    g.sync()
+    ms_resident = e0.elapsed_time(e1)
+
+    # dominant kernel: the pair kernel, timed alone on the context's stream
+    work = pair_work(g, cfg)
+    reps = 20
+    pk = []
+    for k in range(reps):
+        with torch.cuda.stream(ext):
+            flush.fill_(k & 0xff)
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(ext)
+        g.fluid_fluid()
+        p1.record(ext)
+        pk.append((p0, p1))
+    g.sync()
+    torch.cuda.synchronize(dev)
+    pair_ms = sum(x.elapsed_time(y) for x, y in pk) / reps
+    # algorithmic HBM bytes of one launch: each particle's sorted position and
+    # velocity records (16 + 16 B), its row length (4 B), its force record
+    # read and written (16 + 16 B) and its list row (4 B per entry)
+    pair_bytes = n * (16 + 16 + 4 + 16 + 16) + 4 * work["list_entries"]
+    # algorithmic flops (canonical counts): 17 per listed half-pair, 38 (LJ) + 29 (DPD) per in-cutoff half-pair
+    pair_flops = 17 * work["listed_half_pairs"] + (38 + 29) * work["incut_half_pairs"]
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = pair_bytes / (pair_ms * 1e-3) / 1e9
+    traffic = None
+    try:
+        prof = json.load(open(os.path.join(ROOT, "profiles", "pair_traffic.json")))
+        if prof.get("workload") == meta["workload"]:
+            traffic = prof.get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        pass
+    g.close()
+
+    # plain FP64 GPU path, same protocol
+    g64, ms_fp64, _, _, _ = timed_run(_abi.FP64, a.steps, a.warmup)
+    g64.close()
+    value_fp64 = world * n * a.steps / (ms_fp64 * 1e-3)
+
+    # end to end through the public API with host buffers
+    import ctypes as C
+    pinned = torch.empty((3, n, 3), dtype=torch.float64, pin_memory=True)
+    pinned[0].copy_(torch.from_numpy(cfg.r0))
+    pinned[1].copy_(torch.from_numpy(cfg.v))
+    ge = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=_abi.MIXED, device=dev)
+    if cfg.params.charged:
+        ge.ewald_k(0)
+    ge.init_forces()
+    ge.step(a.equil)
+    st = ge.download()
+    pinned[0].copy_(torch.from_numpy(st["r0"]))
+    pinned[1].copy_(torch.from_numpy(st["v"]))
+    pinned[2].copy_(torch.from_numpy(st["a"]))
+    host = pinned.numpy()
+    ge.sync()
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    ge.upload(r0=host[0], v=host[1], a=host[2])
+    for k in range(a.steps):
+        ge.step(1)
+        ge.scalars()                         # the step's energies (fort.60 quantities) to the host
+    out = ge.download(_abi.R0 | _abi.V)
+    t_e2e = time.perf_counter() - t0
+    ge.close()
+    if dist is not None:
+        t = torch.tensor([t_e2e], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e = world * n * a.steps / t_e2e
+    scal_bytes = 16 * 8 + 8 * 4
+    e2e_obj = {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": int(72 * n / a.steps),
+               "d2h_bytes_per_step": int(scal_bytes + 48 * n / a.steps)}
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not a.no_cpu:
+            rate, steps, dt = run_oracle(cfg, a.cpu_seconds, 100000)
+            model, ncpu = cpu_info()
+            cpu = {"value": rate, "unit": METRIC, "cores": 1, "kind": "port",
+                   "sample": f"{steps} full time steps ({dt:.1f} s) of the same {n}-bead workload, serial C "
+                             f"restatement of the reference loop on 1 core of {model} ({ncpu} host threads)"}
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded generator, no reference data)",
+            "config": dict(meta, beads=n, precision="mixed", dt=cfg.params.dt, skin=cfg.params.skin,
+                           thermostat="dpd", replicas=world,
+                           l2="flushed between timed steps (256 MiB write on the context stream)",
+                           parallelism=f"replicas x{world}"),
+            "fp64": {"value": value_fp64, "ms_per_step": ms_fp64 / a.steps},
+            "mixed_over_fp64": value / value_fp64,
+            "value_l2_resident": world * n * a.steps / (ms_resident * 1e-3),
+            "roofline": {"bound": "hbm", "kernel": "k_pair (fluid_fluid + dpd_forces + walls)",
+                         "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                         "traffic": traffic, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"
+                         if "hbm_gbs" in peaks else "fallback 6650 GB/s",
+                         "launch_ms": pair_ms, "algorithmic_bytes": pair_bytes,
+                         "fp32_tflops": pair_flops / (pair_ms * 1e-3) / 1e12, **work},
+            "e2e": e2e_obj,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,245 @@
+/*
+ * mfa_gpu.h -- C ABI of the B200 (sm_100a) implementation of mfa's per-timestep
+ * force and integration loop.
+ *
+ * The reference program (feindas/mfa) drives one MD/DPD time step from
+ * md_main.f90:68-157 by calling argument-less Fortran subroutines that read and
+ * write the global module `commons` (mfa_common.f90).  Every entry point below
+ * replaces one of those subroutines; a Fortran shim with the same subroutine
+ * name calls it through iso_c_binding.  After mfa_init the GPU owns all
+ * particle state; host arrays are mirrors that are valid after mfa_download.
+ *
+ * Conventions at this boundary (they follow the Fortran layouts):
+ *   - positions/velocities/accelerations/forces are double[3*n_part], xyz
+ *     contiguous per particle (Fortran r0(3,n_part), column-major);
+ *   - mic_count is int32[3*n_part] (Fortran mic_count(3,n_part));
+ *   - a_type is int32[n_part] with values 1..n_type (Fortran a_type);
+ *   - particle ids in lists are 1-based (Fortran ff_list / bin_fluid);
+ *   - pair tables are indexed [(ti-1)*MFA_MAX_TYPES + (tj-1)].
+ * Every function returns an mfa_status code (0 = ok).  Calls are asynchronous on
+ * the context's CUDA stream; mfa_check_skin, mfa_get_scalars, mfa_download and
+ * mfa_sync synchronise and report device-side errors.
+ */
+#ifndef MFA_GPU_H
+#define MFA_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MFA_MAX_TYPES 8
+#define MFA_ABI_VERSION 1
+
+typedef enum mfa_status {
+    MFA_OK = 0,
+    MFA_ERR_ARGS = 1,            /* bad argument or parameter combination        */
+    MFA_ERR_CUDA = 2,            /* a CUDA runtime call failed                   */
+    MFA_ERR_CELL_RANGE = 3,      /* particle outside the binning grid (z<0 ...)  */
+    MFA_ERR_NEIGH_OVERFLOW = 4,  /* neighbour list capacity exceeded             */
+    MFA_ERR_NONFINITE = 5,       /* NaN/Inf in positions or forces               */
+    MFA_ERR_TIMEOUT = 6,         /* a bounded device wait gave up                */
+    MFA_ERR_NOMEM = 7,           /* device allocation failed                     */
+    MFA_ERR_STATE = 8,           /* call order violated (e.g. forces before lists) */
+    MFA_ERR_UNSUPPORTED = 9      /* feature not built for this parameter set     */
+} mfa_status;
+
+typedef enum mfa_precision {
+    MFA_FP64 = 0,   /* every quantity in FP64 (plain FP64 GPU path)                   */
+    MFA_MIXED = 1   /* FP32 pair/bond forces; FP64 positions, VV, reductions, Ewald-k */
+} mfa_precision;
+
+/* Reference quirk switches (mfa_params.quirks).  Set = reproduce the reference. */
+#define MFA_Q_EWALD_REAL_IN_LJ  0x1  /* fluid_fluid.f90:94,166: Ewald real only inside range_2 */
+#define MFA_Q_WALL_ENERGY_AW    0x2  /* fluid_wall.f90:98,116: energy uses a_w, force a_wall(t) */
+
+/* Thermostat selector (control_simulation.h:45 THERMOSTAT) */
+#define MFA_THERMO_DPD  0
+#define MFA_THERMO_LGV  1
+#define MFA_THERMO_NONE 2
+
+/* Noise shape for DPD / Langevin random forces */
+#define MFA_NOISE_GAUSS   0   /* Box-Muller on Philox-4x32-10 (stands in for rnor())   */
+#define MFA_NOISE_UNIFORM 1   /* sqrt(3)*(2u-1), the alternative of dpd_forces.f90:278 */
+
+/*
+ * Run parameters.  These are the *derived* constants the reference computes in
+ * init_params.f90 / init_config.f90 / make_binning_boxes.f90 (epsilon already
+ * multiplied by 4, k_chain already multiplied by R0^2, range_2 with the
+ * single-precision 2.**(1./6.) literal, ...).  A Fortran shim fills this struct
+ * from the `commons` module variables of the same names.
+ */
+typedef struct mfa_params {
+    /* sizes and topology */
+    int32_t n_part;          /* particles (= n_mon_tot; explicit wall atoms unsupported) */
+    int32_t n_type;          /* 1..MFA_MAX_TYPES                                        */
+    int32_t n_mon, n_chain;  /* grafted/bulk chains, ids 1..n_mon*n_chain               */
+    int32_t n_mon_d, n_chain_d; /* melt/droplet chains, ids part_init_d+1..            */
+    /* control_simulation.h switches as runtime fields */
+    int32_t symmetry;        /* 0 channel (PBC x,y), 1 bulk (PBC x,y,z)                 */
+    int32_t thermostat;      /* MFA_THERMO_*                                            */
+    int32_t dpd_weight;      /* 0: w_r = 1-r/rc, w_d = w_r^2; 1: w_r = w_d = 1          */
+    int32_t wall;            /* 0 none, 2: 9-3 both walls, 3: 9-3 bottom + hard top,
+                                4: hard walls (fluid_wall.f90 inter_type)                */
+    int32_t charged;         /* Ewald real + k-space (SYSTEM 2,3)                       */
+    int32_t bending;         /* bending(2) over the grafted/bulk chains                 */
+    int32_t force_switch_on; /* FORCE_SWITCH_ON clamp r^2 = max(r^2, r_2_min)           */
+    int32_t pin_heads;       /* brush heads pinned (verlet_velocities.f90:269-282)      */
+    int32_t quirks;          /* MFA_Q_* bits                                            */
+    int32_t noise;           /* MFA_NOISE_*                                             */
+    /* geometry and cell grid */
+    double  boundary[3];
+    int32_t n_bin[3];        /* cells per axis (make_binning_boxes.f90:175-177)         */
+    int32_t delta_bin[3];    /* upper neighbour-cell offset (make_binning_boxes.f90:145-168) */
+    int32_t pad0;
+    /* pair tables [(ti-1)*MFA_MAX_TYPES + (tj-1)] */
+    double  range_2[MFA_MAX_TYPES * MFA_MAX_TYPES];
+    double  epsil[MFA_MAX_TYPES * MFA_MAX_TYPES];      /* already x4              */
+    double  sigma_2[MFA_MAX_TYPES * MFA_MAX_TYPES];
+    double  e_shift[MFA_MAX_TYPES * MFA_MAX_TYPES];
+    double  inv_range_2[MFA_MAX_TYPES * MFA_MAX_TYPES];
+    double  skin, skin_2;    /* check_skin.f90:18, init_params.f90:807-808              */
+    /* integrator and thermostat */
+    double  dt, temp, friction, sig;  /* sig = sqrt(2 T friction / dt) (init_params.f90:845) */
+    /* bonds */
+    double  k_chain;         /* FENE k * R0^2 (init_params.f90:398), grafted chains     */
+    double  k_ring;          /* FENE constant used for melt/droplet chains (intra_molec.f90:133) */
+    double  r_chain_2, inv_r_chain_2;
+    double  fene_clamp;      /* 0.98 (single-precision literal, intra_molec.f90:248)    */
+    double  k_bend, alpha_eq;
+    /* walls */
+    double  a_wall[MFA_MAX_TYPES], sigma_wall[MFA_MAX_TYPES];
+    double  a_w, z_space_wall, z_head;
+    double  wall_cut;        /* 0: no cutoff (reference); >0: truncate+shift at z = wall_cut */
+    double  va_spring_twall[3];
+    /* force switch-on (fluid_fluid.f90:42-49, init_force_switch_on.f90:15-22) */
+    double  r_2_min_init, r_2_min_time;
+    int64_t s_time;
+    /* Ewald (init_config.f90:217-246, ewald_k.f90) */
+    double  alpha_c;         /* the code's alpha_c (= alpha^2)                          */
+    double  sqrt_alpha;
+    double  inv_sqrt_pi;     /* 1/pi in the reference (init_config.f90:230)             */
+    double  pi;              /* value of pi used in the k-space sums                    */
+    double  ewald_rc_2;      /* real-space cutoff^2 when MFA_Q_EWALD_REAL_IN_LJ is off  */
+    int32_t n_kmax;
+    int32_t pad1;
+    /* counter-based noise */
+    uint64_t seed;
+} mfa_params;
+
+/* Scalars after a step (the `commons` variables of the same name). */
+typedef struct mfa_scalars {
+    double  v_fluid_fluid;   /* LJ energy, pairs counted once                    */
+    double  v_fluid_wall;
+    double  v_intra_molec;   /* FENE, brush + melt                               */
+    double  v_bend;
+    double  v_coul;          /* real + k-space + self                            */
+    double  t_fluid;         /* 0.5 * sum m v^2 over n_part                      */
+    double  v_total;         /* v_fluid_wall + v_fluid_fluid + v_intra_molec     */
+    double  e_total;         /* v_total + t_fluid                                */
+    double  virial;          /* sum over pairs of r_ij . F_ij (LJ + DPD + Coulomb real) */
+    int64_t i_time;          /* step counter of the context                      */
+    int32_t f_skin;
+    int32_t n_rebuilds;      /* neighbour-list rebuilds since mfa_init           */
+    int32_t max_neigh;       /* largest list row seen at the last rebuild        */
+    int32_t max_cell;        /* largest cell occupancy at the last rebuild       */
+    int32_t fene_clamped;    /* bonds that hit the 0.98 clamp since mfa_init     */
+    int32_t error_bits;      /* device error word                                */
+    int64_t kernel_launches; /* kernels this context launched since mfa_init
+                                (each kernel of a replayed graph counted)       */
+} mfa_scalars;
+
+typedef struct mfa_ctx mfa_ctx;
+
+/* Download / upload masks */
+#define MFA_R0   0x01
+#define MFA_V    0x02
+#define MFA_A    0x04
+#define MFA_F    0x08
+#define MFA_MIC  0x10
+
+/* ---------------- lifetime ---------------- */
+
+/* Replaces the allocation in init_system.f90:228-299 plus the state upload that
+ * follows init_config (md_main.f90:51-53).  q may be NULL unless p->charged;
+ * mic_count may be NULL (zeros).  device < 0 keeps the current device. */
+int mfa_init(const mfa_params* p, int precision, int device,
+             const double* r0, const double* v, const double* a,
+             const int32_t* a_type, const double* mass, const double* q,
+             const int32_t* mic_count, mfa_ctx** out);
+int mfa_finalize(mfa_ctx* ctx);
+int mfa_abi_version(void);
+/* sizeof(mfa_params) and sizeof(mfa_scalars) as compiled into the library, so a
+ * binding (Fortran iso_c_binding, ctypes) can check its struct mirrors. */
+int mfa_abi_sizes(int32_t* params_bytes, int32_t* scalars_bytes);
+const char* mfa_status_string(int status);
+
+/* Sets the step counter i_time (md_main.f90:68); r_time = (s_time+i_time-1)*dt. */
+int mfa_set_step(mfa_ctx* ctx, int64_t i_time);
+
+/* ---------------- the per-step subroutines ---------------- */
+
+/* verlet_positions.f90:146-171,237-251: r += dt v + dt^2/2 a; v += dt/2 a; wrap.
+ * Also advances i_time by one (the loop counter of md_main.f90:68). */
+int mfa_verlet_positions(mfa_ctx* ctx);
+/* check_skin.f90:4-24.  Synchronises; *f_skin = 1 if a rebuild is due. */
+int mfa_check_skin(mfa_ctx* ctx, int32_t* f_skin);
+/* binning.f90:2-131 (BIN_TYPE 0).  Cell binning + Verlet list, f_skin = 0,
+ * snapshot r0_old/mic_old.  The list is held as a full (both-direction) list;
+ * as a set of unordered pairs it equals the reference's half list. */
+int mfa_binning(mfa_ctx* ctx);
+/* my_binning.f90:5-140 (BIN_TYPE 1).  Same cells and pairs; the full list is
+ * what my_binning builds. */
+int mfa_my_binning(mfa_ctx* ctx);
+/* force(:,:) = 0 (md_main.f90:88). */
+int mfa_zero_forces(mfa_ctx* ctx);
+/* fluid_fluid.f90:1-254 with dpd_forces (THERMOSTAT 0), lgv_forces
+ * (THERMOSTAT 1) and ewald_real (charged) fused in.  Adds to force. */
+int mfa_fluid_fluid(mfa_ctx* ctx);
+/* fluid_wall.f90:2-204, inter_type 2, 3 or 4.  Adds to force (2,3), reflects v (3,4). */
+int mfa_fluid_wall(mfa_ctx* ctx, int32_t inter_type);
+/* intra_molec.f90:1-300: FENE bonds of grafted and melt chains.  Adds to force. */
+int mfa_intra_molec(mfa_ctx* ctx);
+/* bending.f90:2-149 (mode 0: no-op, mode 2: angle forces).  Adds to force. */
+int mfa_bending(mfa_ctx* ctx, int32_t mode);
+/* ewald_k.f90:1-211 (mode 0: build k-vectors, mode 1: k-space energy + force). */
+int mfa_ewald_k(mfa_ctx* ctx, int32_t mode);
+/* verlet_velocities.f90:1-246: a = F/m, v += dt/2 a, heads pinned, energies. */
+int mfa_verlet_velocities(mfa_ctx* ctx);
+
+/* ---------------- fast path ---------------- */
+
+/* Runs nsteps complete time steps (md_main.f90:69-147) on the device: fused
+ * kernels, rebuild decided on the device, each step replayed as a captured
+ * CUDA graph.  No host synchronisation inside. */
+int mfa_step(mfa_ctx* ctx, int32_t nsteps);
+/* Records e_total/v_total/t_fluid every `every` steps of mfa_step into a device
+ * log of `capacity` entries (0 disables).  Read back with mfa_read_energy_log. */
+int mfa_set_energy_log(mfa_ctx* ctx, int32_t every, int32_t capacity);
+int mfa_read_energy_log(mfa_ctx* ctx, double* out3, int32_t max_entries, int32_t* n_out);
+
+/* ---------------- host mirrors ---------------- */
+
+int mfa_get_scalars(mfa_ctx* ctx, mfa_scalars* out);
+int mfa_download(mfa_ctx* ctx, uint32_t mask, double* r0, double* v, double* a,
+                 double* force, int32_t* mic_count);
+int mfa_upload(mfa_ctx* ctx, uint32_t mask, const double* r0, const double* v,
+               const double* a, const double* force, const int32_t* mic_count);
+int mfa_sync(mfa_ctx* ctx);
+/* The CUDA stream (cudaStream_t) all of the context's work is ordered on, for
+ * callers that time it with events or order their own copies after it. */
+int mfa_stream(mfa_ctx* ctx, void** cuda_stream);
+
+/* Parity hooks: cell index per particle (0-based ix + nbx*(iy + nby*iz)) and the
+ * Verlet list, full (both directions), rows in particle order, 1-based ids,
+ * row i = nbr[i*max_per .. i*max_per + nbr_count[i]). */
+int mfa_debug_lists(mfa_ctx* ctx, int32_t* cell_of, int32_t* nbr_count,
+                    int32_t* nbr, int32_t max_per);
+/* Number of k-vectors and their components (after mfa_ewald_k(ctx, 0)). */
+int mfa_debug_kvecs(mfa_ctx* ctx, int32_t* nk, double* kvecs3, int32_t max_k);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MFA_GPU_H */

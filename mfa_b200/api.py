@@ -1,0 +1,219 @@
+"""Host-side mirror of the reference's per-step subroutine interface.
+
+``System`` owns one device context (``mfa_ctx``) and exposes the subroutines
+md_main.f90 calls, under the same names and in the same roles:
+
+    verlet_positions, check_skin, binning, my_binning, fluid_fluid,
+    fluid_wall(inter_type), intra_molec, bending(mode), ewald_k(mode),
+    verlet_velocities
+
+plus ``md_step`` (one iteration of md_main.f90:68-147 through those calls),
+``step(n)`` (the fused, graph-captured device loop) and the host mirrors.
+Every call goes through the C ABI of libmfa_gpu.so; errors raise MfaError,
+the way the reference stops.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _abi
+from ._abi import MfaParams, MfaScalars, check, load
+
+
+def _dp(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+class System:
+    """One simulated system resident on one GPU."""
+
+    def __init__(self, params: MfaParams, r0, v, a_type, mass, q=None, a=None, mic=None,
+                 precision: int = _abi.MIXED, device: int = 0):
+        self.lib = load()
+        self.params = params.copy()
+        self.n = int(params.n_part)
+        self.precision = precision
+        r0 = np.ascontiguousarray(r0, dtype=np.float64).reshape(self.n, 3)
+        v = np.ascontiguousarray(v, dtype=np.float64).reshape(self.n, 3)
+        acc = None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(self.n, 3)
+        t = np.ascontiguousarray(a_type, dtype=np.int32)
+        m = np.ascontiguousarray(mass, dtype=np.float64)
+        qq = None if q is None else np.ascontiguousarray(q, dtype=np.float64)
+        mc = None if mic is None else np.ascontiguousarray(mic, dtype=np.int32).reshape(self.n, 3)
+        ctx = C.c_void_p()
+        check(self.lib.mfa_init(C.byref(self.params), precision, device, _dp(r0), _dp(v), _dp(acc),
+                                _ip(t), _dp(m), _dp(qq), _ip(mc), C.byref(ctx)), "mfa_init")
+        self.ctx = ctx
+        self.mass = m
+
+    # ---- lifetime ----
+    def close(self) -> None:
+        if getattr(self, "ctx", None):
+            self.lib.mfa_finalize(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- the subroutines of md_main.f90:68-147 ----
+    def set_step(self, i_time: int) -> None:
+        check(self.lib.mfa_set_step(self.ctx, int(i_time)), "mfa_set_step")
+
+    def verlet_positions(self) -> None:
+        check(self.lib.mfa_verlet_positions(self.ctx), "verlet_positions")
+
+    def check_skin(self) -> int:
+        f = C.c_int32(0)
+        check(self.lib.mfa_check_skin(self.ctx, C.byref(f)), "check_skin")
+        return int(f.value)
+
+    def binning(self) -> None:
+        check(self.lib.mfa_binning(self.ctx), "binning")
+
+    def my_binning(self) -> None:
+        check(self.lib.mfa_my_binning(self.ctx), "my_binning")
+
+    def zero_forces(self) -> None:
+        check(self.lib.mfa_zero_forces(self.ctx), "zero_forces")
+
+    def fluid_fluid(self) -> None:
+        check(self.lib.mfa_fluid_fluid(self.ctx), "fluid_fluid")
+
+    def fluid_wall(self, inter_type: int) -> None:
+        check(self.lib.mfa_fluid_wall(self.ctx, int(inter_type)), "fluid_wall")
+
+    def intra_molec(self) -> None:
+        check(self.lib.mfa_intra_molec(self.ctx), "intra_molec")
+
+    def bending(self, mode: int) -> None:
+        check(self.lib.mfa_bending(self.ctx, int(mode)), "bending")
+
+    def ewald_k(self, mode: int) -> None:
+        check(self.lib.mfa_ewald_k(self.ctx, int(mode)), "ewald_k")
+
+    def verlet_velocities(self) -> None:
+        check(self.lib.mfa_verlet_velocities(self.ctx), "verlet_velocities")
+
+    # ---- compositions ----
+    def init_forces(self) -> None:
+        """The start-up sequence of conf_default.f90:254-299: lists, the forces
+        fluid_fluid / fluid_wall / intra_molec, then a = F/m."""
+        p = self.params
+        if p.charged:
+            self.ewald_k(0)
+        self.binning()
+        self.zero_forces()
+        self.fluid_fluid()
+        if p.symmetry == 0 and p.wall in (2, 3, 4):
+            self.fluid_wall(p.wall)
+        self.intra_molec()
+        f = self.download(_abi.F)["force"]
+        self.upload(a=f / self.mass[:, None])
+
+    def md_step(self) -> int:
+        """One md_main.f90:68-147 iteration through the individual entry points.
+        Returns f_skin as check_skin saw it."""
+        p = self.params
+        self.verlet_positions()
+        f_skin = self.check_skin()
+        if f_skin == 1:
+            self.binning()
+        self.zero_forces()
+        self.fluid_fluid()
+        if p.symmetry == 0 and p.wall in (2, 3, 4):
+            self.fluid_wall(p.wall)
+        self.intra_molec()
+        if p.bending:
+            self.bending(2)
+        if p.charged:
+            self.ewald_k(1)
+        self.verlet_velocities()
+        return f_skin
+
+    def step(self, nsteps: int) -> None:
+        """nsteps time steps on the device (fused kernels, captured graphs)."""
+        check(self.lib.mfa_step(self.ctx, int(nsteps)), "mfa_step")
+
+    # ---- mirrors ----
+    def stream_ptr(self) -> int:
+        """cudaStream_t of the context (for event timing on the launching stream)."""
+        s = C.c_void_p()
+        check(self.lib.mfa_stream(self.ctx, C.byref(s)), "mfa_stream")
+        return int(s.value or 0)
+
+    def sync(self) -> None:
+        check(self.lib.mfa_sync(self.ctx), "mfa_sync")
+
+    def scalars(self) -> dict:
+        s = MfaScalars()
+        check(self.lib.mfa_get_scalars(self.ctx, C.byref(s)), "mfa_get_scalars")
+        return s.as_dict()
+
+    def download(self, mask: int = _abi.R0 | _abi.V | _abi.A | _abi.F | _abi.MIC) -> dict:
+        n = self.n
+        r0 = np.empty((n, 3)) if mask & _abi.R0 else None
+        v = np.empty((n, 3)) if mask & _abi.V else None
+        a = np.empty((n, 3)) if mask & _abi.A else None
+        f = np.empty((n, 3)) if mask & _abi.F else None
+        mic = np.empty((n, 3), dtype=np.int32) if mask & _abi.MIC else None
+        check(self.lib.mfa_download(self.ctx, mask, _dp(r0), _dp(v), _dp(a), _dp(f), _ip(mic)),
+              "mfa_download")
+        return {"r0": r0, "v": v, "a": a, "force": f, "mic": mic}
+
+    def upload(self, r0=None, v=None, a=None, force=None, mic=None) -> None:
+        mask = 0
+        arrs = []
+        for bit, x, dt in ((_abi.R0, r0, np.float64), (_abi.V, v, np.float64), (_abi.A, a, np.float64),
+                           (_abi.F, force, np.float64), (_abi.MIC, mic, np.int32)):
+            if x is not None:
+                mask |= bit
+                arrs.append(np.ascontiguousarray(x, dtype=dt).reshape(self.n, 3))
+            else:
+                arrs.append(None)
+        check(self.lib.mfa_upload(self.ctx, mask, _dp(arrs[0]), _dp(arrs[1]), _dp(arrs[2]),
+                                  _dp(arrs[3]), _ip(arrs[4])), "mfa_upload")
+
+    def debug_lists(self, max_per: int = 256):
+        n = self.n
+        cell = np.empty(n, dtype=np.int32)
+        cnt = np.empty(n, dtype=np.int32)
+        nbr = np.zeros((n, max_per), dtype=np.int32)
+        check(self.lib.mfa_debug_lists(self.ctx, _ip(cell), _ip(cnt), _ip(nbr), max_per), "mfa_debug_lists")
+        return cell, cnt, nbr
+
+    def kvecs(self, max_k: int = 100000) -> np.ndarray:
+        nk = C.c_int32(0)
+        out = np.empty((max_k, 3))
+        check(self.lib.mfa_debug_kvecs(self.ctx, C.byref(nk), _dp(out), max_k), "mfa_debug_kvecs")
+        return out[: nk.value].copy()
+
+    def set_energy_log(self, every: int, capacity: int) -> None:
+        check(self.lib.mfa_set_energy_log(self.ctx, every, capacity), "mfa_set_energy_log")
+
+    def energy_log(self, max_entries: int = 1 << 20) -> np.ndarray:
+        out = np.empty((max_entries, 4))
+        n = C.c_int32(0)
+        check(self.lib.mfa_read_energy_log(self.ctx, _dp(out), max_entries, C.byref(n)), "mfa_read_energy_log")
+        return out[: n.value].copy()
+
+
+def from_config(cfg, precision: int = _abi.MIXED, device: int = 0) -> System:
+    """A System holding a generated configuration (mfa_b200.configs)."""
+    return System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q,
+                  precision=precision, device=device)

@@ -1,0 +1,650 @@
+// C ABI entry points (include/mfa_gpu.h): context lifetime, the per-step
+// subroutines of md_main.f90:68-147, the captured-graph fast path, host mirrors.
+#include "mfa_internal.cuh"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <vector>
+
+int mfa_ewald_download_kvecs(mfa_ctx* c, double* out3, int max_k);
+
+namespace {
+
+template <typename T>
+int dalloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    if (cudaMalloc((void**)p, count * sizeof(T)) != cudaSuccess) return MFA_ERR_NOMEM;
+    return MFA_OK;
+}
+
+#define TRY(x)                          \
+    do {                                \
+        int s__ = (x);                  \
+        if (s__ != MFA_OK) return s__;  \
+    } while (0)
+
+size_t esz(const mfa_ctx* c) { return c->prec == MFA_MIXED ? sizeof(float) : sizeof(double); }
+
+int first_error(int bits) {
+    for (int s = 1; s < 31; ++s)
+        if (bits & (1 << s)) return s;
+    return MFA_OK;
+}
+
+int check_params(const mfa_params* p, int precision) {
+    if (!p) return MFA_ERR_ARGS;
+    if (precision != MFA_FP64 && precision != MFA_MIXED) return MFA_ERR_ARGS;
+    if (p->n_part <= 0 || p->n_part >= (1 << 23)) return MFA_ERR_ARGS;
+    if (p->n_type < 1 || p->n_type > MFA_MAX_TYPES) return MFA_ERR_ARGS;
+    for (int d = 0; d < 3; ++d) {
+        if (!(p->boundary[d] > 0.0) || p->n_bin[d] < 1) return MFA_ERR_ARGS;
+        if (p->delta_bin[d] < -1 || p->delta_bin[d] > 1) return MFA_ERR_ARGS;
+    }
+    if (p->n_mon < 0 || p->n_chain < 0 || p->n_mon_d < 0 || p->n_chain_d < 0) return MFA_ERR_ARGS;
+    if ((long long)p->n_mon * p->n_chain + (long long)p->n_mon_d * p->n_chain_d > p->n_part) return MFA_ERR_ARGS;
+    if (p->symmetry != 0 && p->symmetry != 1) return MFA_ERR_ARGS;
+    if (p->thermostat < 0 || p->thermostat > 2) return MFA_ERR_ARGS;
+    if (p->dpd_weight != 0 && p->dpd_weight != 1) return MFA_ERR_UNSUPPORTED;
+    if (p->wall != 0 && p->wall != 2 && p->wall != 3 && p->wall != 4) return MFA_ERR_ARGS;
+    if (!(p->dt > 0.0)) return MFA_ERR_ARGS;
+    return MFA_OK;
+}
+
+void invalidate_graph(mfa_ctx* c) {
+    for (int k = 0; k < 3; ++k) {
+        if (c->gexec[k]) cudaGraphExecDestroy(c->gexec[k]);
+        if (c->graph[k]) cudaGraphDestroy(c->graph[k]);
+        c->gexec[k] = nullptr;
+        c->graph[k] = nullptr;
+        c->graph_kernels[k] = 0;
+    }
+}
+
+void free_all(mfa_ctx* c) {
+    invalidate_graph(c);
+    void* ptrs[] = {c->rx, c->mx, c->type, c->mass, c->force, c->pos_s, c->vel_s, c->pos64,
+                    c->ids, c->cell_count, c->nbr, c->nnb, c->partials, c->counters, c->dscal,
+                    c->dflags, c->dstep, c->kvec, c->rho, c->rho_part, c->elog, c->elog_n, c->tabs};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    if (c->st) cudaStreamDestroy(c->st);
+}
+
+int alloc_list(mfa_ctx* c, int maxnb) {
+    if (c->nbr) cudaFree(c->nbr);
+    c->nbr = nullptr;
+    c->maxnb = maxnb;
+    return dalloc(&c->nbr, (size_t)maxnb * c->n);
+}
+
+int read_flags(mfa_ctx* c, int32_t* f) {
+    MFA_CUDA_TRY(cudaMemcpyAsync(f, c->dflags, F_NFLAG * sizeof(int32_t), cudaMemcpyDeviceToHost, c->st));
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    return MFA_OK;
+}
+
+// rebuild through the ABI (unconditional) with capacity growth on overflow
+int rebuild_abi(mfa_ctx* c, int rule) {
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        c->bin_type = rule;
+        TRY(launch_rebuild(c, rule, 0));
+        c->lists_valid = 1;
+        int32_t f[F_NFLAG];
+        TRY(read_flags(c, f));
+        const int bits = f[F_ERR];
+        if (bits & (1 << MFA_ERR_NEIGH_OVERFLOW)) {
+            const int need = f[F_NEEDNB];
+            int grow = ((need + need / 4 + 32) + 31) / 32 * 32;
+            TRY(alloc_list(c, grow));
+            invalidate_graph(c);
+            int32_t zero[2] = {0, 0};
+            const int32_t clear = bits & ~(1 << MFA_ERR_NEIGH_OVERFLOW);
+            MFA_CUDA_TRY(cudaMemcpy(c->dflags + F_ERR, &clear, sizeof(int32_t), cudaMemcpyHostToDevice));
+            MFA_CUDA_TRY(cudaMemcpy(c->dflags + F_NEEDNB, zero, sizeof(int32_t), cudaMemcpyHostToDevice));
+            continue;
+        }
+        return first_error(bits);
+    }
+    return MFA_ERR_NEIGH_OVERFLOW;
+}
+
+int forces_fused(mfa_ctx* c) {
+    TRY(launch_pair(c, 1, 0));
+    if (c->p.wall == 3 || c->p.wall == 4) TRY(launch_wall(c, c->p.wall));
+    const bool chains = c->p.n_chain > 0 || (c->p.n_chain_d > 0 && c->p.n_mon_d >= 2);
+    if (chains) TRY(launch_bonds(c, 1, 1));
+    if (c->p.charged) TRY(launch_ewald(c));
+    return MFA_OK;
+}
+
+constexpr int GRAPH_BODY = 10;
+
+// One time step as the reference orders it (md_main.f90:73-147), with the
+// rebuild decided on the device: positions (+ skin check), rebuild if due,
+// forces, velocities.
+int launch_full_step(mfa_ctx* c) {
+    TRY(launch_vv_positions(c, 1));
+    TRY(launch_rebuild(c, c->bin_type, 1));
+    TRY(forces_fused(c));
+    return launch_vv_velocities(c);
+}
+
+// A body step of a run of steps: forces of step n, then velocities of n fused
+// with positions of n+1, then the rebuild of n+1 if due.
+int launch_body_step(mfa_ctx* c) {
+    TRY(forces_fused(c));
+    TRY(launch_vv_fused(c));
+    return launch_rebuild(c, c->bin_type, 1);
+}
+
+// kind 0: one full step; 1: one body step; 2: GRAPH_BODY body steps
+int capture(mfa_ctx* c, int kind) {
+    cudaGraph_t g;
+    MFA_CUDA_TRY(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    c->capturing = 1;
+    c->cap_count = 0;
+    int rc = MFA_OK;
+    if (kind == 0) rc = launch_full_step(c);
+    else
+        for (int s = 0; s < (kind == 1 ? 1 : GRAPH_BODY) && rc == MFA_OK; ++s) rc = launch_body_step(c);
+    c->capturing = 0;
+    cudaError_t e = cudaStreamEndCapture(c->st, &g);
+    if (rc != MFA_OK) return rc;
+    MFA_CUDA_TRY(e);
+    MFA_CUDA_TRY(cudaGraphInstantiate(&c->gexec[kind], g, 0));
+    c->graph[kind] = g;
+    c->graph_kernels[kind] = (int)c->cap_count;
+    return MFA_OK;
+}
+
+int replay(mfa_ctx* c, int kind) {
+    const void* key[4] = {c->nbr, c->elog, c->kvec, (const void*)(intptr_t)(c->bin_type + 1)};
+    if (memcmp(key, c->graph_key, sizeof(key)) != 0) {
+        invalidate_graph(c);
+        memcpy(c->graph_key, key, sizeof(key));
+    }
+    if (!c->gexec[kind]) TRY(capture(c, kind));
+    MFA_CUDA_TRY(cudaGraphLaunch(c->gexec[kind], c->st));
+    c->launches += c->graph_kernels[kind];
+    return MFA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mfa_abi_version(void) { return MFA_ABI_VERSION; }
+
+int mfa_abi_sizes(int32_t* params_bytes, int32_t* scalars_bytes) {
+    if (params_bytes) *params_bytes = (int32_t)sizeof(mfa_params);
+    if (scalars_bytes) *scalars_bytes = (int32_t)sizeof(mfa_scalars);
+    return MFA_OK;
+}
+
+const char* mfa_status_string(int s) {
+    switch (s) {
+        case MFA_OK: return "ok";
+        case MFA_ERR_ARGS: return "invalid argument or parameter combination";
+        case MFA_ERR_CUDA: return "CUDA runtime error";
+        case MFA_ERR_CELL_RANGE: return "particle outside the binning grid";
+        case MFA_ERR_NEIGH_OVERFLOW: return "neighbour list capacity exceeded";
+        case MFA_ERR_NONFINITE: return "non-finite position or force";
+        case MFA_ERR_TIMEOUT: return "bounded device wait timed out";
+        case MFA_ERR_NOMEM: return "device allocation failed";
+        case MFA_ERR_STATE: return "call order violated";
+        case MFA_ERR_UNSUPPORTED: return "unsupported parameter set";
+        default: return "unknown status";
+    }
+}
+
+int mfa_init(const mfa_params* p, int precision, int device, const double* r0, const double* v,
+             const double* a, const int32_t* a_type, const double* mass, const double* q,
+             const int32_t* mic_count, mfa_ctx** out) {
+    if (!out) return MFA_ERR_ARGS;
+    *out = nullptr;
+    TRY(check_params(p, precision));
+    if (!r0 || !a_type || !mass) return MFA_ERR_ARGS;
+    if (p->charged && !q) return MFA_ERR_ARGS;
+    const int n = p->n_part;
+    for (int i = 0; i < n; ++i) {
+        if (a_type[i] < 1 || a_type[i] > p->n_type) return MFA_ERR_ARGS;
+        if (!(mass[i] > 0.0)) return MFA_ERR_ARGS;
+    }
+    if (device >= 0) MFA_CUDA_TRY(cudaSetDevice(device));
+    mfa_ctx* c = (mfa_ctx*)calloc(1, sizeof(mfa_ctx));
+    if (!c) return MFA_ERR_NOMEM;
+    c->p = *p;
+    c->prec = precision;
+    MFA_CUDA_TRY(cudaGetDevice(&c->dev));
+    c->n = n;
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) { free(c); return MFA_ERR_CUDA; }
+    int rc = MFA_OK;
+#define A(x) do { if (rc == MFA_OK) rc = (x); } while (0)
+    // FP64 state: r, v, a, r0_old (12 arrays)
+    double* d12 = nullptr;
+    A(dalloc(&d12, (size_t)12 * n));
+    int32_t* i7 = nullptr;
+    A(dalloc(&i7, (size_t)6 * n));
+    if (rc == MFA_OK) {
+        c->rx = d12; c->ry = d12 + n; c->rz = d12 + 2 * n;
+        c->vx = d12 + 3 * n; c->vy = d12 + 4 * n; c->vz = d12 + 5 * n;
+        c->ax = d12 + 6 * n; c->ay = d12 + 7 * n; c->az = d12 + 8 * n;
+        c->ox = d12 + 9 * n; c->oy = d12 + 10 * n; c->oz = d12 + 11 * n;
+        c->mx = i7; c->my = i7 + n; c->mz = i7 + 2 * n;
+        c->omx = i7 + 3 * n; c->omy = i7 + 4 * n; c->omz = i7 + 5 * n;
+    }
+    A(dalloc(&c->type, n));
+    double* d3 = nullptr;
+    A(dalloc(&d3, (size_t)3 * n));
+    if (rc == MFA_OK) { c->mass = d3; c->inv_mass = d3 + n; c->q = d3 + 2 * n; }
+    A(dalloc((unsigned char**)&c->force, (size_t)4 * n * esz(c)));
+    A(dalloc((unsigned char**)&c->pos_s, (size_t)4 * n * esz(c)));
+    A(dalloc((unsigned char**)&c->vel_s, (size_t)4 * n * esz(c)));
+    A(dalloc(&c->pos64, n));
+    int32_t* i2 = nullptr;
+    A(dalloc(&i2, (size_t)2 * n));
+    if (rc == MFA_OK) { c->ids = i2; c->slot = i2 + n; }
+    // cells (make_binning_boxes.f90:188-195)
+    c->ncell = 1;
+    for (int d = 0; d < 3; ++d) {
+        c->nb[d] = p->n_bin[d];
+        c->ncell *= p->n_bin[d];
+        c->rbin[d] = p->boundary[d] / (double)p->n_bin[d];
+        c->inv_rbin[d] = 1.0 / c->rbin[d];
+        c->inv_boundary[d] = 1.0 / p->boundary[d];   // init_config.f90:20
+    }
+    int32_t* cells = nullptr;
+    A(dalloc(&cells, (size_t)3 * c->ncell + 2 + n));
+    if (rc == MFA_OK) {
+        c->cell_count = cells;
+        c->cell_start = cells + c->ncell;
+        c->cell_cursor = cells + 2 * c->ncell + 1;
+        c->cell_of = cells + 3 * c->ncell + 2;
+    }
+    // Verlet list capacity: twice the expected count at the mean density
+    double rc2max = 0.0;
+    for (int k = 0; k < T8 * T8; ++k) rc2max = fmax(rc2max, p->range_2[k]);
+    double rlist2 = rc2max + p->skin_2;
+    if (p->charged && !(p->quirks & MFA_Q_EWALD_REAL_IN_LJ)) {
+        const double re = sqrt(p->ewald_rc_2) + p->skin;
+        rlist2 = fmax(rlist2, re * re);
+    }
+    const double vol = p->boundary[0] * p->boundary[1] * p->boundary[2];
+    const double expect = 4.18879020478639 * pow(rlist2, 1.5) * (double)n / vol;
+    int maxnb = ((int)(2.0 * expect) + 32 + 31) / 32 * 32;
+    if (maxnb > n) maxnb = ((n + 31) / 32) * 32;
+    if (rc == MFA_OK) rc = alloc_list(c, maxnb);
+    A(dalloc(&c->nnb, n));
+    c->max_blocks = (n + 31) / 32 + 64;
+    A(dalloc(&c->partials, (size_t)R_N * 4 * c->max_blocks));
+    A(dalloc(&c->counters, R_N));
+    A(dalloc(&c->dscal, S_NSLOT));
+    A(dalloc(&c->dflags, F_NFLAG));
+    A(dalloc(&c->dstep, 1));
+    A(dalloc(&c->tabs, 6 * T8 * T8));
+    if (rc == MFA_OK && cudaMallocHost((void**)&c->h_stage, (size_t)3 * n * sizeof(double)) != cudaSuccess)
+        rc = MFA_ERR_NOMEM;
+    if (rc != MFA_OK) { free_all(c); free(c); return rc; }
+    // host-side staging
+    std::vector<double> soa((size_t)12 * n, 0.0);
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) {
+            soa[(size_t)d * n + i] = r0[3 * i + d];
+            soa[(size_t)(3 + d) * n + i] = v ? v[3 * i + d] : 0.0;
+            soa[(size_t)(6 + d) * n + i] = a ? a[3 * i + d] : 0.0;
+            soa[(size_t)(9 + d) * n + i] = r0[3 * i + d];
+        }
+    std::vector<int32_t> mic((size_t)6 * n, 0);
+    if (mic_count)
+        for (int i = 0; i < n; ++i)
+            for (int d = 0; d < 3; ++d) { mic[(size_t)d * n + i] = mic_count[3 * i + d]; mic[(size_t)(3 + d) * n + i] = mic_count[3 * i + d]; }
+    std::vector<double> m3((size_t)3 * n, 0.0);
+    double vself = 0.0;
+    for (int i = 0; i < n; ++i) {
+        m3[i] = mass[i];
+        m3[n + i] = 1.0 / mass[i];
+        m3[2 * n + i] = q ? q[i] : 0.0;
+        if (q) vself = vself - q[i] * q[i];
+    }
+    c->v_coul_self = p->charged ? vself * p->sqrt_alpha / sqrt(p->pi) : 0.0;   // init_config.f90:235-239
+    std::vector<double> tabs((size_t)6 * T8 * T8);
+    // list criterion: range_2 + skin_2 (binning.f90:104); with the real-space
+    // Ewald cutoff decoupled from the LJ range, out to rc_ewald + skin as well
+    double ew_list2 = 0.0;
+    if (p->charged && !(p->quirks & MFA_Q_EWALD_REAL_IN_LJ)) {
+        const double re = sqrt(p->ewald_rc_2) + p->skin;
+        ew_list2 = re * re;
+    }
+    for (int k = 0; k < T8 * T8; ++k) {
+        tabs[k] = p->range_2[k] + p->skin_2;
+        if (ew_list2 > tabs[k]) tabs[k] = ew_list2;
+        tabs[T8 * T8 + k] = p->range_2[k];
+        tabs[2 * T8 * T8 + k] = p->epsil[k];
+        tabs[3 * T8 * T8 + k] = p->sigma_2[k];
+        tabs[4 * T8 * T8 + k] = p->e_shift[k];
+        tabs[5 * T8 * T8 + k] = p->inv_range_2[k];
+    }
+    rc = MFA_OK;
+    if (cudaMemcpy(d12, soa.data(), soa.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(i7, mic.data(), mic.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->type, a_type, (size_t)n * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(d3, m3.data(), m3.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->tabs, tabs.data(), tabs.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(c->force, 0, (size_t)4 * n * esz(c)) != cudaSuccess ||
+        cudaMemset(c->cell_count, 0, (size_t)c->ncell * 4) != cudaSuccess ||
+        cudaMemset(c->nnb, 0, (size_t)n * 4) != cudaSuccess ||
+        cudaMemset(c->counters, 0, R_N * sizeof(unsigned)) != cudaSuccess ||
+        cudaMemset(c->dscal, 0, S_NSLOT * 8) != cudaSuccess ||
+        cudaMemset(c->dflags, 0, F_NFLAG * 4) != cudaSuccess ||
+        cudaMemset(c->dstep, 0, 8) != cudaSuccess)
+        rc = MFA_ERR_CUDA;
+    if (rc == MFA_OK) rc = bonds_setup(c);
+    if (rc != MFA_OK) { free_all(c); free(c); return rc; }
+#undef A
+    *out = c;
+    return MFA_OK;
+}
+
+int mfa_finalize(mfa_ctx* c) {
+    if (!c) return MFA_ERR_ARGS;
+    cudaStreamSynchronize(c->st);
+    free_all(c);
+    free(c);
+    return MFA_OK;
+}
+
+int mfa_set_step(mfa_ctx* c, int64_t i_time) {
+    if (!c) return MFA_ERR_ARGS;
+    c->i_time = i_time;
+    MFA_CUDA_TRY(cudaMemcpyAsync(c->dstep, &c->i_time, 8, cudaMemcpyHostToDevice, c->st));
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    return MFA_OK;
+}
+
+int mfa_verlet_positions(mfa_ctx* c) {
+    if (!c) return MFA_ERR_ARGS;
+    c->i_time += 1;
+    return launch_vv_positions(c, 0);
+}
+
+int mfa_check_skin(mfa_ctx* c, int32_t* f_skin) {
+    if (!c || !f_skin) return MFA_ERR_ARGS;
+    TRY(launch_check_skin(c));
+    int32_t f[F_NFLAG];
+    TRY(read_flags(c, f));
+    *f_skin = f[F_SKIN];
+    return first_error(f[F_ERR]);
+}
+
+int mfa_binning(mfa_ctx* c) {
+    if (!c) return MFA_ERR_ARGS;
+    return rebuild_abi(c, 0);
+}
+
+int mfa_my_binning(mfa_ctx* c) {
+    if (!c) return MFA_ERR_ARGS;
+    return rebuild_abi(c, 1);
+}
+
+int mfa_zero_forces(mfa_ctx* c) {
+    if (!c) return MFA_ERR_ARGS;
+    MFA_CUDA_TRY(cudaMemsetAsync(c->force, 0, (size_t)4 * c->n * esz(c), c->st));
+    return MFA_OK;
+}
+
+int mfa_fluid_fluid(mfa_ctx* c) {
+    if (!c) return MFA_ERR_ARGS;
+    // fluid_fluid.f90:17 resets v_coul; the k-space part is added by ewald_k
+    MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VCK, 0, 8, c->st));
+    return launch_pair(c, 0, 1);
+}
+
+int mfa_fluid_wall(mfa_ctx* c, int32_t inter_type) {
+    if (!c) return MFA_ERR_ARGS;
+    return launch_wall(c, inter_type);
+}
+
+int mfa_intra_molec(mfa_ctx* c) {
+    if (!c) return MFA_ERR_ARGS;
+    return launch_bonds(c, 1, 0);
+}
+
+int mfa_bending(mfa_ctx* c, int32_t mode) {
+    if (!c) return MFA_ERR_ARGS;
+    if (mode == 0 || mode == 1) return MFA_OK;   // bending.f90:12-20: report / no-op
+    if (mode != 2) return MFA_ERR_ARGS;
+    if (!c->p.bending) return MFA_OK;
+    return launch_bonds(c, 0, 1);
+}
+
+int mfa_ewald_k(mfa_ctx* c, int32_t mode) {
+    if (!c) return MFA_ERR_ARGS;
+    if (!c->p.charged) return MFA_OK;
+    if (mode == 0) {
+        MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+        return ewald_setup(c);
+    }
+    if (mode != 1) return MFA_ERR_ARGS;
+    return launch_ewald(c);
+}
+
+int mfa_verlet_velocities(mfa_ctx* c) {
+    if (!c) return MFA_ERR_ARGS;
+    return launch_vv_velocities(c);
+}
+
+int mfa_step(mfa_ctx* c, int32_t nsteps) {
+    if (!c || nsteps < 0) return MFA_ERR_ARGS;
+    if (nsteps == 0) return MFA_OK;
+    if (c->p.charged && c->nk == 0) return MFA_ERR_STATE;
+    if (!c->lists_valid) TRY(rebuild_abi(c, c->bin_type));
+    if (nsteps == 1) {
+        TRY(replay(c, 0));
+        c->i_time += 1;
+        return MFA_OK;
+    }
+    // first step: positions (+ skin check), conditional rebuild
+    TRY(launch_vv_positions(c, 1));
+    TRY(launch_rebuild(c, c->bin_type, 1));
+    int body = nsteps - 1;
+    while (body >= GRAPH_BODY) {
+        TRY(replay(c, 2));
+        body -= GRAPH_BODY;
+    }
+    while (body > 0) {
+        TRY(replay(c, 1));
+        --body;
+    }
+    // last step: forces and the velocity half
+    TRY(forces_fused(c));
+    TRY(launch_vv_velocities(c));
+    c->i_time += nsteps;
+    return MFA_OK;
+}
+
+int mfa_set_energy_log(mfa_ctx* c, int32_t every, int32_t capacity) {
+    if (!c || every < 0 || capacity < 0) return MFA_ERR_ARGS;
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    if (c->elog) cudaFree(c->elog);
+    if (c->elog_n) cudaFree(c->elog_n);
+    c->elog = nullptr;
+    c->elog_n = nullptr;
+    c->elog_every = 0;
+    c->elog_cap = 0;
+    invalidate_graph(c);
+    if (every == 0 || capacity == 0) return MFA_OK;
+    TRY(dalloc(&c->elog, (size_t)4 * capacity));
+    TRY(dalloc(&c->elog_n, 1));
+    MFA_CUDA_TRY(cudaMemset(c->elog_n, 0, 4));
+    c->elog_every = every;
+    c->elog_cap = capacity;
+    return MFA_OK;
+}
+
+int mfa_read_energy_log(mfa_ctx* c, double* out, int32_t max_entries, int32_t* n_out) {
+    if (!c || !n_out) return MFA_ERR_ARGS;
+    *n_out = 0;
+    if (!c->elog) return MFA_OK;
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    int32_t k = 0;
+    MFA_CUDA_TRY(cudaMemcpy(&k, c->elog_n, 4, cudaMemcpyDeviceToHost));
+    const int m = k < max_entries ? k : max_entries;
+    if (out && m > 0) MFA_CUDA_TRY(cudaMemcpy(out, c->elog, (size_t)m * 4 * 8, cudaMemcpyDeviceToHost));
+    *n_out = m;
+    return MFA_OK;
+}
+
+int mfa_get_scalars(mfa_ctx* c, mfa_scalars* o) {
+    if (!c || !o) return MFA_ERR_ARGS;
+    double s[S_NSLOT];
+    int32_t f[F_NFLAG];
+    MFA_CUDA_TRY(cudaMemcpyAsync(s, c->dscal, sizeof(s), cudaMemcpyDeviceToHost, c->st));
+    MFA_CUDA_TRY(cudaMemcpyAsync(f, c->dflags, sizeof(f), cudaMemcpyDeviceToHost, c->st));
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    memset(o, 0, sizeof(*o));
+    o->v_fluid_fluid = s[S_VFF];
+    o->v_fluid_wall = s[S_VFW];
+    o->v_intra_molec = s[S_VINTRA];
+    o->v_bend = s[S_VBEND];
+    o->v_coul = c->p.charged ? (s[S_VCR] + c->v_coul_self) + s[S_VCK] : 0.0;
+    o->t_fluid = s[S_TKIN];
+    o->v_total = s[S_VTOT];
+    o->e_total = s[S_ETOT];
+    o->virial = s[S_VIR];
+    o->i_time = c->i_time;
+    o->f_skin = f[F_SKIN];
+    o->n_rebuilds = f[F_REBUILDS];
+    o->max_neigh = f[F_MAXNB];
+    o->max_cell = f[F_MAXCELL];
+    o->fene_clamped = f[F_FENE];
+    o->error_bits = f[F_ERR];
+    o->kernel_launches = c->launches;
+    return first_error(f[F_ERR]);
+}
+
+int mfa_stream(mfa_ctx* c, void** s) {
+    if (!c || !s) return MFA_ERR_ARGS;
+    *s = (void*)c->st;
+    return MFA_OK;
+}
+
+int mfa_sync(mfa_ctx* c) {
+    if (!c) return MFA_ERR_ARGS;
+    int32_t f[F_NFLAG];
+    TRY(read_flags(c, f));
+    MFA_CUDA_TRY(cudaGetLastError());
+    return first_error(f[F_ERR]);
+}
+
+int mfa_download(mfa_ctx* c, uint32_t mask, double* r0, double* v, double* a, double* force, int32_t* mic) {
+    if (!c) return MFA_ERR_ARGS;
+    const int n = c->n;
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    // x, y, z of one quantity are contiguous on the device: one copy through
+    // the pinned staging buffer, then the interleave into the r0(3,n) layout
+    double* buf = c->h_stage;
+    auto get3 = [&](double* dst, const double* x) -> int {
+        MFA_CUDA_TRY(cudaMemcpyAsync(buf, x, (size_t)3 * n * 8, cudaMemcpyDeviceToHost, c->st));
+        MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+        for (int i = 0; i < n; ++i)
+            for (int d = 0; d < 3; ++d) dst[3 * i + d] = buf[(size_t)d * n + i];
+        return MFA_OK;
+    };
+    if ((mask & MFA_R0) && r0) TRY(get3(r0, c->rx));
+    if ((mask & MFA_V) && v) TRY(get3(v, c->vx));
+    if ((mask & MFA_A) && a) TRY(get3(a, c->ax));
+    if ((mask & MFA_F) && force) {
+        if (c->prec == MFA_MIXED) {
+            std::vector<float> f4((size_t)4 * n);
+            MFA_CUDA_TRY(cudaMemcpy(f4.data(), c->force, f4.size() * 4, cudaMemcpyDeviceToHost));
+            for (int i = 0; i < n; ++i)
+                for (int d = 0; d < 3; ++d) force[3 * i + d] = f4[4 * i + d];
+        } else {
+            std::vector<double> f4((size_t)4 * n);
+            MFA_CUDA_TRY(cudaMemcpy(f4.data(), c->force, f4.size() * 8, cudaMemcpyDeviceToHost));
+            for (int i = 0; i < n; ++i)
+                for (int d = 0; d < 3; ++d) force[3 * i + d] = f4[4 * i + d];
+        }
+    }
+    if ((mask & MFA_MIC) && mic) {
+        std::vector<int32_t> m((size_t)3 * n);
+        MFA_CUDA_TRY(cudaMemcpy(m.data(), c->mx, m.size() * 4, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < n; ++i)
+            for (int d = 0; d < 3; ++d) mic[3 * i + d] = m[(size_t)d * n + i];
+    }
+    return MFA_OK;
+}
+
+int mfa_upload(mfa_ctx* c, uint32_t mask, const double* r0, const double* v, const double* a,
+               const double* force, const int32_t* mic) {
+    if (!c) return MFA_ERR_ARGS;
+    const int n = c->n;
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    double* buf = c->h_stage;
+    auto put3 = [&](const double* src, double* x) -> int {
+        for (int i = 0; i < n; ++i)
+            for (int d = 0; d < 3; ++d) buf[(size_t)d * n + i] = src[3 * i + d];
+        MFA_CUDA_TRY(cudaMemcpyAsync(x, buf, (size_t)3 * n * 8, cudaMemcpyHostToDevice, c->st));
+        MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+        return MFA_OK;
+    };
+    if ((mask & MFA_R0) && r0) TRY(put3(r0, c->rx));
+    if ((mask & MFA_V) && v) TRY(put3(v, c->vx));
+    if ((mask & MFA_A) && a) TRY(put3(a, c->ax));
+    if ((mask & MFA_F) && force) {
+        if (c->prec == MFA_MIXED) {
+            std::vector<float> f4((size_t)4 * n, 0.0f);
+            for (int i = 0; i < n; ++i)
+                for (int d = 0; d < 3; ++d) f4[4 * i + d] = (float)force[3 * i + d];
+            MFA_CUDA_TRY(cudaMemcpy(c->force, f4.data(), f4.size() * 4, cudaMemcpyHostToDevice));
+        } else {
+            std::vector<double> f4((size_t)4 * n, 0.0);
+            for (int i = 0; i < n; ++i)
+                for (int d = 0; d < 3; ++d) f4[4 * i + d] = force[3 * i + d];
+            MFA_CUDA_TRY(cudaMemcpy(c->force, f4.data(), f4.size() * 8, cudaMemcpyHostToDevice));
+        }
+    }
+    if ((mask & MFA_MIC) && mic) {
+        std::vector<int32_t> m((size_t)3 * n);
+        for (int i = 0; i < n; ++i)
+            for (int d = 0; d < 3; ++d) m[(size_t)d * n + i] = mic[3 * i + d];
+        MFA_CUDA_TRY(cudaMemcpy(c->mx, m.data(), m.size() * 4, cudaMemcpyHostToDevice));
+    }
+    if (c->lists_valid && (mask & (MFA_R0 | MFA_V))) TRY(launch_refresh_sorted(c));
+    return MFA_OK;
+}
+
+int mfa_debug_lists(mfa_ctx* c, int32_t* cell_of, int32_t* nbr_count, int32_t* nbr, int32_t max_per) {
+    if (!c) return MFA_ERR_ARGS;
+    if (!c->lists_valid) return MFA_ERR_STATE;
+    const int n = c->n;
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    std::vector<int32_t> co(n), ids(n), cnt(n), lst((size_t)c->maxnb * n);
+    MFA_CUDA_TRY(cudaMemcpy(co.data(), c->cell_of, (size_t)n * 4, cudaMemcpyDeviceToHost));
+    MFA_CUDA_TRY(cudaMemcpy(ids.data(), c->ids, (size_t)n * 4, cudaMemcpyDeviceToHost));
+    MFA_CUDA_TRY(cudaMemcpy(cnt.data(), c->nnb, (size_t)n * 4, cudaMemcpyDeviceToHost));
+    MFA_CUDA_TRY(cudaMemcpy(lst.data(), c->nbr, lst.size() * 4, cudaMemcpyDeviceToHost));
+    if (cell_of) memcpy(cell_of, co.data(), (size_t)n * 4);
+    for (int t = 0; t < n; ++t) {
+        const int i = ids[t];
+        const int m = cnt[t] < max_per ? cnt[t] : max_per;
+        if (nbr_count) nbr_count[i] = cnt[t];
+        if (nbr)
+            for (int k = 0; k < m; ++k) nbr[(size_t)i * max_per + k] = ids[lst[(size_t)k * n + t]] + 1;
+    }
+    return MFA_OK;
+}
+
+int mfa_debug_kvecs(mfa_ctx* c, int32_t* nk, double* kvecs3, int32_t max_k) {
+    if (!c || !nk) return MFA_ERR_ARGS;
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    const int r = mfa_ewald_download_kvecs(c, kvecs3, max_k);
+    if (r < 0) return MFA_ERR_CUDA;
+    *nk = r;
+    return MFA_OK;
+}
+
+}  // extern "C"

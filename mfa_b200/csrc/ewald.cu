@@ -1,0 +1,269 @@
+// Ewald k-space (ewald_k.f90), FP64 throughout.
+//
+// mode 0 (host): the half-space set of k-vectors with |k| <= k_c, enumerated
+//   exactly as ewald_k.f90:47-124 does (same FP64 expressions, same int()
+//   truncations, so the same vectors are kept at the boundary of the sphere).
+// mode 1 (device):
+//   k_rho_partial  - structure factors rho(k) = sum_i q_i exp(i k.r_i).  Each
+//                    block takes a contiguous range of particles; for a batch of
+//                    particles it builds exp(i n dk_d r_d), n = 0..kmax_d, per
+//                    axis by a complex power recurrence from one sincos per axis,
+//                    and every thread accumulates a fixed set of k in registers
+//                    (12 FP64 flops per (particle, k)).  Partials per block.
+//   k_rho_reduce   - sums the block partials in block order (deterministic) and
+//                    the energy 4 pi / V sum_k inv_k2 exp(-k2/4a) |rho|^2.
+//   k_ewald_force  - thread per particle, the same per-axis tables in shared
+//                    memory, F_i = -8 pi q_i / V sum_k k inv_k2 exp(..) (cos Im - sin Re).
+#include "mfa_internal.cuh"
+
+#include <math.h>
+#include <vector>
+
+namespace {
+
+constexpr int KM = 16;        // largest |n| per axis held in the tables
+constexpr int RHO_T = 512;    // threads per block in k_rho_partial
+constexpr int KPT = 8;        // k per thread  -> nk <= 4096
+constexpr int CH = 32;        // particles per table batch
+constexpr int FT = 64;        // threads per block in k_ewald_force
+
+struct EwArgs {
+    const double *rx, *ry, *rz, *q;
+    const double4* kvec;      // kx, ky, kz, inv_k2 * exp(-k2 fac_alpha)
+    const int4* kn;           // nx, ny, nz
+    double2* rho_part;
+    double2* rho;
+    void* force;
+    double* partials;
+    unsigned* counter;
+    double* dscal;
+    int max_blocks;
+    int n, nk, nblk, per_blk;
+    int kmax[3];
+    double dk[3];
+    double pi, inv_V;
+};
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// tables t[d*(KM+1) + n] = exp(i n dk_d r_d), n = 0..kmax_d
+__device__ __forceinline__ void build_tables(double2* t, const EwArgs& a, double x, double y, double z) {
+    const double r[3] = {x, y, z};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double s, c;
+        sincos(a.dk[d] * r[d], &s, &c);
+        const double2 e1 = make_double2(c, s);
+        double2 e = make_double2(1.0, 0.0);
+        t[d * (KM + 1)] = e;
+        for (int n = 1; n <= a.kmax[d]; ++n) {
+            e = cmul(e, e1);
+            t[d * (KM + 1) + n] = e;
+        }
+    }
+}
+
+__device__ __forceinline__ double2 phase_from(const double2* t, int4 kn) {
+    double2 ex = t[abs(kn.x)];
+    if (kn.x < 0) ex.y = -ex.y;
+    double2 ey = t[(KM + 1) + abs(kn.y)];
+    if (kn.y < 0) ey.y = -ey.y;
+    const double2 ez = t[2 * (KM + 1) + kn.z];
+    return cmul(cmul(ex, ey), ez);
+}
+
+__global__ void __launch_bounds__(RHO_T) k_rho_partial(EwArgs a) {
+    __shared__ double2 tab[CH][3 * (KM + 1)];
+    __shared__ double sq[CH];
+    const int p0 = blockIdx.x * a.per_blk, p1 = min(a.n, p0 + a.per_blk);
+    double2 acc[KPT];
+    int4 kn[KPT];
+#pragma unroll
+    for (int j = 0; j < KPT; ++j) {
+        acc[j] = make_double2(0.0, 0.0);
+        const int k = threadIdx.x + j * RHO_T;
+        kn[j] = k < a.nk ? a.kn[k] : make_int4(0, 0, 0, 0);
+    }
+    for (int b0 = p0; b0 < p1; b0 += CH) {
+        const int nb = min(CH, p1 - b0);
+        __syncthreads();
+        if (threadIdx.x < nb) {
+            const int i = b0 + threadIdx.x;
+            build_tables(tab[threadIdx.x], a, a.rx[i], a.ry[i], a.rz[i]);
+            sq[threadIdx.x] = a.q[i];
+        }
+        __syncthreads();
+        for (int pp = 0; pp < nb; ++pp) {
+            const double qi = sq[pp];
+#pragma unroll
+            for (int j = 0; j < KPT; ++j) {
+                const double2 e = phase_from(tab[pp], kn[j]);
+                acc[j].x += qi * e.x;
+                acc[j].y += qi * e.y;
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < KPT; ++j) {
+        const int k = threadIdx.x + j * RHO_T;
+        if (k < a.nk) a.rho_part[(size_t)blockIdx.x * a.nk + k] = acc[j];
+    }
+}
+
+__global__ void k_rho_reduce(EwArgs a) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[1] = {0.0};
+    if (k < a.nk) {
+        double2 s = make_double2(0.0, 0.0);
+        for (int b = 0; b < a.nblk; ++b) {
+            const double2 v = a.rho_part[(size_t)b * a.nk + k];
+            s.x += v.x;
+            s.y += v.y;
+        }
+        a.rho[k] = s;
+        acc[0] = a.kvec[k].w * (s.x * s.x + s.y * s.y);   // ewald_k.f90:155-156
+    }
+    if (block_sum_commit<1>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_TMP0 + 2) && threadIdx.x == 0)
+        a.dscal[S_VCK] = ((a.dscal[S_TMP0 + 2] * 4.0) * a.pi) * a.inv_V;   // :159
+}
+
+template <typename R4>
+__global__ void __launch_bounds__(FT) k_ewald_force(EwArgs a) {
+    extern __shared__ double2 ftab[];
+    double2* t = ftab + threadIdx.x * 3 * (KM + 1);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const double qi = a.q[i];
+    if (qi == 0.0) return;
+    build_tables(t, a, a.rx[i], a.ry[i], a.rz[i]);
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    for (int k = 0; k < a.nk; ++k) {
+        const double2 e = phase_from(t, __ldg(&a.kn[k]));
+        const double2 r = __ldg(&a.rho[k]);
+        const double4 kv = ldg4(&a.kvec[k]);
+        const double sc = (e.x * r.y - e.y * r.x) * kv.w;   // (cos Im - sin Re) inv_k2 exp()
+        fx += kv.x * sc;
+        fy += kv.y * sc;
+        fz += kv.z * sc;
+    }
+    const double pre = ((-8.0 * a.pi) * qi) * a.inv_V;   // ewald_k.f90:194
+    R4* f4 = (R4*)a.force;
+    R4 o = f4[i];
+    o.x += pre * fx;
+    o.y += pre * fy;
+    o.z += pre * fz;
+    f4[i] = o;
+}
+
+EwArgs make_args(mfa_ctx* c) {
+    EwArgs a;
+    a.rx = c->rx; a.ry = c->ry; a.rz = c->rz; a.q = c->q;
+    a.kvec = c->kvec; a.kn = (const int4*)(c->kvec + c->nk);
+    a.rho_part = c->rho_part; a.rho = c->rho; a.force = c->force;
+    a.partials = c->partials + (size_t)R_EWALD * 4 * c->max_blocks;
+    a.counter = c->counters + R_EWALD;
+    a.dscal = c->dscal;
+    a.max_blocks = c->max_blocks;
+    a.n = c->n; a.nk = c->nk; a.nblk = c->nblk_rho;
+    a.per_blk = (c->n + c->nblk_rho - 1) / c->nblk_rho;
+    const mfa_params& p = c->p;
+    for (int d = 0; d < 3; ++d) a.kmax[d] = c->kmax[d];
+    a.pi = p.pi;
+    a.inv_V = c->inv_V;
+    // the k components are n * delta_k (ewald_k.f90:117); the tables use delta_k
+    if (p.symmetry == 1) {
+        for (int d = 0; d < 3; ++d) a.dk[d] = (2.0 * p.pi) * c->inv_boundary[d];
+    } else {
+        a.dk[0] = (2.0 * p.pi) * c->inv_boundary[0];
+        a.dk[1] = (2.0 * p.pi) * c->inv_boundary[1];
+        a.dk[2] = (2.0 * p.pi) / (p.boundary[2] + 2.0 * p.boundary[2]);
+    }
+    return a;
+}
+
+}  // namespace
+
+int ewald_setup(mfa_ctx* c) {
+    const mfa_params& p = c->p;
+    if (!p.charged) return MFA_OK;
+    double dk[3], z_slab;
+    if (p.symmetry == 1) {
+        for (int d = 0; d < 3; ++d) dk[d] = (2.0 * p.pi) * c->inv_boundary[d];
+        z_slab = 0.0;
+    } else {
+        z_slab = 2.0;
+        dk[0] = (2.0 * p.pi) * c->inv_boundary[0];
+        dk[1] = (2.0 * p.pi) * c->inv_boundary[1];
+        dk[2] = (2.0 * p.pi) / (p.boundary[2] + z_slab * p.boundary[2]);
+    }
+    volatile double kc_v = ((dk[0] + dk[1]) * (double)p.n_kmax) / 2.0;
+    const double k_c = kc_v;
+    const int nkx = (int)(k_c / dk[0]), nky = (int)(k_c / dk[1]), nkz = (int)(k_c / dk[2]);
+    if (nkx > KM || nky > KM || nkz > KM) return MFA_ERR_UNSUPPORTED;
+    const double kc2 = k_c * k_c;
+    const double fac_alpha = 1.0 / (4.0 * p.alpha_c);
+    std::vector<double4> kv;
+    std::vector<int4> kn;
+    for (int z = 0; z <= nkz; ++z)
+        for (int y = -nky; y <= nky; ++y)
+            for (int x = -nkx; x <= nkx; ++x) {
+                volatile double a0 = (double)x * dk[0], a1 = (double)y * dk[1], a2 = (double)z * dk[2];
+                volatile double s01 = a0 * a0 + a1 * a1;
+                volatile double rk_2 = s01 + a2 * a2;
+                if (rk_2 > kc2) continue;
+                if (z == 0 && y == 0 && x == 0) continue;
+                if (z == 0 && x + y < 0) continue;
+                if (z == 0 && -x == y && y > 0) continue;
+                const double k2 = rk_2;
+                volatile double inv = 1.0 / k2;
+                kv.push_back(make_double4(a0, a1, a2, inv * exp(-k2 * fac_alpha)));
+                kn.push_back(make_int4(x, y, z, 0));
+            }
+    c->nk = (int)kv.size();
+    if (c->nk > KPT * RHO_T) return MFA_ERR_UNSUPPORTED;
+    c->kmax[0] = nkx; c->kmax[1] = nky; c->kmax[2] = nkz;
+    c->inv_V = (c->inv_boundary[0] * c->inv_boundary[1]) / (p.boundary[2] * (1.0 + z_slab));
+    if (c->kvec) cudaFree(c->kvec);
+    if (c->rho) cudaFree(c->rho);
+    if (c->rho_part) cudaFree(c->rho_part);
+    c->kvec = nullptr; c->rho = nullptr; c->rho_part = nullptr;
+    // kvec block: nk double4 followed by nk int4
+    MFA_CUDA_TRY(cudaMalloc(&c->kvec, (size_t)c->nk * (sizeof(double4) + sizeof(int4))));
+    MFA_CUDA_TRY(cudaMemcpy(c->kvec, kv.data(), kv.size() * sizeof(double4), cudaMemcpyHostToDevice));
+    MFA_CUDA_TRY(cudaMemcpy(c->kvec + c->nk, kn.data(), kn.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    int nblk = (c->n + CH - 1) / CH;
+    if (nblk > 2 * 148) nblk = 2 * 148;
+    if (nblk < 1) nblk = 1;
+    c->nblk_rho = nblk;
+    MFA_CUDA_TRY(cudaMalloc(&c->rho, (size_t)c->nk * sizeof(double2)));
+    MFA_CUDA_TRY(cudaMalloc(&c->rho_part, (size_t)nblk * c->nk * sizeof(double2)));
+    const int fsm = FT * 3 * (KM + 1) * (int)sizeof(double2);
+    MFA_CUDA_TRY(cudaFuncSetAttribute(k_ewald_force<float4>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+    MFA_CUDA_TRY(cudaFuncSetAttribute(k_ewald_force<double4>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+    return MFA_OK;
+}
+
+int launch_ewald(mfa_ctx* c) {
+    if (!c->p.charged) return MFA_OK;
+    if (c->nk == 0) return MFA_ERR_STATE;
+    EwArgs a = make_args(c);
+    k_rho_partial<<<c->nblk_rho, RHO_T, 0, c->st>>>(a);
+    k_rho_reduce<<<(c->nk + 255) / 256, 256, 0, c->st>>>(a);
+    const int fsm = FT * 3 * (KM + 1) * (int)sizeof(double2);
+    if (c->prec == MFA_MIXED) k_ewald_force<float4><<<(c->n + FT - 1) / FT, FT, fsm, c->st>>>(a);
+    else k_ewald_force<double4><<<(c->n + FT - 1) / FT, FT, fsm, c->st>>>(a);
+    MFA_CUDA_TRY(cudaGetLastError());
+    note_launch(c, 3);
+    return MFA_OK;
+}
+
+int mfa_ewald_download_kvecs(mfa_ctx* c, double* out3, int max_k) {
+    if (!c->kvec) return 0;
+    std::vector<double4> kv(c->nk);
+    if (cudaMemcpy(kv.data(), c->kvec, kv.size() * sizeof(double4), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    const int m = c->nk < max_k ? c->nk : max_k;
+    for (int k = 0; k < m; ++k) { out3[3 * k] = kv[k].x; out3[3 * k + 1] = kv[k].y; out3[3 * k + 2] = kv[k].z; }
+    return c->nk;
+}

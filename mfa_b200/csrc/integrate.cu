@@ -1,0 +1,265 @@
+// Velocity-Verlet integration (verlet_positions.f90, verlet_velocities.f90) and
+// the skin check (check_skin.f90).  FP64 state, streamed once per call:
+// thread per particle, SoA arrays, coalesced.  The FP64 arithmetic uses explicit
+// round-to-nearest intrinsics so that no multiply-add is contracted and the
+// update rounds exactly like the Fortran statement order.
+#include "mfa_internal.cuh"
+
+namespace {
+
+struct VVArgs {
+    double *rx, *ry, *rz, *vx, *vy, *vz, *ax, *ay, *az;
+    const double *ox, *oy, *oz;
+    int32_t *mx, *my, *mz;
+    const int32_t *omx, *omy, *omz;
+    const int32_t* slot;
+    const int32_t* type;
+    const double* q;
+    const double *mass, *inv_mass;
+    void* pos_s;
+    void* vel_s;
+    void* force;
+    int32_t* flags;
+    int64_t* dstep;
+    double* partials;
+    unsigned* counter;
+    double* dscal;
+    double* elog;
+    int32_t* elog_n;
+    int elog_every, elog_cap;
+    int max_blocks;
+    int n;
+    int symmetry;
+    int write_sorted;
+    int pin_heads, n_chain, n_mon;
+    double L[3];
+    double dt, skin_lim;
+    double va[3];
+};
+
+// r += dt v + (0.5 dt^2) a ; v += (0.5 dt) a   (verlet_positions.f90:153,169)
+__device__ __forceinline__ void drift_kick(double& r, double& v, double a, double dt, double hdt2, double hdt) {
+    r = __dadd_rn(__dadd_rn(r, __dmul_rn(dt, v)), __dmul_rn(hdt2, a));
+    v = __dadd_rn(v, __dmul_rn(hdt, a));
+}
+
+// verlet_positions.f90:237-251
+__device__ __forceinline__ void wrap(double& r, int32_t& m, double L) {
+    if (r > L) { r = __dsub_rn(r, L); m += 1; }
+    else if (r < 0.0) { r = __dadd_rn(r, L); m -= 1; }
+}
+
+template <typename R4>
+__device__ __forceinline__ void store_sorted(const VVArgs& a, int i, double x, double y, double z,
+                                             double vx, double vy, double vz) {
+    const int s = a.slot[i];
+    R4* ps = (R4*)a.pos_s;
+    R4* vs = (R4*)a.vel_s;
+    R4 pw;
+    pw.x = x; pw.y = y; pw.z = z;
+    packw(pw, i, a.type[i]);
+    ps[s] = pw;
+    R4 vw;
+    vw.x = vx; vw.y = vy; vw.z = vz; vw.w = a.q ? a.q[i] : 0.0;
+    vs[s] = vw;
+}
+
+// check_skin.f90:8-21 on one particle
+__device__ __forceinline__ bool skin_tripped(const VVArgs& a, int i, double x, double y, double z,
+                                             int mx, int my, int mz) {
+    double d0 = __dsub_rn(__dsub_rn(__dadd_rn(a.ox[i], __dmul_rn((double)a.omx[i], a.L[0])), x), __dmul_rn((double)mx, a.L[0]));
+    double d1 = __dsub_rn(__dsub_rn(__dadd_rn(a.oy[i], __dmul_rn((double)a.omy[i], a.L[1])), y), __dmul_rn((double)my, a.L[1]));
+    double d2 = __dsub_rn(__dsub_rn(__dadd_rn(a.oz[i], __dmul_rn((double)a.omz[i], a.L[2])), z), __dmul_rn((double)mz, a.L[2]));
+    double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
+    return r2 > a.skin_lim;
+}
+
+template <typename R4>
+__device__ __forceinline__ void position_half(const VVArgs& a, int i, double x, double y, double z,
+                                              double vx, double vy, double vz, double ax, double ay, double az,
+                                              bool fused_skin) {
+    const double dt = a.dt, hdt2 = 0.5 * (dt * dt), hdt = 0.5 * dt;
+    drift_kick(x, vx, ax, dt, hdt2, hdt);
+    drift_kick(y, vy, ay, dt, hdt2, hdt);
+    drift_kick(z, vz, az, dt, hdt2, hdt);
+    int32_t mx = a.mx[i], my = a.my[i], mz = a.mz[i];
+    wrap(x, mx, a.L[0]);
+    wrap(y, my, a.L[1]);
+    if (a.symmetry == 1) wrap(z, mz, a.L[2]);
+    a.rx[i] = x; a.ry[i] = y; a.rz[i] = z;
+    a.vx[i] = vx; a.vy[i] = vy; a.vz[i] = vz;
+    a.mx[i] = mx; a.my[i] = my; a.mz[i] = mz;
+    if (fused_skin && skin_tripped(a, i, x, y, z, mx, my, mz)) a.flags[F_SKIN] = 1;
+    if (a.write_sorted) store_sorted<R4>(a, i, x, y, z, vx, vy, vz);
+}
+
+template <typename R4>
+__global__ void k_vv_positions(VVArgs a, int fused_skin) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *a.dstep += 1;
+    if (i >= a.n) return;
+    position_half<R4>(a, i, a.rx[i], a.ry[i], a.rz[i], a.vx[i], a.vy[i], a.vz[i],
+                      a.ax[i], a.ay[i], a.az[i], fused_skin != 0);
+}
+
+__global__ void k_check_skin(VVArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    if (skin_tripped(a, i, a.rx[i], a.ry[i], a.rz[i], a.mx[i], a.my[i], a.mz[i])) a.flags[F_SKIN] = 1;
+}
+
+// velocity half of verlet_velocities.f90:174-185 and the head rules :269-282.
+// Returns the kinetic contribution m v^2 of particle i.
+template <typename R4>
+__device__ __forceinline__ double velocity_half(const VVArgs& a, int i, double& vx, double& vy, double& vz,
+                                                double& ax, double& ay, double& az) {
+    R4* f = (R4*)a.force;
+    R4 fi = f[i];
+    const double im = a.inv_mass[i];
+    const double hdt = 0.5 * a.dt;
+    ax = __dmul_rn((double)fi.x, im);
+    ay = __dmul_rn((double)fi.y, im);
+    az = __dmul_rn((double)fi.z, im);
+    vx = __dadd_rn(vx, __dmul_rn(hdt, ax));
+    vy = __dadd_rn(vy, __dmul_rn(hdt, ay));
+    vz = __dadd_rn(vz, __dmul_rn(hdt, az));
+    if (a.pin_heads && i < a.n_chain * a.n_mon && (i % a.n_mon) == 0) {
+        const double sg = (i / a.n_mon < a.n_chain / 2) ? 1.0 : -1.0;
+        vx = sg * a.va[0];
+        vy = sg * a.va[1];
+        vz = 0.0;
+        ax = ay = az = 0.0;
+        R4 z4; z4.x = 0; z4.y = 0; z4.z = 0; z4.w = 0;
+        f[i] = z4;
+    }
+    const double m = a.mass[i];
+    return __dmul_rn(m, __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz)));
+}
+
+__device__ __forceinline__ void finish_energies(const VVArgs& a) {
+    // verlet_velocities.f90:334-347 (v_wall_wall = 0, t_wall = 0)
+    double* s = a.dscal;
+    s[S_TKIN] = 0.5 * s[S_TKIN];
+    s[S_VTOT] = (s[S_VFW] + s[S_VFF]) + s[S_VINTRA];
+    s[S_ETOT] = s[S_VTOT] + s[S_TKIN];
+    if (a.elog && a.elog_every > 0) {
+        const long long st = *a.dstep;
+        if (st % a.elog_every == 0) {
+            const int k = *a.elog_n;
+            if (k < a.elog_cap) {
+                a.elog[4 * k + 0] = (double)st;
+                a.elog[4 * k + 1] = s[S_ETOT];
+                a.elog[4 * k + 2] = s[S_VTOT];
+                a.elog[4 * k + 3] = s[S_TKIN];
+                *a.elog_n = k + 1;
+            }
+        }
+    }
+}
+
+template <typename R4>
+__global__ void k_vv_velocities(VVArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double ke[1] = {0.0};
+    if (i < a.n) {
+        double vx = a.vx[i], vy = a.vy[i], vz = a.vz[i], ax, ay, az;
+        ke[0] = velocity_half<R4>(a, i, vx, vy, vz, ax, ay, az);
+        a.vx[i] = vx; a.vy[i] = vy; a.vz[i] = vz;
+        a.ax[i] = ax; a.ay[i] = ay; a.az[i] = az;
+    }
+    if (block_sum_commit<1>(ke, a.partials, a.max_blocks, a.counter, a.dscal + S_TKIN)) {
+        if (threadIdx.x == 0) finish_energies(a);
+    }
+}
+
+// verlet_velocities of step n followed by verlet_positions of step n+1 in one
+// pass over the state (the skin check of n+1 fused in).
+template <typename R4>
+__global__ void k_vv_fused(VVArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double ke[1] = {0.0};
+    if (i < a.n) {
+        double vx = a.vx[i], vy = a.vy[i], vz = a.vz[i], ax, ay, az;
+        ke[0] = velocity_half<R4>(a, i, vx, vy, vz, ax, ay, az);
+        a.ax[i] = ax; a.ay[i] = ay; a.az[i] = az;
+        position_half<R4>(a, i, a.rx[i], a.ry[i], a.rz[i], vx, vy, vz, ax, ay, az, true);
+    }
+    if (block_sum_commit<1>(ke, a.partials, a.max_blocks, a.counter, a.dscal + S_TKIN)) {
+        if (threadIdx.x == 0) {
+            finish_energies(a);
+            *a.dstep += 1;  // the next step has begun
+        }
+    }
+}
+
+VVArgs make_args(mfa_ctx* c) {
+    VVArgs a;
+    a.rx = c->rx; a.ry = c->ry; a.rz = c->rz;
+    a.vx = c->vx; a.vy = c->vy; a.vz = c->vz;
+    a.ax = c->ax; a.ay = c->ay; a.az = c->az;
+    a.ox = c->ox; a.oy = c->oy; a.oz = c->oz;
+    a.mx = c->mx; a.my = c->my; a.mz = c->mz;
+    a.omx = c->omx; a.omy = c->omy; a.omz = c->omz;
+    a.slot = c->slot; a.type = c->type; a.q = c->p.charged ? c->q : nullptr;
+    a.mass = c->mass; a.inv_mass = c->inv_mass;
+    a.pos_s = c->pos_s; a.vel_s = c->vel_s; a.force = c->force;
+    a.flags = c->dflags; a.dstep = c->dstep;
+    a.partials = c->partials + (size_t)R_VV * 4 * c->max_blocks;
+    a.counter = c->counters + R_VV;
+    a.dscal = c->dscal;
+    a.elog = c->elog; a.elog_n = c->elog_n; a.elog_every = c->elog_every; a.elog_cap = c->elog_cap;
+    a.max_blocks = c->max_blocks;
+    a.n = c->n;
+    a.symmetry = c->p.symmetry;
+    a.write_sorted = c->lists_valid;
+    a.pin_heads = c->p.pin_heads; a.n_chain = c->p.n_chain; a.n_mon = c->p.n_mon;
+    for (int d = 0; d < 3; ++d) { a.L[d] = c->p.boundary[d]; a.va[d] = c->p.va_spring_twall[d]; }
+    a.dt = c->p.dt;
+    a.skin_lim = (c->p.skin / 2.0) * (c->p.skin / 2.0);
+    return a;
+}
+
+constexpr int TPB = 256;
+
+}  // namespace
+
+int launch_vv_positions(mfa_ctx* c, int fused_skin) {
+    VVArgs a = make_args(c);
+    const int nb = (c->n + TPB - 1) / TPB;
+    if (c->prec == MFA_MIXED) k_vv_positions<float4><<<nb, TPB, 0, c->st>>>(a, fused_skin);
+    else k_vv_positions<double4><<<nb, TPB, 0, c->st>>>(a, fused_skin);
+    MFA_CUDA_TRY(cudaGetLastError());
+    note_launch(c, 1);
+    return MFA_OK;
+}
+
+int launch_check_skin(mfa_ctx* c) {
+    VVArgs a = make_args(c);
+    const int nb = (c->n + TPB - 1) / TPB;
+    k_check_skin<<<nb, TPB, 0, c->st>>>(a);
+    MFA_CUDA_TRY(cudaGetLastError());
+    note_launch(c, 1);
+    return MFA_OK;
+}
+
+int launch_vv_velocities(mfa_ctx* c) {
+    VVArgs a = make_args(c);
+    const int nb = (c->n + TPB - 1) / TPB;
+    if (nb > c->max_blocks) return MFA_ERR_ARGS;
+    if (c->prec == MFA_MIXED) k_vv_velocities<float4><<<nb, TPB, 0, c->st>>>(a);
+    else k_vv_velocities<double4><<<nb, TPB, 0, c->st>>>(a);
+    MFA_CUDA_TRY(cudaGetLastError());
+    note_launch(c, 1);
+    return MFA_OK;
+}
+
+int launch_vv_fused(mfa_ctx* c) {
+    VVArgs a = make_args(c);
+    const int nb = (c->n + TPB - 1) / TPB;
+    if (nb > c->max_blocks) return MFA_ERR_ARGS;
+    if (c->prec == MFA_MIXED) k_vv_fused<float4><<<nb, TPB, 0, c->st>>>(a);
+    else k_vv_fused<double4><<<nb, TPB, 0, c->st>>>(a);
+    MFA_CUDA_TRY(cudaGetLastError());
+    note_launch(c, 1);
+    return MFA_OK;
+}

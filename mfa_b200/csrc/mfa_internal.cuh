@@ -1,0 +1,250 @@
+// Internal declarations of the B200 implementation of mfa's per-step loop.
+// Device data layout (all resident in HBM for the life of a context):
+//   FP64 SoA state in particle order: r (x,y,z), v, a, mic_count, r0_old, mic_old
+//   force:   one 4-wide record per particle (float4 in MIXED, double4 in FP64)
+//   pos_s:   cell-sorted copy of positions, w = (id << 8 | type)   (float4 / double4)
+//   vel_s:   cell-sorted copy of velocities, w = charge             (float4 / double4)
+//   ids:     slot -> particle, slot: particle -> slot (counting sort by cell)
+//   nbr:     full Verlet list in slot space, column k of row t at nbr[k*n + t]
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "../../include/mfa_gpu.h"
+
+#define T8 MFA_MAX_TYPES
+
+// scalar slots in ctx->dscal (device FP64)
+enum {
+    S_VFF = 0,      // LJ energy
+    S_VIR = 1,      // pair virial
+    S_VCR = 2,      // Coulomb real-space energy (without self term)
+    S_VFW = 3,      // wall energy
+    S_VINTRA = 4,   // FENE energy (already multiplied by k)
+    S_VBEND = 5,
+    S_TKIN = 6,     // 0.5 sum m v^2
+    S_VCK = 7,      // Coulomb k-space energy
+    S_VTOT = 8,
+    S_ETOT = 9,
+    S_VCOUL = 10,   // real + self + k
+    S_TMP0 = 12,    // 12..15: staging for kernels that publish a subset of slots
+    S_NSLOT = 16
+};
+
+// int flags in ctx->dflags
+enum {
+    F_ERR = 0,       // error bits (1 << mfa_status)
+    F_SKIN = 1,      // rebuild due
+    F_MAXNB = 2,     // largest list row at the last rebuild
+    F_MAXCELL = 3,   // largest cell at the last rebuild
+    F_NEEDNB = 4,    // list capacity that would have been needed
+    F_REBUILDS = 5,  // rebuild counter
+    F_FENE = 6,      // FENE bonds at the clamp in the last bond pass
+    F_NFLAG = 8
+};
+
+// reduction counters (last-block-done pattern), one per reducing kernel
+enum { R_PAIR = 0, R_BOND = 1, R_WALL = 2, R_VV = 3, R_EWALD = 4, R_N = 8 };
+
+struct mfa_ctx {
+    mfa_params p;
+    int prec;            // MFA_FP64 / MFA_MIXED
+    int dev;
+    cudaStream_t st;
+    int n;
+    // FP64 state
+    double *rx, *ry, *rz, *vx, *vy, *vz, *ax, *ay, *az;
+    double *ox, *oy, *oz;               // r0_old
+    int32_t *mx, *my, *mz, *omx, *omy, *omz;
+    int32_t* type;
+    double *mass, *inv_mass, *q;
+    void* force;                        // float4 / double4 [n]
+    void* pos_s;                        // float4 / double4 [n]
+    void* vel_s;                        // float4 / double4 [n]
+    double4* pos64;                     // FP64 sorted positions for the list builder (scratch)
+    int32_t *ids, *slot;
+    // cells
+    int nb[3], ncell;
+    double rbin[3], inv_rbin[3], inv_boundary[3];
+    int32_t *cell_count, *cell_start, *cell_cursor, *cell_of;
+    // pair tables on the device: range_2+skin_2, range_2, epsil, sigma_2, e_shift, inv_range_2
+    double* tabs;                       // 6 x T8*T8
+    // Verlet list
+    int maxnb;
+    int32_t *nbr, *nnb;
+    // reductions / flags
+    double* partials;                   // R_N regions x max_blocks x 4 quantities
+    int max_blocks;
+    unsigned* counters;                 // R_N
+    double* dscal;                      // S_NSLOT
+    int32_t* dflags;                    // F_NFLAG
+    int64_t* dstep;                     // device copy of i_time
+    // Ewald
+    int nk;
+    double4* kvec;                      // (kx, ky, kz, inv_k2*exp(-k2/(4 alpha_c)))
+    double2* rho;                       // nk
+    double2* rho_part;                  // nblk_rho x nk
+    int nblk_rho;
+    int kmax[3];
+    double inv_V, v_coul_self;
+    // host-side bookkeeping
+    int64_t i_time;
+    int bin_type;                       // 0 after binning, 1 after my_binning
+    int lists_valid;
+    int n_rebuilds_host;
+    // fast path: captured graphs (0: one full step, 1: one fused body step,
+    // 2: GRAPH_BODY fused body steps) and the number of kernels in each
+    cudaGraphExec_t gexec[3];
+    cudaGraph_t graph[3];
+    int graph_kernels[3];
+    const void* graph_key[4];           // what the captured arguments depend on
+    // kernel launch accounting
+    long long launches;
+    long long cap_count;
+    int capturing;
+    // energy log
+    double* elog;
+    int elog_every, elog_cap;
+    int32_t* elog_n;
+    // pinned host staging for uploads/downloads (3 x n doubles)
+    double* h_stage;
+    // bonds launch geometry
+    int bond_warps_per_block;
+    size_t bond_smem;
+};
+
+// ---------- launchers (each file) ----------
+// integrate.cu
+int launch_vv_positions(mfa_ctx* c, int fused_skin);
+int launch_check_skin(mfa_ctx* c);
+int launch_vv_velocities(mfa_ctx* c);
+int launch_vv_fused(mfa_ctx* c);
+// binning.cu
+int launch_rebuild(mfa_ctx* c, int rule, int conditional);
+int launch_refresh_sorted(mfa_ctx* c);
+// pair.cu
+int launch_pair(mfa_ctx* c, int fuse_wall, int accumulate);
+// bonds.cu
+int launch_bonds(mfa_ctx* c, int do_fene, int do_bend);
+int bonds_setup(mfa_ctx* c);
+// wall.cu
+int launch_wall(mfa_ctx* c, int inter_type);
+// ewald.cu
+int ewald_setup(mfa_ctx* c);
+int launch_ewald(mfa_ctx* c);
+
+// every kernel launch is recorded (graph captures count towards their graph)
+inline void note_launch(mfa_ctx* c, int k) {
+    if (c->capturing) c->cap_count += k;
+    else c->launches += k;
+}
+
+#define MFA_CUDA_TRY(x)                                   \
+    do {                                                  \
+        cudaError_t e__ = (x);                            \
+        if (e__ != cudaSuccess) return MFA_ERR_CUDA;      \
+    } while (0)
+
+// ---------- device helpers ----------
+__device__ __forceinline__ double mimage64(double d, double L, double invL) {
+    // d - L*int(2d/L) with int() truncating toward zero (fluid_fluid.f90:84-88);
+    // explicit round-to-nearest ops so that no multiply-add is fused.
+    double t = __dmul_rn(__dmul_rn(2.0, d), invL);
+    return __dsub_rn(d, __dmul_rn(L, (double)(int)t));
+}
+__device__ __forceinline__ float mimage32(float d, float L, float invL) {
+    float t = 2.0f * d * invL;
+    return d - L * (float)(int)t;
+}
+
+__device__ __forceinline__ void set_err(int32_t* flags, int status) {
+    atomicOr(&flags[F_ERR], 1 << status);
+}
+
+// Philox-4x32-10 (Salmon et al., SC'11), counter (c0..c3), key (k0, k1).
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+    const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+        uint32_t hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+        uint4 o;
+        o.x = hi1 ^ c.y ^ k0;
+        o.y = lo1;
+        o.z = hi0 ^ c.w ^ k1;
+        o.w = lo0;
+        c = o;
+        k0 += W0;
+        k1 += W1;
+    }
+    return c;
+}
+#define TAG_DPD 0x44504400u
+#define TAG_LGV 0x4C475600u
+
+// Block-wide FP64 sums of NQ values, committed deterministically: each block
+// writes its partials, the last block to finish adds them in block order and
+// stores the result in out[0..NQ).  Requires blockDim.x a multiple of 32, <= 1024.
+template <int NQ>
+__device__ __forceinline__ bool block_sum_commit(double (&v)[NQ], double* partials, int max_blocks,
+                                                 unsigned* counter, double* out) {
+    __shared__ double sm[NQ][32];
+    __shared__ bool am_last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+        double x = v[q];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sm[q][wid] = x;
+    }
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            double x = lane < nw ? sm[q][lane] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            if (lane == 0) partials[q * max_blocks + blockIdx.x] = x;
+        }
+    }
+    __threadfence();
+    if (threadIdx.x == 0) am_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!am_last) return false;
+    __threadfence();
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+        double x = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+            x += __ldcg(&partials[q * max_blocks + b]);
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        __syncthreads();
+        if (lane == 0) sm[q][wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            double y = lane < nw ? sm[q][lane] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) y += __shfl_down_sync(0xffffffffu, y, o);
+            if (lane == 0) out[q] = y;
+        }
+    }
+    if (threadIdx.x == 0) *counter = 0u;
+    return true;
+}
+
+// read-only-path loads of 4-wide records
+__device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ double4 ldg4(const double4* p) {
+    const double2* q = (const double2*)p;
+    const double2 a = __ldg(q), b = __ldg(q + 1);
+    double4 r;
+    r.x = a.x; r.y = a.y; r.z = b.x; r.w = b.y;
+    return r;
+}
+
+// The w lane of the sorted position record carries (particle id << 8 | type)
+// as raw bits; no arithmetic is ever done on it.
+__device__ __forceinline__ void packw(float4& p, int id, int t) { p.w = __int_as_float((id << 8) | t); }
+__device__ __forceinline__ void packw(double4& p, int id, int t) {
+    p.w = __longlong_as_double((long long)((id << 8) | t));
+}
+__device__ __forceinline__ int wbits(float w) { return __float_as_int(w); }
+__device__ __forceinline__ int wbits(double w) { return (int)__double_as_longlong(w); }

@@ -1,0 +1,261 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle.
+
+Tolerances (max-norm relative error unless stated):
+  FP64 path   forces 1e-12; trajectories over 100 steps 1e-10 (thermostat off
+              and DPD with Philox noise); neighbour lists and cells bit-exact.
+  MIXED path  forces 1e-4 (FP32 pair/bond math); positions after 100 steps 1e-5
+              (relative to the box), energies 1e-5.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from conftest import relerr
+from mfa_b200 import _abi, configs
+from mfa_b200._abi import FP64, MIXED, MfaError
+from mfa_b200.api import System
+from oracle import Oracle, pair_multiset_full, pair_multiset_half
+
+pytestmark = pytest.mark.gpu
+
+CFGS = ["melt_cfg", "brush_small_cfg", "charged_small_cfg", "charged_ref_cfg"]
+
+
+def pair(cfg, prec, params=None, list_cap=512):
+    p = cfg.params if params is None else params
+    o = Oracle(p, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, list_cap=list_cap)
+    g = System(p, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=prec)
+    return o, g
+
+
+@pytest.mark.parametrize("name", CFGS)
+def test_binning_bit_exact(name, request):
+    cfg = request.getfixturevalue(name)
+    o, g = pair(cfg, MIXED)
+    o.binning()
+    g.binning()
+    cell_o, _, ff = o.lists()
+    cell_g, cnt, nbr = g.debug_lists(512)
+    assert (cell_o == cell_g).all()
+    half = pair_multiset_half(ff)
+    full = pair_multiset_full(cnt, nbr)
+    assert half.shape == full.shape and (half == full).all()
+    # the full list is symmetric
+    assert cnt.sum() == 2 * half.shape[0]
+    g.close()
+
+
+@pytest.mark.parametrize("name", ["melt_cfg", "charged_small_cfg"])
+def test_my_binning_bit_exact(name, request):
+    cfg = request.getfixturevalue(name)
+    o, g = pair(cfg, FP64)
+    o.my_binning()
+    g.my_binning()
+    cell_o, _, ff = o.lists()
+    cell_g, cnt, nbr = g.debug_lists(512)
+    assert (cell_o == cell_g).all()
+    ref = pair_multiset_full(ff[:, 0], ff[:, 1:])
+    got = pair_multiset_full(cnt, nbr)
+    assert ref.shape == got.shape and (ref == got).all()
+    g.close()
+
+
+def test_binning_duplicate_cell_visits():
+    """n_bin = 2 with delta_bin = 1 (make_binning_boxes.f90:145-168): pairs in
+    the other cell are listed twice, as in the reference."""
+    cfg = configs.melt(seed=5, n_chain=10, n_mon=8, density=0.5)
+    p = cfg.params.copy()
+    p.n_bin[:] = [2, 2, 2]
+    p.delta_bin[:] = [1, 1, 1]
+    o, g = pair(cfg, FP64, params=p)
+    o.binning()
+    g.binning()
+    half = pair_multiset_half(o.lists()[2])
+    cnt, nbr = g.debug_lists(512)[1:]
+    full = pair_multiset_full(cnt, nbr)
+    assert half.shape == full.shape and (half == full).all()
+    assert len({tuple(x) for x in half}) < half.shape[0]   # duplicates present
+    g.close()
+
+
+@pytest.mark.parametrize("name", CFGS)
+@pytest.mark.parametrize("prec,tol", [(FP64, 1e-12), (MIXED, 1e-4)])
+def test_initial_forces_and_energies(name, prec, tol, request):
+    cfg = request.getfixturevalue(name)
+    o, g = pair(cfg, prec)
+    o.init_forces()
+    g.init_forces()
+    assert relerr(g.download(_abi.F)["force"], o.state()["force"]) < tol
+    so, sg = o.scalars(), g.scalars()
+    for k in ("v_fluid_fluid", "v_fluid_wall", "v_intra_molec", "v_coul"):
+        assert sg[k] == pytest.approx(so[k], rel=tol * 10, abs=tol * 10 * cfg.n), k
+    g.close()
+
+
+def run_both(o, g, nsteps):
+    fo, fg = [], []
+    for _ in range(nsteps):
+        o.md_step()
+        fg.append(g.md_step())
+        fo.append(o.scalars()["f_skin"])
+    return fo, fg
+
+
+@pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg", "charged_small_cfg"])
+@pytest.mark.parametrize("thermo", [_abi.THERMO_NONE, _abi.THERMO_DPD])
+def test_fp64_trajectory_100_steps(name, thermo, request):
+    cfg = request.getfixturevalue(name)
+    p = cfg.params.copy()
+    p.thermostat = thermo
+    o, g = pair(cfg, FP64, params=p)
+    o.init_forces()
+    g.init_forces()
+    run_both(o, g, 100)
+    so, sg = o.state(), g.download()
+    assert relerr(sg["r0"], so["r0"]) < 1e-10
+    assert relerr(sg["v"], so["v"]) < 1e-10
+    assert (sg["mic"] == so["mic"]).all()
+    eo, eg = o.scalars(), g.scalars()
+    assert eg["e_total"] == pytest.approx(eo["e_total"], rel=1e-10)
+    assert eg["n_rebuilds"] == eo["n_rebuilds"]
+    g.close()
+
+
+@pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg", "charged_small_cfg"])
+def test_mixed_trajectory_100_steps(name, request):
+    cfg = request.getfixturevalue(name)
+    o, g = pair(cfg, MIXED)
+    o.init_forces()
+    g.init_forces()
+    run_both(o, g, 100)
+    so, sg = o.state(), g.download()
+    L = max(cfg.params.boundary)
+    assert np.abs(sg["r0"] - so["r0"]).max() / L < 1e-5
+    assert g.scalars()["e_total"] == pytest.approx(o.scalars()["e_total"], rel=1e-5)
+    g.close()
+
+
+@pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg", "charged_small_cfg"])
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+def test_fast_path_equals_subroutine_path(name, prec, request):
+    """mfa_step (fused kernels, captured graphs, device-side rebuild decision)
+    gives bit-identical states to the per-subroutine path."""
+    cfg = request.getfixturevalue(name)
+    g1 = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=prec)
+    g2 = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=prec)
+    g1.init_forces()
+    g2.init_forces()
+    for _ in range(57):
+        g1.md_step()
+    g2.step(57)
+    s1, s2 = g1.download(), g2.download()
+    assert (s1["r0"] == s2["r0"]).all() and (s1["v"] == s2["v"]).all()
+    e1, e2 = g1.scalars(), g2.scalars()
+    assert e1["e_total"] == e2["e_total"] and e1["i_time"] == e2["i_time"] == 57
+    assert e1["n_rebuilds"] == e2["n_rebuilds"]
+    g1.close()
+    g2.close()
+
+
+@pytest.mark.parametrize("name", ["charged_small_cfg", "charged_ref_cfg"])
+def test_ewald_kspace(name, request):
+    cfg = request.getfixturevalue(name)
+    o, g = pair(cfg, FP64)
+    o.ewald_k(0)
+    g.ewald_k(0)
+    ko, kg = o.kvecs(), g.kvecs()
+    assert ko.shape == kg.shape and (ko == kg).all()     # same vectors, bit for bit
+    o.binning()
+    g.binning()
+    for x in (o, g):
+        x.zero_forces()
+        x.fluid_fluid()
+    o.zero_forces()
+    g.zero_forces()
+    o.ewald_k(1)
+    g.ewald_k(1)
+    assert relerr(g.download(_abi.F)["force"], o.state()["force"]) < 1e-10
+    assert g.scalars()["v_coul"] == pytest.approx(o.scalars()["v_coul"], rel=1e-11)
+    g.close()
+
+
+def test_walls_hard_and_half_hard(brush_small_cfg):
+    cfg = brush_small_cfg
+    for it in (3, 4):
+        p = cfg.params.copy()
+        p.wall = it
+        r0 = cfg.r0.copy()
+        v = cfg.v.copy()
+        r0[:20, 2] = np.linspace(0.001, 0.009, 20)
+        v[:20, 2] = -1.0
+        r0[20:40, 2] = p.z_space_wall - 0.005
+        v[20:40, 2] = 1.0
+        o = Oracle(p, r0, v, cfg.a_type, cfg.mass, list_cap=512)
+        g = System(p, r0, v, cfg.a_type, cfg.mass, precision=FP64)
+        for x in (o, g):
+            x.zero_forces()
+            x.fluid_wall(it)
+        assert relerr(g.download()["v"], o.state()["v"]) == 0.0
+        assert relerr(g.download(_abi.F)["force"], o.state()["force"]) < 1e-12
+        g.close()
+
+
+def test_error_particle_outside_grid(brush_small_cfg):
+    cfg = brush_small_cfg
+    r0 = cfg.r0.copy()
+    r0[5, 2] = -3.0     # inside the bottom wall: mod(int(z/r_bin), n) < 0 (binning.f90:29)
+    g = System(cfg.params, r0, cfg.v, cfg.a_type, cfg.mass, precision=MIXED)
+    with pytest.raises(MfaError) as e:
+        g.binning()
+    assert e.value.status == _abi.ERR_CELL_RANGE
+    g.close()
+
+
+def test_error_nonfinite_position(melt_cfg):
+    cfg = melt_cfg
+    r0 = cfg.r0.copy()
+    r0[7, 0] = np.nan
+    g = System(cfg.params, r0, cfg.v, cfg.a_type, cfg.mass, precision=MIXED)
+    with pytest.raises(MfaError) as e:
+        g.binning()
+    assert e.value.status == _abi.ERR_NONFINITE
+    g.close()
+
+
+def test_neighbour_capacity_grows():
+    """A clustered configuration overflows the list capacity estimated from the
+    mean density; mfa_binning grows it and the list still matches."""
+    cfg = configs.melt(seed=6, n_chain=40, n_mon=20, density=0.85)
+    p = cfg.params.copy()
+    L = 3.0 * p.boundary[0]
+    p.boundary[:] = [L, L, L]
+    for d in range(3):
+        p.n_bin[d] = int(L / (math.sqrt(p.range_2[0]) + 0.4))
+    # squeeze the beads into a corner at ~4x the density the capacity is sized for
+    cfg = configs.Config(cfg.name, cfg.spec, p, cfg.r0 * 0.6, cfg.v, cfg.a_type, cfg.mass)
+    o, g = pair(cfg, FP64, params=p)
+    o.binning()
+    g.binning()
+    half = pair_multiset_half(o.lists()[2])
+    cnt, nbr = g.debug_lists(512)[1:]
+    full = pair_multiset_full(cnt, nbr)
+    assert half.shape == full.shape and (half == full).all()
+    g.close()
+
+
+def test_energy_log_and_dpd_temperature(melt_cfg):
+    """Thermostat-on physics is checked statistically: the DPD thermostat holds
+    kT = 1 (the reference draws its noise in traversal order, so trajectories
+    cannot be compared)."""
+    cfg = melt_cfg
+    g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, precision=MIXED)
+    g.init_forces()
+    g.set_energy_log(10, 1000)
+    g.step(4000)
+    log = g.energy_log()
+    assert log.shape[0] == 400
+    assert (np.diff(log[:, 0]) == 10).all()
+    T = 2.0 * log[200:, 3] / (3.0 * cfg.n)
+    assert T.mean() == pytest.approx(1.0, abs=0.05)
+    g.close()
