@@ -44,11 +44,59 @@ def args_():
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="brush", choices=["brush", "melt", "charged"])
-    ap.add_argument("--equil", type=int, default=2000, help="untimed relaxation steps of the fresh configuration")
+    ap.add_argument("--equil", type=int, default=10000, help="untimed relaxation steps of the fresh configuration")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--drift", action="store_true",
+                    help="energy drift of FP64 vs mixed over --drift-steps NVE steps (not a throughput run)")
+    ap.add_argument("--drift-steps", type=int, default=100000)
+    ap.add_argument("--drift-equil", type=int, default=20000)
     return ap.parse_args()
+
+
+def drift(a):
+    """Equilibrate with the thermostat (FP64), then run the same state without
+    thermostat (NVE) in FP64 and in mixed precision and report the energy
+    drift per bead, a linear-fit slope per 1e5 steps and the step time."""
+    import numpy as np
+    import torch
+    from mfa_b200 import _abi
+    from mfa_b200.api import System
+    cfg, meta = make_config(a.workload, a.seed)
+    g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=_abi.FP64)
+    g.init_forces()
+    g.step(a.drift_equil)
+    st = g.download()
+    g.close()
+    p = cfg.params.copy()
+    p.thermostat = _abi.THERMO_NONE
+    every = max(1, a.drift_steps // 1000)
+    res = {}
+    for name, prec in (("fp64", _abi.FP64), ("mixed", _abi.MIXED)):
+        h = System(p, st["r0"], st["v"], cfg.a_type, cfg.mass, q=cfg.q, mic=st["mic"], precision=prec)
+        h.init_forces(full=True)
+        h.set_energy_log(every, a.drift_steps // every + 8)
+        ext = torch.cuda.ExternalStream(h.stream_ptr())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        h.step(a.drift_steps)
+        e1.record(ext)
+        h.sync()
+        log = h.energy_log()
+        t, E, T = log[:, 0], log[:, 1], log[:, 3]
+        slope = float(np.polyfit(t, E, 1)[0])
+        res[name] = {"drift_per_bead": float((E[-1] - E[0]) / cfg.n),
+                     "fit_slope_per_bead_per_1e5_steps": slope * 1e5 / cfg.n,
+                     "fluct_rms_per_bead": float(np.std(E) / cfg.n),
+                     "kT_mean": float(2.0 * T.mean() / (3.0 * cfg.n)),
+                     "ms_per_step": e0.elapsed_time(e1) / a.drift_steps,
+                     "bead_steps_per_s": cfg.n * a.drift_steps / (e0.elapsed_time(e1) * 1e-3)}
+        h.close()
+    print(json.dumps({"mode": "drift", "workload": meta["workload"], "beads": cfg.n, "nve_steps": a.drift_steps,
+                      "dt": cfg.params.dt, "equilibration_steps_dpd": a.drift_equil, **res,
+                      "mixed_over_fp64_speed": res["mixed"]["bead_steps_per_s"] / res["fp64"]["bead_steps_per_s"]}))
+    return 0
 
 
 def make_config(name, seed):
@@ -173,6 +221,8 @@ def pair_work(g, cfg):
 
 def main():
     a = args_()
+    if a.drift:
+        return drift(a)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -202,6 +252,7 @@ def main():
     import torch
     from mfa_b200 import _abi
     from mfa_b200.api import System
+    from mfa_b200.tune import tune_pair_shape
 
     dist = None
     if world > 1:
@@ -223,6 +274,8 @@ def main():
         g.init_forces()
         if a.equil:
             g.step(a.equil)
+        tuned = tune_pair_shape(g)
+        g.tuned = min(tuned, key=tuned.get)
         ext = torch.cuda.ExternalStream(g.stream_ptr(), device=f"cuda:{dev}")
         for k in range(warmup):
             with torch.cuda.stream(ext):
@@ -230,12 +283,14 @@ def main():
             g.step(1)
         g.sync()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-        launches0 = g.scalars()["kernel_launches"]
+        s0 = g.scalars()
+        launches0 = s0["kernel_launches"]
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize(dev)
         sampler = ClockSampler(dev)
         sampler.start()
+        torch.cuda.nvtx.range_push(f"timed_{'mixed' if prec == _abi.MIXED else 'fp64'}")
         for k in range(steps):
             if flush_l2:
                 with torch.cuda.stream(ext):
@@ -243,6 +298,7 @@ def main():
             ev[k][0].record(ext)
             g.step(1)
             ev[k][1].record(ext)
+        torch.cuda.nvtx.range_pop()
         g.sync()
         torch.cuda.synchronize(dev)
         clocks = sampler.stop()
@@ -250,10 +306,12 @@ def main():
             dist.barrier()
         ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
         s = g.scalars()
+        s["rebuilds_timed"] = s["n_rebuilds"] - s0["n_rebuilds"]
         return g, ms, s["kernel_launches"] - launches0, clocks, s
 
     # headline: mixed precision
     g, ms_mixed, launches, clocks, s_mixed = timed_run(_abi.MIXED, a.steps, a.warmup)
+    shape_mixed = g.tuned
     ms_max = ms_mixed
     if dist is not None:
         t = torch.tensor([ms_mixed], dtype=torch.float64, device=f"cuda:{dev}")
@@ -362,6 +420,7 @@ def main():
             "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded generator, no reference data)",
             "config": dict(meta, beads=n, precision="mixed", dt=cfg.params.dt, skin=cfg.params.skin,
+                           pair_shape=f"{shape_mixed[0]} threads/particle x {shape_mixed[1]}-thread blocks (autotuned)",
                            thermostat="dpd", replicas=world,
                            l2="flushed between timed steps (256 MiB write on the context stream)",
                            parallelism=f"replicas x{world}"),
@@ -376,6 +435,7 @@ def main():
                          "fp32_tflops": pair_flops / (pair_ms * 1e-3) / 1e12, **work},
             "e2e": e2e_obj,
             "gpu_launches": int(launches),
+            "list_rebuilds_in_timed_steps": int(s_mixed["rebuilds_timed"]),
             "clocks": clocks,
         }
         if cpu is not None:

@@ -219,6 +219,12 @@ int mfa_step(mfa_ctx* ctx, int32_t nsteps);
 int mfa_set_energy_log(mfa_ctx* ctx, int32_t every, int32_t capacity);
 int mfa_read_energy_log(mfa_ctx* ctx, double* out3, int32_t max_entries, int32_t* n_out);
 
+/* Launch shape of the pair kernel: threads that share one particle's
+ * neighbour list (1, 2 or 4) and threads per block (32..256, multiple of 32).
+ * Results do not depend on it beyond floating-point summation order; it is
+ * what the autotuner (mfa_b200.tune) chooses. */
+int mfa_set_pair_shape(mfa_ctx* ctx, int32_t threads_per_particle, int32_t block);
+
 /* ---------------- host mirrors ---------------- */
 
 int mfa_get_scalars(mfa_ctx* ctx, mfa_scalars* out);

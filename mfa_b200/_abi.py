@@ -124,6 +124,7 @@ SIGNATURES = {
     "mfa_upload": (C.c_int, [_P, C.c_uint32, _DP, _DP, _DP, _DP, _IP]),
     "mfa_sync": (C.c_int, [_P]),
     "mfa_stream": (C.c_int, [_P, C.POINTER(_P)]),
+    "mfa_set_pair_shape": (C.c_int, [_P, C.c_int32, C.c_int32]),
     "mfa_debug_lists": (C.c_int, [_P, _IP, _IP, _IP, C.c_int32]),
     "mfa_debug_kvecs": (C.c_int, [_P, _IP, _DP, C.c_int32]),
 }

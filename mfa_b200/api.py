@@ -111,9 +111,11 @@ class System:
         check(self.lib.mfa_verlet_velocities(self.ctx), "verlet_velocities")
 
     # ---- compositions ----
-    def init_forces(self) -> None:
+    def init_forces(self, full: bool = False) -> None:
         """The start-up sequence of conf_default.f90:254-299: lists, the forces
-        fluid_fluid / fluid_wall / intra_molec, then a = F/m."""
+        fluid_fluid / fluid_wall / intra_molec, then a = F/m.  full=True also
+        adds bending and the Ewald k-space forces (the complete per-step force
+        set), for starting a run from a state produced elsewhere."""
         p = self.params
         if p.charged:
             self.ewald_k(0)
@@ -123,6 +125,10 @@ class System:
         if p.symmetry == 0 and p.wall in (2, 3, 4):
             self.fluid_wall(p.wall)
         self.intra_molec()
+        if full and p.bending:
+            self.bending(2)
+        if full and p.charged:
+            self.ewald_k(1)
         f = self.download(_abi.F)["force"]
         self.upload(a=f / self.mass[:, None])
 
@@ -149,6 +155,9 @@ class System:
     def step(self, nsteps: int) -> None:
         """nsteps time steps on the device (fused kernels, captured graphs)."""
         check(self.lib.mfa_step(self.ctx, int(nsteps)), "mfa_step")
+
+    def set_pair_shape(self, threads_per_particle: int, block: int) -> None:
+        check(self.lib.mfa_set_pair_shape(self.ctx, int(threads_per_particle), int(block)), "mfa_set_pair_shape")
 
     # ---- mirrors ----
     def stream_ptr(self) -> int:

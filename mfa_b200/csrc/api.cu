@@ -106,6 +106,15 @@ int rebuild_abi(mfa_ctx* c, int rule) {
             MFA_CUDA_TRY(cudaMemcpy(c->dflags + F_NEEDNB, zero, sizeof(int32_t), cudaMemcpyHostToDevice));
             continue;
         }
+        // size the pair kernel's shared-memory tile for the largest row seen
+        // (with headroom); rows that outgrow it later are read from global memory
+        const long long want = f[F_MAXTILE];
+        if (want > c->tile_cap && c->tile_cap < pair_tile_limit(c)) {
+            long long cap = want + want / 8 + 32;
+            if (cap > pair_tile_limit(c)) cap = pair_tile_limit(c);
+            TRY(pair_set_shape(c, c->pair_tpp, c->pair_block, (int)cap));
+            invalidate_graph(c);
+        }
         return first_error(bits);
     }
     return MFA_ERR_NEIGH_OVERFLOW;
@@ -256,13 +265,15 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
         c->inv_rbin[d] = 1.0 / c->rbin[d];
         c->inv_boundary[d] = 1.0 / p->boundary[d];   // init_config.f90:20
     }
+    const int nrow = p->n_bin[1] * p->n_bin[2];
     int32_t* cells = nullptr;
-    A(dalloc(&cells, (size_t)3 * c->ncell + 2 + n));
+    A(dalloc(&cells, (size_t)3 * c->ncell + 2 + n + nrow));
     if (rc == MFA_OK) {
         c->cell_count = cells;
         c->cell_start = cells + c->ncell;
         c->cell_cursor = cells + 2 * c->ncell + 1;
         c->cell_of = cells + 3 * c->ncell + 2;
+        c->row_count = cells + 3 * c->ncell + 2 + n;
     }
     // Verlet list capacity: twice the expected count at the mean density
     double rc2max = 0.0;
@@ -278,7 +289,11 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
     if (maxnb > n) maxnb = ((n + 31) / 32) * 32;
     if (rc == MFA_OK) rc = alloc_list(c, maxnb);
     A(dalloc(&c->nnb, n));
+    // partial-sum slots: enough for the largest grid of any reducing kernel
+    // (particles / 32, cell rows, chains)
     c->max_blocks = (n + 31) / 32 + 64;
+    if (nrow + 64 > c->max_blocks) c->max_blocks = nrow + 64;
+    if (p->n_chain + p->n_chain_d + 64 > c->max_blocks) c->max_blocks = p->n_chain + p->n_chain_d + 64;
     A(dalloc(&c->partials, (size_t)R_N * 4 * c->max_blocks));
     A(dalloc(&c->counters, R_N));
     A(dalloc(&c->dscal, S_NSLOT));
@@ -334,7 +349,7 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
         cudaMemcpy(d3, m3.data(), m3.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(c->tabs, tabs.data(), tabs.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(c->force, 0, (size_t)4 * n * esz(c)) != cudaSuccess ||
-        cudaMemset(c->cell_count, 0, (size_t)c->ncell * 4) != cudaSuccess ||
+        cudaMemset(c->cell_count, 0, ((size_t)3 * c->ncell + 2 + n + nrow) * 4) != cudaSuccess ||
         cudaMemset(c->nnb, 0, (size_t)n * 4) != cudaSuccess ||
         cudaMemset(c->counters, 0, R_N * sizeof(unsigned)) != cudaSuccess ||
         cudaMemset(c->dscal, 0, S_NSLOT * 8) != cudaSuccess ||
@@ -342,6 +357,12 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
         cudaMemset(c->dstep, 0, 8) != cudaSuccess)
         rc = MFA_ERR_CUDA;
     if (rc == MFA_OK) rc = bonds_setup(c);
+    if (rc == MFA_OK) {
+        // pair kernel: 2 threads per particle, 256-thread blocks, a tile sized
+        // for 1.2x the mean neighbourhood of a row (grown at a rebuild if needed)
+        const long long cap = 9LL * (6LL * n / (5LL * nrow) + 8);
+        rc = pair_set_shape(c, 2, 256, (int)(cap < pair_tile_limit(c) ? cap : pair_tile_limit(c)));
+    }
     if (rc != MFA_OK) { free_all(c); free(c); return rc; }
 #undef A
     *out = c;
@@ -525,6 +546,14 @@ int mfa_get_scalars(mfa_ctx* c, mfa_scalars* o) {
     return first_error(f[F_ERR]);
 }
 
+int mfa_set_pair_shape(mfa_ctx* c, int32_t tpp, int32_t block) {
+    if (!c) return MFA_ERR_ARGS;
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    TRY(pair_set_shape(c, tpp, block, c->tile_cap));
+    invalidate_graph(c);
+    return MFA_OK;
+}
+
 int mfa_stream(mfa_ctx* c, void** s) {
     if (!c || !s) return MFA_ERR_ARGS;
     *s = (void*)c->st;
@@ -622,18 +651,30 @@ int mfa_debug_lists(mfa_ctx* c, int32_t* cell_of, int32_t* nbr_count, int32_t* n
     if (!c->lists_valid) return MFA_ERR_STATE;
     const int n = c->n;
     MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
-    std::vector<int32_t> co(n), ids(n), cnt(n), lst((size_t)c->maxnb * n);
+    std::vector<int32_t> co(n), ids(n), cnt(n), lst((size_t)c->maxnb * n), cs(c->ncell + 1);
     MFA_CUDA_TRY(cudaMemcpy(co.data(), c->cell_of, (size_t)n * 4, cudaMemcpyDeviceToHost));
     MFA_CUDA_TRY(cudaMemcpy(ids.data(), c->ids, (size_t)n * 4, cudaMemcpyDeviceToHost));
     MFA_CUDA_TRY(cudaMemcpy(cnt.data(), c->nnb, (size_t)n * 4, cudaMemcpyDeviceToHost));
     MFA_CUDA_TRY(cudaMemcpy(lst.data(), c->nbr, lst.size() * 4, cudaMemcpyDeviceToHost));
+    MFA_CUDA_TRY(cudaMemcpy(cs.data(), c->cell_start, cs.size() * 4, cudaMemcpyDeviceToHost));
     if (cell_of) memcpy(cell_of, co.data(), (size_t)n * 4);
+    const int nx = c->nb[0], ny = c->nb[1], nz = c->nb[2];
+    const int wy = c->bin_type == 0 ? c->p.delta_bin[1] + 2 : 3;
     for (int t = 0; t < n; ++t) {
         const int i = ids[t];
         const int m = cnt[t] < max_per ? cnt[t] : max_per;
         if (nbr_count) nbr_count[i] = cnt[t];
-        if (nbr)
-            for (int k = 0; k < m; ++k) nbr[(size_t)i * max_per + k] = ids[lst[(size_t)k * n + t]] + 1;
+        if (!nbr) continue;
+        const int cy = (co[i] / nx) % ny, cz = co[i] / (nx * ny);
+        for (int k = 0; k < m; ++k) {
+            // entry = (segment << 27 | offset inside that neighbouring row)
+            const int e = lst[(size_t)k * n + t];
+            const int seg = e >> 27, off = e & 0x7ffffff;
+            int ky, kz;
+            neighbour_row(c->bin_type, cy, cz, seg % wy, seg / wy, ny, nz, ky, kz);
+            const int s = cs[nx * (ky + ny * kz)] + off;
+            nbr[(size_t)i * max_per + k] = (s >= 0 && s < n) ? ids[s] + 1 : 0;
+        }
     }
     return MFA_OK;
 }

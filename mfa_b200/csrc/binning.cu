@@ -1,13 +1,22 @@
 // Cell binning and Verlet-list construction (binning.f90 / my_binning.f90).
 //
-// Integer work, HBM/L2 bound: a counting sort of the particles by cell
-// (histogram with atomics, one-block exclusive scan, scatter, a per-cell sort by
-// particle id so that the order is deterministic), a gather of the sorted
-// position/velocity records, and a thread-per-particle scan of the neighbouring
-// cells that keeps j with r^2 < range_2(ti,tj) + skin_2.  The distance test is
-// the reference's FP64 expression evaluated without contraction, so the pair
-// set equals the reference's bit for bit.  The list is stored full (both
-// directions) in slot space, column-major: nbr[k*n + t].
+// Integer work, HBM/L2 bound.  A counting sort of the particles by cell:
+//   k_cell_assign   cell per particle (the reference's FP64 formula), cell and
+//                   row histograms with atomics, r0_old/mic_old snapshot;
+//   k_scan_rows     multi-block: each block gets its row offset from the row
+//                   histogram, then one warp per row scans that row's cells;
+//   k_cell_scatter  slot per particle (atomic cursor per cell);
+//   k_cell_sort     per-cell sort by particle id, so the order is deterministic;
+//   k_gather_sorted the cell-sorted position/velocity records.
+// A "row" is the run of cells at fixed (y, z); cells are numbered x-fastest, so
+// a row is a contiguous range of slots.
+//   k_build_nbr     thread per slot: scans the neighbouring cells and keeps j with
+//                   r^2 < range_2(ti,tj) + skin_2, the reference's FP64
+//                   expression evaluated without contraction (bit-exact pair set).
+// The list is full (both directions), column-major (entry k of slot t at
+// nbr[k*n + t]).  An entry is (segment << 27 | offset): segment = which of the
+// neighbouring rows (in the order the pair kernel stages them), offset = the
+// slot's position inside that row.
 #include "mfa_internal.cuh"
 
 namespace {
@@ -19,7 +28,7 @@ struct BinArgs {
     int32_t *omx, *omy, *omz;
     const int32_t* type;
     const double* q;
-    int32_t *cell_count, *cell_start, *cell_cursor, *cell_of;
+    int32_t *cell_count, *cell_start, *cell_cursor, *cell_of, *row_count;
     int32_t *ids, *slot;
     void* pos_s;
     void* vel_s;
@@ -27,7 +36,7 @@ struct BinArgs {
     int32_t *nbr, *nnb;
     int32_t* flags;
     unsigned* counter;
-    int n, ncell, maxnb;
+    int n, ncell, nrow, maxnb;
     int nb[3], dl[3];
     double L[3], invL[3], rbin[3], inv_rbin[3];
     int symmetry;
@@ -54,58 +63,88 @@ __device__ __forceinline__ int cell_coord(const BinArgs& a, double x, int d, boo
 __global__ void k_cell_assign(BinArgs a) {
     if (skip(a)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        a.flags[F_MAXCELL] = 0;
+        a.flags[F_MAXROW] = 0;
+        a.flags[F_MAXTILE] = 0;
+        a.flags[F_MAXNB] = 0;
+    }
     if (i >= a.n) return;
     const double x = a.rx[i], y = a.ry[i], z = a.rz[i];
     bool bad = false;
     const int cx = cell_coord(a, x, 0, bad), cy = cell_coord(a, y, 1, bad), cz = cell_coord(a, z, 2, bad);
     if (!(isfinite(x) && isfinite(y) && isfinite(z))) set_err(a.flags, MFA_ERR_NONFINITE);
     else if (bad) set_err(a.flags, MFA_ERR_CELL_RANGE);
-    const int c = cx + a.nb[0] * (cy + a.nb[1] * cz);
+    const int r = cy + a.nb[1] * cz;
+    const int c = cx + a.nb[0] * r;
     a.cell_of[i] = c;
     atomicAdd(&a.cell_count[c], 1);
+    atomicAdd(&a.row_count[r], 1);
     // binning.f90:126-127 snapshot
     a.ox[i] = x; a.oy[i] = y; a.oz[i] = z;
     a.omx[i] = a.mx[i]; a.omy[i] = a.my[i]; a.omz[i] = a.mz[i];
 }
 
-// One block: exclusive scan of cell_count into cell_start[0..ncell] and
-// cell_cursor, largest occupancy, and cell_count cleared for the next rebuild.
-__global__ void k_scan_cells(BinArgs a) {
+// Exclusive scan of the cell histogram into cell_start[0..ncell] (and the
+// scatter cursors).  Block b owns rows [b*W, b*W + W), one warp per row; its
+// starting offset is the sum of the row histogram below its first row.
+__global__ void k_scan_rows(BinArgs a) {
     if (skip(a)) return;
-    __shared__ int wsum[32];
-    __shared__ int wmax[32];
-    const int T = blockDim.x, tid = threadIdx.x;
-    const int chunk = (a.ncell + T - 1) / T;
-    const int b0 = tid * chunk, b1 = min(a.ncell, b0 + chunk);
-    int local = 0, lmax = 0;
-    for (int c = b0; c < b1; ++c) { int k = a.cell_count[c]; local += k; lmax = max(lmax, k); }
-    // inclusive warp scan
-    const int lane = tid & 31, wid = tid >> 5;
-    int x = local;
-    for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
-    int m = lmax;
-    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, o));
-    if (lane == 31) wsum[wid] = x;
-    if (lane == 0) wmax[wid] = m;
+    __shared__ int wpart[32];
+    __shared__ int rpre[33];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, W = blockDim.x >> 5;
+    const int r0 = blockIdx.x * W;
+    // offset of this block: sum of row_count[0 .. r0)
+    int s = 0;
+    for (int r = threadIdx.x; r < r0; r += blockDim.x) s += a.row_count[r];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) wpart[wid] = s;
     __syncthreads();
-    if (wid == 0) {
-        int s = lane < (T >> 5) ? wsum[lane] : 0;
-        for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, s, o); if (lane >= o) s += y; }
-        wsum[lane] = s;
-        int mm = lane < (T >> 5) ? wmax[lane] : 0;
-        for (int o = 16; o > 0; o >>= 1) mm = max(mm, __shfl_down_sync(0xffffffffu, mm, o));
-        if (lane == 0) a.flags[F_MAXCELL] = mm;
+    if (threadIdx.x == 0) {
+        int base = 0;
+        for (int w = 0; w < W; ++w) base += wpart[w];
+        rpre[0] = base;
+        for (int w = 0; w < W; ++w) rpre[w + 1] = rpre[w] + (r0 + w < a.nrow ? a.row_count[r0 + w] : 0);
     }
     __syncthreads();
-    int run = (x - local) + (wid > 0 ? wsum[wid - 1] : 0);
-    for (int c = b0; c < b1; ++c) {
-        const int k = a.cell_count[c];
-        a.cell_start[c] = run;
-        a.cell_cursor[c] = run;
-        a.cell_count[c] = 0;
-        run += k;
+    const int r = r0 + wid;
+    if (r >= a.nrow) return;
+    const int nx = a.nb[0];
+    int carry = rpre[wid];
+    int cmax = 0;
+    for (int x0 = 0; x0 < nx; x0 += 32) {
+        const int x = x0 + lane;
+        const int k = x < nx ? a.cell_count[nx * r + x] : 0;
+        cmax = max(cmax, k);
+        int incl = k;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (x < nx) {
+            const int st = carry + incl - k;
+            a.cell_start[nx * r + x] = st;
+            a.cell_cursor[nx * r + x] = st;
+            a.cell_count[nx * r + x] = 0;
+        }
+        carry += __shfl_sync(0xffffffffu, incl, 31);
     }
-    if (tid == T - 1) a.cell_start[a.ncell] = run;
+    for (int o = 16; o > 0; o >>= 1) cmax = max(cmax, __shfl_down_sync(0xffffffffu, cmax, o));
+    // records of this row's neighbourhood (the pair kernel's tile)
+    const int wy = a.rule == 0 ? a.dl[1] + 2 : 3, wz = a.rule == 0 ? a.dl[2] + 2 : 3;
+    int tile = 0;
+    if (lane < wy * wz) {
+        int ky, kz;
+        neighbour_row(a.rule, r % a.nb[1], r / a.nb[1], lane % wy, lane / wy, a.nb[1], a.nb[2], ky, kz);
+        tile = a.row_count[ky + a.nb[1] * kz];
+    }
+    for (int o = 16; o > 0; o >>= 1) tile += __shfl_down_sync(0xffffffffu, tile, o);
+    if (lane == 0) {
+        atomicMax(&a.flags[F_MAXCELL], cmax);
+        atomicMax(&a.flags[F_MAXROW], rpre[wid + 1] - rpre[wid]);
+        atomicMax(&a.flags[F_MAXTILE], tile);
+        if (r == a.nrow - 1) a.cell_start[a.ncell] = carry;
+    }
 }
 
 __global__ void k_cell_scatter(BinArgs a) {
@@ -116,10 +155,12 @@ __global__ void k_cell_scatter(BinArgs a) {
     a.ids[p] = i;
 }
 
-// insertion sort of each cell's ids (cells hold a few to a few tens of particles)
+// insertion sort of each cell's ids (cells hold a few to a few tens of
+// particles); the row histogram is cleared here for the next rebuild
 __global__ void k_cell_sort(BinArgs a) {
     if (skip(a)) return;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < a.nrow) a.row_count[c] = 0;
     if (c >= a.ncell) return;
     const int b = a.cell_start[c], e = a.cell_start[c + 1];
     for (int k = b + 1; k < e; ++k) {
@@ -165,37 +206,42 @@ __global__ void k_build_nbr(BinArgs a, const double* __restrict__ cut2 /*T8*T8*/
         const int wi = wbits(pi.w);
         const int ti = wi & 0xff, ii = wi >> 8;
         const int c = a.cell_of[ii];
-        const int cx = c % a.nb[0], cy = (c / a.nb[0]) % a.nb[1], cz = c / (a.nb[0] * a.nb[1]);
-        int cnt = 0;
         const int nx = a.nb[0], ny = a.nb[1], nz = a.nb[2];
-        const int ncells = a.rule == 0 ? (a.dl[0] + 2) * (a.dl[1] + 2) * (a.dl[2] + 2) : 27;
-        for (int k = 0; k < ncells; ++k) {
-            int kx, ky, kz;
-            if (a.rule == 0) {
-                // binning.f90:71-76: j = i-1 .. i+delta_bin, k = mod(j+n, n)
-                const int wx = a.dl[0] + 2, wy = a.dl[1] + 2;
-                const int jx = cx - 1 + k % wx, jy = cy - 1 + (k / wx) % wy, jz = cz - 1 + k / (wx * wy);
-                kx = (jx + nx) % nx; ky = (jy + ny) % ny; kz = (jz + nz) % nz;
-            } else {
-                // my_binning.f90:70-80
-                kx = cx + k % 3 - 1; if (kx < 0) kx = nx - 1; if (kx == nx) kx = 0;
-                ky = cy + (k / 3) % 3 - 1; if (ky < 0) ky = ny - 1; if (ky == ny) ky = 0;
-                kz = cz + k / 9 - 1; if (kz < 0) kz = nz - 1; if (kz == nz) kz = 0;
-            }
-            const int c2 = kx + nx * (ky + ny * kz);
-            const int s0 = a.cell_start[c2], s1 = a.cell_start[c2 + 1];
-            for (int s = s0; s < s1; ++s) {
-                if (s == t) continue;
-                const double4 pj = a.pos64[s];
-                const int tj = wbits(pj.w) & 0xff;
-                double d0 = __dsub_rn(pi.x, pj.x), d1 = __dsub_rn(pi.y, pj.y), d2 = __dsub_rn(pi.z, pj.z);
-                d0 = mimage64(d0, a.L[0], a.invL[0]);
-                d1 = mimage64(d1, a.L[1], a.invL[1]);
-                if (a.symmetry == 1) d2 = mimage64(d2, a.L[2], a.invL[2]);
-                const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
-                if (r2 < sc[(ti - 1) * T8 + (tj - 1)]) {
-                    if (cnt < a.maxnb) a.nbr[(size_t)cnt * a.n + t] = s;
-                    ++cnt;
+        const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
+        int cnt = 0;
+        const int wx = a.rule == 0 ? a.dl[0] + 2 : 3;
+        const int wy = a.rule == 0 ? a.dl[1] + 2 : 3;
+        const int wz = a.rule == 0 ? a.dl[2] + 2 : 3;
+        for (int iz = 0; iz < wz; ++iz)
+        for (int iy = 0; iy < wy; ++iy) {
+            int ky, kz;
+            neighbour_row(a.rule, cy, cz, iy, iz, ny, nz, ky, kz);
+            const int seg = iz * wy + iy;
+            const int row0 = a.cell_start[nx * (ky + ny * kz)];
+            for (int ix = 0; ix < wx; ++ix) {
+                int kx;
+                if (a.rule == 0) {
+                    kx = (cx - 1 + ix + nx) % nx;        // binning.f90:71-76
+                } else {
+                    kx = cx + ix - 1;                    // my_binning.f90:70-72
+                    if (kx < 0) kx = nx - 1;
+                    if (kx == nx) kx = 0;
+                }
+                const int c2 = kx + nx * (ky + ny * kz);
+                const int s0 = a.cell_start[c2], s1 = a.cell_start[c2 + 1];
+                for (int s = s0; s < s1; ++s) {
+                    if (s == t) continue;
+                    const double4 pj = a.pos64[s];
+                    const int tj = wbits(pj.w) & 0xff;
+                    double d0 = __dsub_rn(pi.x, pj.x), d1 = __dsub_rn(pi.y, pj.y), d2 = __dsub_rn(pi.z, pj.z);
+                    d0 = mimage64(d0, a.L[0], a.invL[0]);
+                    d1 = mimage64(d1, a.L[1], a.invL[1]);
+                    if (a.symmetry == 1) d2 = mimage64(d2, a.L[2], a.invL[2]);
+                    const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
+                    if (r2 < sc[(ti - 1) * T8 + (tj - 1)]) {
+                        if (cnt < a.maxnb) a.nbr[(size_t)cnt * a.n + t] = (seg << 27) | (s - row0);
+                        ++cnt;
+                    }
                 }
             }
         }
@@ -227,11 +273,11 @@ BinArgs make_args(mfa_ctx* c, int rule, int conditional) {
     a.omx = c->omx; a.omy = c->omy; a.omz = c->omz;
     a.type = c->type; a.q = c->p.charged ? c->q : nullptr;
     a.cell_count = c->cell_count; a.cell_start = c->cell_start; a.cell_cursor = c->cell_cursor;
-    a.cell_of = c->cell_of; a.ids = c->ids; a.slot = c->slot;
+    a.cell_of = c->cell_of; a.row_count = c->row_count; a.ids = c->ids; a.slot = c->slot;
     a.pos_s = c->pos_s; a.vel_s = c->vel_s; a.pos64 = c->pos64;
     a.nbr = c->nbr; a.nnb = c->nnb; a.flags = c->dflags;
     a.counter = c->counters + R_N - 1;
-    a.n = c->n; a.ncell = c->ncell; a.maxnb = c->maxnb;
+    a.n = c->n; a.ncell = c->ncell; a.nrow = c->nb[1] * c->nb[2]; a.maxnb = c->maxnb;
     for (int d = 0; d < 3; ++d) {
         a.nb[d] = c->nb[d]; a.dl[d] = c->p.delta_bin[d];
         a.L[d] = c->p.boundary[d]; a.invL[d] = c->inv_boundary[d];
@@ -252,8 +298,9 @@ int launch_rebuild(mfa_ctx* c, int rule, int conditional) {
     BinArgs a = make_args(c, rule, conditional);
     const int T = 256;
     const int nbp = (c->n + T - 1) / T;
+    const int nrow = c->nb[1] * c->nb[2];
     k_cell_assign<<<nbp, T, 0, c->st>>>(a);
-    k_scan_cells<<<1, 1024, 0, c->st>>>(a);
+    k_scan_rows<<<(nrow + 7) / 8, 256, 0, c->st>>>(a);
     k_cell_scatter<<<nbp, T, 0, c->st>>>(a);
     k_cell_sort<<<(c->ncell + 127) / 128, 128, 0, c->st>>>(a);
     if (c->prec == MFA_MIXED) k_gather_sorted<float4><<<nbp, T, 0, c->st>>>(a, 1);

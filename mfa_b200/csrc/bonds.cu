@@ -133,22 +133,25 @@ __global__ void k_bonds(BondArgs a) {
         // phase 3: every term that touches bead b
         R4* f4 = (R4*)a.force;
         for (int b = lane; b < nm; b += 32) {
-            R gx = 0, gy = 0, gz = 0;
+            // FENE and bending are added to the force in two steps, so that the
+            // fused pass rounds exactly like intra_molec followed by bending(2)
+            R gx = 0, gy = 0, gz = 0, hx = 0, hy = 0, hz = 0;
             if (a.do_fene) {
                 if (b < nm - 1) { gx -= s_fene[3 * b]; gy -= s_fene[3 * b + 1]; gz -= s_fene[3 * b + 2]; }
                 if (b > 0) { gx += s_fene[3 * (b - 1)]; gy += s_fene[3 * (b - 1) + 1]; gz += s_fene[3 * (b - 1) + 2]; }
             }
             if (bend) {
-                if (b + 1 <= nm - 2) { gx += s_fp[3 * (b + 1)]; gy += s_fp[3 * (b + 1) + 1]; gz += s_fp[3 * (b + 1) + 2]; }
+                if (b + 1 <= nm - 2) { hx += s_fp[3 * (b + 1)]; hy += s_fp[3 * (b + 1) + 1]; hz += s_fp[3 * (b + 1) + 2]; }
                 if (b >= 1 && b <= nm - 2) {
-                    gx -= s_fp[3 * b] + s_fn[3 * b];
-                    gy -= s_fp[3 * b + 1] + s_fn[3 * b + 1];
-                    gz -= s_fp[3 * b + 2] + s_fn[3 * b + 2];
+                    hx -= s_fp[3 * b] + s_fn[3 * b];
+                    hy -= s_fp[3 * b + 1] + s_fn[3 * b + 1];
+                    hz -= s_fp[3 * b + 2] + s_fn[3 * b + 2];
                 }
-                if (b - 1 >= 1) { gx += s_fn[3 * (b - 1)]; gy += s_fn[3 * (b - 1) + 1]; gz += s_fn[3 * (b - 1) + 2]; }
+                if (b - 1 >= 1) { hx += s_fn[3 * (b - 1)]; hy += s_fn[3 * (b - 1) + 1]; hz += s_fn[3 * (b - 1) + 2]; }
             }
             R4 o = f4[base + b];
-            o.x += gx; o.y += gy; o.z += gz;
+            if (a.do_fene) { o.x += gx; o.y += gy; o.z += gz; }
+            if (bend) { o.x += hx; o.y += hy; o.z += hz; }
             f4[base + b] = o;
         }
     }

@@ -38,8 +38,10 @@ enum {
     F_MAXCELL = 3,   // largest cell at the last rebuild
     F_NEEDNB = 4,    // list capacity that would have been needed
     F_REBUILDS = 5,  // rebuild counter
-    F_FENE = 6,      // FENE bonds at the clamp in the last bond pass
-    F_NFLAG = 8
+    F_FENE = 6,      // FENE bonds at the clamp since init
+    F_MAXROW = 7,    // largest cell row (fixed y, z) at the last rebuild
+    F_MAXTILE = 8,   // largest neighbourhood of a row (records) at the last rebuild
+    F_NFLAG = 16
 };
 
 // reduction counters (last-block-done pattern), one per reducing kernel
@@ -65,7 +67,10 @@ struct mfa_ctx {
     // cells
     int nb[3], ncell;
     double rbin[3], inv_rbin[3], inv_boundary[3];
-    int32_t *cell_count, *cell_start, *cell_cursor, *cell_of;
+    int32_t *cell_count, *cell_start, *cell_cursor, *cell_of, *row_count;
+    // pair kernel launch shape (threads per particle, block size) and the
+    // shared-memory capacity of its staged tile, in records
+    int pair_tpp, pair_block, tile_cap;
     // pair tables on the device: range_2+skin_2, range_2, epsil, sigma_2, e_shift, inv_range_2
     double* tabs;                       // 6 x T8*T8
     // Verlet list
@@ -123,6 +128,8 @@ int launch_rebuild(mfa_ctx* c, int rule, int conditional);
 int launch_refresh_sorted(mfa_ctx* c);
 // pair.cu
 int launch_pair(mfa_ctx* c, int fuse_wall, int accumulate);
+int pair_set_shape(mfa_ctx* c, int tpp, int block, int tile_cap);
+int pair_tile_limit(const mfa_ctx* c);
 // bonds.cu
 int launch_bonds(mfa_ctx* c, int do_fene, int do_bend);
 int bonds_setup(mfa_ctx* c);
@@ -228,6 +235,46 @@ __device__ __forceinline__ bool block_sum_commit(double (&v)[NQ], double* partia
     }
     if (threadIdx.x == 0) *counter = 0u;
     return true;
+}
+
+// One 9-3 wall term (fluid_wall.f90:96-101) at inverse distance 1/zz:
+// energy |A| (s/z)^9 - A_e (s/z)^3 and the force along the wall normal
+// 9|A| s^9 / z^10 - 3 A s^3 / z^4; with cut > 0 the energy is shifted to zero at
+// z = cut.  Shared by the stand-alone wall pass and the pair-kernel epilogue so
+// that both round identically.
+template <typename R>
+__device__ __forceinline__ void wall93_term(R zz, R sw, R aw, R ae, R cut, R& f, double& e) {
+    const R faw = aw < (R)0 ? -aw : aw;
+    const R iz = (R)1 / zz;
+    const R rd = sw * iz;
+    const R rd2 = rd * rd, rd4 = rd2 * rd2, rd8 = rd4 * rd4;
+    const R sw2 = sw * sw, sw4 = sw2 * sw2, sw8 = sw4 * sw4;
+    const R iz2 = iz * iz, iz4 = iz2 * iz2, iz8 = iz4 * iz4;
+    e = (double)(faw * (rd8 * rd) - ae * (rd2 * rd));
+    f = (R)9 * faw * (sw8 * sw) * (iz8 * iz2) - (R)3 * aw * (sw2 * sw) * iz4;
+    if (cut > (R)0) {
+        const R rc = sw / cut, rc3 = rc * rc * rc;
+        e -= (double)(faw * rc3 * rc3 * rc3 - ae * rc3);
+    }
+}
+
+// Row (ky, kz) of neighbour-row index (iy, iz) around the row (cy, cz):
+// binning.f90:73-76 for rule 0 (j = c-1 .. c+delta_bin, mod n), my_binning.f90:74-80
+// for rule 1 (c-1 .. c+1 with a single wrap).  The pair kernel stages the rows
+// in this order and the list builder encodes entries with the same index.
+__host__ __device__ __forceinline__ void neighbour_row(int rule, int cy, int cz, int iy, int iz, int ny, int nz,
+                                                       int& ky, int& kz) {
+    if (rule == 0) {
+        ky = (cy - 1 + iy + ny) % ny;
+        kz = (cz - 1 + iz + nz) % nz;
+    } else {
+        ky = cy + iy - 1;
+        if (ky < 0) ky = ny - 1;
+        if (ky == ny) ky = 0;
+        kz = cz + iz - 1;
+        if (kz < 0) kz = nz - 1;
+        if (kz == nz) kz = 0;
+    }
 }
 
 // read-only-path loads of 4-wide records

@@ -2,11 +2,18 @@
 // (charged systems, fused into the same pass) and lgv_forces (THERMOSTAT 1),
 // plus optionally the 9-3 walls of fluid_wall.f90 in the per-particle epilogue.
 //
-// One thread per cell-sorted slot walks its full Verlet list and accumulates
-// the force on its own particle only: no atomics, deterministic order, and the
-// DPD noise of a pair is drawn from Philox keyed by (step, min(i,j), max(i,j))
-// so both sides of a pair see the same random number.  R = float in MIXED mode
-// (FP32 force math, FP64 energy/virial accumulators), double in FP64 mode.
+// One CTA per cell row (fixed y, z).  Its neighbourhood -- the neighbouring
+// cell rows, each a contiguous run of cell-sorted records -- is staged into
+// shared memory with bulk asynchronous copies (cp.async.bulk, completion on an
+// mbarrier, bounded wait), and the Verlet-list entries (segment, offset) index
+// that tile directly.  TPP threads share one particle's list and combine their
+// partial forces with warp shuffles; each particle's force is accumulated by
+// its own group only: no atomics, a fixed summation order, and the DPD noise of
+// a pair is drawn from Philox keyed by (step, min(i,j), max(i,j)) so both sides
+// see the same random number.  If a row's neighbourhood does not fit the
+// shared-memory tile, the CTA reads the same records from global memory.
+// R = float in MIXED mode (FP32 force math, FP64 energy/virial accumulators),
+// double in FP64 mode.
 #include "mfa_internal.cuh"
 
 namespace {
@@ -16,6 +23,8 @@ struct PairArgs {
     const void* vel_s;
     const int32_t* __restrict__ nbr;
     const int32_t* __restrict__ nnb;
+    const int32_t* __restrict__ cell_start;
+    int32_t* flags;
     const double* mass;
     const double* tabs;
     void* force;
@@ -24,9 +33,10 @@ struct PairArgs {
     unsigned* counter;
     double* dscal;
     int n, max_blocks;
+    int nb[3], rule, wy, nseg, tile_cap, need_vtile;
     int symmetry, thermostat, dpd_weight, noise, charged, real_in_lj, fsw;
     int wall_type, wall_e_aw;
-    int accumulate;
+    int accumulate, fuse_wall;
     double coul_energy_factor;
     double L[3], invL[3];
     double sig, friction, dt;
@@ -99,35 +109,134 @@ __device__ __forceinline__ R wall_force(const PairArgs& a, int t, R z, double& e
     R fz = 0;
     const R sw = (R)a.sigma_wall[t - 1], aw = (R)a.a_wall[t - 1];
     const R ae = a.wall_e_aw ? (R)a.a_w : aw;
-    const R sw3 = sw * sw * sw, sw9 = sw3 * sw3 * sw3;
-    const R faw = aw < 0 ? -aw : aw;
     const R cut = (R)a.wall_cut;
-    auto term = [&](R zz, R& f, double& ee) {
-        const R iz = (R)1 / zz;
-        const R rd = sw * iz, rd3 = rd * rd * rd;
-        const R iz2 = iz * iz, iz4 = iz2 * iz2, iz8 = iz4 * iz4;
-        ee = (double)(faw * rd3 * rd3 * rd3 - ae * rd3);
-        f = (R)9 * faw * sw9 * (iz8 * iz2) - (R)3 * aw * sw3 * iz4;
-        if (cut > 0) {
-            const R ic = (R)1 / cut, rc = sw * ic, rc3 = rc * rc * rc;
-            ee -= (double)(faw * rc3 * rc3 * rc3 - ae * rc3);
-        }
-    };
     R f;
     double ee;
-    if (cut <= 0 || z < cut) { term(z, f, ee); fz += f; e += ee; }
+    if (cut <= 0 || z < cut) { wall93_term<R>(z, sw, aw, ae, cut, f, ee); fz += f; e += ee; }
     if (a.wall_type == 2) {
         const R zt = (R)a.z_space_wall - z;
-        if (cut <= 0 || zt < cut) { term(zt, f, ee); fz -= f; e += ee; }
+        if (cut <= 0 || zt < cut) { wall93_term<R>(zt, sw, aw, ae, cut, f, ee); fz -= f; e += ee; }
     }
     return fz;
 }
 
-template <typename R, bool FUSE_WALL>
-__global__ void __launch_bounds__(128) k_pair(PairArgs a) {
+
+// ---- bulk-copy staging (cp.async.bulk global -> shared, mbarrier completion) ----
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(__cvta_generic_to_global(src)), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait: gives up after `limit` polls (each poll may suspend briefly)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long limit) {
+    for (long long it = 0; it < limit; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+constexpr long long WAIT_LIMIT = 1LL << 24;
+
+// Feature bits of a pair-kernel instantiation.  A specialised instantiation
+// compiles only the physics a run uses (fewer registers, more resident warps);
+// FT_GENERIC reads every switch at run time and serves all other combinations.
+enum {
+    FT_DPD = 1,        // DPD thermostat (dpd_forces)
+    FT_LGV = 2,        // Langevin thermostat (lgv_forces)
+    FT_QLJ = 4,        // Ewald real space inside the LJ range (reference)
+    FT_QSEP = 8,       // Ewald real space with its own cutoff
+    FT_FSW = 16,       // force switch-on clamp
+    FT_WALL = 32,      // 9-3 walls in the epilogue
+    FT_ACC = 64,       // add to the force array (else store)
+    FT_GENERIC = 128
+};
+
+template <int FT>
+__device__ __forceinline__ bool has(const PairArgs& a, int bit) {
+    if (FT & FT_GENERIC) {
+        switch (bit) {
+            case FT_DPD: return a.thermostat == MFA_THERMO_DPD;
+            case FT_LGV: return a.thermostat == MFA_THERMO_LGV;
+            case FT_QLJ: return a.charged && a.real_in_lj;
+            case FT_QSEP: return a.charged && !a.real_in_lj;
+            case FT_FSW: return a.fsw != 0;
+            case FT_WALL: return a.fuse_wall != 0;
+            case FT_ACC: return a.accumulate != 0;
+        }
+        return false;
+    }
+    return (FT & bit) != 0;
+}
+
+template <typename R, int TPP, int FT>
+__global__ void __launch_bounds__(256, 3) k_pair(PairArgs a) {
     typedef typename Vec4<R>::T R4;
-    constexpr int NQ = FUSE_WALL ? 4 : 3;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    R4* tpos = (R4*)smem_raw;
+    R4* tvel = tpos + a.tile_cap;
     __shared__ R s_rc2[T8 * T8], s_eps[T8 * T8], s_sig2[T8 * T8], s_esh[T8 * T8], s_irc2[T8 * T8];
+    __shared__ int seg_start[16], seg_base[16];
+    __shared__ int s_mode;   // 1: tile in shared memory, 0: global records
+    __shared__ __align__(8) uint64_t bar;
+    const bool DPD = has<FT>(a, FT_DPD), LGV = has<FT>(a, FT_LGV), QLJ = has<FT>(a, FT_QLJ);
+    const bool QSEP = has<FT>(a, FT_QSEP), FSW = has<FT>(a, FT_FSW), WALL = has<FT>(a, FT_WALL);
+    const bool ACC = has<FT>(a, FT_ACC);
+    const bool need_v = DPD || QLJ || QSEP;
+    const int row = blockIdx.x;
+    const int nx = a.nb[0], ny = a.nb[1], nz = a.nb[2];
+    // staging: lane k of warp 0 finds neighbouring row k; a warp scan places
+    // the rows back to back; every lane then issues the bulk copies of its row
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        int s0 = 0, len = 0;
+        if (lane < a.nseg) {
+            int ky, kz;
+            neighbour_row(a.rule, row % ny, row / ny, lane % a.wy, lane / a.wy, ny, nz, ky, kz);
+            const int c0 = nx * (ky + ny * kz);
+            s0 = a.cell_start[c0];
+            len = a.cell_start[c0 + nx] - s0;
+        }
+        int incl = len;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        if (lane < a.nseg) { seg_start[lane] = s0; seg_base[lane] = incl - len; }
+        const int mode = total <= a.tile_cap ? 1 : 0;
+        if (lane == 0) {
+            s_mode = mode;
+            if (mode) {
+                mbar_init(&bar);
+                mbar_expect_tx(&bar, (uint32_t)total * (uint32_t)sizeof(R4) * (need_v ? 2u : 1u));
+            }
+        }
+        __syncwarp();
+        if (mode && lane < a.nseg && len > 0) {
+            bulk_g2s(tpos + (incl - len), (const R4*)a.pos_s + s0, (uint32_t)len * sizeof(R4), &bar);
+            if (need_v) bulk_g2s(tvel + (incl - len), (const R4*)a.vel_s + s0, (uint32_t)len * sizeof(R4), &bar);
+        }
+    }
     for (int k = threadIdx.x; k < T8 * T8; k += blockDim.x) {
         s_rc2[k] = (R)a.tabs[1 * T8 * T8 + k];
         s_eps[k] = (R)a.tabs[2 * T8 * T8 + k];
@@ -136,136 +245,248 @@ __global__ void __launch_bounds__(128) k_pair(PairArgs a) {
         s_irc2[k] = (R)a.tabs[5 * T8 * T8 + k];
     }
     __syncthreads();
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    double acc[NQ];
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
-    if (t < a.n) {
-        const R4* __restrict__ pos = (const R4*)a.pos_s;
-        const R4* __restrict__ vel = (const R4*)a.vel_s;
-        const long long step = *a.dstep;
+    const bool tile = s_mode != 0;
+    bool valid = true;
+    if (tile && !mbar_wait_bounded(&bar, 0, WAIT_LIMIT)) {
+        // the copies did not complete in time: report, wait for them once more
+        // (the tile must not be released while they are in flight), skip the work
+        set_err(a.flags, MFA_ERR_TIMEOUT);
+        mbar_wait_bounded(&bar, 0, WAIT_LIMIT);
+        valid = false;
+    }
+    const R4* __restrict__ gpos = (const R4*)a.pos_s;
+    const R4* __restrict__ gvel = (const R4*)a.vel_s;
+    const long long step = *a.dstep;
+    R r2min = 0;
+    if (FSW) {
         // fluid_fluid.f90:42-49 force switch-on
-        R r2min = 0;
-        if (a.fsw) {
-            const double r_time = (double)(a.s_time + step - 1) * a.dt;
-            r2min = r_time < a.r_2_min_time ? (R)((1.0 - r_time / a.r_2_min_time) * a.r_2_min_init) : (R)0;
-        }
-        const R4 pi = ldg4(&pos[t]);
-        const int wi = wbits(pi.w);
-        const int ti = wi & 0xff, ii = wi >> 8;
-        const bool need_v = a.thermostat == MFA_THERMO_DPD || a.charged;
-        R4 vi;
-        if (need_v) vi = ldg4(&vel[t]);
-        const R Lx = (R)a.L[0], Ly = (R)a.L[1], Lz = (R)a.L[2];
-        const R iLx = (R)a.invL[0], iLy = (R)a.invL[1], iLz = (R)a.invL[2];
-        const R sig = (R)a.sig, gam = (R)a.friction;
+        const double r_time = (double)(a.s_time + step - 1) * a.dt;
+        r2min = r_time < a.r_2_min_time ? (R)((1.0 - r_time / a.r_2_min_time) * a.r_2_min_init) : (R)0;
+    }
+    const R Lx = (R)a.L[0], Ly = (R)a.L[1], Lz = (R)a.L[2];
+    const R iLx = (R)a.invL[0], iLy = (R)a.invL[1], iLz = (R)a.invL[2];
+    const R sig = (R)a.sig, gam = (R)a.friction;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    const int p0 = a.cell_start[nx * row], p1 = a.cell_start[nx * row + nx];
+    const int sub = threadIdx.x % TPP;
+    const int per_pass = blockDim.x / TPP;
+    for (int base = p0; base < p1 && valid; base += per_pass) {
+        const int t = base + threadIdx.x / TPP;
+        const bool act = t < p1;
         R fx = 0, fy = 0, fz = 0;
         double e_lj = 0.0, vir = 0.0, e_c = 0.0;
-        const int m = a.nnb[t];
-        const int rowi = (ti - 1) * T8;
-        for (int k = 0; k < m; ++k) {
-            const int s = __ldg(&a.nbr[(size_t)k * a.n + t]);
-            const R4 pj = ldg4(&pos[s]);
-            R dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-            dx = mimg(dx, Lx, iLx);
-            dy = mimg(dy, Ly, iLy);
-            if (a.symmetry == 1) dz = mimg(dz, Lz, iLz);
-            const R r2 = dx * dx + dy * dy + dz * dz;
-            const int wj = wbits(pj.w);
-            const int ij = rowi + (wj & 0xff) - 1;
-            if (r2 < s_rc2[ij]) {
-                const R r2c = a.fsw ? (r2 > r2min ? r2 : r2min) : r2;
-                const R inv_r2 = (R)1 / r2c;
-                const R inv_r = rsqrt_(r2c);
-                const R eps = s_eps[ij];
-                const R r61 = s_sig2[ij] * inv_r2;
-                const R r6 = r61 * r61 * r61;
-                const R r12 = r6 * r6;
-                e_lj += (double)(eps * ((r12 - r6) - s_esh[ij]));
-                const R fs = eps * ((R)12 * r12 - (R)6 * r6) * inv_r2;   // force on i along d
-                R fsum = fs;
-                vir += (double)(fs * r2);
-                if (a.thermostat == MFA_THERMO_DPD) {
-                    // dpd_forces.f90:273-348 with Philox noise keyed by the pair
-                    const int jj = wj >> 8;
-                    const uint32_t lo = (uint32_t)min(ii, jj), hi = (uint32_t)max(ii, jj);
-                    const uint4 w = philox4x32_10(make_uint4(lo, hi, (uint32_t)step, TAG_DPD), a.seed0, a.seed1);
-                    const R g = noise1(w.x, w.y, a.noise, R(0));
-                    R wr, wd;
-                    if (a.dpd_weight == 1) { wr = 1; wd = 1; }
-                    else { wr = (R)1 - sqrt_(r2c * s_irc2[ij]); wd = wr * wr; }
-                    const R4 vj = ldg4(&vel[s]);
-                    const R rd = ((vi.x - vj.x) * dx + (vi.y - vj.y) * dy + (vi.z - vj.z) * dz) * inv_r;
-                    // F_i += (sig w_r g - gamma w_d (dv . rhat)) rhat, rhat = d * inv_r
-                    fsum += (sig * wr * g - gam * wd * rd) * inv_r;
+        R4 pi, vi;
+        int ti = 1, ii = 0;
+        if (act) {
+            pi = ldg4(&gpos[t]);
+            const int wi = wbits(pi.w);
+            ti = wi & 0xff;
+            ii = wi >> 8;
+            if (need_v) vi = ldg4(&gvel[t]);
+            const int m = a.nnb[t];
+            const int rowi = (ti - 1) * T8;
+            for (int k = sub; k < m; k += TPP) {
+                const int e = __ldg(&a.nbr[(size_t)k * a.n + t]);
+                const int seg = e >> 27, off = e & 0x7ffffff;
+                const int lj = seg_base[seg] + off;
+                const int gj = seg_start[seg] + off;
+                const R4 pj = tile ? tpos[lj] : ldg4(&gpos[gj]);
+                R dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                dx = mimg(dx, Lx, iLx);
+                dy = mimg(dy, Ly, iLy);
+                if (a.symmetry == 1) dz = mimg(dz, Lz, iLz);
+                const R r2 = dx * dx + dy * dy + dz * dz;
+                const int wj = wbits(pj.w);
+                const int ij = rowi + (wj & 0xff) - 1;
+                const bool in_lj = r2 < s_rc2[ij];
+                const bool in_ew = QSEP && r2 < (R)a.ewald_rc_2;
+                if (!in_lj && !in_ew) continue;
+                R4 vj;
+                if (need_v) vj = tile ? tvel[lj] : ldg4(&gvel[gj]);
+                if (in_lj) {
+                    const R r2c = FSW ? (r2 > r2min ? r2 : r2min) : r2;
+                    const R inv_r2 = (R)1 / r2c;
+                    const R eps = s_eps[ij];
+                    const R r61 = s_sig2[ij] * inv_r2;
+                    const R r6 = r61 * r61 * r61;
+                    const R r12 = r6 * r6;
+                    e_lj += (double)(eps * ((r12 - r6) - s_esh[ij]));
+                    const R fs = eps * ((R)12 * r12 - (R)6 * r6) * inv_r2;   // force on i along d
+                    R fsum = fs;
+                    vir += (double)(fs * r2);
+                    if (DPD || QLJ) {
+                        const R inv_r = rsqrt_(r2c);
+                        if (DPD) {
+                            // dpd_forces.f90:273-348 with Philox noise keyed by the pair
+                            const int jj = wj >> 8;
+                            const uint32_t lo = (uint32_t)min(ii, jj), hi = (uint32_t)max(ii, jj);
+                            const uint4 w = philox4x32_10(make_uint4(lo, hi, (uint32_t)step, TAG_DPD), a.seed0,
+                                                          a.seed1);
+                            const R g = noise1(w.x, w.y, a.noise, R(0));
+                            R wr, wd;
+                            if (a.dpd_weight == 1) { wr = 1; wd = 1; }
+                            else { wr = (R)1 - sqrt_(r2c * s_irc2[ij]); wd = wr * wr; }
+                            const R rd = ((vi.x - vj.x) * dx + (vi.y - vj.y) * dy + (vi.z - vj.z) * dz) * inv_r;
+                            // F_i += (sig w_r g - gamma w_d (dv . rhat)) rhat, rhat = d * inv_r
+                            fsum += (sig * wr * g - gam * wd * rd) * inv_r;
+                        }
+                        if (QLJ) {
+                            // ewald_real.f90:411-428, inside the LJ range (reference behaviour)
+                            const R qq = vi.w * vj.w;
+                            const R r = (R)1 / inv_r;
+                            const R ec = erfc_((R)a.sqrt_alpha * r);
+                            e_c += (double)(qq * ec * inv_r);
+                            const R fsc = qq * (R)a.sqrt_alpha * (R)a.inv_sqrt_pi * (R)2 * exp_(-(R)a.alpha_c * r2c) *
+                                              inv_r + qq * ec * inv_r * inv_r;
+                            fsum += fsc * inv_r;
+                            vir += (double)(fsc * r2 * inv_r);
+                        }
+                    }
+                    fx += fsum * dx; fy += fsum * dy; fz += fsum * dz;
                 }
-                if (a.charged && a.real_in_lj) {
-                    // ewald_real.f90:411-428, inside the LJ range (reference behaviour)
-                    const R4 vj = ldg4(&vel[s]);
+                if (in_ew) {
                     const R qq = vi.w * vj.w;
-                    const R r = (R)1 / inv_r;
-                    const R ir = inv_r;
+                    const R ir = rsqrt_(r2);
+                    const R r = (R)1 / ir;
                     const R ec = erfc_((R)a.sqrt_alpha * r);
                     e_c += (double)(qq * ec * ir);
-                    const R fsc = qq * (R)a.sqrt_alpha * (R)a.inv_sqrt_pi * (R)2 * exp_(-(R)a.alpha_c * r2c) * ir
+                    const R fsc = qq * (R)a.sqrt_alpha * (R)a.inv_sqrt_pi * (R)2 * exp_(-(R)a.alpha_c * r2) * ir
                                   + qq * ec * ir * ir;
-                    fsum += fsc * ir;
+                    const R f = fsc * ir;
+                    fx += f * dx; fy += f * dy; fz += f * dz;
                     vir += (double)(fsc * r2 * ir);
                 }
-                fx += fsum * dx; fy += fsum * dy; fz += fsum * dz;
-            }
-            if (a.charged && !a.real_in_lj && r2 < (R)a.ewald_rc_2) {
-                const R4 vj = ldg4(&vel[s]);
-                const R qq = vi.w * vj.w;
-                const R ir = rsqrt_(r2);
-                const R r = (R)1 / ir;
-                const R ec = erfc_((R)a.sqrt_alpha * r);
-                e_c += (double)(qq * ec * ir);
-                const R fsc = qq * (R)a.sqrt_alpha * (R)a.inv_sqrt_pi * (R)2 * exp_(-(R)a.alpha_c * r2) * ir
-                              + qq * ec * ir * ir;
-                const R f = fsc * ir;
-                fx += f * dx; fy += f * dy; fz += f * dz;
-                vir += (double)(fsc * r2 * ir);
             }
         }
-        if (a.thermostat == MFA_THERMO_LGV) {
-            // lgv_forces.f90:377-393
-            R g[3];
-            lgv_noise3<R>((uint32_t)ii, (uint32_t)step, a, g);
-            const double mi = a.mass[ii];
-            const R sm = (R)sqrt(mi), gm = (R)(a.friction * mi);
-            if (!need_v) vi = ldg4(&vel[t]);
-            fx += sig * g[0] * sm - gm * vi.x;
-            fy += sig * g[1] * sm - gm * vi.y;
-            fz += sig * g[2] * sm - gm * vi.z;
+        // combine the TPP partial sums of a particle (lanes of one group are adjacent)
+#pragma unroll
+        for (int o = TPP / 2; o > 0; o >>= 1) {
+            fx += __shfl_xor_sync(0xffffffffu, fx, o);
+            fy += __shfl_xor_sync(0xffffffffu, fy, o);
+            fz += __shfl_xor_sync(0xffffffffu, fz, o);
         }
-        if (FUSE_WALL) {
-            double ew = 0.0;
-            fz += wall_force<R>(a, ti, pi.z, ew);
-            acc[NQ - 1] = ew;
+        if (act && sub == 0) {
+            if (LGV) {
+                // lgv_forces.f90:377-393
+                R g[3];
+                lgv_noise3<R>((uint32_t)ii, (uint32_t)step, a, g);
+                const double mi = a.mass[ii];
+                const R sm = (R)sqrt(mi), gm = (R)(a.friction * mi);
+                if (!need_v) vi = ldg4(&gvel[t]);
+                fx += sig * g[0] * sm - gm * vi.x;
+                fy += sig * g[1] * sm - gm * vi.y;
+                fz += sig * g[2] * sm - gm * vi.z;
+            }
+            if (WALL) {
+                double ew = 0.0;
+                fz += wall_force<R>(a, ti, pi.z, ew);
+                acc[3] += ew;
+            }
+            R4* f4 = (R4*)a.force;
+            R4 o;
+            if (ACC) {
+                o = f4[ii];
+                o.x += fx; o.y += fy; o.z += fz;
+            } else {
+                o.x = fx; o.y = fy; o.z = fz; o.w = 0;
+            }
+            f4[ii] = o;
         }
-        acc[0] = 0.5 * e_lj;   // full list: each pair seen from both sides
-        acc[1] = 0.5 * vir;
-        acc[2] = a.coul_energy_factor * e_c;
-        R4* f4 = (R4*)a.force;
-        R4 o;
-        if (a.accumulate) {
-            o = f4[ii];
-            o.x += fx; o.y += fy; o.z += fz;
-        } else {
-            o.x = fx; o.y = fy; o.z = fz; o.w = 0;
-        }
-        f4[ii] = o;
+        acc[0] += 0.5 * e_lj;   // full list: each pair seen from both sides
+        acc[1] += 0.5 * vir;
+        acc[2] += a.coul_energy_factor * e_c;
     }
-    block_sum_commit<NQ>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_VFF);
+    if (WALL) {
+        block_sum_commit<4>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_VFF);
+    } else {
+        double acc3[3] = {acc[0], acc[1], acc[2]};
+        block_sum_commit<3>(acc3, a.partials, a.max_blocks, a.counter, a.dscal + S_VFF);
+    }
+}
+
+// the feature sets the time-step fast path uses, each compiled on its own
+constexpr int FT_SETS[] = {0, FT_DPD, FT_DPD | FT_WALL, FT_WALL, FT_LGV, FT_LGV | FT_WALL, FT_LGV | FT_QSEP,
+                           FT_LGV | FT_QLJ, FT_DPD | FT_QSEP, FT_DPD | FT_QLJ};
+constexpr int N_FT_SETS = sizeof(FT_SETS) / sizeof(int);
+
+template <typename R, int TPP, int I>
+struct Dispatch {
+    static int run(int ft, const PairArgs& a, int grid, int block, size_t smem, cudaStream_t st) {
+        if (ft == FT_SETS[I]) {
+            k_pair<R, TPP, FT_SETS[I]><<<grid, block, smem, st>>>(a);
+            return 1;
+        }
+        return Dispatch<R, TPP, I - 1>::run(ft, a, grid, block, smem, st);
+    }
+    static int attr(size_t smem) {
+        if (cudaFuncSetAttribute(k_pair<R, TPP, FT_SETS[I]>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
+            return MFA_ERR_CUDA;
+        return Dispatch<R, TPP, I - 1>::attr(smem);
+    }
+};
+template <typename R, int TPP>
+struct Dispatch<R, TPP, -1> {
+    static int run(int, const PairArgs& a, int grid, int block, size_t smem, cudaStream_t st) {
+        k_pair<R, TPP, FT_GENERIC><<<grid, block, smem, st>>>(a);
+        return 0;
+    }
+    static int attr(size_t smem) {
+        if (cudaFuncSetAttribute(k_pair<R, TPP, FT_GENERIC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
+            return MFA_ERR_CUDA;
+        return MFA_OK;
+    }
+};
+
+template <typename R>
+int launch_r(int tpp, int ft, const PairArgs& a, int grid, int block, size_t smem, cudaStream_t st) {
+    switch (tpp) {
+        case 1: Dispatch<R, 1, N_FT_SETS - 1>::run(ft, a, grid, block, smem, st); break;
+        case 2: Dispatch<R, 2, N_FT_SETS - 1>::run(ft, a, grid, block, smem, st); break;
+        case 4: Dispatch<R, 4, N_FT_SETS - 1>::run(ft, a, grid, block, smem, st); break;
+        default: return MFA_ERR_ARGS;
+    }
+    return MFA_OK;
+}
+
+template <typename R>
+int attr_r(size_t smem) {
+    int rc = Dispatch<R, 1, N_FT_SETS - 1>::attr(smem);
+    if (rc == MFA_OK) rc = Dispatch<R, 2, N_FT_SETS - 1>::attr(smem);
+    if (rc == MFA_OK) rc = Dispatch<R, 4, N_FT_SETS - 1>::attr(smem);
+    return rc;
 }
 
 }  // namespace
+
+// Largest tile the pair kernel may stage, in records (2 x cap records within
+// 180 KB of dynamic shared memory).
+int pair_tile_limit(const mfa_ctx* c) {
+    const size_t rec = c->prec == MFA_MIXED ? sizeof(float4) : sizeof(double4);
+    return (int)((180 * 1024) / (2 * rec));
+}
+
+int pair_set_shape(mfa_ctx* c, int tpp, int block, int tile_cap) {
+    if (tpp != 1 && tpp != 2 && tpp != 4) return MFA_ERR_ARGS;
+    if (block < 32 || block > 256 || block % 32) return MFA_ERR_ARGS;
+    if (tile_cap < 0) tile_cap = 0;
+    if (tile_cap > pair_tile_limit(c)) tile_cap = pair_tile_limit(c);
+    const size_t rec = c->prec == MFA_MIXED ? sizeof(float4) : sizeof(double4);
+    const size_t smem = 2 * (size_t)tile_cap * rec;
+    const int rc = c->prec == MFA_MIXED ? attr_r<float>(smem) : attr_r<double>(smem);
+    if (rc != MFA_OK) return rc;
+    c->pair_tpp = tpp;
+    c->pair_block = block;
+    c->tile_cap = tile_cap;
+    return MFA_OK;
+}
 
 int launch_pair(mfa_ctx* c, int fuse_wall, int accumulate) {
     if (!c->lists_valid) return MFA_ERR_STATE;
     PairArgs a;
     a.pos_s = c->pos_s; a.vel_s = c->vel_s; a.nbr = c->nbr; a.nnb = c->nnb;
+    a.cell_start = c->cell_start; a.flags = c->dflags;
     a.mass = c->mass; a.tabs = c->tabs; a.force = c->force; a.dstep = c->dstep;
     a.partials = c->partials + (size_t)R_PAIR * 4 * c->max_blocks;
     a.counter = c->counters + R_PAIR;
@@ -273,11 +494,17 @@ int launch_pair(mfa_ctx* c, int fuse_wall, int accumulate) {
     a.n = c->n;
     a.max_blocks = c->max_blocks;
     const mfa_params& p = c->p;
+    for (int d = 0; d < 3; ++d) a.nb[d] = c->nb[d];
+    a.rule = c->bin_type;
+    a.wy = c->bin_type == 0 ? p.delta_bin[1] + 2 : 3;
+    a.nseg = a.wy * (c->bin_type == 0 ? p.delta_bin[2] + 2 : 3);
+    a.tile_cap = c->tile_cap;
     a.symmetry = p.symmetry; a.thermostat = p.thermostat; a.dpd_weight = p.dpd_weight;
     a.noise = p.noise; a.charged = p.charged;
     a.real_in_lj = (p.quirks & MFA_Q_EWALD_REAL_IN_LJ) != 0;
     a.fsw = p.force_switch_on;
     a.wall_type = p.wall; a.wall_e_aw = (p.quirks & MFA_Q_WALL_ENERGY_AW) != 0;
+    a.fuse_wall = fuse_wall && p.wall == 2;
     a.accumulate = accumulate;
     // ewald_real.f90:416 adds every visit; a full list (my_binning) visits each
     // pair twice, the half list once.
@@ -290,17 +517,20 @@ int launch_pair(mfa_ctx* c, int fuse_wall, int accumulate) {
     for (int k = 0; k < T8; ++k) { a.a_wall[k] = p.a_wall[k]; a.sigma_wall[k] = p.sigma_wall[k]; }
     a.a_w = p.a_w; a.z_space_wall = p.z_space_wall; a.wall_cut = p.wall_cut;
     a.seed0 = (uint32_t)p.seed; a.seed1 = (uint32_t)(p.seed >> 32);
-    const int T = 128;
-    const int nb = (c->n + T - 1) / T;
-    if (nb > c->max_blocks) return MFA_ERR_ARGS;
-    const bool fw = fuse_wall && p.wall == 2;
-    if (c->prec == MFA_MIXED) {
-        if (fw) k_pair<float, true><<<nb, T, 0, c->st>>>(a);
-        else k_pair<float, false><<<nb, T, 0, c->st>>>(a);
-    } else {
-        if (fw) k_pair<double, true><<<nb, T, 0, c->st>>>(a);
-        else k_pair<double, false><<<nb, T, 0, c->st>>>(a);
-    }
+    const int grid = c->nb[1] * c->nb[2];
+    if (grid > c->max_blocks) return MFA_ERR_ARGS;
+    const size_t rec = c->prec == MFA_MIXED ? sizeof(float4) : sizeof(double4);
+    const size_t smem = 2 * (size_t)c->tile_cap * rec;
+    int ft = 0;
+    if (p.thermostat == MFA_THERMO_DPD) ft |= FT_DPD;
+    if (p.thermostat == MFA_THERMO_LGV) ft |= FT_LGV;
+    if (p.charged) ft |= a.real_in_lj ? FT_QLJ : FT_QSEP;
+    if (p.force_switch_on) ft |= FT_FSW;
+    if (a.fuse_wall) ft |= FT_WALL;
+    if (accumulate) ft |= FT_ACC;
+    const int rc = c->prec == MFA_MIXED ? launch_r<float>(c->pair_tpp, ft, a, grid, c->pair_block, smem, c->st)
+                                        : launch_r<double>(c->pair_tpp, ft, a, grid, c->pair_block, smem, c->st);
+    if (rc != MFA_OK) return rc;
     MFA_CUDA_TRY(cudaGetLastError());
     note_launch(c, 1);
     return MFA_OK;

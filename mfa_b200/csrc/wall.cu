@@ -21,20 +21,8 @@ struct WallArgs {
 
 template <typename R>
 __device__ __forceinline__ void term93(const WallArgs& a, int t, R zz, R& f, double& e) {
-    const R sw = (R)a.sigma_wall[t - 1], aw = (R)a.a_wall[t - 1];
-    const R ae = a.e_aw ? (R)a.a_w : aw;
-    const R faw = aw < 0 ? -aw : aw;
-    const R iz = (R)1 / zz;
-    const R rd = sw * iz;
-    const R rd2 = rd * rd, rd4 = rd2 * rd2, rd8 = rd4 * rd4;
-    const R sw2 = sw * sw, sw4 = sw2 * sw2, sw8 = sw4 * sw4;
-    const R iz2 = iz * iz, iz4 = iz2 * iz2, iz8 = iz4 * iz4;
-    e = (double)(faw * (rd8 * rd) - ae * (rd2 * rd));
-    f = (R)9 * faw * (sw8 * sw) * (iz8 * iz2) - (R)3 * aw * (sw2 * sw) * iz4;
-    if (a.wall_cut > 0) {
-        const R rc = sw / (R)a.wall_cut, rc3 = rc * rc * rc;
-        e -= (double)(faw * rc3 * rc3 * rc3 - ae * rc3);
-    }
+    const R aw = (R)a.a_wall[t - 1];
+    wall93_term<R>(zz, (R)a.sigma_wall[t - 1], aw, a.e_aw ? (R)a.a_w : aw, (R)a.wall_cut, f, e);
 }
 
 template <typename R, typename R4>
