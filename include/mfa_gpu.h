@@ -42,7 +42,8 @@ typedef enum mfa_status {
     MFA_ERR_TIMEOUT = 6,         /* a bounded device wait gave up                */
     MFA_ERR_NOMEM = 7,           /* device allocation failed                     */
     MFA_ERR_STATE = 8,           /* call order violated (e.g. forces before lists) */
-    MFA_ERR_UNSUPPORTED = 9      /* feature not built for this parameter set     */
+    MFA_ERR_UNSUPPORTED = 9,     /* feature not built for this parameter set     */
+    MFA_ERR_CAPACITY = 10        /* request larger than a fixed-size buffer      */
 } mfa_status;
 
 typedef enum mfa_precision {
@@ -244,6 +245,31 @@ int mfa_debug_lists(mfa_ctx* ctx, int32_t* cell_of, int32_t* nbr_count,
                     int32_t* nbr, int32_t max_per);
 /* Number of k-vectors and their components (after mfa_ewald_k(ctx, 0)). */
 int mfa_debug_kvecs(mfa_ctx* ctx, int32_t* nk, double* kvecs3, int32_t max_k);
+
+/* ---------------- binning without device allocation ---------------- */
+
+/* No counterpart in the reference.  The cell binning that mfa_binning starts
+ * with (binning.f90:25-50 for rule 0, my_binning.f90:26-44 for rule 1), for
+ * callers that must not allocate device memory -- host programs that already
+ * own all of the GPU's memory through their own pools, or that call at a point
+ * where the device-wide synchronisation an allocation may imply is not
+ * acceptable.  Nothing is allocated: the caller passes device buffers
+ *   r0         n particles, xyz interleaved (Fortran r0(3,n)), read only
+ *   cell_of    n, the cell of each particle (0-based, ix + nbx*(iy + nby*iz))
+ *   cell_start n_bin[0]*n_bin[1]*n_bin[2] + 1, first slot of each cell
+ *   sorted_ids n, particle ids (0-based) grouped by cell, ascending in a cell
+ * and the per-cell counters live in a fixed device array inside the library of
+ * at most 131072 cells (1 MiB, held by every GPU that loads the library until
+ * the process exits); larger grids return MFA_ERR_CAPACITY.  All calls share
+ * that array: calls whose work overlaps on the GPU race and must be serialised
+ * by the caller.  boundary and n_bin are host arrays of 3; stream is a
+ * cudaStream_t (NULL for the default stream).  The first call on a device looks
+ * the array's device address up (make it before any stream capture); every
+ * call synchronises `stream` before returning and reports particles outside
+ * the grid (MFA_ERR_CELL_RANGE) or non-finite (MFA_ERR_NONFINITE). */
+int mfa_bin_cells_noalloc(const double* r0, int32_t n, const double* boundary,
+                          const int32_t* n_bin, int32_t rule, int32_t* cell_of,
+                          int32_t* cell_start, int32_t* sorted_ids, void* stream);
 
 #ifdef __cplusplus
 }

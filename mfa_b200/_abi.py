@@ -23,6 +23,7 @@ ERR_TIMEOUT = 6
 ERR_NOMEM = 7
 ERR_STATE = 8
 ERR_UNSUPPORTED = 9
+ERR_CAPACITY = 10
 
 FP64 = 0
 MIXED = 1
@@ -125,6 +126,8 @@ SIGNATURES = {
     "mfa_sync": (C.c_int, [_P]),
     "mfa_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "mfa_set_pair_shape": (C.c_int, [_P, C.c_int32, C.c_int32]),
+    "mfa_bin_cells_noalloc": (C.c_int, [C.c_void_p, C.c_int32, _DP, _IP, C.c_int32, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p]),
     "mfa_debug_lists": (C.c_int, [_P, _IP, _IP, _IP, C.c_int32]),
     "mfa_debug_kvecs": (C.c_int, [_P, _IP, _DP, C.c_int32]),
 }

@@ -205,6 +205,7 @@ const char* mfa_status_string(int s) {
         case MFA_ERR_NOMEM: return "device allocation failed";
         case MFA_ERR_STATE: return "call order violated";
         case MFA_ERR_UNSUPPORTED: return "unsupported parameter set";
+        case MFA_ERR_CAPACITY: return "request larger than a fixed-size buffer";
         default: return "unknown status";
     }
 }
