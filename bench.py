@@ -42,6 +42,7 @@ def args_():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--chunk", type=int, default=10, help="time steps per timed iteration (one mfa_step call)")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="brush", choices=["brush", "melt", "charged"])
     ap.add_argument("--equil", type=int, default=10000, help="untimed relaxation steps of the fresh configuration")
@@ -276,13 +277,18 @@ def main():
             g.step(a.equil)
         tuned = tune_pair_shape(g)
         g.tuned = min(tuned, key=tuned.get)
+        g.tuning = {f"{k}x{b}{'-tiled' if t else ''}": round(1e3 * s / 300, 4) for (k, b, t), s in tuned.items()}
         ext = torch.cuda.ExternalStream(g.stream_ptr(), device=f"cuda:{dev}")
-        for k in range(warmup):
+        # a timed iteration is `chunk` consecutive time steps (one mfa_step call:
+        # fused velocity/position kernels, captured graphs); L2 is flushed
+        # between iterations
+        chunks = [a.chunk] * (steps // a.chunk) + ([steps % a.chunk] if steps % a.chunk else [])
+        for k in range(max(1, -(-warmup // a.chunk))):
             with torch.cuda.stream(ext):
                 flush.fill_(k & 0xff)
-            g.step(1)
+            g.step(a.chunk)
         g.sync()
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in chunks]
         s0 = g.scalars()
         launches0 = s0["kernel_launches"]
         if dist is not None:
@@ -291,12 +297,12 @@ def main():
         sampler = ClockSampler(dev)
         sampler.start()
         torch.cuda.nvtx.range_push(f"timed_{'mixed' if prec == _abi.MIXED else 'fp64'}")
-        for k in range(steps):
+        for k, nst in enumerate(chunks):
             if flush_l2:
                 with torch.cuda.stream(ext):
                     flush.fill_(k & 0xff)
             ev[k][0].record(ext)
-            g.step(1)
+            g.step(nst)
             ev[k][1].record(ext)
         torch.cuda.nvtx.range_pop()
         g.sync()
@@ -312,6 +318,7 @@ def main():
     # headline: mixed precision
     g, ms_mixed, launches, clocks, s_mixed = timed_run(_abi.MIXED, a.steps, a.warmup)
     shape_mixed = g.tuned
+    tuning_mixed = g.tuning
     ms_max = ms_mixed
     if dist is not None:
         t = torch.tensor([ms_mixed], dtype=torch.float64, device=f"cuda:{dev}")
@@ -420,9 +427,13 @@ def main():
             "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded generator, no reference data)",
             "config": dict(meta, beads=n, precision="mixed", dt=cfg.params.dt, skin=cfg.params.skin,
-                           pair_shape=f"{shape_mixed[0]} threads/particle x {shape_mixed[1]}-thread blocks (autotuned)",
+                           pair_shape=f"{shape_mixed[0]} kept pairs per thread x {shape_mixed[1]}-thread blocks, "
+                                      f"{'tiled' if shape_mixed[2] else 'untiled'} (autotuned)",
+                           autotune_ms_per_step=tuning_mixed,
                            thermostat="dpd", replicas=world,
-                           l2="flushed between timed steps (256 MiB write on the context stream)",
+                           steps_per_timed_iteration=a.chunk,
+                           l2=f"flushed between timed iterations of {a.chunk} steps "
+                              "(256 MiB write on the context stream)",
                            parallelism=f"replicas x{world}"),
             "fp64": {"value": value_fp64, "ms_per_step": ms_fp64 / a.steps},
             "mixed_over_fp64": value / value_fp64,

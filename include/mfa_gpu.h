@@ -220,11 +220,13 @@ int mfa_step(mfa_ctx* ctx, int32_t nsteps);
 int mfa_set_energy_log(mfa_ctx* ctx, int32_t every, int32_t capacity);
 int mfa_read_energy_log(mfa_ctx* ctx, double* out3, int32_t max_entries, int32_t* n_out);
 
-/* Launch shape of the pair kernel: threads that share one particle's
- * neighbour list (1, 2 or 4) and threads per block (32..256, multiple of 32).
- * Results do not depend on it beyond floating-point summation order; it is
- * what the autotuner (mfa_b200.tune) chooses. */
-int mfa_set_pair_shape(mfa_ctx* ctx, int32_t threads_per_particle, int32_t block);
+/* Launch shape of the pair kernel: how many in-range neighbours a thread keeps
+ * per pass before its warp evaluates the kept pairs together (2, 4 or 8),
+ * threads per block (32..256, multiple of 32), and whether each block stages
+ * its neighbourhood in shared memory (tiled = 1) or reads neighbours through
+ * the cache hierarchy (tiled = 0).  Results do not depend on it; it is what the
+ * autotuner (mfa_b200.tune) chooses. */
+int mfa_set_pair_shape(mfa_ctx* ctx, int32_t pairs_per_thread, int32_t block, int32_t tiled);
 
 /* ---------------- host mirrors ---------------- */
 

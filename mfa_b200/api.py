@@ -156,8 +156,9 @@ class System:
         """nsteps time steps on the device (fused kernels, captured graphs)."""
         check(self.lib.mfa_step(self.ctx, int(nsteps)), "mfa_step")
 
-    def set_pair_shape(self, threads_per_particle: int, block: int) -> None:
-        check(self.lib.mfa_set_pair_shape(self.ctx, int(threads_per_particle), int(block)), "mfa_set_pair_shape")
+    def set_pair_shape(self, pairs_per_thread: int, block: int, tiled: bool = True) -> None:
+        check(self.lib.mfa_set_pair_shape(self.ctx, int(pairs_per_thread), int(block), int(bool(tiled))),
+              "mfa_set_pair_shape")
 
     # ---- mirrors ----
     def stream_ptr(self) -> int:

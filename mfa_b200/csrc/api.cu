@@ -359,10 +359,12 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
         rc = MFA_ERR_CUDA;
     if (rc == MFA_OK) rc = bonds_setup(c);
     if (rc == MFA_OK) {
-        // pair kernel: 2 threads per particle, 256-thread blocks, a tile sized
-        // for 1.2x the mean neighbourhood of a row (grown at a rebuild if needed)
+        // pair kernel: up to 4 kept pairs per lane and chunk, 128-thread blocks,
+        // a tile sized for 1.2x the mean neighbourhood of a row (grown at a
+        // rebuild if needed)
         const long long cap = 9LL * (6LL * n / (5LL * nrow) + 8);
-        rc = pair_set_shape(c, 2, 256, (int)(cap < pair_tile_limit(c) ? cap : pair_tile_limit(c)));
+        c->pair_tiled = 1;
+        rc = pair_set_shape(c, 4, 128, (int)(cap < pair_tile_limit(c) ? cap : pair_tile_limit(c)));
     }
     if (rc != MFA_OK) { free_all(c); free(c); return rc; }
 #undef A
@@ -547,10 +549,11 @@ int mfa_get_scalars(mfa_ctx* c, mfa_scalars* o) {
     return first_error(f[F_ERR]);
 }
 
-int mfa_set_pair_shape(mfa_ctx* c, int32_t tpp, int32_t block) {
-    if (!c) return MFA_ERR_ARGS;
+int mfa_set_pair_shape(mfa_ctx* c, int32_t k, int32_t block, int32_t tiled) {
+    if (!c || (tiled != 0 && tiled != 1)) return MFA_ERR_ARGS;
     MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
-    TRY(pair_set_shape(c, tpp, block, c->tile_cap));
+    c->pair_tiled = tiled;
+    TRY(pair_set_shape(c, k, block, c->tile_cap));
     invalidate_graph(c);
     return MFA_OK;
 }

@@ -70,7 +70,7 @@ struct mfa_ctx {
     int32_t *cell_count, *cell_start, *cell_cursor, *cell_of, *row_count;
     // pair kernel launch shape (threads per particle, block size) and the
     // shared-memory capacity of its staged tile, in records
-    int pair_tpp, pair_block, tile_cap;
+    int pair_tpp, pair_block, tile_cap, pair_tiled;
     // pair tables on the device: range_2+skin_2, range_2, epsil, sigma_2, e_shift, inv_range_2
     double* tabs;                       // 6 x T8*T8
     // Verlet list

@@ -6,12 +6,19 @@
 // cell rows, each a contiguous run of cell-sorted records -- is staged into
 // shared memory with bulk asynchronous copies (cp.async.bulk, completion on an
 // mbarrier, bounded wait), and the Verlet-list entries (segment, offset) index
-// that tile directly.  TPP threads share one particle's list and combine their
-// partial forces with warp shuffles; each particle's force is accumulated by
-// its own group only: no atomics, a fixed summation order, and the DPD noise of
-// a pair is drawn from Philox keyed by (step, min(i,j), max(i,j)) so both sides
-// see the same random number.  If a row's neighbourhood does not fit the
-// shared-memory tile, the CTA reads the same records from global memory.
+// that tile directly.  A warp works on 32 particles of the row at a time in
+// three passes per chunk of their lists:
+//   1. each lane tests its own listed neighbours (distance only) and keeps up
+//      to K in-range ones in its slice of shared memory;
+//   2. the warp's kept pairs are laid out back to back and the lanes take them
+//      32 at a time, so the expensive pair physics (LJ, Philox noise, DPD,
+//      Ewald real) runs with every lane busy instead of once per listed pair
+//      with most lanes idle;
+//   3. each lane adds the results of its own pairs, in list order.
+// Each particle's force is summed by its own lane in a fixed order (no atomics,
+// deterministic), and the DPD noise of a pair is drawn from Philox keyed by
+// (step, min(i,j), max(i,j)) so both sides see the same random number.  If a
+// row's neighbourhood does not fit the tile, the CTA reads global memory.
 // R = float in MIXED mode (FP32 force math, FP64 energy/virial accumulators),
 // double in FP64 mode.
 #include "mfa_internal.cuh"
@@ -56,6 +63,8 @@ __device__ __forceinline__ double mimg(double d, double L, double iL) {
     return d - L * (double)(int)(2.0 * d * iL);
 }
 __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
+__device__ __forceinline__ float rcp_(float x) { return __fdividef(1.0f, x); }
+__device__ __forceinline__ double rcp_(double x) { return 1.0 / x; }
 __device__ __forceinline__ double rsqrt_(double x) { return sqrt(1.0 / x); }
 __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
 __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
@@ -70,9 +79,14 @@ __device__ __forceinline__ float noise1(uint32_t x0, uint32_t x1, int shape, flo
         const float u = (float)(x0 >> 9) * 1.1920928955078125e-07f + 5.9604644775390625e-08f;
         return 1.7320508075688772f * (2.0f * u - 1.0f);
     }
+    // FP32 (mixed) path: the hardware approximations of log, cos and 1/sqrt;
+    // their ~1e-6 relative error is far below the statistical noise they model.
+    // cos(2 pi u2) = -cos(2 pi u2 - pi) keeps __cosf inside [-pi, pi].
     const float u1 = fmaf((float)x0, 2.3283064365386963e-10f, 1.16415321826934814e-10f);
     const float u2 = fmaf((float)x1, 2.3283064365386963e-10f, 1.16415321826934814e-10f);
-    return sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
+    const float s = -2.0f * __logf(u1);
+    const float r = s > 0.0f ? s * rsqrtf(s) : 0.0f;
+    return -r * __cosf(fmaf(6.283185307179586f, u2, -3.14159265358979f));
 }
 __device__ __forceinline__ double noise1(uint32_t x0, uint32_t x1, int shape, double) {
     if (shape == MFA_NOISE_UNIFORM) {
@@ -149,13 +163,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// bounded wait: gives up after `limit` polls (each poll may suspend briefly)
+// bounded wait: gives up after `limit` polls; between polls the warp sleeps
+// (32 ns doubling to 512 ns), so waiting warps do not take issue slots from
+// the CTAs on the same SM that have their data
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long limit) {
-    for (long long it = 0; it < limit; ++it)
+    unsigned ns = 32;
+    for (long long it = 0; it < limit; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
+        __nanosleep(ns);
+        if (ns < 512) ns <<= 1;
+    }
     return false;
 }
-constexpr long long WAIT_LIMIT = 1LL << 24;
+constexpr long long WAIT_LIMIT = 1LL << 23;   // ~4 s of polls at the longest sleep
 
 // Feature bits of a pair-kernel instantiation.  A specialised instantiation
 // compiles only the physics a run uses (fewer registers, more resident warps);
@@ -188,12 +208,28 @@ __device__ __forceinline__ bool has(const PairArgs& a, int bit) {
     return (FT & bit) != 0;
 }
 
-template <typename R, int TPP, int FT>
+template <typename R> struct Vec3;
+template <> struct Vec3<float> { typedef float3 T; };
+template <> struct Vec3<double> { typedef double3 T; };
+
+// K: in-range pairs a lane may keep per chunk (pass 1 capacity)
+template <typename R, int K, int FT>
 __global__ void __launch_bounds__(256, 3) k_pair(PairArgs a) {
     typedef typename Vec4<R>::T R4;
+    typedef typename Vec3<R>::T R3;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     R4* tpos = (R4*)smem_raw;
     R4* tvel = tpos + a.tile_cap;
+    // per-warp work space after the two tile arrays
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    unsigned char* wbase = (unsigned char*)(tvel + a.tile_cap);
+    const size_t wbytes = 32 * sizeof(R4) * 2 + 32 * K * (sizeof(int) * 2 + sizeof(R3));
+    unsigned char* wmem = wbase + warp * wbytes;
+    R4* own_p = (R4*)wmem;                         // 32 owner positions
+    R4* own_v = own_p + 32;                        // 32 owner velocities
+    int* q1 = (int*)(own_v + 32);                  // lane-private kept entries [lane*K + j]
+    int* q2 = q1 + 32 * K;                         // kept entries back to back (owner << 24 | index)
+    R3* qres = (R3*)(q2 + 32 * K);                 // pair results, back to back
     __shared__ R s_rc2[T8 * T8], s_eps[T8 * T8], s_sig2[T8 * T8], s_esh[T8 * T8], s_irc2[T8 * T8];
     __shared__ int seg_start[16], seg_base[16];
     __shared__ int s_mode;   // 1: tile in shared memory, 0: global records
@@ -206,8 +242,7 @@ __global__ void __launch_bounds__(256, 3) k_pair(PairArgs a) {
     const int nx = a.nb[0], ny = a.nb[1], nz = a.nb[2];
     // staging: lane k of warp 0 finds neighbouring row k; a warp scan places
     // the rows back to back; every lane then issues the bulk copies of its row
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
+    if (warp == 0) {
         int s0 = 0, len = 0;
         if (lane < a.nseg) {
             int ky, kz;
@@ -256,6 +291,8 @@ __global__ void __launch_bounds__(256, 3) k_pair(PairArgs a) {
     }
     const R4* __restrict__ gpos = (const R4*)a.pos_s;
     const R4* __restrict__ gvel = (const R4*)a.vel_s;
+    const R4* spos = tile ? tpos : gpos;           // where pass 2 reads neighbour records
+    const R4* svel = tile ? tvel : gvel;
     const long long step = *a.dstep;
     R r2min = 0;
     if (FSW) {
@@ -268,72 +305,100 @@ __global__ void __launch_bounds__(256, 3) k_pair(PairArgs a) {
     const R sig = (R)a.sig, gam = (R)a.friction;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     const int p0 = a.cell_start[nx * row], p1 = a.cell_start[nx * row + nx];
-    const int sub = threadIdx.x % TPP;
-    const int per_pass = blockDim.x / TPP;
-    for (int base = p0; base < p1 && valid; base += per_pass) {
-        const int t = base + threadIdx.x / TPP;
+    for (int base = p0 + 32 * warp; base < p1 && valid; base += 32 * nwarp) {
+        const int t = base + lane;
         const bool act = t < p1;
-        R fx = 0, fy = 0, fz = 0;
-        double e_lj = 0.0, vir = 0.0, e_c = 0.0;
         R4 pi, vi;
-        int ti = 1, ii = 0;
+        int m = 0;
         if (act) {
             pi = ldg4(&gpos[t]);
-            const int wi = wbits(pi.w);
-            ti = wi & 0xff;
-            ii = wi >> 8;
             if (need_v) vi = ldg4(&gvel[t]);
-            const int m = a.nnb[t];
-            const int rowi = (ti - 1) * T8;
-            for (int k = sub; k < m; k += TPP) {
+            m = a.nnb[t];
+        } else {
+            pi.x = pi.y = pi.z = 0; pi.w = 0;
+        }
+        own_p[lane] = pi;
+        if (need_v) own_v[lane] = vi;
+        const int ti = wbits(pi.w) & 0xff;
+        const int rowi = (ti > 0 ? ti - 1 : 0) * T8;
+        R fx = 0, fy = 0, fz = 0;
+        double e_lj = 0.0, vir = 0.0, e_c = 0.0;
+        int k = 0;
+        while (__any_sync(0xffffffffu, k < m)) {
+            // pass 1: distance test of this lane's next listed neighbours
+            int c = 0;
+            while (k < m && c < K) {
                 const int e = __ldg(&a.nbr[(size_t)k * a.n + t]);
+                ++k;
                 const int seg = e >> 27, off = e & 0x7ffffff;
-                const int lj = seg_base[seg] + off;
-                const int gj = seg_start[seg] + off;
-                const R4 pj = tile ? tpos[lj] : ldg4(&gpos[gj]);
+                const int idx = tile ? seg_base[seg] + off : seg_start[seg] + off;
+                const R4 pj = tile ? tpos[idx] : ldg4(&gpos[idx]);
                 R dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
                 dx = mimg(dx, Lx, iLx);
                 dy = mimg(dy, Ly, iLy);
                 if (a.symmetry == 1) dz = mimg(dz, Lz, iLz);
                 const R r2 = dx * dx + dy * dy + dz * dz;
-                const int wj = wbits(pj.w);
-                const int ij = rowi + (wj & 0xff) - 1;
-                const bool in_lj = r2 < s_rc2[ij];
+                const bool in_lj = r2 < s_rc2[rowi + (wbits(pj.w) & 0xff) - 1];
                 const bool in_ew = QSEP && r2 < (R)a.ewald_rc_2;
-                if (!in_lj && !in_ew) continue;
-                R4 vj;
-                if (need_v) vj = tile ? tvel[lj] : ldg4(&gvel[gj]);
-                if (in_lj) {
+                if (in_lj || in_ew) q1[lane * K + c++] = idx;
+            }
+            // lay the kept pairs out back to back (owner lane in the top bits)
+            int incl = c;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            const int first = incl - c;
+            for (int j = 0; j < c; ++j) q2[first + j] = (lane << 24) | q1[lane * K + j];
+            __syncwarp();
+            // pass 2: every lane takes pairs first+lane, +32, ...
+            for (int q = lane; q < total; q += 32) {
+                const int w = q2[q];
+                const int ol = w >> 24, idx = w & 0xffffff;
+                const R4 qi = own_p[ol];
+                const R4 pj = spos[idx];
+                R dx = qi.x - pj.x, dy = qi.y - pj.y, dz = qi.z - pj.z;
+                dx = mimg(dx, Lx, iLx);
+                dy = mimg(dy, Ly, iLy);
+                if (a.symmetry == 1) dz = mimg(dz, Lz, iLz);
+                const R r2 = dx * dx + dy * dy + dz * dz;
+                const int wi = wbits(qi.w), wj = wbits(pj.w);
+                const int ij = ((wi & 0xff) - 1) * T8 + (wj & 0xff) - 1;
+                R4 vq, vj;
+                if (need_v) { vq = own_v[ol]; vj = svel[idx]; }
+                R fsum = 0;
+                if (r2 < s_rc2[ij]) {
                     const R r2c = FSW ? (r2 > r2min ? r2 : r2min) : r2;
-                    const R inv_r2 = (R)1 / r2c;
+                    const R inv_r2 = rcp_(r2c);
                     const R eps = s_eps[ij];
                     const R r61 = s_sig2[ij] * inv_r2;
                     const R r6 = r61 * r61 * r61;
                     const R r12 = r6 * r6;
                     e_lj += (double)(eps * ((r12 - r6) - s_esh[ij]));
                     const R fs = eps * ((R)12 * r12 - (R)6 * r6) * inv_r2;   // force on i along d
-                    R fsum = fs;
+                    fsum = fs;
                     vir += (double)(fs * r2);
                     if (DPD || QLJ) {
                         const R inv_r = rsqrt_(r2c);
                         if (DPD) {
                             // dpd_forces.f90:273-348 with Philox noise keyed by the pair
-                            const int jj = wj >> 8;
+                            const int ii = wi >> 8, jj = wj >> 8;
                             const uint32_t lo = (uint32_t)min(ii, jj), hi = (uint32_t)max(ii, jj);
-                            const uint4 w = philox4x32_10(make_uint4(lo, hi, (uint32_t)step, TAG_DPD), a.seed0,
-                                                          a.seed1);
-                            const R g = noise1(w.x, w.y, a.noise, R(0));
+                            const uint4 ph = philox4x32_10(make_uint4(lo, hi, (uint32_t)step, TAG_DPD), a.seed0,
+                                                           a.seed1);
+                            const R g = noise1(ph.x, ph.y, a.noise, R(0));
                             R wr, wd;
                             if (a.dpd_weight == 1) { wr = 1; wd = 1; }
                             else { wr = (R)1 - sqrt_(r2c * s_irc2[ij]); wd = wr * wr; }
-                            const R rd = ((vi.x - vj.x) * dx + (vi.y - vj.y) * dy + (vi.z - vj.z) * dz) * inv_r;
+                            const R rd = ((vq.x - vj.x) * dx + (vq.y - vj.y) * dy + (vq.z - vj.z) * dz) * inv_r;
                             // F_i += (sig w_r g - gamma w_d (dv . rhat)) rhat, rhat = d * inv_r
                             fsum += (sig * wr * g - gam * wd * rd) * inv_r;
                         }
                         if (QLJ) {
                             // ewald_real.f90:411-428, inside the LJ range (reference behaviour)
-                            const R qq = vi.w * vj.w;
-                            const R r = (R)1 / inv_r;
+                            const R qq = vq.w * vj.w;
+                            const R r = r2c * inv_r;
                             const R ec = erfc_((R)a.sqrt_alpha * r);
                             e_c += (double)(qq * ec * inv_r);
                             const R fsc = qq * (R)a.sqrt_alpha * (R)a.inv_sqrt_pi * (R)2 * exp_(-(R)a.alpha_c * r2c) *
@@ -342,30 +407,32 @@ __global__ void __launch_bounds__(256, 3) k_pair(PairArgs a) {
                             vir += (double)(fsc * r2 * inv_r);
                         }
                     }
-                    fx += fsum * dx; fy += fsum * dy; fz += fsum * dz;
                 }
-                if (in_ew) {
-                    const R qq = vi.w * vj.w;
+                if (QSEP && r2 < (R)a.ewald_rc_2) {
+                    const R qq = vq.w * vj.w;
                     const R ir = rsqrt_(r2);
-                    const R r = (R)1 / ir;
+                    const R r = r2 * ir;
                     const R ec = erfc_((R)a.sqrt_alpha * r);
                     e_c += (double)(qq * ec * ir);
                     const R fsc = qq * (R)a.sqrt_alpha * (R)a.inv_sqrt_pi * (R)2 * exp_(-(R)a.alpha_c * r2) * ir
                                   + qq * ec * ir * ir;
-                    const R f = fsc * ir;
-                    fx += f * dx; fy += f * dy; fz += f * dz;
+                    fsum += fsc * ir;
                     vir += (double)(fsc * r2 * ir);
                 }
+                R3 rs;
+                rs.x = fsum * dx; rs.y = fsum * dy; rs.z = fsum * dz;
+                qres[q] = rs;
             }
+            __syncwarp();
+            // pass 3: this lane's pairs, in list order
+            for (int j = 0; j < c; ++j) {
+                const R3 rs = qres[first + j];
+                fx += rs.x; fy += rs.y; fz += rs.z;
+            }
+            __syncwarp();
         }
-        // combine the TPP partial sums of a particle (lanes of one group are adjacent)
-#pragma unroll
-        for (int o = TPP / 2; o > 0; o >>= 1) {
-            fx += __shfl_xor_sync(0xffffffffu, fx, o);
-            fy += __shfl_xor_sync(0xffffffffu, fy, o);
-            fz += __shfl_xor_sync(0xffffffffu, fz, o);
-        }
-        if (act && sub == 0) {
+        if (act) {
+            const int ii = wbits(pi.w) >> 8;
             if (LGV) {
                 // lgv_forces.f90:377-393
                 R g[3];
@@ -395,6 +462,7 @@ __global__ void __launch_bounds__(256, 3) k_pair(PairArgs a) {
         acc[0] += 0.5 * e_lj;   // full list: each pair seen from both sides
         acc[1] += 0.5 * vir;
         acc[2] += a.coul_energy_factor * e_c;
+        __syncwarp();
     }
     if (WALL) {
         block_sum_commit<4>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_VFF);
@@ -404,35 +472,41 @@ __global__ void __launch_bounds__(256, 3) k_pair(PairArgs a) {
     }
 }
 
+template <typename R, int K>
+size_t warp_space() {
+    typedef typename Vec4<R>::T R4;
+    typedef typename Vec3<R>::T R3;
+    return 32 * sizeof(R4) * 2 + 32 * K * (sizeof(int) * 2 + sizeof(R3));
+}
+
 // the feature sets the time-step fast path uses, each compiled on its own
 constexpr int FT_SETS[] = {0, FT_DPD, FT_DPD | FT_WALL, FT_WALL, FT_LGV, FT_LGV | FT_WALL, FT_LGV | FT_QSEP,
                            FT_LGV | FT_QLJ, FT_DPD | FT_QSEP, FT_DPD | FT_QLJ};
 constexpr int N_FT_SETS = sizeof(FT_SETS) / sizeof(int);
 
-template <typename R, int TPP, int I>
+template <typename R, int K, int I>
 struct Dispatch {
-    static int run(int ft, const PairArgs& a, int grid, int block, size_t smem, cudaStream_t st) {
+    static void run(int ft, const PairArgs& a, int grid, int block, size_t smem, cudaStream_t st) {
         if (ft == FT_SETS[I]) {
-            k_pair<R, TPP, FT_SETS[I]><<<grid, block, smem, st>>>(a);
-            return 1;
+            k_pair<R, K, FT_SETS[I]><<<grid, block, smem, st>>>(a);
+            return;
         }
-        return Dispatch<R, TPP, I - 1>::run(ft, a, grid, block, smem, st);
+        Dispatch<R, K, I - 1>::run(ft, a, grid, block, smem, st);
     }
     static int attr(size_t smem) {
-        if (cudaFuncSetAttribute(k_pair<R, TPP, FT_SETS[I]>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(k_pair<R, K, FT_SETS[I]>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem) != cudaSuccess)
             return MFA_ERR_CUDA;
-        return Dispatch<R, TPP, I - 1>::attr(smem);
+        return Dispatch<R, K, I - 1>::attr(smem);
     }
 };
-template <typename R, int TPP>
-struct Dispatch<R, TPP, -1> {
-    static int run(int, const PairArgs& a, int grid, int block, size_t smem, cudaStream_t st) {
-        k_pair<R, TPP, FT_GENERIC><<<grid, block, smem, st>>>(a);
-        return 0;
+template <typename R, int K>
+struct Dispatch<R, K, -1> {
+    static void run(int, const PairArgs& a, int grid, int block, size_t smem, cudaStream_t st) {
+        k_pair<R, K, FT_GENERIC><<<grid, block, smem, st>>>(a);
     }
     static int attr(size_t smem) {
-        if (cudaFuncSetAttribute(k_pair<R, TPP, FT_GENERIC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(k_pair<R, K, FT_GENERIC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem) != cudaSuccess)
             return MFA_ERR_CUDA;
         return MFA_OK;
@@ -440,43 +514,55 @@ struct Dispatch<R, TPP, -1> {
 };
 
 template <typename R>
-int launch_r(int tpp, int ft, const PairArgs& a, int grid, int block, size_t smem, cudaStream_t st) {
-    switch (tpp) {
-        case 1: Dispatch<R, 1, N_FT_SETS - 1>::run(ft, a, grid, block, smem, st); break;
+size_t smem_bytes(int k, int block, int tile_cap) {
+    typedef typename Vec4<R>::T R4;
+    const size_t ws = k == 2 ? warp_space<R, 2>() : (k == 4 ? warp_space<R, 4>() : warp_space<R, 8>());
+    return 2 * (size_t)tile_cap * sizeof(R4) + (size_t)(block / 32) * ws;
+}
+
+template <typename R>
+int launch_r(int k, int ft, const PairArgs& a, int grid, int block, size_t smem, cudaStream_t st) {
+    switch (k) {
         case 2: Dispatch<R, 2, N_FT_SETS - 1>::run(ft, a, grid, block, smem, st); break;
         case 4: Dispatch<R, 4, N_FT_SETS - 1>::run(ft, a, grid, block, smem, st); break;
+        case 8: Dispatch<R, 8, N_FT_SETS - 1>::run(ft, a, grid, block, smem, st); break;
         default: return MFA_ERR_ARGS;
     }
     return MFA_OK;
 }
 
 template <typename R>
-int attr_r(size_t smem) {
-    int rc = Dispatch<R, 1, N_FT_SETS - 1>::attr(smem);
-    if (rc == MFA_OK) rc = Dispatch<R, 2, N_FT_SETS - 1>::attr(smem);
-    if (rc == MFA_OK) rc = Dispatch<R, 4, N_FT_SETS - 1>::attr(smem);
-    return rc;
+int attr_r(int k, size_t smem) {
+    switch (k) {
+        case 2: return Dispatch<R, 2, N_FT_SETS - 1>::attr(smem);
+        case 4: return Dispatch<R, 4, N_FT_SETS - 1>::attr(smem);
+        case 8: return Dispatch<R, 8, N_FT_SETS - 1>::attr(smem);
+    }
+    return MFA_ERR_ARGS;
 }
+
+constexpr size_t SMEM_LIMIT = 200 * 1024;   // dynamic shared memory per CTA
 
 }  // namespace
 
-// Largest tile the pair kernel may stage, in records (2 x cap records within
-// 180 KB of dynamic shared memory).
+// Largest tile the pair kernel may stage, in records, next to the work space
+// of the largest launch shape.
 int pair_tile_limit(const mfa_ctx* c) {
     const size_t rec = c->prec == MFA_MIXED ? sizeof(float4) : sizeof(double4);
-    return (int)((180 * 1024) / (2 * rec));
+    const size_t ws = c->prec == MFA_MIXED ? smem_bytes<float>(8, 256, 0) : smem_bytes<double>(8, 256, 0);
+    return (int)((SMEM_LIMIT - ws) / (2 * rec));
 }
 
-int pair_set_shape(mfa_ctx* c, int tpp, int block, int tile_cap) {
-    if (tpp != 1 && tpp != 2 && tpp != 4) return MFA_ERR_ARGS;
+int pair_set_shape(mfa_ctx* c, int k, int block, int tile_cap) {
+    if (k != 2 && k != 4 && k != 8) return MFA_ERR_ARGS;
     if (block < 32 || block > 256 || block % 32) return MFA_ERR_ARGS;
     if (tile_cap < 0) tile_cap = 0;
     if (tile_cap > pair_tile_limit(c)) tile_cap = pair_tile_limit(c);
-    const size_t rec = c->prec == MFA_MIXED ? sizeof(float4) : sizeof(double4);
-    const size_t smem = 2 * (size_t)tile_cap * rec;
-    const int rc = c->prec == MFA_MIXED ? attr_r<float>(smem) : attr_r<double>(smem);
+    const size_t smem = c->prec == MFA_MIXED ? smem_bytes<float>(k, block, tile_cap)
+                                             : smem_bytes<double>(k, block, tile_cap);
+    const int rc = c->prec == MFA_MIXED ? attr_r<float>(k, smem) : attr_r<double>(k, smem);
     if (rc != MFA_OK) return rc;
-    c->pair_tpp = tpp;
+    c->pair_tpp = k;
     c->pair_block = block;
     c->tile_cap = tile_cap;
     return MFA_OK;
@@ -498,7 +584,9 @@ int launch_pair(mfa_ctx* c, int fuse_wall, int accumulate) {
     a.rule = c->bin_type;
     a.wy = c->bin_type == 0 ? p.delta_bin[1] + 2 : 3;
     a.nseg = a.wy * (c->bin_type == 0 ? p.delta_bin[2] + 2 : 3);
-    a.tile_cap = c->tile_cap;
+    // untiled: capacity 0, every block reads its neighbourhood from global memory
+    const int cap = c->pair_tiled ? c->tile_cap : 0;
+    a.tile_cap = cap;
     a.symmetry = p.symmetry; a.thermostat = p.thermostat; a.dpd_weight = p.dpd_weight;
     a.noise = p.noise; a.charged = p.charged;
     a.real_in_lj = (p.quirks & MFA_Q_EWALD_REAL_IN_LJ) != 0;
@@ -519,8 +607,8 @@ int launch_pair(mfa_ctx* c, int fuse_wall, int accumulate) {
     a.seed0 = (uint32_t)p.seed; a.seed1 = (uint32_t)(p.seed >> 32);
     const int grid = c->nb[1] * c->nb[2];
     if (grid > c->max_blocks) return MFA_ERR_ARGS;
-    const size_t rec = c->prec == MFA_MIXED ? sizeof(float4) : sizeof(double4);
-    const size_t smem = 2 * (size_t)c->tile_cap * rec;
+    const size_t smem = c->prec == MFA_MIXED ? smem_bytes<float>(c->pair_tpp, c->pair_block, cap)
+                                             : smem_bytes<double>(c->pair_tpp, c->pair_block, cap);
     int ft = 0;
     if (p.thermostat == MFA_THERMO_DPD) ft |= FT_DPD;
     if (p.thermostat == MFA_THERMO_LGV) ft |= FT_LGV;

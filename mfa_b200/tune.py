@@ -1,24 +1,27 @@
 """Autotuner for the launch shape of the pair kernel.
 
 The pair kernel's work per particle is set by the neighbour count, which
-varies with density and cutoff, so the best number of threads sharing one
-particle's list and the best block size are measured rather than assumed:
-each candidate runs a few hundred real time steps of the system (the state
-advances; tuning doubles as equilibration) and the fastest shape is kept.
+varies with density and cutoff, so its launch shape is measured rather than
+assumed: the number of in-range pairs a thread keeps per pass, the block size,
+and whether each block stages its neighbourhood in shared memory or reads it
+through the caches.  Each candidate runs a few hundred real time steps of the
+system (the state advances; tuning doubles as equilibration) and the fastest
+shape is kept.  Results do not depend on the shape.
 """
 from __future__ import annotations
 
 import time
 
-CANDIDATES = ((1, 128), (1, 256), (2, 128), (2, 256), (4, 128), (4, 256))
+CANDIDATES = ((4, 128, True), (8, 128, True), (4, 64, True),
+              (2, 128, False), (4, 128, False), (4, 256, False), (8, 256, False))
 
 
 def tune_pair_shape(system, steps: int = 300, candidates=CANDIDATES, repeats: int = 2) -> dict:
     """Time `steps` fused time steps per candidate (best of `repeats`), set the
     fastest shape on `system` and return {shape: seconds}."""
     timings = {}
-    for tpp, block in candidates:
-        system.set_pair_shape(tpp, block)
+    for k, block, tiled in candidates:
+        system.set_pair_shape(k, block, tiled)
         system.step(10)          # capture the graphs outside the timed window
         system.sync()
         best = float("inf")
@@ -27,7 +30,7 @@ def tune_pair_shape(system, steps: int = 300, candidates=CANDIDATES, repeats: in
             system.step(steps)
             system.sync()
             best = min(best, time.perf_counter() - t0)
-        timings[(tpp, block)] = best
-    tpp, block = min(timings, key=timings.get)
-    system.set_pair_shape(tpp, block)
+        timings[(k, block, tiled)] = best
+    k, block, tiled = min(timings, key=timings.get)
+    system.set_pair_shape(k, block, tiled)
     return timings

@@ -142,7 +142,11 @@ def test_mixed_trajectory_100_steps(name, request):
 @pytest.mark.parametrize("prec", [FP64, MIXED])
 def test_fast_path_equals_subroutine_path(name, prec, request):
     """mfa_step (fused kernels, captured graphs, device-side rebuild decision)
-    gives bit-identical states to the per-subroutine path."""
+    computes the same physics as the per-subroutine path.  The two paths run
+    different instantiations of the pair kernel (store + fused wall vs. add to
+    the force array), which the compiler may contract differently, so after 57
+    steps they agree to rounding (FP64: 1e-12 sigma; MIXED: 1e-5 sigma, FP32
+    differences amplified by the dynamics) rather than bit for bit."""
     cfg = request.getfixturevalue(name)
     g1 = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=prec)
     g2 = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=prec)
@@ -151,16 +155,36 @@ def test_fast_path_equals_subroutine_path(name, prec, request):
     for _ in range(57):
         g1.md_step()
     g2.step(57)
+    e1, e2 = g1.scalars(), g2.scalars()       # raises on a device-side error
     s1, s2 = g1.download(), g2.download()
-    assert (s1["r0"] == s2["r0"]).all() and (s1["v"] == s2["v"]).all()
-    e1, e2 = g1.scalars(), g2.scalars()
+    dr = float(np.abs(s1["r0"] - s2["r0"]).max())
+    dv = float(np.abs(s1["v"] - s2["v"]).max())
+    tol = 1e-12 if prec == FP64 else 1e-5
+    assert dr < tol and dv < 100 * tol, (dr, dv)
+    assert (s1["mic"] == s2["mic"]).all()
     # energies are reduced over different block shapes when the wall is fused
     # into the pair kernel, so they agree to rounding rather than bit for bit
-    assert e1["e_total"] == pytest.approx(e2["e_total"], rel=1e-13)
+    assert e1["e_total"] == pytest.approx(e2["e_total"], rel=1e-11 if prec == FP64 else 1e-6)
     assert e1["i_time"] == e2["i_time"] == 57
     assert e1["n_rebuilds"] == e2["n_rebuilds"]
     g1.close()
     g2.close()
+
+
+@pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg"])
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+def test_runs_are_bitwise_reproducible(name, prec, request):
+    """No atomics in any force sum: two runs of the fast path agree bit for bit."""
+    cfg = request.getfixturevalue(name)
+    out = []
+    for _ in range(2):
+        g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=prec)
+        g.init_forces()
+        g.step(123)
+        g.scalars()
+        out.append(g.download())
+        g.close()
+    assert (out[0]["r0"] == out[1]["r0"]).all() and (out[0]["v"] == out[1]["v"]).all()
 
 
 @pytest.mark.parametrize("name", ["charged_small_cfg", "charged_ref_cfg"])
