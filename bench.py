@@ -253,7 +253,7 @@ def main():
     import torch
     from mfa_b200 import _abi
     from mfa_b200.api import System
-    from mfa_b200.tune import tune_pair_shape
+    from mfa_b200.tune import autotune
 
     dist = None
     if world > 1:
@@ -275,9 +275,11 @@ def main():
         g.init_forces()
         if a.equil:
             g.step(a.equil)
-        tuned = tune_pair_shape(g)
-        g.tuned = min(tuned, key=tuned.get)
-        g.tuning = {f"{k}x{b}{'-tiled' if t else ''}": round(1e3 * s / 300, 4) for (k, b, t), s in tuned.items()}
+        tuned = autotune(g)
+        shapes = tuned["pair_shape"]
+        g.tuned = min(shapes, key=shapes.get)
+        g.tuning = {f"{k}x{b}{'-tiled' if t else ''}": round(1e3 * s / 300, 4) for (k, b, t), s in shapes.items()}
+        g.skin_tuning = {f"{s:g}": round(1e3 * v / 300, 4) for s, v in tuned["skin"].items()}
         ext = torch.cuda.ExternalStream(g.stream_ptr(), device=f"cuda:{dev}")
         # a timed iteration is `chunk` consecutive time steps (one mfa_step call:
         # fused velocity/position kernels, captured graphs); L2 is flushed
@@ -319,6 +321,7 @@ def main():
     g, ms_mixed, launches, clocks, s_mixed = timed_run(_abi.MIXED, a.steps, a.warmup)
     shape_mixed = g.tuned
     tuning_mixed = g.tuning
+    skin_mixed, nbin_mixed, skin_tuning = g.params.skin, list(g.params.n_bin), g.skin_tuning
     ms_max = ms_mixed
     if dist is not None:
         t = torch.tensor([ms_mixed], dtype=torch.float64, device=f"cuda:{dev}")
@@ -426,7 +429,8 @@ def main():
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded generator, no reference data)",
-            "config": dict(meta, beads=n, precision="mixed", dt=cfg.params.dt, skin=cfg.params.skin,
+            "config": dict(meta, beads=n, precision="mixed", dt=cfg.params.dt, skin=skin_mixed,
+                           cells=nbin_mixed, autotune_skin_ms_per_step=skin_tuning,
                            pair_shape=f"{shape_mixed[0]} kept pairs per thread x {shape_mixed[1]}-thread blocks, "
                                       f"{'tiled' if shape_mixed[2] else 'untiled'} (autotuned)",
                            autotune_ms_per_step=tuning_mixed,

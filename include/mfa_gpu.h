@@ -228,6 +228,13 @@ int mfa_read_energy_log(mfa_ctx* ctx, double* out3, int32_t max_entries, int32_t
  * autotuner (mfa_b200.tune) chooses. */
 int mfa_set_pair_shape(mfa_ctx* ctx, int32_t pairs_per_thread, int32_t block, int32_t tiled);
 
+/* Re-grids the cell list (n_bin cells per axis) and sets the Verlet skin
+ * (skin_2 derived as init_params.f90:807-808 does).  Cells must be at least as
+ * wide as the list radius wherever n_bin >= 3, or MFA_ERR_ARGS is returned.
+ * The lists are rebuilt at the next step (mfa_check_skin reports 1).  The
+ * forces do not depend on either choice; the autotuner uses it. */
+int mfa_set_cells(mfa_ctx* ctx, const int32_t* n_bin, double skin);
+
 /* ---------------- host mirrors ---------------- */
 
 int mfa_get_scalars(mfa_ctx* ctx, mfa_scalars* out);

@@ -160,6 +160,13 @@ class System:
         check(self.lib.mfa_set_pair_shape(self.ctx, int(pairs_per_thread), int(block), int(bool(tiled))),
               "mfa_set_pair_shape")
 
+    def set_cells(self, n_bin, skin: float) -> None:
+        nb = (C.c_int32 * 3)(*[int(x) for x in n_bin])
+        check(self.lib.mfa_set_cells(self.ctx, nb, float(skin)), "mfa_set_cells")
+        self.params.skin = float(skin)
+        for d in range(3):
+            self.params.n_bin[d] = int(n_bin[d])
+
     # ---- mirrors ----
     def stream_ptr(self) -> int:
         """cudaStream_t of the context (for event timing on the launching stream)."""

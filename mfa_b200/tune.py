@@ -1,19 +1,69 @@
-"""Autotuner for the launch shape of the pair kernel.
+"""Autotuner: cell size, Verlet skin and the pair kernel's launch shape.
 
-The pair kernel's work per particle is set by the neighbour count, which
-varies with density and cutoff, so its launch shape is measured rather than
-assumed: the number of in-range pairs a thread keeps per pass, the block size,
-and whether each block stages its neighbourhood in shared memory or reads it
-through the caches.  Each candidate runs a few hundred real time steps of the
-system (the state advances; tuning doubles as equilibration) and the fastest
-shape is kept.  Results do not depend on the shape.
+A larger skin lists more pairs per particle but rebuilds the lists less often;
+the pair kernel's best shape (in-range pairs a thread keeps per pass, block
+size, shared-memory tiling or not) depends on the neighbour count.  Neither
+changes the forces, so both are measured rather than assumed: each candidate
+runs a few hundred real time steps of the system (the state advances; tuning
+doubles as equilibration) and the fastest is kept.
 """
 from __future__ import annotations
 
 import time
 
+import math
+
 CANDIDATES = ((4, 128, True), (8, 128, True), (4, 64, True),
               (2, 128, False), (4, 128, False), (4, 256, False), (8, 256, False))
+SKINS = (0.2, 0.3, 0.4, 0.5, 0.6)
+
+
+def list_radius(params, skin: float) -> float:
+    """Verlet-list radius for a skin: max LJ range + skin (or the Ewald
+    real-space cutoff + skin when that is decoupled from the LJ range)."""
+    rcm = math.sqrt(max(params.range_2[k] for k in range(64)))
+    r = rcm + skin
+    if params.charged and not (params.quirks & 1):
+        r = max(r, math.sqrt(params.ewald_rc_2) + skin)
+    return r
+
+
+def cells_for(params, skin: float):
+    """Finest grid whose cells still hold the list radius (at least 1 cell)."""
+    r = list_radius(params, skin)
+    return [max(1, int(params.boundary[d] / r)) for d in range(3)]
+
+
+def _time(system, steps, repeats):
+    system.step(10)              # rebuild / capture outside the timed window
+    system.sync()
+    best = float("inf")
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        system.step(steps)
+        system.sync()
+        best = min(best, time.perf_counter() - t0)
+    return best
+
+
+def tune_cells(system, steps: int = 300, skins=SKINS, repeats: int = 2) -> dict:
+    """Try each skin with the finest valid cell grid, keep the fastest.
+    Returns {skin: seconds}."""
+    timings = {}
+    for skin in skins:
+        nb = cells_for(system.params, skin)
+        system.set_cells(nb, skin)
+        timings[skin] = _time(system, steps, repeats)
+    best = min(timings, key=timings.get)
+    system.set_cells(cells_for(system.params, best), best)
+    return timings
+
+
+def autotune(system, steps: int = 300) -> dict:
+    """Cell size and skin first, then the pair kernel's launch shape."""
+    cells = tune_cells(system, steps)
+    shape = tune_pair_shape(system, steps)
+    return {"skin": cells, "pair_shape": shape}
 
 
 def tune_pair_shape(system, steps: int = 300, candidates=CANDIDATES, repeats: int = 2) -> dict:
@@ -22,15 +72,7 @@ def tune_pair_shape(system, steps: int = 300, candidates=CANDIDATES, repeats: in
     timings = {}
     for k, block, tiled in candidates:
         system.set_pair_shape(k, block, tiled)
-        system.step(10)          # capture the graphs outside the timed window
-        system.sync()
-        best = float("inf")
-        for _ in range(repeats):
-            t0 = time.perf_counter()
-            system.step(steps)
-            system.sync()
-            best = min(best, time.perf_counter() - t0)
-        timings[(k, block, tiled)] = best
+        timings[(k, block, tiled)] = _time(system, steps, repeats)
     k, block, tiled = min(timings, key=timings.get)
     system.set_pair_shape(k, block, tiled)
     return timings

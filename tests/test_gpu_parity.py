@@ -187,6 +187,22 @@ def test_runs_are_bitwise_reproducible(name, prec, request):
     assert (out[0]["r0"] == out[1]["r0"]).all() and (out[0]["v"] == out[1]["v"]).all()
 
 
+@pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg", "charged_small_cfg"])
+def test_regridding_keeps_the_forces(name, request):
+    """mfa_set_cells (the autotuner's knob) changes cells and skin, not physics."""
+    from mfa_b200.tune import cells_for
+    cfg = request.getfixturevalue(name)
+    g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=FP64)
+    g.init_forces()
+    f0 = g.download(_abi.F)["force"]
+    for skin in (0.15, 0.55):
+        g.set_cells(cells_for(g.params, skin), skin)
+        assert g.check_skin() == 1
+        g.init_forces()
+        assert relerr(g.download(_abi.F)["force"], f0) < 1e-12
+    g.close()
+
+
 @pytest.mark.parametrize("name", ["charged_small_cfg", "charged_ref_cfg"])
 def test_ewald_kspace(name, request):
     cfg = request.getfixturevalue(name)
