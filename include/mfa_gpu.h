@@ -198,6 +198,11 @@ int mfa_zero_forces(mfa_ctx* ctx);
 /* fluid_fluid.f90:1-254 with dpd_forces (THERMOSTAT 0), lgv_forces
  * (THERMOSTAT 1) and ewald_real (charged) fused in.  Adds to force. */
 int mfa_fluid_fluid(mfa_ctx* ctx);
+/* md_main.f90:88-97 in one pass: force(:,:) = 0, fluid_fluid (with the
+ * thermostat and Ewald real space, as mfa_fluid_fluid) and, for WALL 2, the
+ * 9-3 walls of fluid_wall.f90:77-125 (WALL 3/4 as mfa_fluid_wall).  Stores
+ * force; the same kernel the time-step loop of mfa_step runs. */
+int mfa_pair_forces(mfa_ctx* ctx);
 /* fluid_wall.f90:2-204, inter_type 2, 3 or 4.  Adds to force (2,3), reflects v (3,4). */
 int mfa_fluid_wall(mfa_ctx* ctx, int32_t inter_type);
 /* intra_molec.f90:1-300: FENE bonds of grafted and melt chains.  Adds to force. */

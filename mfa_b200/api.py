@@ -95,6 +95,10 @@ class System:
     def fluid_fluid(self) -> None:
         check(self.lib.mfa_fluid_fluid(self.ctx), "fluid_fluid")
 
+    def pair_forces(self) -> None:
+        """force = 0; fluid_fluid; fluid_wall (WALL 2 fused) in one pass."""
+        check(self.lib.mfa_pair_forces(self.ctx), "pair_forces")
+
     def fluid_wall(self, inter_type: int) -> None:
         check(self.lib.mfa_fluid_wall(self.ctx, int(inter_type)), "fluid_wall")
 

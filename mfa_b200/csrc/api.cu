@@ -121,8 +121,9 @@ int rebuild_abi(mfa_ctx* c, int rule) {
 }
 
 int forces_fused(mfa_ctx* c) {
-    TRY(launch_pair(c, 1, 0));
-    if (c->p.wall == 3 || c->p.wall == 4) TRY(launch_wall(c, c->p.wall));
+    // fluid_wall is called for SYMMETRY 0 only (md_main.f90:97)
+    TRY(launch_pair(c, c->p.symmetry == 0, 0));
+    if (c->p.symmetry == 0 && (c->p.wall == 3 || c->p.wall == 4)) TRY(launch_wall(c, c->p.wall));
     const bool chains = c->p.n_chain > 0 || (c->p.n_chain_d > 0 && c->p.n_mon_d >= 2);
     if (chains) TRY(launch_bonds(c, 1, 1));
     if (c->p.charged) TRY(launch_ewald(c));
@@ -424,6 +425,15 @@ int mfa_fluid_fluid(mfa_ctx* c) {
     // fluid_fluid.f90:17 resets v_coul; the k-space part is added by ewald_k
     MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VCK, 0, 8, c->st));
     return launch_pair(c, 0, 1);
+}
+
+int mfa_pair_forces(mfa_ctx* c) {
+    if (!c) return MFA_ERR_ARGS;
+    MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VCK, 0, 8, c->st));
+    if (c->p.symmetry != 0 || c->p.wall != 2) MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VFW, 0, 8, c->st));
+    TRY(launch_pair(c, c->p.symmetry == 0, 0));
+    if (c->p.symmetry == 0 && (c->p.wall == 3 || c->p.wall == 4)) TRY(launch_wall(c, c->p.wall));
+    return MFA_OK;
 }
 
 int mfa_fluid_wall(mfa_ctx* c, int32_t inter_type) {
