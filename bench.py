@@ -152,6 +152,11 @@ class ClockSampler:
         self.gpu_id = gpu_id
         self.proc = None
         self.lines = []
+        self.window = (0.0, float("inf"))
+
+    def mark(self, begin, end):
+        """Only samples taken between these host times describe the timed region."""
+        self.window = (begin, end)
 
     def start(self):
         try:
@@ -166,7 +171,7 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
 
     def stop(self):
         if self.proc is None:
@@ -179,7 +184,13 @@ class ClockSampler:
         self.thread.join(timeout=2)
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        b, e = self.window
+        inside = [ln for ts, ln in self.lines if b <= ts <= e + 0.2]
+        if not inside and self.lines:
+            # a timed region shorter than the sampling period: the first sample after it began
+            later = [ln for ts, ln in self.lines if ts >= b]
+            inside = later[:1] if later else [self.lines[-1][1]]
+        for ln in inside:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 8:
                 continue
@@ -198,7 +209,8 @@ class ClockSampler:
 
 def pair_work(g, cfg):
     """Counts behind the algorithmic figures of one pair-kernel launch: listed
-    half-pairs, in-cutoff half-pairs and the sum of list rows."""
+    half-pairs, in-cutoff half-pairs and the sum of list rows (binning's half
+    list holds every pair once)."""
     import numpy as np
     from mfa_b200 import _abi
     p = cfg.params
@@ -216,7 +228,7 @@ def pair_work(g, cfg):
     r2 = (d * d).sum(1)
     rc2 = np.array(p.range_2[:]).reshape(8, 8)[t[ii] - 1, t[jj] - 1]
     inside = int((r2 < rc2).sum())
-    return {"listed_half_pairs": int(cnt.sum()) // 2, "incut_half_pairs": inside // 2,
+    return {"listed_half_pairs": int(cnt.sum()), "incut_half_pairs": inside,
             "list_entries": int(cnt.sum())}
 
 
@@ -285,6 +297,10 @@ def main():
         # fused velocity/position kernels, captured graphs); L2 is flushed
         # between iterations
         chunks = [a.chunk] * (steps // a.chunk) + ([steps % a.chunk] if steps % a.chunk else [])
+        # the clock sampler starts before the warm-up, so that starting
+        # nvidia-smi does not overlap the timed region
+        sampler = ClockSampler(dev)
+        sampler.start()
         for k in range(max(1, -(-warmup // a.chunk))):
             with torch.cuda.stream(ext):
                 flush.fill_(k & 0xff)
@@ -296,8 +312,7 @@ def main():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize(dev)
-        sampler = ClockSampler(dev)
-        sampler.start()
+        t_begin = time.time()
         torch.cuda.nvtx.range_push(f"timed_{'mixed' if prec == _abi.MIXED else 'fp64'}")
         for k, nst in enumerate(chunks):
             if flush_l2:
@@ -309,6 +324,7 @@ def main():
         torch.cuda.nvtx.range_pop()
         g.sync()
         torch.cuda.synchronize(dev)
+        sampler.mark(t_begin, time.time())
         clocks = sampler.stop()
         if dist is not None:
             dist.barrier()
@@ -347,9 +363,10 @@ def main():
     for k in range(reps):
         with torch.cuda.stream(ext):
             flush.fill_(k & 0xff)
+        g.zero_forces()
         p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         p0.record(ext)
-        g.pair_forces()      # the time step's own pair kernel (walls fused)
+        g.pair_forces()      # the time step's own pair kernel (walls fused), adding to force
         p1.record(ext)
         pk.append((p0, p1))
     torch.cuda.nvtx.range_pop()
@@ -373,7 +390,8 @@ def main():
     rebuild_ms = sum(x.elapsed_time(y) for x, y in rb) / len(rb)
     # algorithmic HBM bytes of one launch: each particle's sorted position and
     # velocity records (16 + 16 B), its row length (4 B), its force record
-    # read and written (16 + 16 B) and its list row (4 B per entry)
+    # read and written once by the reductions (16 + 16 B) and its list row
+    # (4 B per entry)
     pair_bytes = n * (16 + 16 + 4 + 16 + 16) + 4 * work["list_entries"]
     # algorithmic flops (canonical counts): 17 per listed half-pair, 38 (LJ) + 29 (DPD) per in-cutoff half-pair
     pair_flops = 17 * work["listed_half_pairs"] + (38 + 29) * work["incut_half_pairs"]
@@ -448,7 +466,7 @@ def main():
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded generator, no reference data)",
             "config": dict(meta, beads=n, precision="mixed", dt=cfg.params.dt, skin=skin_mixed,
                            cells=nbin_mixed, autotune_skin_ms_per_step=skin_tuning,
-                           pair_shape=f"{shape_mixed[0]} kept pairs per thread x {shape_mixed[1]}-thread blocks, "
+                           pair_shape=f"{shape_mixed[0]} list entries per thread and round x {shape_mixed[1]}-thread blocks, "
                                       f"{'tiled' if shape_mixed[2] else 'untiled'} (autotuned)",
                            autotune_ms_per_step=tuning_mixed,
                            thermostat="dpd", replicas=world,

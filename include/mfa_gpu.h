@@ -198,10 +198,12 @@ int mfa_zero_forces(mfa_ctx* ctx);
 /* fluid_fluid.f90:1-254 with dpd_forces (THERMOSTAT 0), lgv_forces
  * (THERMOSTAT 1) and ewald_real (charged) fused in.  Adds to force. */
 int mfa_fluid_fluid(mfa_ctx* ctx);
-/* md_main.f90:88-97 in one pass: force(:,:) = 0, fluid_fluid (with the
- * thermostat and Ewald real space, as mfa_fluid_fluid) and, for WALL 2, the
- * 9-3 walls of fluid_wall.f90:77-125 (WALL 3/4 as mfa_fluid_wall).  Stores
- * force; the same kernel the time-step loop of mfa_step runs. */
+/* md_main.f90:93-97 in one pass: fluid_fluid (with the thermostat and Ewald
+ * real space, as mfa_fluid_fluid) and, for SYMMETRY 0, fluid_wall(wall): the
+ * 9-3 walls of WALL 2 (fluid_wall.f90:77-125) in the same kernel, WALL 3/4 as
+ * mfa_fluid_wall.  Adds to force (after mfa_zero_forces it replaces
+ * force = 0; fluid_fluid; fluid_wall).  The kernel the time-step loop of
+ * mfa_step runs. */
 int mfa_pair_forces(mfa_ctx* ctx);
 /* fluid_wall.f90:2-204, inter_type 2, 3 or 4.  Adds to force (2,3), reflects v (3,4). */
 int mfa_fluid_wall(mfa_ctx* ctx, int32_t inter_type);
@@ -218,20 +220,26 @@ int mfa_verlet_velocities(mfa_ctx* ctx);
 
 /* Runs nsteps complete time steps (md_main.f90:69-147) on the device: fused
  * kernels, rebuild decided on the device, each step replayed as a captured
- * CUDA graph.  No host synchronisation inside. */
+ * CUDA graph.  No host synchronisation inside.  The rebuild of a captured
+ * step sits in a conditional graph node that the integrator opens when the
+ * skin check trips; with the environment variable MFA_GRAPH_CONDITIONAL=0 at
+ * mfa_init the rebuild kernels are launched every step instead and return at
+ * once when no rebuild is due (for profilers that replay graph nodes one by
+ * one, which do not handle conditional nodes). */
 int mfa_step(mfa_ctx* ctx, int32_t nsteps);
 /* Records e_total/v_total/t_fluid every `every` steps of mfa_step into a device
  * log of `capacity` entries (0 disables).  Read back with mfa_read_energy_log. */
 int mfa_set_energy_log(mfa_ctx* ctx, int32_t every, int32_t capacity);
 int mfa_read_energy_log(mfa_ctx* ctx, double* out3, int32_t max_entries, int32_t* n_out);
 
-/* Launch shape of the pair kernel: how many in-range neighbours a thread keeps
- * per pass before its warp evaluates the kept pairs together (2, 4 or 8),
- * threads per block (32..256, multiple of 32), and whether each block stages
- * its neighbourhood in shared memory (tiled = 1) or reads neighbours through
- * the cache hierarchy (tiled = 0).  Results do not depend on it; it is what the
+/* Launch shape of the pair kernel: how many list entries a thread tests per
+ * round before its warp evaluates the in-range pairs 32 at a time (1, 2 or 4),
+ * threads per block (32..256, multiple of 32), and whether each block (one
+ * cell row) stages its neighbourhood in shared memory (tiled = 1) or blocks
+ * of consecutive particles read neighbours through the cache hierarchy
+ * (tiled = 0).  The forces do not depend on it beyond rounding; it is what the
  * autotuner (mfa_b200.tune) chooses. */
-int mfa_set_pair_shape(mfa_ctx* ctx, int32_t pairs_per_thread, int32_t block, int32_t tiled);
+int mfa_set_pair_shape(mfa_ctx* ctx, int32_t entries_per_round, int32_t block, int32_t tiled);
 
 /* Re-grids the cell list (n_bin cells per axis) and sets the Verlet skin
  * (skin_2 derived as init_params.f90:807-808 does).  Cells must be at least as

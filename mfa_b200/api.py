@@ -96,7 +96,7 @@ class System:
         check(self.lib.mfa_fluid_fluid(self.ctx), "fluid_fluid")
 
     def pair_forces(self) -> None:
-        """force = 0; fluid_fluid; fluid_wall (WALL 2 fused) in one pass."""
+        """fluid_fluid and fluid_wall (WALL 2 fused) in one pass; adds to force."""
         check(self.lib.mfa_pair_forces(self.ctx), "pair_forces")
 
     def fluid_wall(self, inter_type: int) -> None:
@@ -160,8 +160,8 @@ class System:
         """nsteps time steps on the device (fused kernels, captured graphs)."""
         check(self.lib.mfa_step(self.ctx, int(nsteps)), "mfa_step")
 
-    def set_pair_shape(self, pairs_per_thread: int, block: int, tiled: bool = True) -> None:
-        check(self.lib.mfa_set_pair_shape(self.ctx, int(pairs_per_thread), int(block), int(bool(tiled))),
+    def set_pair_shape(self, entries_per_round: int, block: int, tiled: bool = True) -> None:
+        check(self.lib.mfa_set_pair_shape(self.ctx, int(entries_per_round), int(block), int(bool(tiled))),
               "mfa_set_pair_shape")
 
     def set_cells(self, n_bin, skin: float) -> None:

@@ -64,13 +64,14 @@ void invalidate_graph(mfa_ctx* c) {
 
 void free_all(mfa_ctx* c) {
     invalidate_graph(c);
-    void* ptrs[] = {c->rx, c->mx, c->type, c->mass, c->force, c->pos_s, c->vel_s, c->pos64,
+    void* ptrs[] = {c->rx, c->mx, c->type, c->mass, c->force, c->pos_s, c->vel_s, c->pos64, c->pos32,
                     c->ids, c->cell_count, c->nbr, c->nnb, c->partials, c->counters, c->dscal,
                     c->dflags, c->dstep, c->kvec, c->rho, c->rho_part, c->elog, c->elog_n, c->tabs};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->st) cudaStreamDestroy(c->st);
+    if (c->st_body) cudaStreamDestroy(c->st_body);
 }
 
 int alloc_list(mfa_ctx* c, int maxnb) {
@@ -122,7 +123,7 @@ int rebuild_abi(mfa_ctx* c, int rule) {
 
 int forces_fused(mfa_ctx* c) {
     // fluid_wall is called for SYMMETRY 0 only (md_main.f90:97)
-    TRY(launch_pair(c, c->p.symmetry == 0, 0));
+    TRY(launch_pair(c, c->p.symmetry == 0));
     if (c->p.symmetry == 0 && (c->p.wall == 3 || c->p.wall == 4)) TRY(launch_wall(c, c->p.wall));
     const bool chains = c->p.n_chain > 0 || (c->p.n_chain_d > 0 && c->p.n_mon_d >= 2);
     if (chains) TRY(launch_bonds(c, 1, 1));
@@ -136,17 +137,50 @@ constexpr int GRAPH_BODY = 10;
 // rebuild decided on the device: positions (+ skin check), rebuild if due,
 // forces, velocities.
 int launch_full_step(mfa_ctx* c) {
-    TRY(launch_vv_positions(c, 1));
+    TRY(launch_vv_positions(c, 1, 1));
     TRY(launch_rebuild(c, c->bin_type, 1));
     TRY(forces_fused(c));
     return launch_vv_velocities(c);
+}
+
+// The rebuild of a captured body step as a conditional graph node: the
+// integrator's last block sets the node's condition from the skin check, and
+// the six rebuild kernels run only when it tripped (no launches otherwise).
+int capture_vv_and_conditional_rebuild(mfa_ctx* c) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    MFA_CUDA_TRY(cudaStreamGetCaptureInfo(c->st, &cs, nullptr, &g, &deps, &nd));
+    if (cs != cudaStreamCaptureStatusActive) return MFA_ERR_STATE;
+    cudaGraphConditionalHandle h;
+    MFA_CUDA_TRY(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    TRY(launch_vv_fused(c, h));
+    MFA_CUDA_TRY(cudaStreamGetCaptureInfo(c->st, &cs, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeIf;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    MFA_CUDA_TRY(cudaGraphAddNode(&node, g, deps, nd, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    MFA_CUDA_TRY(cudaStreamBeginCaptureToGraph(c->st_body, body, nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal));
+    const int rc = launch_rebuild_on(c, c->bin_type, 0, c->st_body, 1);
+    cudaGraph_t out;
+    const cudaError_t e = cudaStreamEndCapture(c->st_body, &out);
+    if (rc != MFA_OK) return rc;
+    MFA_CUDA_TRY(e);
+    MFA_CUDA_TRY(cudaStreamUpdateCaptureDependencies(c->st, &node, 1, cudaStreamSetCaptureDependencies));
+    return MFA_OK;
 }
 
 // A body step of a run of steps: forces of step n, then velocities of n fused
 // with positions of n+1, then the rebuild of n+1 if due.
 int launch_body_step(mfa_ctx* c) {
     TRY(forces_fused(c));
-    TRY(launch_vv_fused(c));
+    if (c->capturing && c->cond_rebuild) return capture_vv_and_conditional_rebuild(c);
+    TRY(launch_vv_fused(c, 0));
     return launch_rebuild(c, c->bin_type, 1);
 }
 
@@ -176,7 +210,18 @@ int replay(mfa_ctx* c, int kind) {
         invalidate_graph(c);
         memcpy(c->graph_key, key, sizeof(key));
     }
-    if (!c->gexec[kind]) TRY(capture(c, kind));
+    if (!c->gexec[kind]) {
+        int rc = capture(c, kind);
+        if (rc != MFA_OK && c->cond_rebuild) {
+            // a runtime without conditional graph nodes: rebuild kernels that
+            // return at once when no rebuild is due
+            cudaGetLastError();
+            c->cond_rebuild = 0;
+            invalidate_graph(c);
+            rc = capture(c, kind);
+        }
+        TRY(rc);
+    }
     MFA_CUDA_TRY(cudaGraphLaunch(c->gexec[kind], c->st));
     c->launches += c->graph_kernels[kind];
     return MFA_OK;
@@ -232,6 +277,19 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
     MFA_CUDA_TRY(cudaGetDevice(&c->dev));
     c->n = n;
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) { free(c); return MFA_ERR_CUDA; }
+    if (cudaStreamCreateWithFlags(&c->st_body, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaStreamDestroy(c->st);
+        free(c);
+        return MFA_ERR_CUDA;
+    }
+    // MFA_GRAPH_CONDITIONAL=0: the captured steps launch the rebuild kernels
+    // every step and they return at once when no rebuild is due, instead of
+    // holding them in conditional graph nodes (for tools that replay graph
+    // nodes one at a time, such as kernel profilers)
+    {
+        const char* e = getenv("MFA_GRAPH_CONDITIONAL");
+        c->cond_rebuild = (e && e[0] == '0') ? 0 : 1;
+    }
     int rc = MFA_OK;
 #define A(x) do { if (rc == MFA_OK) rc = (x); } while (0)
     // FP64 state: r, v, a, r0_old (12 arrays)
@@ -255,6 +313,7 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
     A(dalloc((unsigned char**)&c->pos_s, (size_t)4 * n * esz(c)));
     A(dalloc((unsigned char**)&c->vel_s, (size_t)4 * n * esz(c)));
     A(dalloc(&c->pos64, n));
+    A(dalloc(&c->pos32, n));
     int32_t* i2 = nullptr;
     A(dalloc(&i2, (size_t)2 * n));
     if (rc == MFA_OK) { c->ids = i2; c->slot = i2 + n; }
@@ -360,12 +419,12 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
         rc = MFA_ERR_CUDA;
     if (rc == MFA_OK) rc = bonds_setup(c);
     if (rc == MFA_OK) {
-        // pair kernel: up to 4 kept pairs per lane and chunk, 128-thread blocks,
-        // a tile sized for 1.2x the mean neighbourhood of a row (grown at a
-        // rebuild if needed)
+        // pair kernel: 2 list entries per lane and round, 128-thread blocks
+        // of consecutive slots; the tile (used when tiling is switched on) is
+        // sized for 1.2x the mean neighbourhood of a row and grown at a rebuild
         const long long cap = 9LL * (6LL * n / (5LL * nrow) + 8);
-        c->pair_tiled = 1;
-        rc = pair_set_shape(c, 4, 128, (int)(cap < pair_tile_limit(c) ? cap : pair_tile_limit(c)));
+        c->pair_tiled = 0;
+        rc = pair_set_shape(c, 2, 128, (int)(cap < pair_tile_limit(c) ? cap : pair_tile_limit(c)));
     }
     if (rc != MFA_OK) { free_all(c); free(c); return rc; }
 #undef A
@@ -392,7 +451,7 @@ int mfa_set_step(mfa_ctx* c, int64_t i_time) {
 int mfa_verlet_positions(mfa_ctx* c) {
     if (!c) return MFA_ERR_ARGS;
     c->i_time += 1;
-    return launch_vv_positions(c, 0);
+    return launch_vv_positions(c, 0, 0);
 }
 
 int mfa_check_skin(mfa_ctx* c, int32_t* f_skin) {
@@ -424,14 +483,14 @@ int mfa_fluid_fluid(mfa_ctx* c) {
     if (!c) return MFA_ERR_ARGS;
     // fluid_fluid.f90:17 resets v_coul; the k-space part is added by ewald_k
     MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VCK, 0, 8, c->st));
-    return launch_pair(c, 0, 1);
+    return launch_pair(c, 0);
 }
 
 int mfa_pair_forces(mfa_ctx* c) {
     if (!c) return MFA_ERR_ARGS;
     MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VCK, 0, 8, c->st));
     if (c->p.symmetry != 0 || c->p.wall != 2) MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VFW, 0, 8, c->st));
-    TRY(launch_pair(c, c->p.symmetry == 0, 0));
+    TRY(launch_pair(c, c->p.symmetry == 0));
     if (c->p.symmetry == 0 && (c->p.wall == 3 || c->p.wall == 4)) TRY(launch_wall(c, c->p.wall));
     return MFA_OK;
 }
@@ -480,8 +539,8 @@ int mfa_step(mfa_ctx* c, int32_t nsteps) {
         c->i_time += 1;
         return MFA_OK;
     }
-    // first step: positions (+ skin check), conditional rebuild
-    TRY(launch_vv_positions(c, 1));
+    // first step: positions (+ skin check, force reset), conditional rebuild
+    TRY(launch_vv_positions(c, 1, 1));
     TRY(launch_rebuild(c, c->bin_type, 1));
     int body = nsteps - 1;
     while (body >= GRAPH_BODY) {
@@ -555,7 +614,8 @@ int mfa_get_scalars(mfa_ctx* c, mfa_scalars* o) {
     o->max_cell = f[F_MAXCELL];
     o->fene_clamped = f[F_FENE];
     o->error_bits = f[F_ERR];
-    o->kernel_launches = c->launches;
+    // kernels of rebuilds that ran inside conditional graph nodes are counted on the device
+    o->kernel_launches = c->launches + 6LL * f[F_CONDREB];
     return first_error(f[F_ERR]);
 }
 
@@ -742,21 +802,13 @@ int mfa_debug_lists(mfa_ctx* c, int32_t* cell_of, int32_t* nbr_count, int32_t* n
     MFA_CUDA_TRY(cudaMemcpy(lst.data(), c->nbr, lst.size() * 4, cudaMemcpyDeviceToHost));
     MFA_CUDA_TRY(cudaMemcpy(cs.data(), c->cell_start, cs.size() * 4, cudaMemcpyDeviceToHost));
     if (cell_of) memcpy(cell_of, co.data(), (size_t)n * 4);
-    const int nx = c->nb[0], ny = c->nb[1], nz = c->nb[2];
-    const int wy = c->bin_type == 0 ? c->p.delta_bin[1] + 2 : 3;
     for (int t = 0; t < n; ++t) {
         const int i = ids[t];
         const int m = cnt[t] < max_per ? cnt[t] : max_per;
         if (nbr_count) nbr_count[i] = cnt[t];
         if (!nbr) continue;
-        const int cy = (co[i] / nx) % ny, cz = co[i] / (nx * ny);
         for (int k = 0; k < m; ++k) {
-            // entry = (segment << 27 | offset inside that neighbouring row)
-            const int e = lst[(size_t)k * n + t];
-            const int seg = e >> 27, off = e & 0x7ffffff;
-            int ky, kz;
-            neighbour_row(c->bin_type, cy, cz, seg % wy, seg / wy, ny, nz, ky, kz);
-            const int s = cs[nx * (ky + ny * kz)] + off;
+            const int s = lst[(size_t)k * n + t];   // the partner's slot
             nbr[(size_t)i * max_per + k] = (s >= 0 && s < n) ? ids[s] + 1 : 0;
         }
     }

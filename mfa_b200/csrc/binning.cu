@@ -13,10 +13,12 @@
 //   k_build_nbr     thread per slot: scans the neighbouring cells and keeps j with
 //                   r^2 < range_2(ti,tj) + skin_2, the reference's FP64
 //                   expression evaluated without contraction (bit-exact pair set).
-// The list is full (both directions), column-major (entry k of slot t at
-// nbr[k*n + t]).  An entry is (segment << 27 | offset): segment = which of the
-// neighbouring rows (in the order the pair kernel stages them), offset = the
-// slot's position inside that row.
+// binning.f90 keeps each pair once (i < j, binning.f90:81-104); here the pair is
+// kept in the row of its lower slot (the pair kernel applies Newton's third
+// law), so the set of unordered pairs -- with the reference's repeats when a
+// cell is scanned twice -- is the reference's.  my_binning.f90 keeps both
+// directions (a full list).  Column-major (entry k of slot t at nbr[k*n + t]);
+// an entry is the partner's slot.
 #include "mfa_internal.cuh"
 
 namespace {
@@ -33,6 +35,7 @@ struct BinArgs {
     void* pos_s;
     void* vel_s;
     double4* pos64;
+    float4* pos32;             // FP32 copy of pos64 for the list builder's prefilter
     int32_t *nbr, *nnb;
     int32_t* flags;
     unsigned* counter;
@@ -42,6 +45,9 @@ struct BinArgs {
     int symmetry;
     int conditional;
     int rule;            // 0: binning.f90, 1: my_binning.f90
+    int prefilter;       // FP32 prefilter of list candidates (n_bin >= 3 on every axis)
+    float prefilter_margin;
+    int in_cond_body;    // launched from a conditional graph node: count the rebuild there
 };
 
 __device__ __forceinline__ bool skip(const BinArgs& a) {
@@ -192,17 +198,57 @@ __global__ void k_gather_sorted(BinArgs a, int with_pos64) {
         d.x = x; d.y = y; d.z = z;
         packw(d, i, ty);
         a.pos64[t] = d;
+        float4 f;
+        f.x = (float)x; f.y = (float)y; f.z = (float)z;
+        packw(f, i, ty);
+        a.pos32[t] = f;
     }
 }
 
+// The x neighbours of cell column cx, as runs of consecutive cells [x0, x1)
+// (a run breaks where the periodic wrap does, and repeats stay repeats: with
+// nx = 2 the reference visits the other cell twice).
+__device__ __forceinline__ int x_runs(const BinArgs& a, int cx, int nx, int wx, int* x0, int* x1) {
+    int nr = 0;
+    for (int ix = 0; ix < wx; ++ix) {
+        int kx;
+        if (a.rule == 0) {
+            kx = (cx - 1 + ix + nx) % nx;        // binning.f90:71-76
+        } else {
+            kx = cx + ix - 1;                    // my_binning.f90:70-72
+            if (kx < 0) kx = nx - 1;
+            if (kx == nx) kx = 0;
+        }
+        if (nr > 0 && kx == x1[nr - 1]) {
+            x1[nr - 1] = kx + 1;
+        } else {
+            x0[nr] = kx;
+            x1[nr] = kx + 1;
+            ++nr;
+        }
+    }
+    return nr;
+}
+
+// Thread per slot: the neighbouring cells are visited as runs of consecutive
+// slots (one to three per neighbouring row).  A candidate is first tested in
+// FP32 against the list radius plus a margin far above FP32 rounding; only
+// those that pass get the reference's FP64 test, so the kept set is exactly
+// the FP64 criterion's.  Grids with fewer than 3 cells on an axis (where a
+// pair's nearest image can be ambiguous in FP32) test every candidate in FP64.
 __global__ void k_build_nbr(BinArgs a, const double* __restrict__ cut2 /*T8*T8*/) {
     if (skip(a)) return;
     __shared__ double sc[T8 * T8];
-    for (int k = threadIdx.x; k < T8 * T8; k += blockDim.x) sc[k] = cut2[k];
+    __shared__ float scf[T8 * T8];
+    for (int k = threadIdx.x; k < T8 * T8; k += blockDim.x) {
+        sc[k] = cut2[k];
+        scf[k] = (float)cut2[k] + a.prefilter_margin;
+    }
     __syncthreads();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < a.n) {
         const double4 pi = a.pos64[t];
+        const float4 pf = a.pos32[t];
         const int wi = wbits(pi.w);
         const int ti = wi & 0xff, ii = wi >> 8;
         const int c = a.cell_of[ii];
@@ -212,34 +258,43 @@ __global__ void k_build_nbr(BinArgs a, const double* __restrict__ cut2 /*T8*T8*/
         const int wx = a.rule == 0 ? a.dl[0] + 2 : 3;
         const int wy = a.rule == 0 ? a.dl[1] + 2 : 3;
         const int wz = a.rule == 0 ? a.dl[2] + 2 : 3;
+        int x0[3], x1[3];
+        const int nr = x_runs(a, cx, nx, wx, x0, x1);
+        const bool pre = a.prefilter != 0;
+        const float Lx = (float)a.L[0], Ly = (float)a.L[1], Lz = (float)a.L[2];
+        const float iLx = (float)a.invL[0], iLy = (float)a.invL[1], iLz = (float)a.invL[2];
+        const int trow = (ti - 1) * T8 - 1;
         for (int iz = 0; iz < wz; ++iz)
         for (int iy = 0; iy < wy; ++iy) {
             int ky, kz;
             neighbour_row(a.rule, cy, cz, iy, iz, ny, nz, ky, kz);
-            const int seg = iz * wy + iy;
-            const int row0 = a.cell_start[nx * (ky + ny * kz)];
-            for (int ix = 0; ix < wx; ++ix) {
-                int kx;
-                if (a.rule == 0) {
-                    kx = (cx - 1 + ix + nx) % nx;        // binning.f90:71-76
-                } else {
-                    kx = cx + ix - 1;                    // my_binning.f90:70-72
-                    if (kx < 0) kx = nx - 1;
-                    if (kx == nx) kx = 0;
-                }
-                const int c2 = kx + nx * (ky + ny * kz);
-                const int s0 = a.cell_start[c2], s1 = a.cell_start[c2 + 1];
+            const int rb = nx * (ky + ny * kz);
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                if (r >= nr) break;
+                int s0 = a.cell_start[rb + x0[r]];
+                const int s1 = a.cell_start[rb + x1[r]];
+                // half list: only partners at higher slots (the lower slot owns the pair)
+                if (a.rule == 0 && s0 <= t) s0 = t + 1;
                 for (int s = s0; s < s1; ++s) {
                     if (s == t) continue;
+                    const float4 qf = a.pos32[s];
+                    const int tj = wbits(qf.w) & 0xff;
+                    if (pre) {
+                        float e0 = pf.x - qf.x, e1 = pf.y - qf.y, e2 = pf.z - qf.z;
+                        e0 = fmaf(-Lx, truncf(2.0f * e0 * iLx), e0);
+                        e1 = fmaf(-Ly, truncf(2.0f * e1 * iLy), e1);
+                        if (a.symmetry == 1) e2 = fmaf(-Lz, truncf(2.0f * e2 * iLz), e2);
+                        if (!(e0 * e0 + e1 * e1 + e2 * e2 < scf[trow + tj])) continue;
+                    }
                     const double4 pj = a.pos64[s];
-                    const int tj = wbits(pj.w) & 0xff;
                     double d0 = __dsub_rn(pi.x, pj.x), d1 = __dsub_rn(pi.y, pj.y), d2 = __dsub_rn(pi.z, pj.z);
                     d0 = mimage64(d0, a.L[0], a.invL[0]);
                     d1 = mimage64(d1, a.L[1], a.invL[1]);
                     if (a.symmetry == 1) d2 = mimage64(d2, a.L[2], a.invL[2]);
                     const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
-                    if (r2 < sc[(ti - 1) * T8 + (tj - 1)]) {
-                        if (cnt < a.maxnb) a.nbr[(size_t)cnt * a.n + t] = (seg << 27) | (s - row0);
+                    if (r2 < sc[trow + tj]) {
+                        if (cnt < a.maxnb) a.nbr[(size_t)cnt * a.n + t] = s;
                         ++cnt;
                     }
                 }
@@ -262,6 +317,7 @@ __global__ void k_build_nbr(BinArgs a, const double* __restrict__ cut2 /*T8*T8*/
         *a.counter = 0u;
         a.flags[F_SKIN] = 0;
         a.flags[F_REBUILDS] += 1;
+        if (a.in_cond_body) a.flags[F_CONDREB] += 1;
     }
 }
 
@@ -274,7 +330,7 @@ BinArgs make_args(mfa_ctx* c, int rule, int conditional) {
     a.type = c->type; a.q = c->p.charged ? c->q : nullptr;
     a.cell_count = c->cell_count; a.cell_start = c->cell_start; a.cell_cursor = c->cell_cursor;
     a.cell_of = c->cell_of; a.row_count = c->row_count; a.ids = c->ids; a.slot = c->slot;
-    a.pos_s = c->pos_s; a.vel_s = c->vel_s; a.pos64 = c->pos64;
+    a.pos_s = c->pos_s; a.vel_s = c->vel_s; a.pos64 = c->pos64; a.pos32 = c->pos32;
     a.nbr = c->nbr; a.nnb = c->nnb; a.flags = c->dflags;
     a.counter = c->counters + R_N - 1;
     a.n = c->n; a.ncell = c->ncell; a.nrow = c->nb[1] * c->nb[2]; a.maxnb = c->maxnb;
@@ -286,33 +342,46 @@ BinArgs make_args(mfa_ctx* c, int rule, int conditional) {
     a.symmetry = c->p.symmetry;
     a.conditional = conditional;
     a.rule = rule;
+    // FP32 candidate test: |r2_fp32 - r2| stays below ~1e-5 (L + 1) r_list for
+    // positions in [0, L); the margin is orders of magnitude above that
+    double lmax = 0.0, c2max = 0.0;
+    for (int d = 0; d < 3; ++d) lmax = fmax(lmax, c->p.boundary[d]);
+    for (int k = 0; k < T8 * T8; ++k) c2max = fmax(c2max, c->p.range_2[k] + c->p.skin_2);
+    a.prefilter = c->nb[0] >= 3 && c->nb[1] >= 3 && c->nb[2] >= 3;
+    a.prefilter_margin = (float)(0.01 + 1e-4 * (lmax + 1.0) * sqrt(c2max));
     return a;
 }
 
 }  // namespace
 
 int launch_rebuild(mfa_ctx* c, int rule, int conditional) {
+    return launch_rebuild_on(c, rule, conditional, c->st, 0);
+}
+
+int launch_rebuild_on(mfa_ctx* c, int rule, int conditional, cudaStream_t st, int in_cond_body) {
     if (rule == 0)
         for (int d = 0; d < 3; ++d)
             if (c->p.delta_bin[d] < -1 || c->p.delta_bin[d] > 1) return MFA_ERR_ARGS;
     BinArgs a = make_args(c, rule, conditional);
+    a.in_cond_body = in_cond_body;
     const int T = 256;
     const int nbp = (c->n + T - 1) / T;
     const int nrow = c->nb[1] * c->nb[2];
-    k_cell_assign<<<nbp, T, 0, c->st>>>(a);
-    k_scan_rows<<<(nrow + 7) / 8, 256, 0, c->st>>>(a);
-    k_cell_scatter<<<nbp, T, 0, c->st>>>(a);
-    k_cell_sort<<<(c->ncell + 127) / 128, 128, 0, c->st>>>(a);
-    if (c->prec == MFA_MIXED) k_gather_sorted<float4><<<nbp, T, 0, c->st>>>(a, 1);
-    else k_gather_sorted<double4><<<nbp, T, 0, c->st>>>(a, 1);
-    k_build_nbr<<<(c->n + 127) / 128, 128, 0, c->st>>>(a, c->tabs);
+    k_cell_assign<<<nbp, T, 0, st>>>(a);
+    k_scan_rows<<<(nrow + 7) / 8, 256, 0, st>>>(a);
+    k_cell_scatter<<<nbp, T, 0, st>>>(a);
+    k_cell_sort<<<(c->ncell + 127) / 128, 128, 0, st>>>(a);
+    if (c->prec == MFA_MIXED) k_gather_sorted<float4><<<nbp, T, 0, st>>>(a, 1);
+    else k_gather_sorted<double4><<<nbp, T, 0, st>>>(a, 1);
+    k_build_nbr<<<(c->n + 127) / 128, 128, 0, st>>>(a, c->tabs);
     MFA_CUDA_TRY(cudaGetLastError());
-    note_launch(c, 6);
+    if (!in_cond_body) note_launch(c, 6);
     return MFA_OK;
 }
 
 int launch_refresh_sorted(mfa_ctx* c) {
     BinArgs a = make_args(c, 0, 0);
+    a.in_cond_body = 0;
     const int T = 256;
     const int nbp = (c->n + T - 1) / T;
     if (c->prec == MFA_MIXED) k_gather_sorted<float4><<<nbp, T, 0, c->st>>>(a, 0);

@@ -35,6 +35,9 @@ struct VVArgs {
     double L[3];
     double dt, skin_lim;
     double va[3];
+    // conditional graph node that holds the next rebuild (0: none): the last
+    // block opens it when the skin check tripped
+    cudaGraphConditionalHandle rebuild_cond;
 };
 
 // r += dt v + (0.5 dt^2) a ; v += (0.5 dt) a   (verlet_positions.f90:153,169)
@@ -93,13 +96,19 @@ __device__ __forceinline__ void position_half(const VVArgs& a, int i, double x, 
     if (a.write_sorted) store_sorted<R4>(a, i, x, y, z, vx, vy, vz);
 }
 
+// zero_force: the fast path resets the force array here (md_main.f90:88), so
+// that the force kernels of the step only ever add to it
 template <typename R4>
-__global__ void k_vv_positions(VVArgs a, int fused_skin) {
+__global__ void k_vv_positions(VVArgs a, int fused_skin, int zero_force) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) *a.dstep += 1;
     if (i >= a.n) return;
     position_half<R4>(a, i, a.rx[i], a.ry[i], a.rz[i], a.vx[i], a.vy[i], a.vz[i],
                       a.ax[i], a.ay[i], a.az[i], fused_skin != 0);
+    if (zero_force) {
+        R4 z4; z4.x = 0; z4.y = 0; z4.z = 0; z4.w = 0;
+        ((R4*)a.force)[i] = z4;
+    }
 }
 
 __global__ void k_check_skin(VVArgs a) {
@@ -173,7 +182,8 @@ __global__ void k_vv_velocities(VVArgs a) {
 }
 
 // verlet_velocities of step n followed by verlet_positions of step n+1 in one
-// pass over the state (the skin check of n+1 fused in).
+// pass over the state (the skin check of n+1 fused in); the force array is
+// reset for the force kernels of step n+1 (md_main.f90:88).
 template <typename R4>
 __global__ void k_vv_fused(VVArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -181,13 +191,19 @@ __global__ void k_vv_fused(VVArgs a) {
     if (i < a.n) {
         double vx = a.vx[i], vy = a.vy[i], vz = a.vz[i], ax, ay, az;
         ke[0] = velocity_half<R4>(a, i, vx, vy, vz, ax, ay, az);
-        a.ax[i] = ax; a.ay[i] = ay; a.az[i] = az;
+        R4 z4; z4.x = 0; z4.y = 0; z4.z = 0; z4.w = 0;
+        ((R4*)a.force)[i] = z4;
+        // a = F/m is used at once by the position half; the stored copy of a
+        // is written by the velocity half that closes a run of steps
         position_half<R4>(a, i, a.rx[i], a.ry[i], a.rz[i], vx, vy, vz, ax, ay, az, true);
     }
     if (block_sum_commit<1>(ke, a.partials, a.max_blocks, a.counter, a.dscal + S_TKIN)) {
         if (threadIdx.x == 0) {
             finish_energies(a);
             *a.dstep += 1;  // the next step has begun
+            // every block's skin verdict is visible here (each fenced before
+            // taking its turn on the counter)
+            if (a.rebuild_cond) cudaGraphSetConditional(a.rebuild_cond, *(volatile int32_t*)&a.flags[F_SKIN] != 0);
         }
     }
 }
@@ -216,6 +232,7 @@ VVArgs make_args(mfa_ctx* c) {
     for (int d = 0; d < 3; ++d) { a.L[d] = c->p.boundary[d]; a.va[d] = c->p.va_spring_twall[d]; }
     a.dt = c->p.dt;
     a.skin_lim = (c->p.skin / 2.0) * (c->p.skin / 2.0);
+    a.rebuild_cond = 0;
     return a;
 }
 
@@ -223,11 +240,11 @@ constexpr int TPB = 256;
 
 }  // namespace
 
-int launch_vv_positions(mfa_ctx* c, int fused_skin) {
+int launch_vv_positions(mfa_ctx* c, int fused_skin, int zero_force) {
     VVArgs a = make_args(c);
     const int nb = (c->n + TPB - 1) / TPB;
-    if (c->prec == MFA_MIXED) k_vv_positions<float4><<<nb, TPB, 0, c->st>>>(a, fused_skin);
-    else k_vv_positions<double4><<<nb, TPB, 0, c->st>>>(a, fused_skin);
+    if (c->prec == MFA_MIXED) k_vv_positions<float4><<<nb, TPB, 0, c->st>>>(a, fused_skin, zero_force);
+    else k_vv_positions<double4><<<nb, TPB, 0, c->st>>>(a, fused_skin, zero_force);
     MFA_CUDA_TRY(cudaGetLastError());
     note_launch(c, 1);
     return MFA_OK;
@@ -253,8 +270,9 @@ int launch_vv_velocities(mfa_ctx* c) {
     return MFA_OK;
 }
 
-int launch_vv_fused(mfa_ctx* c) {
+int launch_vv_fused(mfa_ctx* c, cudaGraphConditionalHandle rebuild_cond) {
     VVArgs a = make_args(c);
+    a.rebuild_cond = rebuild_cond;
     const int nb = (c->n + TPB - 1) / TPB;
     if (nb > c->max_blocks) return MFA_ERR_ARGS;
     if (c->prec == MFA_MIXED) k_vv_fused<float4><<<nb, TPB, 0, c->st>>>(a);

@@ -5,7 +5,8 @@
 //   pos_s:   cell-sorted copy of positions, w = (id << 8 | type)   (float4 / double4)
 //   vel_s:   cell-sorted copy of velocities, w = charge             (float4 / double4)
 //   ids:     slot -> particle, slot: particle -> slot (counting sort by cell)
-//   nbr:     full Verlet list in slot space, column k of row t at nbr[k*n + t]
+//   nbr:     Verlet list in slot space (half list for binning, full for
+//            my_binning), column k of row t at nbr[k*n + t], entries = slots
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -41,6 +42,7 @@ enum {
     F_FENE = 6,      // FENE bonds at the clamp since init
     F_MAXROW = 7,    // largest cell row (fixed y, z) at the last rebuild
     F_MAXTILE = 8,   // largest neighbourhood of a row (records) at the last rebuild
+    F_CONDREB = 9,   // rebuilds run inside conditional graph nodes (launch accounting)
     F_NFLAG = 16
 };
 
@@ -52,6 +54,7 @@ struct mfa_ctx {
     int prec;            // MFA_FP64 / MFA_MIXED
     int dev;
     cudaStream_t st;
+    cudaStream_t st_body;               // captures the bodies of conditional graph nodes
     int n;
     // FP64 state
     double *rx, *ry, *rz, *vx, *vy, *vz, *ax, *ay, *az;
@@ -63,6 +66,7 @@ struct mfa_ctx {
     void* pos_s;                        // float4 / double4 [n]
     void* vel_s;                        // float4 / double4 [n]
     double4* pos64;                     // FP64 sorted positions for the list builder (scratch)
+    float4* pos32;                      // FP32 copy of pos64 (the builder's prefilter)
     int32_t *ids, *slot;
     // cells
     int nb[3], ncell;
@@ -102,6 +106,7 @@ struct mfa_ctx {
     cudaGraph_t graph[3];
     int graph_kernels[3];
     const void* graph_key[4];           // what the captured arguments depend on
+    int cond_rebuild;                   // rebuilds in conditional graph nodes (1) or early-exit kernels (0)
     // kernel launch accounting
     long long launches;
     long long cap_count;
@@ -119,15 +124,16 @@ struct mfa_ctx {
 
 // ---------- launchers (each file) ----------
 // integrate.cu
-int launch_vv_positions(mfa_ctx* c, int fused_skin);
+int launch_vv_positions(mfa_ctx* c, int fused_skin, int zero_force);
 int launch_check_skin(mfa_ctx* c);
 int launch_vv_velocities(mfa_ctx* c);
-int launch_vv_fused(mfa_ctx* c);
+int launch_vv_fused(mfa_ctx* c, cudaGraphConditionalHandle rebuild_cond);
 // binning.cu
 int launch_rebuild(mfa_ctx* c, int rule, int conditional);
+int launch_rebuild_on(mfa_ctx* c, int rule, int conditional, cudaStream_t st, int in_cond_body);
 int launch_refresh_sorted(mfa_ctx* c);
 // pair.cu
-int launch_pair(mfa_ctx* c, int fuse_wall, int accumulate);
+int launch_pair(mfa_ctx* c, int fuse_wall);   // adds to force
 int pair_set_shape(mfa_ctx* c, int tpp, int block, int tile_cap);
 int pair_tile_limit(const mfa_ctx* c);
 // bonds.cu
@@ -183,6 +189,34 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1
         c = o;
         k0 += W0;
         k1 += W1;
+    }
+    return c;
+}
+// The same generator with the key schedule (k0 + r W0, k1 + r W1), r = 0..9,
+// precomputed on the host and passed in the kernel parameters, so that the
+// round keys are constant-bank operands instead of per-round additions.
+struct PhiloxKeys {
+    uint32_t k[20];
+};
+inline PhiloxKeys philox_round_keys(uint32_t k0, uint32_t k1) {
+    PhiloxKeys r;
+    for (int i = 0; i < 10; ++i) {
+        r.k[2 * i] = k0 + (uint32_t)i * 0x9E3779B9u;
+        r.k[2 * i + 1] = k1 + (uint32_t)i * 0xBB67AE85u;
+    }
+    return r;
+}
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, const PhiloxKeys& key) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)M0 * c.x, p1 = (uint64_t)M1 * c.z;
+        uint4 o;
+        o.x = (uint32_t)(p1 >> 32) ^ c.y ^ key.k[2 * r];
+        o.y = (uint32_t)p1;
+        o.z = (uint32_t)(p0 >> 32) ^ c.w ^ key.k[2 * r + 1];
+        o.w = (uint32_t)p0;
+        c = o;
     }
     return c;
 }

@@ -2,23 +2,36 @@
 // (charged systems, fused into the same pass) and lgv_forces (THERMOSTAT 1),
 // plus optionally the 9-3 walls of fluid_wall.f90 in the per-particle epilogue.
 //
-// One CTA per cell row (fixed y, z).  Its neighbourhood -- the neighbouring
-// cell rows, each a contiguous run of cell-sorted records -- is staged into
-// shared memory with bulk asynchronous copies (cp.async.bulk, completion on an
-// mbarrier, bounded wait), and the Verlet-list entries (segment, offset) index
-// that tile directly.  A warp works on 32 particles of the row at a time in
-// three passes per chunk of their lists:
-//   1. each lane tests its own listed neighbours (distance only) and keeps up
-//      to K in-range ones in its slice of shared memory;
-//   2. the warp's kept pairs are laid out back to back and the lanes take them
-//      32 at a time, so the expensive pair physics (LJ, Philox noise, DPD,
-//      Ewald real) runs with every lane busy instead of once per listed pair
-//      with most lanes idle;
-//   3. each lane adds the results of its own pairs, in list order.
-// Each particle's force is summed by its own lane in a fixed order (no atomics,
-// deterministic), and the DPD noise of a pair is drawn from Philox keyed by
-// (step, min(i,j), max(i,j)) so both sides see the same random number.  If a
-// row's neighbourhood does not fit the tile, the CTA reads global memory.
+// Work unit: a warp takes 32 consecutive cell-sorted slots ("owners") and walks
+// their Verlet rows column by column, K entries per lane per round (the K
+// position gathers of a lane are in flight together):
+//   test   each lane forms d = r_i - r_j (minimum image) and r^2 for its
+//          entries; the in-range ones are appended to the warp's queue in shared
+//          memory (ballot + popc: no holes), with d, r^2, j and j's id/type;
+//   batch  whenever the queue holds 32 pairs, every lane evaluates one of them
+//          (LJ/WCA, Philox noise + DPD, Ewald real space): the expensive physics
+//          always runs with all 32 lanes busy.
+// Newton's third law: with the half list of binning.f90 (pair listed once, in
+// the row of its lower slot) the partner j receives -f through a vector
+// reduction on the force array (red.global.add.v4.f32 in MIXED), the owner's
+// share is summed in shared memory and added once per owner at the end.  With
+// the full list of my_binning.f90 only the owner side is updated, as the
+// reference does (fluid_fluid.f90:236).  The force array is only ever added
+// to; the caller zeroes it (mfa_zero_forces, or the integrator on the fast
+// path), so the summation order of a particle's force is not fixed: forces
+// agree with a fixed-order sum to rounding, not bit for bit.
+//
+// DPD noise of a pair is drawn from Philox-4x32-10 keyed by (step, min(i,j),
+// max(i,j)) (both sides would see the same number; each pair is evaluated once).
+//
+// Two launch modes (the autotuner picks):
+//   untiled  CTA = blockDim consecutive slots, neighbour records read through
+//            L1/L2;
+//   tiled    CTA = one cell row (fixed y, z); the neighbouring cell rows, merged
+//            into contiguous slot runs, are staged into shared memory with bulk
+//            asynchronous copies (cp.async.bulk, completion on an mbarrier,
+//            bounded wait) and list entries are translated into tile indices.
+//            A row whose neighbourhood does not fit the tile reads global memory.
 // R = float in MIXED mode (FP32 force math, FP64 energy/virial accumulators),
 // double in FP64 mode.
 #include "mfa_internal.cuh"
@@ -40,11 +53,11 @@ struct PairArgs {
     unsigned* counter;
     double* dscal;
     int n, max_blocks;
-    int nb[3], rule, wy, nseg, tile_cap, need_vtile;
+    int nb[3], rule, wy, nseg, tile_cap, rowmode;
+    int half;                 // 1: half list (partner gets -f), 0: full list
     int symmetry, thermostat, dpd_weight, noise, charged, real_in_lj, fsw;
-    int wall_type, wall_e_aw;
-    int accumulate, fuse_wall;
-    double coul_energy_factor;
+    int wall_type, wall_e_aw, fuse_wall;
+    double lj_energy_factor;  // 1 (half list) or 1/2 (full list: every pair seen twice)
     double L[3], invL[3];
     double sig, friction, dt;
     double r_2_min_init, r_2_min_time;
@@ -52,13 +65,15 @@ struct PairArgs {
     double sqrt_alpha, alpha_c, inv_sqrt_pi, ewald_rc_2;
     double a_wall[T8], sigma_wall[T8], a_w, z_space_wall, wall_cut;
     uint32_t seed0, seed1;
+    PhiloxKeys key;           // Philox round keys of (seed0, seed1)
 };
 
 template <typename R> struct Vec4;
 template <> struct Vec4<float> { typedef float4 T; };
 template <> struct Vec4<double> { typedef double4 T; };
 
-__device__ __forceinline__ float mimg(float d, float L, float iL) { return mimage32(d, L, iL); }
+// d - L*int(2d/L) (fluid_fluid.f90:84-88); truncf rounds toward zero like int()
+__device__ __forceinline__ float mimg(float d, float L, float iL) { return fmaf(-L, truncf(2.0f * d * iL), d); }
 __device__ __forceinline__ double mimg(double d, double L, double iL) {
     return d - L * (double)(int)(2.0 * d * iL);
 }
@@ -134,6 +149,16 @@ __device__ __forceinline__ R wall_force(const PairArgs& a, int t, R z, double& e
     return fz;
 }
 
+// force[i] += (x, y, z) by a reduction in L2 (no return value: RED, not ATOM)
+__device__ __forceinline__ void red_add(float4* f, float x, float y, float z) {
+    atomicAdd(f, make_float4(x, y, z, 0.0f));
+}
+__device__ __forceinline__ void red_add(double4* f, double x, double y, double z) {
+    double* p = (double*)f;
+    atomicAdd(p, x);
+    atomicAdd(p + 1, y);
+    atomicAdd(p + 2, z);
+}
 
 // ---- bulk-copy staging (cp.async.bulk global -> shared, mbarrier completion) ----
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -187,7 +212,6 @@ enum {
     FT_QSEP = 8,       // Ewald real space with its own cutoff
     FT_FSW = 16,       // force switch-on clamp
     FT_WALL = 32,      // 9-3 walls in the epilogue
-    FT_ACC = 64,       // add to the force array (else store)
     FT_GENERIC = 128
 };
 
@@ -201,76 +225,99 @@ __device__ __forceinline__ bool has(const PairArgs& a, int bit) {
             case FT_QSEP: return a.charged && !a.real_in_lj;
             case FT_FSW: return a.fsw != 0;
             case FT_WALL: return a.fuse_wall != 0;
-            case FT_ACC: return a.accumulate != 0;
         }
         return false;
     }
     return (FT & bit) != 0;
 }
 
-template <typename R> struct Vec3;
-template <> struct Vec3<float> { typedef float3 T; };
-template <> struct Vec3<double> { typedef double3 T; };
+// queue capacity of a warp: up to 31 pairs left over from the previous round
+// plus 32 lanes x K tested entries
+template <int K> constexpr int qcap() { return 32 * K + 32; }
 
-// K: in-range pairs a lane may keep per chunk (pass 1 capacity)
+// per-warp shared memory: queue (d, r^2), queue (j, id/type of j), owner
+// velocities, owner id/type, owner force accumulators
+template <typename R, int K>
+constexpr size_t warp_bytes() {
+    return (size_t)qcap<K>() * (sizeof(typename Vec4<R>::T) + sizeof(int2)) + 32 * sizeof(typename Vec4<R>::T) +
+           32 * sizeof(int) + 96 * sizeof(R);
+}
+
+constexpr int MAXPC = 16;   // staged slot runs (at most 9 neighbouring rows)
+
+// 48 registers in FP32 (40 resident warps per SM: one wave for ~190k
+// particles), 128 in FP64, where the doubled operands would otherwise spill
 template <typename R, int K, int FT>
-__global__ void __launch_bounds__(256, 3) k_pair(PairArgs a) {
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 2) k_pair(PairArgs a) {
     typedef typename Vec4<R>::T R4;
-    typedef typename Vec3<R>::T R3;
+    constexpr int QC = qcap<K>();
     extern __shared__ __align__(128) unsigned char smem_raw[];
     R4* tpos = (R4*)smem_raw;
     R4* tvel = tpos + a.tile_cap;
-    // per-warp work space after the two tile arrays
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    unsigned char* wbase = (unsigned char*)(tvel + a.tile_cap);
-    const size_t wbytes = 32 * sizeof(R4) * 2 + 32 * K * (sizeof(int) * 2 + sizeof(R3));
-    unsigned char* wmem = wbase + warp * wbytes;
-    R4* own_p = (R4*)wmem;                         // 32 owner positions
-    R4* own_v = own_p + 32;                        // 32 owner velocities
-    int* q1 = (int*)(own_v + 32);                  // lane-private kept entries [lane*K + j]
-    int* q2 = q1 + 32 * K;                         // kept entries back to back (owner << 24 | index)
-    R3* qres = (R3*)(q2 + 32 * K);                 // pair results, back to back
+    unsigned char* wmem = (unsigned char*)(tvel + a.tile_cap) + (size_t)warp * warp_bytes<R, K>();
+    R4* qd = (R4*)wmem;                          // QC x (dx, dy, dz, r^2)
+    R4* own_v = qd + QC;                         // 32 owner velocities (w = charge)
+    int2* qw = (int2*)(own_v + 32);              // QC x (owner << 23 | j index, id << 8 | type of j)
+    int* own_w = (int*)(qw + QC);                // 32 owner id << 8 | type
+    R* facc = (R*)(own_w + 32);                  // 3 x 32 owner force accumulators
     __shared__ R s_rc2[T8 * T8], s_eps[T8 * T8], s_sig2[T8 * T8], s_esh[T8 * T8], s_irc2[T8 * T8];
-    __shared__ int seg_start[16], seg_base[16];
-    __shared__ int s_mode;   // 1: tile in shared memory, 0: global records
+    __shared__ int pc_start[MAXPC], pc_len[MAXPC], pc_base[MAXPC];
+    __shared__ int row_r[MAXPC], row_s[MAXPC], row_l[MAXPC];
+    __shared__ int s_npc, s_mode;
     __shared__ __align__(8) uint64_t bar;
     const bool DPD = has<FT>(a, FT_DPD), LGV = has<FT>(a, FT_LGV), QLJ = has<FT>(a, FT_QLJ);
     const bool QSEP = has<FT>(a, FT_QSEP), FSW = has<FT>(a, FT_FSW), WALL = has<FT>(a, FT_WALL);
-    const bool ACC = has<FT>(a, FT_ACC);
     const bool need_v = DPD || QLJ || QSEP;
-    const int row = blockIdx.x;
     const int nx = a.nb[0], ny = a.nb[1], nz = a.nb[2];
-    // staging: lane k of warp 0 finds neighbouring row k; a warp scan places
-    // the rows back to back; every lane then issues the bulk copies of its row
-    if (warp == 0) {
-        int s0 = 0, len = 0;
-        if (lane < a.nseg) {
-            int ky, kz;
-            neighbour_row(a.rule, row % ny, row / ny, lane % a.wy, lane / a.wy, ny, nz, ky, kz);
-            const int c0 = nx * (ky + ny * kz);
-            s0 = a.cell_start[c0];
-            len = a.cell_start[c0 + nx] - s0;
-        }
-        int incl = len;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        const int total = __shfl_sync(0xffffffffu, incl, 31);
-        if (lane < a.nseg) { seg_start[lane] = s0; seg_base[lane] = incl - len; }
-        const int mode = total <= a.tile_cap ? 1 : 0;
-        if (lane == 0) {
-            s_mode = mode;
-            if (mode) {
-                mbar_init(&bar);
-                mbar_expect_tx(&bar, (uint32_t)total * (uint32_t)sizeof(R4) * (need_v ? 2u : 1u));
+    int p0, p1;
+    if (a.rowmode) {
+        const int row = blockIdx.x;
+        p0 = a.cell_start[nx * row];
+        p1 = a.cell_start[nx * row + nx];
+        // staging: the neighbouring rows (in the order the list builder scans
+        // them), merged into runs of consecutive slots, copied back to back
+        if (warp == 0) {
+            if (lane < a.nseg) {
+                int ky, kz;
+                neighbour_row(a.rule, row % ny, row / ny, lane % a.wy, lane / a.wy, ny, nz, ky, kz);
+                const int r = ky + ny * kz;
+                row_r[lane] = r;
+                row_s[lane] = a.cell_start[nx * r];
+                row_l[lane] = a.cell_start[nx * r + nx] - row_s[lane];
+            }
+            __syncwarp();
+            if (lane == 0) {
+                int npc = 0, total = 0;
+                for (int k = 0; k < a.nseg; ++k) {
+                    if (k > 0 && row_r[k] == row_r[k - 1] + 1) {
+                        pc_len[npc - 1] += row_l[k];
+                    } else {
+                        pc_start[npc] = row_s[k];
+                        pc_len[npc] = row_l[k];
+                        ++npc;
+                    }
+                }
+                for (int p = 0; p < npc; ++p) { pc_base[p] = total; total += pc_len[p]; }
+                const int mode = total <= a.tile_cap ? 1 : 0;
+                s_npc = npc;
+                s_mode = mode;
+                if (mode) {
+                    mbar_init(&bar);
+                    mbar_expect_tx(&bar, (uint32_t)total * (uint32_t)sizeof(R4) * (need_v ? 2u : 1u));
+                }
+            }
+            __syncwarp();
+            if (s_mode && lane < s_npc && pc_len[lane] > 0) {
+                const uint32_t bytes = (uint32_t)pc_len[lane] * (uint32_t)sizeof(R4);
+                bulk_g2s(tpos + pc_base[lane], (const R4*)a.pos_s + pc_start[lane], bytes, &bar);
+                if (need_v) bulk_g2s(tvel + pc_base[lane], (const R4*)a.vel_s + pc_start[lane], bytes, &bar);
             }
         }
-        __syncwarp();
-        if (mode && lane < a.nseg && len > 0) {
-            bulk_g2s(tpos + (incl - len), (const R4*)a.pos_s + s0, (uint32_t)len * sizeof(R4), &bar);
-            if (need_v) bulk_g2s(tvel + (incl - len), (const R4*)a.vel_s + s0, (uint32_t)len * sizeof(R4), &bar);
-        }
+    } else {
+        p0 = blockIdx.x * blockDim.x;
+        p1 = min(p0 + (int)blockDim.x, a.n);
+        if (threadIdx.x == 0) { s_mode = 0; s_npc = 0; }
     }
     for (int k = threadIdx.x; k < T8 * T8; k += blockDim.x) {
         s_rc2[k] = (R)a.tabs[1 * T8 * T8 + k];
@@ -281,18 +328,21 @@ __global__ void __launch_bounds__(256, 3) k_pair(PairArgs a) {
     }
     __syncthreads();
     const bool tile = s_mode != 0;
-    bool valid = true;
+    const int npc = s_npc;
+    bool ok = true;
     if (tile && !mbar_wait_bounded(&bar, 0, WAIT_LIMIT)) {
         // the copies did not complete in time: report, wait for them once more
         // (the tile must not be released while they are in flight), skip the work
         set_err(a.flags, MFA_ERR_TIMEOUT);
         mbar_wait_bounded(&bar, 0, WAIT_LIMIT);
-        valid = false;
+        ok = false;
     }
+    const bool valid = __syncthreads_and(ok) != 0;   // uniform over the CTA
     const R4* __restrict__ gpos = (const R4*)a.pos_s;
     const R4* __restrict__ gvel = (const R4*)a.vel_s;
-    const R4* spos = tile ? tpos : gpos;           // where pass 2 reads neighbour records
+    const R4* spos = tile ? tpos : gpos;           // where neighbour records are read
     const R4* svel = tile ? tvel : gvel;
+    R4* f4 = (R4*)a.force;
     const long long step = *a.dstep;
     R r2min = 0;
     if (FSW) {
@@ -303,180 +353,184 @@ __global__ void __launch_bounds__(256, 3) k_pair(PairArgs a) {
     const R Lx = (R)a.L[0], Ly = (R)a.L[1], Lz = (R)a.L[2];
     const R iLx = (R)a.invL[0], iLy = (R)a.invL[1], iLz = (R)a.invL[2];
     const R sig = (R)a.sig, gam = (R)a.friction;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    const int p0 = a.cell_start[nx * row], p1 = a.cell_start[nx * row + nx];
-    for (int base = p0 + 32 * warp; base < p1 && valid; base += 32 * nwarp) {
+    const R ewrc2 = (R)a.ewald_rc_2;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    double e_lj = 0.0, vir = 0.0, e_c = 0.0, e_w = 0.0;
+
+    // one queued pair: physics, owner share into shared memory, partner share
+    // into the force array
+    auto evaluate = [&](int q) {
+        const R4 d = qd[q];
+        const int2 w = qw[q];
+        const int ol = w.x >> 23, jx = w.x & 0x7fffff, wj = w.y;
+        const int wi = own_w[ol];
+        const int ij = ((wi & 0xff) - 1) * T8 + (wj & 0xff) - 1;
+        const R r2 = d.w;
+        R4 vq, vj;
+        if (need_v) { vq = own_v[ol]; vj = svel[jx]; }
+        R fsum = 0;
+        if (r2 < s_rc2[ij]) {
+            const R r2c = FSW ? (r2 > r2min ? r2 : r2min) : r2;
+            const R inv_r2 = rcp_(r2c);
+            const R eps = s_eps[ij];
+            const R r61 = s_sig2[ij] * inv_r2;
+            const R r6 = r61 * r61 * r61;
+            const R r12 = r6 * r6;
+            e_lj += (double)(eps * ((r12 - r6) - s_esh[ij]));
+            const R fs = eps * ((R)12 * r12 - (R)6 * r6) * inv_r2;   // force on i along d
+            fsum = fs;
+            vir += (double)(fs * r2);
+            if (DPD || QLJ) {
+                const R inv_r = rsqrt_(r2c);
+                if (DPD) {
+                    // dpd_forces.f90:273-348 with Philox noise keyed by the pair
+                    const int ii = wi >> 8, jj = wj >> 8;
+                    const uint32_t lo = (uint32_t)min(ii, jj), hi = (uint32_t)max(ii, jj);
+                    const uint4 ph = philox4x32_10(make_uint4(lo, hi, (uint32_t)step, TAG_DPD), a.key);
+                    const R g = noise1(ph.x, ph.y, a.noise, R(0));
+                    R wr, wd;
+                    if (a.dpd_weight == 1) { wr = 1; wd = 1; }
+                    else { wr = (R)1 - sqrt_(r2c * s_irc2[ij]); wd = wr * wr; }
+                    const R rd = ((vq.x - vj.x) * d.x + (vq.y - vj.y) * d.y + (vq.z - vj.z) * d.z) * inv_r;
+                    // F_i += (sig w_r g - gamma w_d (dv . rhat)) rhat, rhat = d * inv_r
+                    fsum += (sig * wr * g - gam * wd * rd) * inv_r;
+                }
+                if (QLJ) {
+                    // ewald_real.f90:411-428, inside the LJ range (reference behaviour)
+                    const R qq = vq.w * vj.w;
+                    const R r = r2c * inv_r;
+                    const R ec = erfc_((R)a.sqrt_alpha * r);
+                    e_c += (double)(qq * ec * inv_r);
+                    const R fsc = qq * (R)a.sqrt_alpha * (R)a.inv_sqrt_pi * (R)2 * exp_(-(R)a.alpha_c * r2c) * inv_r +
+                                  qq * ec * inv_r * inv_r;
+                    fsum += fsc * inv_r;
+                    vir += (double)(fsc * r2 * inv_r);
+                }
+            }
+        }
+        if (QSEP && r2 < ewrc2) {
+            const R qq = vq.w * vj.w;
+            const R ir = rsqrt_(r2);
+            const R r = r2 * ir;
+            const R ec = erfc_((R)a.sqrt_alpha * r);
+            e_c += (double)(qq * ec * ir);
+            const R fsc = qq * (R)a.sqrt_alpha * (R)a.inv_sqrt_pi * (R)2 * exp_(-(R)a.alpha_c * r2) * ir +
+                          qq * ec * ir * ir;
+            fsum += fsc * ir;
+            vir += (double)(fsc * r2 * ir);
+        }
+        const R fx = fsum * d.x, fy = fsum * d.y, fz = fsum * d.z;
+        atomicAdd(&facc[ol], fx);
+        atomicAdd(&facc[32 + ol], fy);
+        atomicAdd(&facc[64 + ol], fz);
+        if (a.half) red_add(&f4[wj >> 8], -fx, -fy, -fz);
+    };
+
+    for (int base = p0 + 32 * warp; valid && base < p1; base += 32 * nwarp) {
         const int t = base + lane;
         const bool act = t < p1;
-        R4 pi, vi;
+        R4 pi;
         int m = 0;
         if (act) {
             pi = ldg4(&gpos[t]);
-            if (need_v) vi = ldg4(&gvel[t]);
             m = a.nnb[t];
+            if (need_v || LGV) own_v[lane] = ldg4(&gvel[t]);
         } else {
-            pi.x = pi.y = pi.z = 0; pi.w = 0;
+            pi.x = pi.y = pi.z = 0;
+            pi.w = 0;
         }
-        own_p[lane] = pi;
-        if (need_v) own_v[lane] = vi;
-        const int ti = wbits(pi.w) & 0xff;
-        const int rowi = (ti > 0 ? ti - 1 : 0) * T8;
-        R fx = 0, fy = 0, fz = 0;
-        double e_lj = 0.0, vir = 0.0, e_c = 0.0;
-        int k = 0;
-        while (__any_sync(0xffffffffu, k < m)) {
-            // pass 1: distance test of this lane's next listed neighbours
-            int c = 0;
-            while (k < m && c < K) {
-                const int e = __ldg(&a.nbr[(size_t)k * a.n + t]);
-                ++k;
-                const int seg = e >> 27, off = e & 0x7ffffff;
-                const int idx = tile ? seg_base[seg] + off : seg_start[seg] + off;
-                const R4 pj = tile ? tpos[idx] : ldg4(&gpos[idx]);
-                R dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                dx = mimg(dx, Lx, iLx);
-                dy = mimg(dy, Ly, iLy);
-                if (a.symmetry == 1) dz = mimg(dz, Lz, iLz);
-                const R r2 = dx * dx + dy * dy + dz * dz;
-                const bool in_lj = r2 < s_rc2[rowi + (wbits(pj.w) & 0xff) - 1];
-                const bool in_ew = QSEP && r2 < (R)a.ewald_rc_2;
-                if (in_lj || in_ew) q1[lane * K + c++] = idx;
+        const int wi = wbits(pi.w);
+        own_w[lane] = wi;
+        facc[lane] = 0;
+        facc[32 + lane] = 0;
+        facc[64 + lane] = 0;
+        const int rowi = act ? ((wi & 0xff) - 1) * T8 - 1 : 0;
+        const int mmax = __reduce_max_sync(0xffffffffu, m);
+        int qn = 0;
+        __syncwarp();
+        for (int k0 = 0; k0 < mmax; k0 += K) {
+            int jx[K];
+            R4 pj[K];
+#pragma unroll
+            for (int u = 0; u < K; ++u) {
+                jx[u] = -1;
+                if (k0 + u < m) jx[u] = __ldg(&a.nbr[(size_t)(k0 + u) * a.n + t]);
             }
-            // lay the kept pairs out back to back (owner lane in the top bits)
-            int incl = c;
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += y;
-            }
-            const int total = __shfl_sync(0xffffffffu, incl, 31);
-            const int first = incl - c;
-            for (int j = 0; j < c; ++j) q2[first + j] = (lane << 24) | q1[lane * K + j];
-            __syncwarp();
-            // pass 2: every lane takes pairs first+lane, +32, ...
-            for (int q = lane; q < total; q += 32) {
-                const int w = q2[q];
-                const int ol = w >> 24, idx = w & 0xffffff;
-                const R4 qi = own_p[ol];
-                const R4 pj = spos[idx];
-                R dx = qi.x - pj.x, dy = qi.y - pj.y, dz = qi.z - pj.z;
-                dx = mimg(dx, Lx, iLx);
-                dy = mimg(dy, Ly, iLy);
-                if (a.symmetry == 1) dz = mimg(dz, Lz, iLz);
-                const R r2 = dx * dx + dy * dy + dz * dz;
-                const int wi = wbits(qi.w), wj = wbits(pj.w);
-                const int ij = ((wi & 0xff) - 1) * T8 + (wj & 0xff) - 1;
-                R4 vq, vj;
-                if (need_v) { vq = own_v[ol]; vj = svel[idx]; }
-                R fsum = 0;
-                if (r2 < s_rc2[ij]) {
-                    const R r2c = FSW ? (r2 > r2min ? r2 : r2min) : r2;
-                    const R inv_r2 = rcp_(r2c);
-                    const R eps = s_eps[ij];
-                    const R r61 = s_sig2[ij] * inv_r2;
-                    const R r6 = r61 * r61 * r61;
-                    const R r12 = r6 * r6;
-                    e_lj += (double)(eps * ((r12 - r6) - s_esh[ij]));
-                    const R fs = eps * ((R)12 * r12 - (R)6 * r6) * inv_r2;   // force on i along d
-                    fsum = fs;
-                    vir += (double)(fs * r2);
-                    if (DPD || QLJ) {
-                        const R inv_r = rsqrt_(r2c);
-                        if (DPD) {
-                            // dpd_forces.f90:273-348 with Philox noise keyed by the pair
-                            const int ii = wi >> 8, jj = wj >> 8;
-                            const uint32_t lo = (uint32_t)min(ii, jj), hi = (uint32_t)max(ii, jj);
-                            const uint4 ph = philox4x32_10(make_uint4(lo, hi, (uint32_t)step, TAG_DPD), a.seed0,
-                                                           a.seed1);
-                            const R g = noise1(ph.x, ph.y, a.noise, R(0));
-                            R wr, wd;
-                            if (a.dpd_weight == 1) { wr = 1; wd = 1; }
-                            else { wr = (R)1 - sqrt_(r2c * s_irc2[ij]); wd = wr * wr; }
-                            const R rd = ((vq.x - vj.x) * dx + (vq.y - vj.y) * dy + (vq.z - vj.z) * dz) * inv_r;
-                            // F_i += (sig w_r g - gamma w_d (dv . rhat)) rhat, rhat = d * inv_r
-                            fsum += (sig * wr * g - gam * wd * rd) * inv_r;
+#pragma unroll
+            for (int u = 0; u < K; ++u) {
+                if (jx[u] >= 0) {
+                    if (tile) {
+                        // list entries are slots; find the staged run holding the slot
+                        int ix = -1;
+                        for (int p = 0; p < npc; ++p) {
+                            const unsigned off = (unsigned)(jx[u] - pc_start[p]);
+                            if (off < (unsigned)pc_len[p]) { ix = pc_base[p] + (int)off; break; }
                         }
-                        if (QLJ) {
-                            // ewald_real.f90:411-428, inside the LJ range (reference behaviour)
-                            const R qq = vq.w * vj.w;
-                            const R r = r2c * inv_r;
-                            const R ec = erfc_((R)a.sqrt_alpha * r);
-                            e_c += (double)(qq * ec * inv_r);
-                            const R fsc = qq * (R)a.sqrt_alpha * (R)a.inv_sqrt_pi * (R)2 * exp_(-(R)a.alpha_c * r2c) *
-                                              inv_r + qq * ec * inv_r * inv_r;
-                            fsum += fsc * inv_r;
-                            vir += (double)(fsc * r2 * inv_r);
-                        }
+                        if (ix < 0) set_err(a.flags, MFA_ERR_STATE);
+                        jx[u] = ix;
                     }
+                    if (jx[u] >= 0) pj[u] = spos[jx[u]];
                 }
-                if (QSEP && r2 < (R)a.ewald_rc_2) {
-                    const R qq = vq.w * vj.w;
-                    const R ir = rsqrt_(r2);
-                    const R r = r2 * ir;
-                    const R ec = erfc_((R)a.sqrt_alpha * r);
-                    e_c += (double)(qq * ec * ir);
-                    const R fsc = qq * (R)a.sqrt_alpha * (R)a.inv_sqrt_pi * (R)2 * exp_(-(R)a.alpha_c * r2) * ir
-                                  + qq * ec * ir * ir;
-                    fsum += fsc * ir;
-                    vir += (double)(fsc * r2 * ir);
+            }
+#pragma unroll
+            for (int u = 0; u < K; ++u) {
+                bool keep = false;
+                R dx = 0, dy = 0, dz = 0, r2 = 0;
+                int wj = 0;
+                if (jx[u] >= 0) {
+                    dx = mimg(pi.x - pj[u].x, Lx, iLx);
+                    dy = mimg(pi.y - pj[u].y, Ly, iLy);
+                    dz = pi.z - pj[u].z;
+                    if (a.symmetry == 1) dz = mimg(dz, Lz, iLz);
+                    r2 = dx * dx + dy * dy + dz * dz;
+                    wj = wbits(pj[u].w);
+                    keep = r2 < s_rc2[rowi + (wj & 0xff)] || (QSEP && r2 < ewrc2);
                 }
-                R3 rs;
-                rs.x = fsum * dx; rs.y = fsum * dy; rs.z = fsum * dz;
-                qres[q] = rs;
+                const unsigned mask = __ballot_sync(0xffffffffu, keep);
+                if (keep) {
+                    const int pos = qn + __popc(mask & lt_mask);
+                    R4 e;
+                    e.x = dx; e.y = dy; e.z = dz; e.w = r2;
+                    qd[pos] = e;
+                    qw[pos] = make_int2((lane << 23) | jx[u], wj);
+                }
+                qn += __popc(mask);
             }
             __syncwarp();
-            // pass 3: this lane's pairs, in list order
-            for (int j = 0; j < c; ++j) {
-                const R3 rs = qres[first + j];
-                fx += rs.x; fy += rs.y; fz += rs.z;
+            while (qn >= 32) {
+                evaluate(qn - 32 + lane);
+                qn -= 32;
+                __syncwarp();
             }
-            __syncwarp();
         }
+        if (lane < qn) evaluate(lane);
+        __syncwarp();
         if (act) {
-            const int ii = wbits(pi.w) >> 8;
+            R fx = facc[lane], fy = facc[32 + lane], fz = facc[64 + lane];
+            const int ti = wi & 0xff, ii = wi >> 8;
             if (LGV) {
                 // lgv_forces.f90:377-393
                 R g[3];
                 lgv_noise3<R>((uint32_t)ii, (uint32_t)step, a, g);
                 const double mi = a.mass[ii];
                 const R sm = (R)sqrt(mi), gm = (R)(a.friction * mi);
-                if (!need_v) vi = ldg4(&gvel[t]);
+                const R4 vi = own_v[lane];
                 fx += sig * g[0] * sm - gm * vi.x;
                 fy += sig * g[1] * sm - gm * vi.y;
                 fz += sig * g[2] * sm - gm * vi.z;
             }
-            if (WALL) {
-                double ew = 0.0;
-                fz += wall_force<R>(a, ti, pi.z, ew);
-                acc[3] += ew;
-            }
-            R4* f4 = (R4*)a.force;
-            R4 o;
-            if (ACC) {
-                o = f4[ii];
-                o.x += fx; o.y += fy; o.z += fz;
-            } else {
-                o.x = fx; o.y = fy; o.z = fz; o.w = 0;
-            }
-            f4[ii] = o;
+            if (WALL) fz += wall_force<R>(a, ti, pi.z, e_w);
+            red_add(&f4[ii], fx, fy, fz);
         }
-        acc[0] += 0.5 * e_lj;   // full list: each pair seen from both sides
-        acc[1] += 0.5 * vir;
-        acc[2] += a.coul_energy_factor * e_c;
         __syncwarp();
     }
     if (WALL) {
+        double acc[4] = {a.lj_energy_factor * e_lj, a.lj_energy_factor * vir, e_c, e_w};
         block_sum_commit<4>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_VFF);
     } else {
-        double acc3[3] = {acc[0], acc[1], acc[2]};
-        block_sum_commit<3>(acc3, a.partials, a.max_blocks, a.counter, a.dscal + S_VFF);
+        double acc[3] = {a.lj_energy_factor * e_lj, a.lj_energy_factor * vir, e_c};
+        block_sum_commit<3>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_VFF);
     }
-}
-
-template <typename R, int K>
-size_t warp_space() {
-    typedef typename Vec4<R>::T R4;
-    typedef typename Vec3<R>::T R3;
-    return 32 * sizeof(R4) * 2 + 32 * K * (sizeof(int) * 2 + sizeof(R3));
 }
 
 // the feature sets the time-step fast path uses, each compiled on its own
@@ -516,16 +570,16 @@ struct Dispatch<R, K, -1> {
 template <typename R>
 size_t smem_bytes(int k, int block, int tile_cap) {
     typedef typename Vec4<R>::T R4;
-    const size_t ws = k == 2 ? warp_space<R, 2>() : (k == 4 ? warp_space<R, 4>() : warp_space<R, 8>());
+    const size_t ws = k == 1 ? warp_bytes<R, 1>() : (k == 2 ? warp_bytes<R, 2>() : warp_bytes<R, 4>());
     return 2 * (size_t)tile_cap * sizeof(R4) + (size_t)(block / 32) * ws;
 }
 
 template <typename R>
 int launch_r(int k, int ft, const PairArgs& a, int grid, int block, size_t smem, cudaStream_t st) {
     switch (k) {
+        case 1: Dispatch<R, 1, N_FT_SETS - 1>::run(ft, a, grid, block, smem, st); break;
         case 2: Dispatch<R, 2, N_FT_SETS - 1>::run(ft, a, grid, block, smem, st); break;
         case 4: Dispatch<R, 4, N_FT_SETS - 1>::run(ft, a, grid, block, smem, st); break;
-        case 8: Dispatch<R, 8, N_FT_SETS - 1>::run(ft, a, grid, block, smem, st); break;
         default: return MFA_ERR_ARGS;
     }
     return MFA_OK;
@@ -534,9 +588,9 @@ int launch_r(int k, int ft, const PairArgs& a, int grid, int block, size_t smem,
 template <typename R>
 int attr_r(int k, size_t smem) {
     switch (k) {
+        case 1: return Dispatch<R, 1, N_FT_SETS - 1>::attr(smem);
         case 2: return Dispatch<R, 2, N_FT_SETS - 1>::attr(smem);
         case 4: return Dispatch<R, 4, N_FT_SETS - 1>::attr(smem);
-        case 8: return Dispatch<R, 8, N_FT_SETS - 1>::attr(smem);
     }
     return MFA_ERR_ARGS;
 }
@@ -549,12 +603,12 @@ constexpr size_t SMEM_LIMIT = 200 * 1024;   // dynamic shared memory per CTA
 // of the largest launch shape.
 int pair_tile_limit(const mfa_ctx* c) {
     const size_t rec = c->prec == MFA_MIXED ? sizeof(float4) : sizeof(double4);
-    const size_t ws = c->prec == MFA_MIXED ? smem_bytes<float>(8, 256, 0) : smem_bytes<double>(8, 256, 0);
+    const size_t ws = c->prec == MFA_MIXED ? smem_bytes<float>(4, 256, 0) : smem_bytes<double>(4, 256, 0);
     return (int)((SMEM_LIMIT - ws) / (2 * rec));
 }
 
 int pair_set_shape(mfa_ctx* c, int k, int block, int tile_cap) {
-    if (k != 2 && k != 4 && k != 8) return MFA_ERR_ARGS;
+    if (k != 1 && k != 2 && k != 4) return MFA_ERR_ARGS;
     if (block < 32 || block > 256 || block % 32) return MFA_ERR_ARGS;
     if (tile_cap < 0) tile_cap = 0;
     if (tile_cap > pair_tile_limit(c)) tile_cap = pair_tile_limit(c);
@@ -568,7 +622,7 @@ int pair_set_shape(mfa_ctx* c, int k, int block, int tile_cap) {
     return MFA_OK;
 }
 
-int launch_pair(mfa_ctx* c, int fuse_wall, int accumulate) {
+int launch_pair(mfa_ctx* c, int fuse_wall) {
     if (!c->lists_valid) return MFA_ERR_STATE;
     PairArgs a;
     a.pos_s = c->pos_s; a.vel_s = c->vel_s; a.nbr = c->nbr; a.nnb = c->nnb;
@@ -584,19 +638,19 @@ int launch_pair(mfa_ctx* c, int fuse_wall, int accumulate) {
     a.rule = c->bin_type;
     a.wy = c->bin_type == 0 ? p.delta_bin[1] + 2 : 3;
     a.nseg = a.wy * (c->bin_type == 0 ? p.delta_bin[2] + 2 : 3);
-    // untiled: capacity 0, every block reads its neighbourhood from global memory
+    // untiled: capacity 0, blocks of consecutive slots read neighbours through the caches
+    a.rowmode = c->pair_tiled;
     const int cap = c->pair_tiled ? c->tile_cap : 0;
     a.tile_cap = cap;
+    // binning.f90 builds a half list (Newton 3); my_binning.f90 a full list
+    a.half = c->bin_type == 0;
+    a.lj_energy_factor = c->bin_type == 0 ? 1.0 : 0.5;
     a.symmetry = p.symmetry; a.thermostat = p.thermostat; a.dpd_weight = p.dpd_weight;
     a.noise = p.noise; a.charged = p.charged;
     a.real_in_lj = (p.quirks & MFA_Q_EWALD_REAL_IN_LJ) != 0;
     a.fsw = p.force_switch_on;
     a.wall_type = p.wall; a.wall_e_aw = (p.quirks & MFA_Q_WALL_ENERGY_AW) != 0;
     a.fuse_wall = fuse_wall && p.wall == 2;
-    a.accumulate = accumulate;
-    // ewald_real.f90:416 adds every visit; a full list (my_binning) visits each
-    // pair twice, the half list once.
-    a.coul_energy_factor = c->bin_type == 1 ? 1.0 : 0.5;
     for (int d = 0; d < 3; ++d) { a.L[d] = p.boundary[d]; a.invL[d] = c->inv_boundary[d]; }
     a.sig = p.sig; a.friction = p.friction; a.dt = p.dt;
     a.r_2_min_init = p.r_2_min_init; a.r_2_min_time = p.r_2_min_time; a.s_time = p.s_time;
@@ -605,7 +659,8 @@ int launch_pair(mfa_ctx* c, int fuse_wall, int accumulate) {
     for (int k = 0; k < T8; ++k) { a.a_wall[k] = p.a_wall[k]; a.sigma_wall[k] = p.sigma_wall[k]; }
     a.a_w = p.a_w; a.z_space_wall = p.z_space_wall; a.wall_cut = p.wall_cut;
     a.seed0 = (uint32_t)p.seed; a.seed1 = (uint32_t)(p.seed >> 32);
-    const int grid = c->nb[1] * c->nb[2];
+    a.key = philox_round_keys(a.seed0, a.seed1);
+    const int grid = c->pair_tiled ? c->nb[1] * c->nb[2] : (c->n + c->pair_block - 1) / c->pair_block;
     if (grid > c->max_blocks) return MFA_ERR_ARGS;
     const size_t smem = c->prec == MFA_MIXED ? smem_bytes<float>(c->pair_tpp, c->pair_block, cap)
                                              : smem_bytes<double>(c->pair_tpp, c->pair_block, cap);
@@ -615,7 +670,6 @@ int launch_pair(mfa_ctx* c, int fuse_wall, int accumulate) {
     if (p.charged) ft |= a.real_in_lj ? FT_QLJ : FT_QSEP;
     if (p.force_switch_on) ft |= FT_FSW;
     if (a.fuse_wall) ft |= FT_WALL;
-    if (accumulate) ft |= FT_ACC;
     const int rc = c->prec == MFA_MIXED ? launch_r<float>(c->pair_tpp, ft, a, grid, c->pair_block, smem, c->st)
                                         : launch_r<double>(c->pair_tpp, ft, a, grid, c->pair_block, smem, c->st);
     if (rc != MFA_OK) return rc;

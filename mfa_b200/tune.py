@@ -1,7 +1,7 @@
 """Autotuner: cell size, Verlet skin and the pair kernel's launch shape.
 
 A larger skin lists more pairs per particle but rebuilds the lists less often;
-the pair kernel's best shape (in-range pairs a thread keeps per pass, block
+the pair kernel's best shape (list entries a thread tests per round, block
 size, shared-memory tiling or not) depends on the neighbour count.  Neither
 changes the forces, so both are measured rather than assumed: each candidate
 runs a few hundred real time steps of the system (the state advances; tuning
@@ -13,8 +13,8 @@ import time
 
 import math
 
-CANDIDATES = ((4, 128, True), (8, 128, True), (4, 64, True),
-              (2, 128, False), (4, 128, False), (4, 256, False), (8, 256, False))
+CANDIDATES = ((2, 128, True), (4, 64, True),
+              (1, 128, False), (2, 128, False), (4, 128, False), (2, 256, False), (4, 256, False))
 SKINS = (0.2, 0.3, 0.4, 0.5, 0.6)
 
 

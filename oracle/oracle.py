@@ -213,6 +213,17 @@ def pair_multiset_half(ff_list: np.ndarray) -> np.ndarray:
     return arr[np.lexsort((arr[:, 1], arr[:, 0]))]
 
 
+def pair_multiset_rows(counts: np.ndarray, nbr: np.ndarray) -> np.ndarray:
+    """Unordered pairs of every entry of a list given as (counts, nbr), ids
+    1-based: one (min, max) row per entry, repeats kept."""
+    n = counts.shape[0]
+    ii = np.repeat(np.arange(1, n + 1), counts)
+    mask = np.arange(nbr.shape[1])[None, :] < counts[:, None]
+    jj = nbr[mask]
+    arr = np.stack([np.minimum(ii, jj), np.maximum(ii, jj)], axis=1).astype(np.int64)
+    return arr[np.lexsort((arr[:, 1], arr[:, 0]))]
+
+
 def pair_multiset_full(counts: np.ndarray, nbr: np.ndarray) -> np.ndarray:
     """Unordered pairs of a full list (each pair in both rows); keeps i < j entries."""
     n = counts.shape[0]

@@ -15,7 +15,7 @@ from conftest import relerr
 from mfa_b200 import _abi, configs
 from mfa_b200._abi import FP64, MIXED, MfaError
 from mfa_b200.api import System
-from oracle import Oracle, pair_multiset_full, pair_multiset_half
+from oracle import Oracle, pair_multiset_full, pair_multiset_half, pair_multiset_rows
 
 pytestmark = pytest.mark.gpu
 
@@ -38,11 +38,11 @@ def test_binning_bit_exact(name, request):
     cell_o, _, ff = o.lists()
     cell_g, cnt, nbr = g.debug_lists(512)
     assert (cell_o == cell_g).all()
-    half = pair_multiset_half(ff)
-    full = pair_multiset_full(cnt, nbr)
-    assert half.shape == full.shape and (half == full).all()
-    # the full list is symmetric
-    assert cnt.sum() == 2 * half.shape[0]
+    # both are half lists: every unordered pair once (the row that holds it
+    # differs: the reference's shorter row, the lower cell slot here)
+    ref = pair_multiset_half(ff)
+    got = pair_multiset_rows(cnt, nbr)
+    assert ref.shape == got.shape and (ref == got).all()
     g.close()
 
 
@@ -73,8 +73,8 @@ def test_binning_duplicate_cell_visits():
     g.binning()
     half = pair_multiset_half(o.lists()[2])
     cnt, nbr = g.debug_lists(512)[1:]
-    full = pair_multiset_full(cnt, nbr)
-    assert half.shape == full.shape and (half == full).all()
+    got = pair_multiset_rows(cnt, nbr)
+    assert half.shape == got.shape and (half == got).all()
     assert len({tuple(x) for x in half}) < half.shape[0]   # duplicates present
     g.close()
 
@@ -143,10 +143,10 @@ def test_mixed_trajectory_100_steps(name, request):
 def test_fast_path_equals_subroutine_path(name, prec, request):
     """mfa_step (fused kernels, captured graphs, device-side rebuild decision)
     computes the same physics as the per-subroutine path.  The two paths run
-    different instantiations of the pair kernel (store + fused wall vs. add to
-    the force array), which the compiler may contract differently, so after 57
-    steps they agree to rounding (FP64: 1e-12 sigma; MIXED: 1e-5 sigma, FP32
-    differences amplified by the dynamics) rather than bit for bit."""
+    different instantiations of the pair kernel (wall fused or not), and the
+    pair kernel's reductions add into the force array in no fixed order, so
+    after 57 steps they agree to rounding (FP64: 1e-12 sigma; MIXED: 1e-4
+    sigma, FP32 differences amplified by the dynamics) rather than bit for bit."""
     cfg = request.getfixturevalue(name)
     g1 = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=prec)
     g2 = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=prec)
@@ -159,12 +159,12 @@ def test_fast_path_equals_subroutine_path(name, prec, request):
     s1, s2 = g1.download(), g2.download()
     dr = float(np.abs(s1["r0"] - s2["r0"]).max())
     dv = float(np.abs(s1["v"] - s2["v"]).max())
-    tol = 1e-12 if prec == FP64 else 1e-5
+    tol = 1e-12 if prec == FP64 else 1e-4
     assert dr < tol and dv < 100 * tol, (dr, dv)
     assert (s1["mic"] == s2["mic"]).all()
     # energies are reduced over different block shapes when the wall is fused
     # into the pair kernel, so they agree to rounding rather than bit for bit
-    assert e1["e_total"] == pytest.approx(e2["e_total"], rel=1e-11 if prec == FP64 else 1e-6)
+    assert e1["e_total"] == pytest.approx(e2["e_total"], rel=1e-11 if prec == FP64 else 1e-5)
     assert e1["i_time"] == e2["i_time"] == 57
     assert e1["n_rebuilds"] == e2["n_rebuilds"]
     g1.close()
@@ -173,18 +173,24 @@ def test_fast_path_equals_subroutine_path(name, prec, request):
 
 @pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg"])
 @pytest.mark.parametrize("prec", [FP64, MIXED])
-def test_runs_are_bitwise_reproducible(name, prec, request):
-    """No atomics in any force sum: two runs of the fast path agree bit for bit."""
+def test_runs_are_reproducible(name, prec, request):
+    """Two runs of the fast path see the same noise (Philox keyed by step and
+    pair) and the same lists; only the order in which the pair kernel's
+    reductions add into the force array differs, so after 123 steps they agree
+    to rounding amplified by the dynamics (FP64 1e-11 sigma, MIXED 1e-4 sigma)."""
     cfg = request.getfixturevalue(name)
     out = []
     for _ in range(2):
         g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=prec)
         g.init_forces()
         g.step(123)
-        g.scalars()
-        out.append(g.download())
+        s = g.scalars()
+        out.append((g.download(), s))
         g.close()
-    assert (out[0]["r0"] == out[1]["r0"]).all() and (out[0]["v"] == out[1]["v"]).all()
+    tol = 1e-11 if prec == FP64 else 1e-4
+    assert float(np.abs(out[0][0]["r0"] - out[1][0]["r0"]).max()) < tol
+    assert float(np.abs(out[0][0]["v"] - out[1][0]["v"]).max()) < 100 * tol
+    assert out[0][1]["n_rebuilds"] == out[1][1]["n_rebuilds"]
 
 
 @pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg", "charged_small_cfg"])
@@ -284,8 +290,8 @@ def test_neighbour_capacity_grows():
     g.binning()
     half = pair_multiset_half(o.lists()[2])
     cnt, nbr = g.debug_lists(512)[1:]
-    full = pair_multiset_full(cnt, nbr)
-    assert half.shape == full.shape and (half == full).all()
+    got = pair_multiset_rows(cnt, nbr)
+    assert half.shape == got.shape and (half == got).all()
     g.close()
 
 
@@ -311,8 +317,8 @@ def test_energy_log_and_dpd_temperature(melt_cfg):
 
 @pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg", "charged_small_cfg"])
 @pytest.mark.parametrize("prec", [FP64, MIXED])
-def test_pair_forces_is_zero_fluid_fluid_fluid_wall(name, prec, request):
-    """mfa_pair_forces (one pass, walls fused) = force = 0; fluid_fluid; fluid_wall."""
+def test_pair_forces_is_fluid_fluid_plus_fluid_wall(name, prec, request):
+    """mfa_pair_forces (one pass, walls fused) = fluid_fluid; fluid_wall."""
     cfg = request.getfixturevalue(name)
     g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=prec)
     g.binning()
@@ -322,6 +328,7 @@ def test_pair_forces_is_zero_fluid_fluid_fluid_wall(name, prec, request):
     if p.symmetry == 0 and p.wall in (2, 3, 4):
         g.fluid_wall(p.wall)
     f1, s1 = g.download(_abi.F)["force"], g.scalars()
+    g.zero_forces()
     g.pair_forces()
     f2, s2 = g.download(_abi.F)["force"], g.scalars()
     assert relerr(f2, f1) < (1e-13 if prec == FP64 else 1e-6)
@@ -333,15 +340,17 @@ def test_pair_forces_is_zero_fluid_fluid_fluid_wall(name, prec, request):
 @pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg", "charged_small_cfg"])
 @pytest.mark.parametrize("prec", [FP64, MIXED])
 def test_tiled_and_untiled_pair_kernels_agree(name, prec, request):
-    """The pair kernel reads neighbour records from its shared-memory tile or
-    from global memory; both read the same records in the same order, so the
-    forces agree bit for bit, and so do 40 steps of the fast path."""
+    """The pair kernel reads neighbour records from its shared-memory tile (one
+    block per cell row) or through the caches (blocks of consecutive particles);
+    the forces agree to the rounding of the reductions' order, and so do 40
+    steps of the fast path."""
     cfg = request.getfixturevalue(name)
     out = []
-    for tiled in (True, False):
+    for k, block, tiled in ((2, 128, True), (4, 64, True), (1, 128, False), (4, 256, False)):
         g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=prec)
-        g.set_pair_shape(4, 128, tiled)
+        g.set_pair_shape(k, block, tiled)
         g.binning()
+        g.zero_forces()
         g.pair_forces()
         f = g.download(_abi.F)["force"]
         g.init_forces()
@@ -349,5 +358,6 @@ def test_tiled_and_untiled_pair_kernels_agree(name, prec, request):
         g.scalars()
         out.append((f, g.download(_abi.R0)["r0"]))
         g.close()
-    assert (out[0][0] == out[1][0]).all()
-    assert (out[0][1] == out[1][1]).all()
+    for f, r in out[1:]:
+        assert relerr(f, out[0][0]) < (1e-13 if prec == FP64 else 1e-5)
+        assert float(np.abs(r - out[0][1]).max()) < (1e-12 if prec == FP64 else 1e-4)
