@@ -366,7 +366,7 @@ def main():
         g.zero_forces()
         p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         p0.record(ext)
-        g.pair_forces()      # the time step's own pair kernel (walls fused), adding to force
+        g.pair_forces()      # the time step's pair kernel (9-3 walls fused), adding to force
         p1.record(ext)
         pk.append((p0, p1))
     torch.cuda.nvtx.range_pop()
@@ -477,7 +477,7 @@ def main():
             "fp64": {"value": value_fp64, "ms_per_step": ms_fp64 / a.steps},
             "mixed_over_fp64": value / value_fp64,
             "value_l2_resident": world * n * a.steps / (ms_resident * 1e-3),
-            "roofline": {"bound": "hbm", "kernel": "k_pair (fluid_fluid + dpd_forces + walls)",
+            "roofline": {"bound": "hbm", "kernel": "k_pair (fluid_fluid + dpd_forces + 9-3 walls)",
                          "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                          "traffic": traffic, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"
                          if "hbm_gbs" in peaks else "fallback 6650 GB/s",

@@ -201,10 +201,13 @@ int mfa_fluid_fluid(mfa_ctx* ctx);
 /* md_main.f90:93-97 in one pass: fluid_fluid (with the thermostat and Ewald
  * real space, as mfa_fluid_fluid) and, for SYMMETRY 0, fluid_wall(wall): the
  * 9-3 walls of WALL 2 (fluid_wall.f90:77-125) in the same kernel, WALL 3/4 as
- * mfa_fluid_wall.  Adds to force (after mfa_zero_forces it replaces
- * force = 0; fluid_fluid; fluid_wall).  The kernel the time-step loop of
+ * mfa_fluid_wall.  Adds to force.  The pair kernel the time-step loop of
  * mfa_step runs. */
 int mfa_pair_forces(mfa_ctx* ctx);
+/* Every force of a step, md_main.f90:93-131: mfa_pair_forces, ewald_k(1) and
+ * the chains' intra_molec + bending(2) (one pass, thread per bead).  Adds to
+ * force (after mfa_zero_forces it replaces the six subroutine calls). */
+int mfa_forces(mfa_ctx* ctx);
 /* fluid_wall.f90:2-204, inter_type 2, 3 or 4.  Adds to force (2,3), reflects v (3,4). */
 int mfa_fluid_wall(mfa_ctx* ctx, int32_t inter_type);
 /* intra_molec.f90:1-300: FENE bonds of grafted and melt chains.  Adds to force. */
@@ -233,7 +236,7 @@ int mfa_set_energy_log(mfa_ctx* ctx, int32_t every, int32_t capacity);
 int mfa_read_energy_log(mfa_ctx* ctx, double* out3, int32_t max_entries, int32_t* n_out);
 
 /* Launch shape of the pair kernel: how many list entries a thread tests per
- * round before its warp evaluates the in-range pairs 32 at a time (1, 2 or 4),
+ * round before its warp evaluates the in-range pairs 32 at a time (2 or 4),
  * threads per block (32..256, multiple of 32), and whether each block (one
  * cell row) stages its neighbourhood in shared memory (tiled = 1) or blocks
  * of consecutive particles read neighbours through the cache hierarchy

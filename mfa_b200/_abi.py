@@ -113,6 +113,7 @@ SIGNATURES = {
     "mfa_zero_forces": (C.c_int, [_P]),
     "mfa_fluid_fluid": (C.c_int, [_P]),
     "mfa_pair_forces": (C.c_int, [_P]),
+    "mfa_forces": (C.c_int, [_P]),
     "mfa_fluid_wall": (C.c_int, [_P, C.c_int32]),
     "mfa_intra_molec": (C.c_int, [_P]),
     "mfa_bending": (C.c_int, [_P, C.c_int32]),

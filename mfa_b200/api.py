@@ -99,6 +99,11 @@ class System:
         """fluid_fluid and fluid_wall (WALL 2 fused) in one pass; adds to force."""
         check(self.lib.mfa_pair_forces(self.ctx), "pair_forces")
 
+    def forces(self) -> None:
+        """All forces of a step (fluid_fluid, fluid_wall, intra_molec, bending,
+        ewald_k) in the fused passes of the time-step loop; adds to force."""
+        check(self.lib.mfa_forces(self.ctx), "forces")
+
     def fluid_wall(self, inter_type: int) -> None:
         check(self.lib.mfa_fluid_wall(self.ctx, int(inter_type)), "fluid_wall")
 

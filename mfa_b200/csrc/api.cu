@@ -27,6 +27,20 @@ int dalloc(T** p, size_t count) {
 
 size_t esz(const mfa_ctx* c) { return c->prec == MFA_MIXED ? sizeof(float) : sizeof(double); }
 
+// Host -> device copy ordered on the context's stream.  The stream is created
+// non-blocking, so a copy or memset on the legacy default stream would not be
+// ordered before the context's kernels (cudaMemcpy may return before its DMA
+// lands); every upload and reset goes through the context's stream instead.
+int h2d(mfa_ctx* c, void* dst, const void* src, size_t bytes) {
+    MFA_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->st));
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));   // the host buffer may be temporary
+    return MFA_OK;
+}
+int dzero(mfa_ctx* c, void* dst, size_t bytes) {
+    MFA_CUDA_TRY(cudaMemsetAsync(dst, 0, bytes, c->st));
+    return MFA_OK;
+}
+
 int first_error(int bits) {
     for (int s = 1; s < 31; ++s)
         if (bits & (1 << s)) return s;
@@ -103,8 +117,8 @@ int rebuild_abi(mfa_ctx* c, int rule) {
             invalidate_graph(c);
             int32_t zero[2] = {0, 0};
             const int32_t clear = bits & ~(1 << MFA_ERR_NEIGH_OVERFLOW);
-            MFA_CUDA_TRY(cudaMemcpy(c->dflags + F_ERR, &clear, sizeof(int32_t), cudaMemcpyHostToDevice));
-            MFA_CUDA_TRY(cudaMemcpy(c->dflags + F_NEEDNB, zero, sizeof(int32_t), cudaMemcpyHostToDevice));
+            TRY(h2d(c, c->dflags + F_ERR, &clear, sizeof(int32_t)));
+            TRY(h2d(c, c->dflags + F_NEEDNB, zero, sizeof(int32_t)));
             continue;
         }
         // size the pair kernel's shared-memory tile for the largest row seen
@@ -121,12 +135,15 @@ int rebuild_abi(mfa_ctx* c, int rule) {
     return MFA_ERR_NEIGH_OVERFLOW;
 }
 
+// The non-bonded forces of a step (md_main.f90:93-97, 129) in the fewest
+// passes: the pair kernel with the 9-3 walls (WALL 2) in its per-particle
+// epilogue, then hard walls (WALL 3/4) and Ewald k-space if used.  The chains'
+// FENE and bending forces (md_main.f90:106-111) are added bead by bead by the
+// integrator kernel that consumes the force (launch_vv_* with fuse_bonds).
 int forces_fused(mfa_ctx* c) {
     // fluid_wall is called for SYMMETRY 0 only (md_main.f90:97)
     TRY(launch_pair(c, c->p.symmetry == 0));
     if (c->p.symmetry == 0 && (c->p.wall == 3 || c->p.wall == 4)) TRY(launch_wall(c, c->p.wall));
-    const bool chains = c->p.n_chain > 0 || (c->p.n_chain_d > 0 && c->p.n_mon_d >= 2);
-    if (chains) TRY(launch_bonds(c, 1, 1));
     if (c->p.charged) TRY(launch_ewald(c));
     return MFA_OK;
 }
@@ -140,7 +157,7 @@ int launch_full_step(mfa_ctx* c) {
     TRY(launch_vv_positions(c, 1, 1));
     TRY(launch_rebuild(c, c->bin_type, 1));
     TRY(forces_fused(c));
-    return launch_vv_velocities(c);
+    return launch_vv_velocities(c, 1);
 }
 
 // The rebuild of a captured body step as a conditional graph node: the
@@ -155,7 +172,7 @@ int capture_vv_and_conditional_rebuild(mfa_ctx* c) {
     if (cs != cudaStreamCaptureStatusActive) return MFA_ERR_STATE;
     cudaGraphConditionalHandle h;
     MFA_CUDA_TRY(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
-    TRY(launch_vv_fused(c, h));
+    TRY(launch_vv_fused(c, h, 1));
     MFA_CUDA_TRY(cudaStreamGetCaptureInfo(c->st, &cs, nullptr, &g, &deps, &nd));
     cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
     np.conditional.handle = h;
@@ -180,7 +197,7 @@ int capture_vv_and_conditional_rebuild(mfa_ctx* c) {
 int launch_body_step(mfa_ctx* c) {
     TRY(forces_fused(c));
     if (c->capturing && c->cond_rebuild) return capture_vv_and_conditional_rebuild(c);
-    TRY(launch_vv_fused(c, 0));
+    TRY(launch_vv_fused(c, 0, 1));
     return launch_rebuild(c, c->bin_type, 1);
 }
 
@@ -404,19 +421,18 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
         tabs[5 * T8 * T8 + k] = p->inv_range_2[k];
     }
     rc = MFA_OK;
-    if (cudaMemcpy(d12, soa.data(), soa.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(i7, mic.data(), mic.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(c->type, a_type, (size_t)n * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(d3, m3.data(), m3.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(c->tabs, tabs.data(), tabs.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemset(c->force, 0, (size_t)4 * n * esz(c)) != cudaSuccess ||
-        cudaMemset(c->cell_count, 0, ((size_t)3 * c->ncell + 2 + n + nrow) * 4) != cudaSuccess ||
-        cudaMemset(c->nnb, 0, (size_t)n * 4) != cudaSuccess ||
-        cudaMemset(c->counters, 0, R_N * sizeof(unsigned)) != cudaSuccess ||
-        cudaMemset(c->dscal, 0, S_NSLOT * 8) != cudaSuccess ||
-        cudaMemset(c->dflags, 0, F_NFLAG * 4) != cudaSuccess ||
-        cudaMemset(c->dstep, 0, 8) != cudaSuccess)
-        rc = MFA_ERR_CUDA;
+    A(dzero(c, c->force, (size_t)4 * n * esz(c)));
+    A(dzero(c, c->cell_count, ((size_t)3 * c->ncell + 2 + n + nrow) * 4));
+    A(dzero(c, c->nnb, (size_t)n * 4));
+    A(dzero(c, c->counters, R_N * sizeof(unsigned)));
+    A(dzero(c, c->dscal, S_NSLOT * 8));
+    A(dzero(c, c->dflags, F_NFLAG * 4));
+    A(dzero(c, c->dstep, 8));
+    A(h2d(c, d12, soa.data(), soa.size() * 8));
+    A(h2d(c, i7, mic.data(), mic.size() * 4));
+    A(h2d(c, c->type, a_type, (size_t)n * 4));
+    A(h2d(c, d3, m3.data(), m3.size() * 8));
+    A(h2d(c, c->tabs, tabs.data(), tabs.size() * 8));
     if (rc == MFA_OK) rc = bonds_setup(c);
     if (rc == MFA_OK) {
         // pair kernel: 2 list entries per lane and round, 128-thread blocks
@@ -489,9 +505,21 @@ int mfa_fluid_fluid(mfa_ctx* c) {
 int mfa_pair_forces(mfa_ctx* c) {
     if (!c) return MFA_ERR_ARGS;
     MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VCK, 0, 8, c->st));
-    if (c->p.symmetry != 0 || c->p.wall != 2) MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VFW, 0, 8, c->st));
+    if (c->p.symmetry != 0 || (c->p.wall != 2 && c->p.wall != 3 && c->p.wall != 4))
+        MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VFW, 0, 8, c->st));
     TRY(launch_pair(c, c->p.symmetry == 0));
     if (c->p.symmetry == 0 && (c->p.wall == 3 || c->p.wall == 4)) TRY(launch_wall(c, c->p.wall));
+    return MFA_OK;
+}
+
+int mfa_forces(mfa_ctx* c) {
+    if (!c) return MFA_ERR_ARGS;
+    if (c->p.charged && c->nk == 0) return MFA_ERR_STATE;
+    if (c->p.symmetry != 0 || (c->p.wall != 2 && c->p.wall != 3 && c->p.wall != 4))
+        MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VFW, 0, 8, c->st));
+    TRY(forces_fused(c));
+    const bool chains = c->p.n_chain > 0 || (c->p.n_chain_d > 0 && c->p.n_mon_d >= 2);
+    if (chains) TRY(launch_bonds(c, 1, 1));
     return MFA_OK;
 }
 
@@ -526,7 +554,7 @@ int mfa_ewald_k(mfa_ctx* c, int32_t mode) {
 
 int mfa_verlet_velocities(mfa_ctx* c) {
     if (!c) return MFA_ERR_ARGS;
-    return launch_vv_velocities(c);
+    return launch_vv_velocities(c, 0);
 }
 
 int mfa_step(mfa_ctx* c, int32_t nsteps) {
@@ -553,7 +581,7 @@ int mfa_step(mfa_ctx* c, int32_t nsteps) {
     }
     // last step: forces and the velocity half
     TRY(forces_fused(c));
-    TRY(launch_vv_velocities(c));
+    TRY(launch_vv_velocities(c, 1));
     c->i_time += nsteps;
     return MFA_OK;
 }
@@ -571,7 +599,8 @@ int mfa_set_energy_log(mfa_ctx* c, int32_t every, int32_t capacity) {
     if (every == 0 || capacity == 0) return MFA_OK;
     TRY(dalloc(&c->elog, (size_t)4 * capacity));
     TRY(dalloc(&c->elog_n, 1));
-    MFA_CUDA_TRY(cudaMemset(c->elog_n, 0, 4));
+    TRY(dzero(c, c->elog_n, 4));
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
     c->elog_every = every;
     c->elog_cap = capacity;
     return MFA_OK;
@@ -647,7 +676,8 @@ int mfa_set_cells(mfa_ctx* c, const int32_t* n_bin, double skin) {
     const int nrow = n_bin[1] * n_bin[2];
     int32_t* cells = nullptr;
     TRY(dalloc(&cells, (size_t)3 * ncell + 2 + n + nrow));
-    MFA_CUDA_TRY(cudaMemset(cells, 0, ((size_t)3 * ncell + 2 + n + nrow) * 4));
+    TRY(dzero(c, cells, ((size_t)3 * ncell + 2 + n + nrow) * 4));
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
     if (nrow + 64 > c->max_blocks) {
         double* part = nullptr;
         TRY(dalloc(&part, (size_t)R_N * 4 * (nrow + 64)));
@@ -673,7 +703,7 @@ int mfa_set_cells(mfa_ctx* c, const int32_t* n_bin, double skin) {
     // list criterion table and capacity for the new radius
     double tab0[T8 * T8];
     for (int k = 0; k < T8 * T8; ++k) tab0[k] = fmax(p.range_2[k] + p.skin_2, rlist2 > rc2max + p.skin_2 ? rlist2 : 0.0);
-    MFA_CUDA_TRY(cudaMemcpy(c->tabs, tab0, sizeof(tab0), cudaMemcpyHostToDevice));
+    TRY(h2d(c, c->tabs, tab0, sizeof(tab0)));
     const double vol = p.boundary[0] * p.boundary[1] * p.boundary[2];
     int maxnb = ((int)(2.0 * 4.18879020478639 * rlist2 * rlist * n / vol) + 32 + 31) / 32 * 32;
     if (maxnb > n) maxnb = ((n + 31) / 32) * 32;
@@ -684,7 +714,7 @@ int mfa_set_cells(mfa_ctx* c, const int32_t* n_bin, double skin) {
     // and check_skin reports the rebuild as due to a subroutine-level driver
     c->lists_valid = 0;
     const int32_t one = 1;
-    MFA_CUDA_TRY(cudaMemcpy(c->dflags + F_SKIN, &one, sizeof(one), cudaMemcpyHostToDevice));
+    TRY(h2d(c, c->dflags + F_SKIN, &one, sizeof(one)));
     invalidate_graph(c);
     return MFA_OK;
 }
@@ -772,19 +802,19 @@ int mfa_upload(mfa_ctx* c, uint32_t mask, const double* r0, const double* v, con
             std::vector<float> f4((size_t)4 * n, 0.0f);
             for (int i = 0; i < n; ++i)
                 for (int d = 0; d < 3; ++d) f4[4 * i + d] = (float)force[3 * i + d];
-            MFA_CUDA_TRY(cudaMemcpy(c->force, f4.data(), f4.size() * 4, cudaMemcpyHostToDevice));
+            TRY(h2d(c, c->force, f4.data(), f4.size() * 4));
         } else {
             std::vector<double> f4((size_t)4 * n, 0.0);
             for (int i = 0; i < n; ++i)
                 for (int d = 0; d < 3; ++d) f4[4 * i + d] = force[3 * i + d];
-            MFA_CUDA_TRY(cudaMemcpy(c->force, f4.data(), f4.size() * 8, cudaMemcpyHostToDevice));
+            TRY(h2d(c, c->force, f4.data(), f4.size() * 8));
         }
     }
     if ((mask & MFA_MIC) && mic) {
         std::vector<int32_t> m((size_t)3 * n);
         for (int i = 0; i < n; ++i)
             for (int d = 0; d < 3; ++d) m[(size_t)d * n + i] = mic[3 * i + d];
-        MFA_CUDA_TRY(cudaMemcpy(c->mx, m.data(), m.size() * 4, cudaMemcpyHostToDevice));
+        TRY(h2d(c, c->mx, m.data(), m.size() * 4));
     }
     if (c->lists_valid && (mask & (MFA_R0 | MFA_V))) TRY(launch_refresh_sorted(c));
     return MFA_OK;

@@ -231,8 +231,10 @@ int ewald_setup(mfa_ctx* c) {
     c->kvec = nullptr; c->rho = nullptr; c->rho_part = nullptr;
     // kvec block: nk double4 followed by nk int4
     MFA_CUDA_TRY(cudaMalloc(&c->kvec, (size_t)c->nk * (sizeof(double4) + sizeof(int4))));
-    MFA_CUDA_TRY(cudaMemcpy(c->kvec, kv.data(), kv.size() * sizeof(double4), cudaMemcpyHostToDevice));
-    MFA_CUDA_TRY(cudaMemcpy(c->kvec + c->nk, kn.data(), kn.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    // on the context's (non-blocking) stream, so that the kernels see the table
+    MFA_CUDA_TRY(cudaMemcpyAsync(c->kvec, kv.data(), kv.size() * sizeof(double4), cudaMemcpyHostToDevice, c->st));
+    MFA_CUDA_TRY(cudaMemcpyAsync(c->kvec + c->nk, kn.data(), kn.size() * sizeof(int4), cudaMemcpyHostToDevice, c->st));
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
     int nblk = (c->n + CH - 1) / CH;
     if (nblk > 2 * 148) nblk = 2 * 148;
     if (nblk < 1) nblk = 1;

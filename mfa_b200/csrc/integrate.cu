@@ -4,6 +4,7 @@
 // round-to-nearest intrinsics so that no multiply-add is contracted and the
 // update rounds exactly like the Fortran statement order.
 #include "mfa_internal.cuh"
+#include "bonded.cuh"
 
 namespace {
 
@@ -38,6 +39,10 @@ struct VVArgs {
     // conditional graph node that holds the next rebuild (0: none): the last
     // block opens it when the skin check tripped
     cudaGraphConditionalHandle rebuild_cond;
+    // time-step fast path: the chains' FENE and bending forces are computed
+    // here, bead by bead, and added to the force before a = F/m
+    int fuse_bonds;
+    BondParams bond;
 };
 
 // r += dt v + (0.5 dt^2) a ; v += (0.5 dt) a   (verlet_positions.f90:153,169)
@@ -121,9 +126,20 @@ __global__ void k_check_skin(VVArgs a) {
 // Returns the kinetic contribution m v^2 of particle i.
 template <typename R4>
 __device__ __forceinline__ double velocity_half(const VVArgs& a, int i, double& vx, double& vy, double& vz,
-                                                double& ax, double& ay, double& az) {
+                                                double& ax, double& ay, double& az, double eb[2], int& clamped,
+                                                bool store_force) {
     R4* f = (R4*)a.force;
     R4 fi = f[i];
+    if (a.fuse_bonds) {
+        // intra_molec + bending(2) (md_main.f90:106-111) for bead i
+        typedef decltype(fi.x) R;
+        R fb[3] = {0, 0, 0};
+        bonded_on_bead<R>(a.bond, i, fb, eb[0], eb[1], clamped);
+        fi.x += fb[0];
+        fi.y += fb[1];
+        fi.z += fb[2];
+        if (store_force) f[i] = fi;
+    }
     const double im = a.inv_mass[i];
     const double hdt = 0.5 * a.dt;
     ax = __dmul_rn((double)fi.x, im);
@@ -146,9 +162,14 @@ __device__ __forceinline__ double velocity_half(const VVArgs& a, int i, double& 
 }
 
 __device__ __forceinline__ void finish_energies(const VVArgs& a) {
-    // verlet_velocities.f90:334-347 (v_wall_wall = 0, t_wall = 0)
+    // verlet_velocities.f90:334-347 (v_wall_wall = 0, t_wall = 0); the block
+    // sums arrive in S_TMP0.. (kinetic, and FENE, bending when fused)
     double* s = a.dscal;
-    s[S_TKIN] = 0.5 * s[S_TKIN];
+    s[S_TKIN] = 0.5 * s[S_TMP0];
+    if (a.fuse_bonds) {
+        s[S_VINTRA] = s[S_TMP0 + 1];
+        s[S_VBEND] = s[S_TMP0 + 2];
+    }
     s[S_VTOT] = (s[S_VFW] + s[S_VFF]) + s[S_VINTRA];
     s[S_ETOT] = s[S_VTOT] + s[S_TKIN];
     if (a.elog && a.elog_every > 0) {
@@ -166,17 +187,27 @@ __device__ __forceinline__ void finish_energies(const VVArgs& a) {
     }
 }
 
+// the FENE bonds at the clamp counted by the warp, and the block sums of
+// m v^2, FENE (times k_chain, intra_molec.f90:272,300) and bending energy
+__device__ __forceinline__ bool vv_commit(const VVArgs& a, double ke, const double eb[2], int clamped) {
+    for (int o = 16; o > 0; o >>= 1) clamped += __shfl_down_sync(0xffffffffu, clamped, o);
+    if ((threadIdx.x & 31) == 0 && clamped) atomicAdd(&a.flags[F_FENE], clamped);
+    double acc[3] = {ke, a.bond.k_chain * eb[0], eb[1]};
+    return block_sum_commit<3>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_TMP0);
+}
+
 template <typename R4>
 __global__ void k_vv_velocities(VVArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double ke[1] = {0.0};
+    double ke = 0.0, eb[2] = {0.0, 0.0};
+    int clamped = 0;
     if (i < a.n) {
         double vx = a.vx[i], vy = a.vy[i], vz = a.vz[i], ax, ay, az;
-        ke[0] = velocity_half<R4>(a, i, vx, vy, vz, ax, ay, az);
+        ke = velocity_half<R4>(a, i, vx, vy, vz, ax, ay, az, eb, clamped, true);
         a.vx[i] = vx; a.vy[i] = vy; a.vz[i] = vz;
         a.ax[i] = ax; a.ay[i] = ay; a.az[i] = az;
     }
-    if (block_sum_commit<1>(ke, a.partials, a.max_blocks, a.counter, a.dscal + S_TKIN)) {
+    if (vv_commit(a, ke, eb, clamped)) {
         if (threadIdx.x == 0) finish_energies(a);
     }
 }
@@ -187,17 +218,18 @@ __global__ void k_vv_velocities(VVArgs a) {
 template <typename R4>
 __global__ void k_vv_fused(VVArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double ke[1] = {0.0};
+    double ke = 0.0, eb[2] = {0.0, 0.0};
+    int clamped = 0;
     if (i < a.n) {
         double vx = a.vx[i], vy = a.vy[i], vz = a.vz[i], ax, ay, az;
-        ke[0] = velocity_half<R4>(a, i, vx, vy, vz, ax, ay, az);
+        ke = velocity_half<R4>(a, i, vx, vy, vz, ax, ay, az, eb, clamped, false);
         R4 z4; z4.x = 0; z4.y = 0; z4.z = 0; z4.w = 0;
         ((R4*)a.force)[i] = z4;
         // a = F/m is used at once by the position half; the stored copy of a
         // is written by the velocity half that closes a run of steps
         position_half<R4>(a, i, a.rx[i], a.ry[i], a.rz[i], vx, vy, vz, ax, ay, az, true);
     }
-    if (block_sum_commit<1>(ke, a.partials, a.max_blocks, a.counter, a.dscal + S_TKIN)) {
+    if (vv_commit(a, ke, eb, clamped)) {
         if (threadIdx.x == 0) {
             finish_energies(a);
             *a.dstep += 1;  // the next step has begun
@@ -233,10 +265,18 @@ VVArgs make_args(mfa_ctx* c) {
     a.dt = c->p.dt;
     a.skin_lim = (c->p.skin / 2.0) * (c->p.skin / 2.0);
     a.rebuild_cond = 0;
+    a.fuse_bonds = 0;
+    a.bond = bond_params(c, 0, 0);
     return a;
 }
 
 constexpr int TPB = 256;
+
+void set_bonds(const mfa_ctx* c, VVArgs& a, int fuse_bonds) {
+    const bool chains = c->p.n_chain > 0 || (c->p.n_chain_d > 0 && c->p.n_mon_d >= 2);
+    a.fuse_bonds = fuse_bonds && chains;
+    a.bond = bond_params(c, a.fuse_bonds, a.fuse_bonds);
+}
 
 }  // namespace
 
@@ -259,8 +299,9 @@ int launch_check_skin(mfa_ctx* c) {
     return MFA_OK;
 }
 
-int launch_vv_velocities(mfa_ctx* c) {
+int launch_vv_velocities(mfa_ctx* c, int fuse_bonds) {
     VVArgs a = make_args(c);
+    set_bonds(c, a, fuse_bonds);
     const int nb = (c->n + TPB - 1) / TPB;
     if (nb > c->max_blocks) return MFA_ERR_ARGS;
     if (c->prec == MFA_MIXED) k_vv_velocities<float4><<<nb, TPB, 0, c->st>>>(a);
@@ -270,9 +311,10 @@ int launch_vv_velocities(mfa_ctx* c) {
     return MFA_OK;
 }
 
-int launch_vv_fused(mfa_ctx* c, cudaGraphConditionalHandle rebuild_cond) {
+int launch_vv_fused(mfa_ctx* c, cudaGraphConditionalHandle rebuild_cond, int fuse_bonds) {
     VVArgs a = make_args(c);
     a.rebuild_cond = rebuild_cond;
+    set_bonds(c, a, fuse_bonds);
     const int nb = (c->n + TPB - 1) / TPB;
     if (nb > c->max_blocks) return MFA_ERR_ARGS;
     if (c->prec == MFA_MIXED) k_vv_fused<float4><<<nb, TPB, 0, c->st>>>(a);

@@ -117,17 +117,14 @@ struct mfa_ctx {
     int32_t* elog_n;
     // pinned host staging for uploads/downloads (3 x n doubles)
     double* h_stage;
-    // bonds launch geometry
-    int bond_warps_per_block;
-    size_t bond_smem;
 };
 
 // ---------- launchers (each file) ----------
 // integrate.cu
 int launch_vv_positions(mfa_ctx* c, int fused_skin, int zero_force);
 int launch_check_skin(mfa_ctx* c);
-int launch_vv_velocities(mfa_ctx* c);
-int launch_vv_fused(mfa_ctx* c, cudaGraphConditionalHandle rebuild_cond);
+int launch_vv_velocities(mfa_ctx* c, int fuse_bonds);
+int launch_vv_fused(mfa_ctx* c, cudaGraphConditionalHandle rebuild_cond, int fuse_bonds);
 // binning.cu
 int launch_rebuild(mfa_ctx* c, int rule, int conditional);
 int launch_rebuild_on(mfa_ctx* c, int rule, int conditional, cudaStream_t st, int in_cond_body);

@@ -32,8 +32,8 @@
 //            asynchronous copies (cp.async.bulk, completion on an mbarrier,
 //            bounded wait) and list entries are translated into tile indices.
 //            A row whose neighbourhood does not fit the tile reads global memory.
-// R = float in MIXED mode (FP32 force math, FP64 energy/virial accumulators),
-// double in FP64 mode.
+// R = float in MIXED mode (FP32 force math; each thread's energy and virial
+// terms summed in FP32, the grid-wide sums in FP64), double in FP64 mode.
 #include "mfa_internal.cuh"
 
 namespace {
@@ -66,7 +66,16 @@ struct PairArgs {
     double a_wall[T8], sigma_wall[T8], a_w, z_space_wall, wall_cut;
     uint32_t seed0, seed1;
     PhiloxKeys key;           // Philox round keys of (seed0, seed1)
+    // the same constants rounded to FP32 once on the host: the FP32 kernels
+    // take them straight from the parameter bank instead of holding converted
+    // copies in registers
+    float fL[3], fiL[3], fsig, fgam, fewrc2, fsqrt_alpha, falpha_c, finv_sqrt_pi;
 };
+
+// a run constant in the kernel's precision
+template <typename R> __device__ __forceinline__ R pv(double d, float f);
+template <> __device__ __forceinline__ float pv<float>(double, float f) { return f; }
+template <> __device__ __forceinline__ double pv<double>(double d, float) { return d; }
 
 template <typename R> struct Vec4;
 template <> struct Vec4<float> { typedef float4 T; };
@@ -133,18 +142,18 @@ __device__ __forceinline__ void lgv_noise3(uint32_t id, uint32_t step, const Pai
 }
 
 // 9-3 wall (fluid_wall.f90:96-121) on one particle: returns F_z, adds energy.
-template <typename R>
-__device__ __forceinline__ R wall_force(const PairArgs& a, int t, R z, double& e) {
+template <typename R, typename E>
+__device__ __forceinline__ R wall_force(const PairArgs& a, int t, R z, E& e) {
     R fz = 0;
     const R sw = (R)a.sigma_wall[t - 1], aw = (R)a.a_wall[t - 1];
     const R ae = a.wall_e_aw ? (R)a.a_w : aw;
     const R cut = (R)a.wall_cut;
     R f;
     double ee;
-    if (cut <= 0 || z < cut) { wall93_term<R>(z, sw, aw, ae, cut, f, ee); fz += f; e += ee; }
+    if (cut <= 0 || z < cut) { wall93_term<R>(z, sw, aw, ae, cut, f, ee); fz += f; e += (E)ee; }
     if (a.wall_type == 2) {
         const R zt = (R)a.z_space_wall - z;
-        if (cut <= 0 || zt < cut) { wall93_term<R>(zt, sw, aw, ae, cut, f, ee); fz -= f; e += ee; }
+        if (cut <= 0 || zt < cut) { wall93_term<R>(zt, sw, aw, ae, cut, f, ee); fz -= f; e += (E)ee; }
     }
     return fz;
 }
@@ -350,12 +359,22 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 2) k_pair(PairArgs a
         const double r_time = (double)(a.s_time + step - 1) * a.dt;
         r2min = r_time < a.r_2_min_time ? (R)((1.0 - r_time / a.r_2_min_time) * a.r_2_min_init) : (R)0;
     }
-    const R Lx = (R)a.L[0], Ly = (R)a.L[1], Lz = (R)a.L[2];
-    const R iLx = (R)a.invL[0], iLy = (R)a.invL[1], iLz = (R)a.invL[2];
-    const R sig = (R)a.sig, gam = (R)a.friction;
-    const R ewrc2 = (R)a.ewald_rc_2;
+#define Lx pv<R>(a.L[0], a.fL[0])
+#define Ly pv<R>(a.L[1], a.fL[1])
+#define Lz pv<R>(a.L[2], a.fL[2])
+#define iLx pv<R>(a.invL[0], a.fiL[0])
+#define iLy pv<R>(a.invL[1], a.fiL[1])
+#define iLz pv<R>(a.invL[2], a.fiL[2])
+#define sig pv<R>(a.sig, a.fsig)
+#define gam pv<R>(a.friction, a.fgam)
+#define ewrc2 pv<R>(a.ewald_rc_2, a.fewrc2)
+#define SQA pv<R>(a.sqrt_alpha, a.fsqrt_alpha)
+#define ALC pv<R>(a.alpha_c, a.falpha_c)
+#define ISP pv<R>(a.inv_sqrt_pi, a.finv_sqrt_pi)
     const unsigned lt_mask = (1u << lane) - 1u;
-    double e_lj = 0.0, vir = 0.0, e_c = 0.0, e_w = 0.0;
+    // per-thread energy sums in R (a thread sums a handful of terms), reduced
+    // over the grid in FP64
+    R e_lj = 0, vir = 0, e_c = 0, e_w = 0;
 
     // one queued pair: physics, owner share into shared memory, partner share
     // into the force array
@@ -376,10 +395,10 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 2) k_pair(PairArgs a
             const R r61 = s_sig2[ij] * inv_r2;
             const R r6 = r61 * r61 * r61;
             const R r12 = r6 * r6;
-            e_lj += (double)(eps * ((r12 - r6) - s_esh[ij]));
+            e_lj += eps * ((r12 - r6) - s_esh[ij]);
             const R fs = eps * ((R)12 * r12 - (R)6 * r6) * inv_r2;   // force on i along d
             fsum = fs;
-            vir += (double)(fs * r2);
+            vir += fs * r2;
             if (DPD || QLJ) {
                 const R inv_r = rsqrt_(r2c);
                 if (DPD) {
@@ -399,12 +418,12 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 2) k_pair(PairArgs a
                     // ewald_real.f90:411-428, inside the LJ range (reference behaviour)
                     const R qq = vq.w * vj.w;
                     const R r = r2c * inv_r;
-                    const R ec = erfc_((R)a.sqrt_alpha * r);
-                    e_c += (double)(qq * ec * inv_r);
-                    const R fsc = qq * (R)a.sqrt_alpha * (R)a.inv_sqrt_pi * (R)2 * exp_(-(R)a.alpha_c * r2c) * inv_r +
+                    const R ec = erfc_(SQA * r);
+                    e_c += qq * ec * inv_r;
+                    const R fsc = qq * SQA * ISP * (R)2 * exp_(-ALC * r2c) * inv_r +
                                   qq * ec * inv_r * inv_r;
                     fsum += fsc * inv_r;
-                    vir += (double)(fsc * r2 * inv_r);
+                    vir += fsc * r2 * inv_r;
                 }
             }
         }
@@ -412,12 +431,12 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 2) k_pair(PairArgs a
             const R qq = vq.w * vj.w;
             const R ir = rsqrt_(r2);
             const R r = r2 * ir;
-            const R ec = erfc_((R)a.sqrt_alpha * r);
-            e_c += (double)(qq * ec * ir);
-            const R fsc = qq * (R)a.sqrt_alpha * (R)a.inv_sqrt_pi * (R)2 * exp_(-(R)a.alpha_c * r2) * ir +
+            const R ec = erfc_(SQA * r);
+            e_c += qq * ec * ir;
+            const R fsc = qq * SQA * ISP * (R)2 * exp_(-ALC * r2) * ir +
                           qq * ec * ir * ir;
             fsum += fsc * ir;
-            vir += (double)(fsc * r2 * ir);
+            vir += fsc * r2 * ir;
         }
         const R fx = fsum * d.x, fy = fsum * d.y, fz = fsum * d.z;
         atomicAdd(&facc[ol], fx);
@@ -525,15 +544,29 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 2) k_pair(PairArgs a
         __syncwarp();
     }
     if (WALL) {
-        double acc[4] = {a.lj_energy_factor * e_lj, a.lj_energy_factor * vir, e_c, e_w};
+        double acc[4] = {a.lj_energy_factor * (double)e_lj, a.lj_energy_factor * (double)vir, (double)e_c,
+                         (double)e_w};
         block_sum_commit<4>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_VFF);
     } else {
-        double acc[3] = {a.lj_energy_factor * e_lj, a.lj_energy_factor * vir, e_c};
+        double acc[3] = {a.lj_energy_factor * (double)e_lj, a.lj_energy_factor * (double)vir, (double)e_c};
         block_sum_commit<3>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_VFF);
     }
 }
+#undef Lx
+#undef Ly
+#undef Lz
+#undef iLx
+#undef iLy
+#undef iLz
+#undef sig
+#undef gam
+#undef ewrc2
+#undef SQA
+#undef ALC
+#undef ISP
 
-// the feature sets the time-step fast path uses, each compiled on its own
+// the feature sets the time-step fast path and the subroutine entry points
+// use, each compiled on its own
 constexpr int FT_SETS[] = {0, FT_DPD, FT_DPD | FT_WALL, FT_WALL, FT_LGV, FT_LGV | FT_WALL, FT_LGV | FT_QSEP,
                            FT_LGV | FT_QLJ, FT_DPD | FT_QSEP, FT_DPD | FT_QLJ};
 constexpr int N_FT_SETS = sizeof(FT_SETS) / sizeof(int);
@@ -570,14 +603,13 @@ struct Dispatch<R, K, -1> {
 template <typename R>
 size_t smem_bytes(int k, int block, int tile_cap) {
     typedef typename Vec4<R>::T R4;
-    const size_t ws = k == 1 ? warp_bytes<R, 1>() : (k == 2 ? warp_bytes<R, 2>() : warp_bytes<R, 4>());
+    const size_t ws = k == 2 ? warp_bytes<R, 2>() : warp_bytes<R, 4>();
     return 2 * (size_t)tile_cap * sizeof(R4) + (size_t)(block / 32) * ws;
 }
 
 template <typename R>
 int launch_r(int k, int ft, const PairArgs& a, int grid, int block, size_t smem, cudaStream_t st) {
     switch (k) {
-        case 1: Dispatch<R, 1, N_FT_SETS - 1>::run(ft, a, grid, block, smem, st); break;
         case 2: Dispatch<R, 2, N_FT_SETS - 1>::run(ft, a, grid, block, smem, st); break;
         case 4: Dispatch<R, 4, N_FT_SETS - 1>::run(ft, a, grid, block, smem, st); break;
         default: return MFA_ERR_ARGS;
@@ -588,7 +620,6 @@ int launch_r(int k, int ft, const PairArgs& a, int grid, int block, size_t smem,
 template <typename R>
 int attr_r(int k, size_t smem) {
     switch (k) {
-        case 1: return Dispatch<R, 1, N_FT_SETS - 1>::attr(smem);
         case 2: return Dispatch<R, 2, N_FT_SETS - 1>::attr(smem);
         case 4: return Dispatch<R, 4, N_FT_SETS - 1>::attr(smem);
     }
@@ -608,7 +639,7 @@ int pair_tile_limit(const mfa_ctx* c) {
 }
 
 int pair_set_shape(mfa_ctx* c, int k, int block, int tile_cap) {
-    if (k != 1 && k != 2 && k != 4) return MFA_ERR_ARGS;
+    if (k != 2 && k != 4) return MFA_ERR_ARGS;
     if (block < 32 || block > 256 || block % 32) return MFA_ERR_ARGS;
     if (tile_cap < 0) tile_cap = 0;
     if (tile_cap > pair_tile_limit(c)) tile_cap = pair_tile_limit(c);
@@ -656,6 +687,9 @@ int launch_pair(mfa_ctx* c, int fuse_wall) {
     a.r_2_min_init = p.r_2_min_init; a.r_2_min_time = p.r_2_min_time; a.s_time = p.s_time;
     a.sqrt_alpha = p.sqrt_alpha; a.alpha_c = p.alpha_c; a.inv_sqrt_pi = p.inv_sqrt_pi;
     a.ewald_rc_2 = p.ewald_rc_2;
+    for (int d = 0; d < 3; ++d) { a.fL[d] = (float)a.L[d]; a.fiL[d] = (float)a.invL[d]; }
+    a.fsig = (float)a.sig; a.fgam = (float)a.friction; a.fewrc2 = (float)a.ewald_rc_2;
+    a.fsqrt_alpha = (float)a.sqrt_alpha; a.falpha_c = (float)a.alpha_c; a.finv_sqrt_pi = (float)a.inv_sqrt_pi;
     for (int k = 0; k < T8; ++k) { a.a_wall[k] = p.a_wall[k]; a.sigma_wall[k] = p.sigma_wall[k]; }
     a.a_w = p.a_w; a.z_space_wall = p.z_space_wall; a.wall_cut = p.wall_cut;
     a.seed0 = (uint32_t)p.seed; a.seed1 = (uint32_t)(p.seed >> 32);

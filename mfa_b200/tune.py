@@ -14,7 +14,7 @@ import time
 import math
 
 CANDIDATES = ((2, 128, True), (4, 64, True),
-              (1, 128, False), (2, 128, False), (4, 128, False), (2, 256, False), (4, 256, False))
+              (2, 128, False), (4, 128, False), (2, 256, False), (4, 256, False))
 SKINS = (0.2, 0.3, 0.4, 0.5, 0.6)
 
 
