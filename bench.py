@@ -44,7 +44,8 @@ def args_():
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--chunk", type=int, default=10, help="time steps per timed iteration (one mfa_step call)")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="brush", choices=["brush", "melt", "charged"])
+    ap.add_argument("--workload", default="brush", choices=["brush", "melt", "charged", "batch"])
+    ap.add_argument("--n-sys", type=int, default=64, help="systems of the batch workload")
     ap.add_argument("--equil", type=int, default=10000, help="untimed relaxation steps of the fresh configuration")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
@@ -232,16 +233,172 @@ def pair_work(g, cfg):
             "list_entries": int(cnt.sum())}
 
 
+def batch_bench(a):
+    """Uneven implicit-solvent brushes (default 64 systems, ~0.95 M beads)
+    advanced together: each kernel stage of a step is one launch for all
+    systems (mfa_batch_step).  Beside it: the same systems stepped one after
+    another through mfa_step (one system per launch sequence), FP64, and the
+    serial CPU restatement on a sample of the systems."""
+    import numpy as np
+    import torch
+    from mfa_b200 import _abi, configs
+    from mfa_b200.api import Batch, System
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    dev = local
+    torch.cuda.set_device(dev)
+    # whole systems are the unit of work: rank r takes every world-th system
+    cfgs = configs.uneven_brushes(seed=a.seed, n_sys=a.n_sys)[rank::world]
+    n = sum(c.n for c in cfgs)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
+
+    def make(prec):
+        ss = []
+        for c in cfgs:
+            g = System(c.params, c.r0, c.v, c.a_type, c.mass, precision=prec, device=dev)
+            g.init_forces()
+            ss.append(g)
+        return ss
+
+    def timed_batch(prec, steps, warmup):
+        ss = make(prec)
+        b = Batch(ss)
+        if a.equil:
+            b.step(a.equil)
+        ext = torch.cuda.ExternalStream(b.stream_ptr(), device=f"cuda:{dev}")
+        sampler = ClockSampler(dev)
+        sampler.start()
+        for k in range(max(1, -(-warmup // a.chunk))):
+            with torch.cuda.stream(ext):
+                flush.fill_(k & 0xff)
+            b.step(a.chunk)
+        b.sync()
+        chunks = [a.chunk] * (steps // a.chunk) + ([steps % a.chunk] if steps % a.chunk else [])
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in chunks]
+        l0 = b.launches()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        t_begin = time.time()
+        for k, nst in enumerate(chunks):
+            with torch.cuda.stream(ext):
+                flush.fill_(k & 0xff)
+            ev[k][0].record(ext)
+            b.step(nst)
+            ev[k][1].record(ext)
+        b.sync()
+        torch.cuda.synchronize(dev)
+        sampler.mark(t_begin, time.time())
+        clocks = sampler.stop()
+        ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
+        launches = b.launches() - l0
+        sc = b.scalars()
+        errs = sum(1 for x in sc if x["error_bits"])
+        b.close()
+        for g in ss:
+            g.close()
+        return ms, launches, clocks, errs
+
+    ms_mixed, launches, clocks, errs = timed_batch(_abi.MIXED, a.steps, a.warmup)
+    ms_max = ms_mixed
+    if dist is not None:
+        t = torch.tensor([ms_mixed], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+        nt = torch.tensor([n], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(nt)
+        n_all = int(nt.item())
+    else:
+        n_all = n
+    value = n_all * a.steps / (ms_max * 1e-3)
+    ms_fp64, _, _, _ = timed_batch(_abi.FP64, a.steps, a.warmup)
+    # the same systems one after another (a launch sequence per system)
+    ss = make(_abi.MIXED)
+    st = torch.cuda.Stream(device=f"cuda:{dev}")
+    for g in ss:
+        g.step(a.chunk)
+    torch.cuda.synchronize(dev)
+    seq_steps = max(a.chunk, a.steps // 4)
+    t0 = time.perf_counter()
+    for g in ss:
+        g.step(seq_steps)
+    for g in ss:
+        g.sync()
+    t_seq = time.perf_counter() - t0
+    for g in ss:
+        g.close()
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not a.no_cpu:
+            # serial CPU restatement on a sample: the smallest systems, a few steps each
+            import statistics
+            sample = sorted(cfgs, key=lambda c: c.n)[:8]
+            tot, done = 0.0, 0
+            for c in sample:
+                rate, steps, dt = run_oracle(c, a.cpu_seconds / len(sample), 1000)
+                tot += dt
+                done += c.n * steps
+            model, ncpu = cpu_info()
+            cpu = {"value": done / tot, "unit": METRIC, "cores": 1, "kind": "port",
+                   "sample": f"{len(sample)} smallest systems of the batch, serial C restatement of the "
+                             f"reference loop one system after another, 1 core of {model} ({ncpu} host threads)"}
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded generator, no reference data)",
+            "config": {"workload": f"uneven_implicit_brushes_x{a.n_sys}", "systems_per_gpu": len(cfgs),
+                       "beads_per_gpu": n, "beads_total": n_all,
+                       "chain_lengths": sorted({c.params.n_mon for c in cfgs}),
+                       "grafting_density": [round(min(c.params.n_chain / (c.params.boundary[0] * c.params.boundary[1])
+                                                      for c in cfgs), 3),
+                                            round(max(c.params.n_chain / (c.params.boundary[0] * c.params.boundary[1])
+                                                      for c in cfgs), 3)],
+                       "precision": "mixed", "dt": 0.005, "thermostat": "dpd",
+                       "steps_per_timed_iteration": a.chunk,
+                       "l2": "flushed between timed iterations (256 MiB write); state is larger than L2",
+                       "parallelism": f"whole systems over {world} GPU(s), no data exchange"},
+            "fp64": {"value": n_all * a.steps / (ms_fp64 * 1e-3), "ms_per_step": ms_fp64 / a.steps},
+            "mixed_over_fp64": ms_fp64 / ms_mixed,
+            "one_system_at_a_time": {"value": n * seq_steps / t_seq,
+                                     "note": "the same systems through mfa_step one after another (wall clock)"},
+            "gpu_launches": int(launches),
+            "systems_with_errors": errs,
+            "clocks": clocks,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     a = args_()
     if a.drift:
         return drift(a)
+    if a.workload == "batch" and a.impl != "reference":
+        return batch_bench(a)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
     if a.impl == "reference":
         if rank != 0:
+            return 0
+        if a.workload == "batch":
+            print(json.dumps({"impl": "reference", "unavailable": "the batch workload has no single reference "
+                              "run; its CPU baseline is the serial restatement per system (cpu_baseline)"}))
             return 0
         cfg, meta = make_config(a.workload, a.seed)
         # each step is one full time step of the workload; the run is capped at

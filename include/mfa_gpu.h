@@ -264,12 +264,40 @@ int mfa_sync(mfa_ctx* ctx);
 int mfa_stream(mfa_ctx* ctx, void** cuda_stream);
 
 /* Parity hooks: cell index per particle (0-based ix + nbx*(iy + nby*iz)) and the
- * Verlet list, full (both directions), rows in particle order, 1-based ids,
- * row i = nbr[i*max_per .. i*max_per + nbr_count[i]). */
+ * Verlet list, rows in particle order, 1-based ids, row i = nbr[i*max_per ..
+ * i*max_per + nbr_count[i]).  After mfa_binning a half list (every pair once,
+ * in the row of the particle with the lower cell-sorted slot); after
+ * mfa_my_binning a full list (both directions), as the reference builds them. */
 int mfa_debug_lists(mfa_ctx* ctx, int32_t* cell_of, int32_t* nbr_count,
                     int32_t* nbr, int32_t max_per);
 /* Number of k-vectors and their components (after mfa_ewald_k(ctx, 0)). */
 int mfa_debug_kvecs(mfa_ctx* ctx, int32_t* nk, double* kvecs3, int32_t max_k);
+
+/* ---------------- many systems in one launch ---------------- */
+
+/* No counterpart in the reference, which runs one system per process (the
+ * md_main.f90:68-184 loop).  Groups n contexts made by mfa_init -- independent
+ * systems of any size and box, same device, precision and physics switches
+ * (thermostat, SYMMETRY, WALL; no Ewald, no WALL 3/4) -- so that
+ * mfa_batch_step advances all of them: each kernel stage of the time step is
+ * ONE launch for the whole batch (a table maps every block to its system),
+ * steps are captured CUDA graphs, and a system's lists are rebuilt when its
+ * own skin check trips.  Every context keeps its state, energies and error
+ * flags; read them with mfa_get_scalars / mfa_download after mfa_batch_sync.
+ * The contexts must outlive the batch; their pair-kernel shape becomes the
+ * first context's. */
+typedef struct mfa_batch mfa_batch;
+int mfa_batch_create(mfa_ctx* const* ctxs, int32_t n, mfa_batch** out);
+/* nsteps time steps of every system of the batch (asynchronous, one stream). */
+int mfa_batch_step(mfa_batch* batch, int32_t nsteps);
+int mfa_batch_sync(mfa_batch* batch);
+/* The batch's CUDA stream (cudaStream_t), for event timing. */
+int mfa_batch_stream(mfa_batch* batch, void** cuda_stream);
+/* Kernels the batch has launched so far (grouped launches; a rebuild node
+ * that opened counts its six kernels once, however many systems rebuilt). */
+int mfa_batch_launches(mfa_batch* batch, int64_t* launches);
+/* Releases the batch (not its contexts). */
+int mfa_batch_destroy(mfa_batch* batch);
 
 /* ---------------- binning without device allocation ---------------- */
 

@@ -11,13 +11,13 @@ from ._abi import FP64, MIXED, MfaError, MfaParams, MfaScalars
 from .params import Spec, derive
 
 __all__ = ["_abi", "FP64", "MIXED", "MfaError", "MfaParams", "MfaScalars", "Spec", "derive",
-           "System", "from_config"]
+           "System", "Batch", "from_config"]
 
 
 def __getattr__(name):
     # the System class needs the CUDA library; load it lazily so that the
     # parameter and configuration helpers import without a GPU build present
-    if name in ("System", "from_config"):
+    if name in ("System", "Batch", "from_config"):
         import importlib
         return getattr(importlib.import_module(".api", __name__), name)
     raise AttributeError(name)

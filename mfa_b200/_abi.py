@@ -133,6 +133,12 @@ SIGNATURES = {
                                         C.c_void_p, C.c_void_p]),
     "mfa_debug_lists": (C.c_int, [_P, _IP, _IP, _IP, C.c_int32]),
     "mfa_debug_kvecs": (C.c_int, [_P, _IP, _DP, C.c_int32]),
+    "mfa_batch_create": (C.c_int, [C.POINTER(_P), C.c_int32, C.POINTER(_P)]),
+    "mfa_batch_step": (C.c_int, [_P, C.c_int32]),
+    "mfa_batch_sync": (C.c_int, [_P]),
+    "mfa_batch_stream": (C.c_int, [_P, C.POINTER(_P)]),
+    "mfa_batch_launches": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "mfa_batch_destroy": (C.c_int, [_P]),
 }
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libmfa_gpu.so")

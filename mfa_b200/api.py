@@ -243,3 +243,49 @@ def from_config(cfg, precision: int = _abi.MIXED, device: int = 0) -> System:
     """A System holding a generated configuration (mfa_b200.configs)."""
     return System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q,
                   precision=precision, device=device)
+
+
+class Batch:
+    """Several Systems advanced together: each kernel stage of the time step is
+    one launch for all of them (mfa_batch_*).  The Systems keep their state,
+    energies and errors; read them after ``sync()``."""
+
+    def __init__(self, systems):
+        self.lib = load()
+        self.systems = list(systems)
+        arr = (C.c_void_p * len(self.systems))(*[s.ctx.value for s in self.systems])
+        b = C.c_void_p()
+        check(self.lib.mfa_batch_create(arr, len(self.systems), C.byref(b)), "mfa_batch_create")
+        self.b = b
+
+    def step(self, nsteps: int) -> None:
+        check(self.lib.mfa_batch_step(self.b, int(nsteps)), "mfa_batch_step")
+
+    def sync(self) -> None:
+        check(self.lib.mfa_batch_sync(self.b), "mfa_batch_sync")
+
+    def stream_ptr(self) -> int:
+        s = C.c_void_p()
+        check(self.lib.mfa_batch_stream(self.b, C.byref(s)), "mfa_batch_stream")
+        return int(s.value or 0)
+
+    def launches(self) -> int:
+        n = C.c_int64(0)
+        check(self.lib.mfa_batch_launches(self.b, C.byref(n)), "mfa_batch_launches")
+        return int(n.value)
+
+    def scalars(self):
+        """Per-system scalars (mfa_get_scalars of each system)."""
+        self.sync()
+        return [s.scalars() for s in self.systems]
+
+    def close(self) -> None:
+        if getattr(self, "b", None):
+            self.lib.mfa_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

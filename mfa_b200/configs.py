@@ -326,3 +326,69 @@ def charged(seed: int = 12345, n_chain: int = 200, n_mon: int = 50, density: flo
             p.n_bin[d] = max(1, int(L / (rc_real + skin)))
             p.delta_bin[d] = 1 if p.n_bin[d] >= 3 else (0 if p.n_bin[d] == 2 else -1)
     return Config("charged", spec, p, r0, _maxwell(rng, mass, 1.0), a_type, mass, q)
+
+
+def brush_stretched(seed: int = 12345, nx: int = 16, ny: int = 16, n_mon: int = 64, graft: float = 0.3,
+                    z_wall: Optional[float] = None, friction: float = 4.5, skin: float = 0.3,
+                    z_head: float = 1.0, jitter: float = 0.15) -> Config:
+    """Implicit-solvent brush between 9-3 walls, chains started fully stretched.
+
+    Heads sit on a square lattice at z = z_head (grafting density `graft`);
+    bead k of a chain sits at height z_head + 0.97 k above its head with an
+    independent lateral jitter of at most `jitter` per bead.  With lattice
+    spacing 1/sqrt(graft) >= 1.41 sigma (graft <= 0.5) beads of different
+    chains stay more than 0.8 sigma apart and bonds stay below 1.1 sigma, so
+    the start is overlap-free by construction at every grafting density (a
+    random-walk growth stalls in dense brushes).  The wall gap defaults to
+    2.2 x the chain length.  Types: 1 = pinned head, 2 = monomer; WCA
+    everywhere, FENE (k = 30, R0 = 1.5), no bending, DPD gamma = friction."""
+    rng = np.random.default_rng(seed)
+    if z_wall is None:
+        z_wall = 2.2 * n_mon
+    a = math.sqrt(1.0 / graft)
+    Lx, Ly = nx * a, ny * a
+    gx, gy = np.meshgrid((np.arange(nx) + 0.5) * a, (np.arange(ny) + 0.5) * a, indexing="ij")
+    heads = np.stack([gx.ravel(), gy.ravel()], axis=1)
+    n_chain = nx * ny
+    k = np.arange(n_mon)
+    r0 = np.empty((n_chain, n_mon, 3))
+    r0[:, :, 0] = heads[:, None, 0]
+    r0[:, :, 1] = heads[:, None, 1]
+    r0[:, :, 2] = z_head + 0.97 * k[None, :]
+    jit = rng.uniform(-jitter, jitter, size=(n_chain, n_mon, 2))
+    jit[:, 0, :] = 0.0
+    r0[:, :, :2] += jit
+    r0[:, :, 0] %= Lx
+    r0[:, :, 1] %= Ly
+    r0 = r0.reshape(-1, 3)
+    n = r0.shape[0]
+    a_type = np.full(n, 2, dtype=np.int32)
+    a_type[0:n:n_mon] = 1
+    mass = np.ones(n)
+    v = _maxwell(rng, mass, 1.0)
+    v[0:n:n_mon] = 0.0
+    eps = np.ones((3, 3))
+    eps[0, 0] = 0.0
+    spec = Spec(n_part=n, boundary=np.array([Lx, Ly, z_wall]), n_type=3, n_mon=n_mon, n_chain=n_chain,
+                symmetry=0, thermostat=_abi.THERMO_DPD, friction=friction, wall=2, bending=0, pin_heads=1,
+                eps=eps, brush_heads=True, wall93_zero_last_type=True, skin=skin, dt=0.005, temp=1.0,
+                k_chain_in=30.0, r_chain=1.5, k_bend=0.0, alpha_eq=0.0, a_w=1.0, sigma_w=1.0, z_head=z_head,
+                wall_cut=2.5, seed=seed)
+    return Config("brush_stretched", spec, derive(spec), r0, v, a_type, mass)
+
+
+def uneven_brushes(seed: int = 2024, n_sys: int = 64, grids=(8, 24), lengths=(16, 32, 64, 128),
+                   graft=(0.05, 0.5)):
+    """Independent implicit-solvent brushes of uneven size for one batched run:
+    per system a grafting density ~ U(graft), a chain length drawn from
+    `lengths`, a square lateral grid of n x n chains with n ~ U{grids}, walls
+    2.2 x the chain length apart, DPD noise seeded per system (seed + 1 + s).
+    Returns the list of Configs (brush_stretched)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for s in range(n_sys):
+        g = float(rng.uniform(*graft))
+        nm = int(rng.choice(lengths))
+        nx = int(rng.integers(grids[0], grids[1] + 1))
+        out.append(brush_stretched(seed=seed + 1 + s, nx=nx, ny=nx, n_mon=nm, graft=g))
+    return out

@@ -21,6 +21,8 @@
 // an entry is the partner's slot.
 #include "mfa_internal.cuh"
 
+#include <string.h>
+
 namespace {
 
 struct BinArgs {
@@ -48,6 +50,8 @@ struct BinArgs {
     int prefilter;       // FP32 prefilter of list candidates (n_bin >= 3 on every axis)
     float prefilter_margin;
     int in_cond_body;    // launched from a conditional graph node: count the rebuild there
+    int with_pos64;      // the gather also writes the list builder's FP64/FP32 copies
+    const double* cut2;  // list criterion range_2 + skin_2 (T8 x T8)
 };
 
 __device__ __forceinline__ bool skip(const BinArgs& a) {
@@ -66,9 +70,9 @@ __device__ __forceinline__ int cell_coord(const BinArgs& a, double x, int d, boo
     return ic;
 }
 
-__global__ void k_cell_assign(BinArgs a) {
+__device__ __forceinline__ void cell_assign_body(const BinArgs& a, Blk blk) {
     if (skip(a)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blk.id * blockDim.x + threadIdx.x;
     if (i == 0) {
         a.flags[F_MAXCELL] = 0;
         a.flags[F_MAXROW] = 0;
@@ -94,12 +98,12 @@ __global__ void k_cell_assign(BinArgs a) {
 // Exclusive scan of the cell histogram into cell_start[0..ncell] (and the
 // scatter cursors).  Block b owns rows [b*W, b*W + W), one warp per row; its
 // starting offset is the sum of the row histogram below its first row.
-__global__ void k_scan_rows(BinArgs a) {
+__device__ __forceinline__ void scan_rows_body(const BinArgs& a, Blk blk) {
     if (skip(a)) return;
     __shared__ int wpart[32];
     __shared__ int rpre[33];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, W = blockDim.x >> 5;
-    const int r0 = blockIdx.x * W;
+    const int r0 = blk.id * W;
     // offset of this block: sum of row_count[0 .. r0)
     int s = 0;
     for (int r = threadIdx.x; r < r0; r += blockDim.x) s += a.row_count[r];
@@ -153,9 +157,9 @@ __global__ void k_scan_rows(BinArgs a) {
     }
 }
 
-__global__ void k_cell_scatter(BinArgs a) {
+__device__ __forceinline__ void cell_scatter_body(const BinArgs& a, Blk blk) {
     if (skip(a)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blk.id * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const int p = atomicAdd(&a.cell_cursor[a.cell_of[i]], 1);
     a.ids[p] = i;
@@ -163,9 +167,9 @@ __global__ void k_cell_scatter(BinArgs a) {
 
 // insertion sort of each cell's ids (cells hold a few to a few tens of
 // particles); the row histogram is cleared here for the next rebuild
-__global__ void k_cell_sort(BinArgs a) {
+__device__ __forceinline__ void cell_sort_body(const BinArgs& a, Blk blk) {
     if (skip(a)) return;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blk.id * blockDim.x + threadIdx.x;
     if (c < a.nrow) a.row_count[c] = 0;
     if (c >= a.ncell) return;
     const int b = a.cell_start[c], e = a.cell_start[c + 1];
@@ -178,9 +182,9 @@ __global__ void k_cell_sort(BinArgs a) {
 }
 
 template <typename R4>
-__global__ void k_gather_sorted(BinArgs a, int with_pos64) {
+__device__ __forceinline__ void gather_sorted_body(const BinArgs& a, Blk blk) {
     if (skip(a)) return;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blk.id * blockDim.x + threadIdx.x;
     if (t >= a.n) return;
     const int i = a.ids[t];
     a.slot[i] = t;
@@ -193,7 +197,7 @@ __global__ void k_gather_sorted(BinArgs a, int with_pos64) {
     R4 v;
     v.x = a.vx[i]; v.y = a.vy[i]; v.z = a.vz[i]; v.w = a.q ? a.q[i] : 0.0;
     ((R4*)a.vel_s)[t] = v;
-    if (with_pos64) {
+    if (a.with_pos64) {
         double4 d;
         d.x = x; d.y = y; d.z = z;
         packw(d, i, ty);
@@ -236,16 +240,16 @@ __device__ __forceinline__ int x_runs(const BinArgs& a, int cx, int nx, int wx, 
 // those that pass get the reference's FP64 test, so the kept set is exactly
 // the FP64 criterion's.  Grids with fewer than 3 cells on an axis (where a
 // pair's nearest image can be ambiguous in FP32) test every candidate in FP64.
-__global__ void k_build_nbr(BinArgs a, const double* __restrict__ cut2 /*T8*T8*/) {
+__device__ __forceinline__ void build_nbr_body(const BinArgs& a, Blk blk) {
     if (skip(a)) return;
     __shared__ double sc[T8 * T8];
     __shared__ float scf[T8 * T8];
     for (int k = threadIdx.x; k < T8 * T8; k += blockDim.x) {
-        sc[k] = cut2[k];
-        scf[k] = (float)cut2[k] + a.prefilter_margin;
+        sc[k] = a.cut2[k];
+        scf[k] = (float)a.cut2[k] + a.prefilter_margin;
     }
     __syncthreads();
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blk.id * blockDim.x + threadIdx.x;
     if (t < a.n) {
         const double4 pi = a.pos64[t];
         const float4 pf = a.pos32[t];
@@ -311,7 +315,7 @@ __global__ void k_build_nbr(BinArgs a, const double* __restrict__ cut2 /*T8*T8*/
     __shared__ bool last;
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) last = (atomicAdd(a.counter, 1u) == gridDim.x - 1);
+    if (threadIdx.x == 0) last = (atomicAdd(a.counter, 1u) == (unsigned)blk.n - 1);
     __syncthreads();
     if (last && threadIdx.x == 0) {
         *a.counter = 0u;
@@ -320,6 +324,36 @@ __global__ void k_build_nbr(BinArgs a, const double* __restrict__ cut2 /*T8*T8*/
         if (a.in_cond_body) a.flags[F_CONDREB] += 1;
     }
 }
+
+// plain launches (one context) and the grouped launch (one stage for several
+// contexts, argument records in device memory)
+__global__ void k_cell_assign(BinArgs a) { cell_assign_body(a, plain_blk()); }
+__global__ void k_scan_rows(BinArgs a) { scan_rows_body(a, plain_blk()); }
+__global__ void k_cell_scatter(BinArgs a) { cell_scatter_body(a, plain_blk()); }
+__global__ void k_cell_sort(BinArgs a) { cell_sort_body(a, plain_blk()); }
+template <typename R4> __global__ void k_gather_sorted(BinArgs a) { gather_sorted_body<R4>(a, plain_blk()); }
+__global__ void k_build_nbr(BinArgs a) { build_nbr_body(a, plain_blk()); }
+
+// node_count (grouped rebuilds in a conditional graph node): counts the times
+// the node ran, for the launch accounting of a batch
+template <typename R4>
+__global__ void k_bin_grouped(const BinArgs* __restrict__ as, const int* __restrict__ off, int nsys, int stage,
+                              int* node_count) {
+    if (node_count && stage == 0 && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(node_count, 1);
+    const int s = group_of(off, nsys, blockIdx.x);
+    const Blk blk = group_blk(off, s);
+    switch (stage) {
+        case 0: cell_assign_body(as[s], blk); break;
+        case 1: scan_rows_body(as[s], blk); break;
+        case 2: cell_scatter_body(as[s], blk); break;
+        case 3: cell_sort_body(as[s], blk); break;
+        case 4: gather_sorted_body<R4>(as[s], blk); break;
+        default: build_nbr_body(as[s], blk); break;
+    }
+}
+
+// block size of each rebuild stage (assign, row scan, scatter, sort, gather, build)
+constexpr int BIN_T[N_BIN_STAGES] = {256, 256, 256, 128, 256, 128};
 
 BinArgs make_args(mfa_ctx* c, int rule, int conditional) {
     BinArgs a;
@@ -354,38 +388,66 @@ BinArgs make_args(mfa_ctx* c, int rule, int conditional) {
 
 }  // namespace
 
-int launch_rebuild(mfa_ctx* c, int rule, int conditional) {
-    return launch_rebuild_on(c, rule, conditional, c->st, 0);
-}
+size_t bin_args_bytes() { return sizeof(BinArgs); }
 
-int launch_rebuild_on(mfa_ctx* c, int rule, int conditional, cudaStream_t st, int in_cond_body) {
+int bin_stage_args(mfa_ctx* c, int rule, int conditional, int in_cond_body, void* out, int nblocks[N_BIN_STAGES]) {
     if (rule == 0)
         for (int d = 0; d < 3; ++d)
             if (c->p.delta_bin[d] < -1 || c->p.delta_bin[d] > 1) return MFA_ERR_ARGS;
     BinArgs a = make_args(c, rule, conditional);
     a.in_cond_body = in_cond_body;
-    const int T = 256;
-    const int nbp = (c->n + T - 1) / T;
+    a.with_pos64 = 1;
+    a.cut2 = c->tabs;
     const int nrow = c->nb[1] * c->nb[2];
-    k_cell_assign<<<nbp, T, 0, st>>>(a);
-    k_scan_rows<<<(nrow + 7) / 8, 256, 0, st>>>(a);
-    k_cell_scatter<<<nbp, T, 0, st>>>(a);
-    k_cell_sort<<<(c->ncell + 127) / 128, 128, 0, st>>>(a);
-    if (c->prec == MFA_MIXED) k_gather_sorted<float4><<<nbp, T, 0, st>>>(a, 1);
-    else k_gather_sorted<double4><<<nbp, T, 0, st>>>(a, 1);
-    k_build_nbr<<<(c->n + 127) / 128, 128, 0, st>>>(a, c->tabs);
+    nblocks[0] = (c->n + BIN_T[0] - 1) / BIN_T[0];
+    nblocks[1] = (nrow + BIN_T[1] / 32 - 1) / (BIN_T[1] / 32);
+    nblocks[2] = (c->n + BIN_T[2] - 1) / BIN_T[2];
+    nblocks[3] = (c->ncell + BIN_T[3] - 1) / BIN_T[3];
+    nblocks[4] = (c->n + BIN_T[4] - 1) / BIN_T[4];
+    nblocks[5] = (c->n + BIN_T[5] - 1) / BIN_T[5];
+    memcpy(out, &a, sizeof(a));
+    return MFA_OK;
+}
+
+int launch_bin_grouped(int prec, int stage, const void* dargs, const int* doff, int nsys, int nblocks,
+                       cudaStream_t st, int* node_count) {
+    if (prec == MFA_MIXED)
+        k_bin_grouped<float4><<<nblocks, BIN_T[stage], 0, st>>>((const BinArgs*)dargs, doff, nsys, stage, node_count);
+    else
+        k_bin_grouped<double4><<<nblocks, BIN_T[stage], 0, st>>>((const BinArgs*)dargs, doff, nsys, stage,
+                                                                  node_count);
     MFA_CUDA_TRY(cudaGetLastError());
-    if (!in_cond_body) note_launch(c, 6);
+    return MFA_OK;
+}
+
+int launch_rebuild(mfa_ctx* c, int rule, int conditional) {
+    return launch_rebuild_on(c, rule, conditional, c->st, 0);
+}
+
+int launch_rebuild_on(mfa_ctx* c, int rule, int conditional, cudaStream_t st, int in_cond_body) {
+    BinArgs a;
+    int nb[N_BIN_STAGES];
+    TRY_(bin_stage_args(c, rule, conditional, in_cond_body, &a, nb));
+    k_cell_assign<<<nb[0], BIN_T[0], 0, st>>>(a);
+    k_scan_rows<<<nb[1], BIN_T[1], 0, st>>>(a);
+    k_cell_scatter<<<nb[2], BIN_T[2], 0, st>>>(a);
+    k_cell_sort<<<nb[3], BIN_T[3], 0, st>>>(a);
+    if (c->prec == MFA_MIXED) k_gather_sorted<float4><<<nb[4], BIN_T[4], 0, st>>>(a);
+    else k_gather_sorted<double4><<<nb[4], BIN_T[4], 0, st>>>(a);
+    k_build_nbr<<<nb[5], BIN_T[5], 0, st>>>(a);
+    MFA_CUDA_TRY(cudaGetLastError());
+    if (!in_cond_body) note_launch(c, N_BIN_STAGES);
     return MFA_OK;
 }
 
 int launch_refresh_sorted(mfa_ctx* c) {
     BinArgs a = make_args(c, 0, 0);
     a.in_cond_body = 0;
-    const int T = 256;
-    const int nbp = (c->n + T - 1) / T;
-    if (c->prec == MFA_MIXED) k_gather_sorted<float4><<<nbp, T, 0, c->st>>>(a, 0);
-    else k_gather_sorted<double4><<<nbp, T, 0, c->st>>>(a, 0);
+    a.with_pos64 = 0;
+    a.cut2 = c->tabs;
+    const int nbp = (c->n + BIN_T[4] - 1) / BIN_T[4];
+    if (c->prec == MFA_MIXED) k_gather_sorted<float4><<<nbp, BIN_T[4], 0, c->st>>>(a);
+    else k_gather_sorted<double4><<<nbp, BIN_T[4], 0, c->st>>>(a);
     MFA_CUDA_TRY(cudaGetLastError());
     note_launch(c, 1);
     return MFA_OK;

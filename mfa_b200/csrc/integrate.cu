@@ -6,6 +6,8 @@
 #include "mfa_internal.cuh"
 #include "bonded.cuh"
 
+#include <string.h>
+
 namespace {
 
 struct VVArgs {
@@ -43,6 +45,7 @@ struct VVArgs {
     // here, bead by bead, and added to the force before a = F/m
     int fuse_bonds;
     BondParams bond;
+    int fused_skin, zero_force;   // position half: skin check, force reset
 };
 
 // r += dt v + (0.5 dt^2) a ; v += (0.5 dt) a   (verlet_positions.f90:153,169)
@@ -104,13 +107,13 @@ __device__ __forceinline__ void position_half(const VVArgs& a, int i, double x, 
 // zero_force: the fast path resets the force array here (md_main.f90:88), so
 // that the force kernels of the step only ever add to it
 template <typename R4>
-__global__ void k_vv_positions(VVArgs a, int fused_skin, int zero_force) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void vv_positions_body(const VVArgs& a, Blk blk) {
+    const int i = blk.id * blockDim.x + threadIdx.x;
     if (i == 0) *a.dstep += 1;
     if (i >= a.n) return;
     position_half<R4>(a, i, a.rx[i], a.ry[i], a.rz[i], a.vx[i], a.vy[i], a.vz[i],
-                      a.ax[i], a.ay[i], a.az[i], fused_skin != 0);
-    if (zero_force) {
+                      a.ax[i], a.ay[i], a.az[i], a.fused_skin != 0);
+    if (a.zero_force) {
         R4 z4; z4.x = 0; z4.y = 0; z4.z = 0; z4.w = 0;
         ((R4*)a.force)[i] = z4;
     }
@@ -189,16 +192,16 @@ __device__ __forceinline__ void finish_energies(const VVArgs& a) {
 
 // the FENE bonds at the clamp counted by the warp, and the block sums of
 // m v^2, FENE (times k_chain, intra_molec.f90:272,300) and bending energy
-__device__ __forceinline__ bool vv_commit(const VVArgs& a, double ke, const double eb[2], int clamped) {
+__device__ __forceinline__ bool vv_commit(const VVArgs& a, double ke, const double eb[2], int clamped, Blk blk) {
     for (int o = 16; o > 0; o >>= 1) clamped += __shfl_down_sync(0xffffffffu, clamped, o);
     if ((threadIdx.x & 31) == 0 && clamped) atomicAdd(&a.flags[F_FENE], clamped);
     double acc[3] = {ke, a.bond.k_chain * eb[0], eb[1]};
-    return block_sum_commit<3>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_TMP0);
+    return block_sum_commit<3>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_TMP0, blk);
 }
 
 template <typename R4>
-__global__ void k_vv_velocities(VVArgs a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void vv_velocities_body(const VVArgs& a, Blk blk) {
+    const int i = blk.id * blockDim.x + threadIdx.x;
     double ke = 0.0, eb[2] = {0.0, 0.0};
     int clamped = 0;
     if (i < a.n) {
@@ -207,7 +210,7 @@ __global__ void k_vv_velocities(VVArgs a) {
         a.vx[i] = vx; a.vy[i] = vy; a.vz[i] = vz;
         a.ax[i] = ax; a.ay[i] = ay; a.az[i] = az;
     }
-    if (vv_commit(a, ke, eb, clamped)) {
+    if (vv_commit(a, ke, eb, clamped, blk)) {
         if (threadIdx.x == 0) finish_energies(a);
     }
 }
@@ -216,8 +219,8 @@ __global__ void k_vv_velocities(VVArgs a) {
 // pass over the state (the skin check of n+1 fused in); the force array is
 // reset for the force kernels of step n+1 (md_main.f90:88).
 template <typename R4>
-__global__ void k_vv_fused(VVArgs a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void vv_fused_body(const VVArgs& a, Blk blk) {
+    const int i = blk.id * blockDim.x + threadIdx.x;
     double ke = 0.0, eb[2] = {0.0, 0.0};
     int clamped = 0;
     if (i < a.n) {
@@ -229,15 +232,32 @@ __global__ void k_vv_fused(VVArgs a) {
         // is written by the velocity half that closes a run of steps
         position_half<R4>(a, i, a.rx[i], a.ry[i], a.rz[i], vx, vy, vz, ax, ay, az, true);
     }
-    if (vv_commit(a, ke, eb, clamped)) {
+    if (vv_commit(a, ke, eb, clamped, blk)) {
         if (threadIdx.x == 0) {
             finish_energies(a);
             *a.dstep += 1;  // the next step has begun
             // every block's skin verdict is visible here (each fenced before
-            // taking its turn on the counter)
-            if (a.rebuild_cond) cudaGraphSetConditional(a.rebuild_cond, *(volatile int32_t*)&a.flags[F_SKIN] != 0);
+            // taking its turn on the counter).  Only a rebuild that is due
+            // opens the node (the condition starts at 0 every graph launch),
+            // so that several contexts may share one node.
+            if (a.rebuild_cond && *(volatile int32_t*)&a.flags[F_SKIN] != 0)
+                cudaGraphSetConditional(a.rebuild_cond, 1u);
         }
     }
+}
+
+// plain launches (one context) and grouped launches (the same stage for
+// several contexts, argument records in device memory)
+template <typename R4> __global__ void k_vv_positions(VVArgs a) { vv_positions_body<R4>(a, plain_blk()); }
+template <typename R4> __global__ void k_vv_velocities(VVArgs a) { vv_velocities_body<R4>(a, plain_blk()); }
+template <typename R4> __global__ void k_vv_fused(VVArgs a) { vv_fused_body<R4>(a, plain_blk()); }
+template <typename R4>
+__global__ void k_vv_grouped(const VVArgs* __restrict__ as, const int* __restrict__ off, int nsys, int stage) {
+    const int s = group_of(off, nsys, blockIdx.x);
+    const Blk blk = group_blk(off, s);
+    if (stage == VV_POSITIONS) vv_positions_body<R4>(as[s], blk);
+    else if (stage == VV_VELOCITIES) vv_velocities_body<R4>(as[s], blk);
+    else vv_fused_body<R4>(as[s], blk);
 }
 
 VVArgs make_args(mfa_ctx* c) {
@@ -267,6 +287,8 @@ VVArgs make_args(mfa_ctx* c) {
     a.rebuild_cond = 0;
     a.fuse_bonds = 0;
     a.bond = bond_params(c, 0, 0);
+    a.fused_skin = 0;
+    a.zero_force = 0;
     return a;
 }
 
@@ -280,11 +302,36 @@ void set_bonds(const mfa_ctx* c, VVArgs& a, int fuse_bonds) {
 
 }  // namespace
 
-int launch_vv_positions(mfa_ctx* c, int fused_skin, int zero_force) {
+int vv_stage_args(mfa_ctx* c, int stage, int fused_skin, int zero_force, int fuse_bonds,
+                  cudaGraphConditionalHandle rebuild_cond, void* out, int* nblocks) {
     VVArgs a = make_args(c);
+    a.fused_skin = fused_skin;
+    a.zero_force = zero_force;
+    a.rebuild_cond = rebuild_cond;
+    set_bonds(c, a, fuse_bonds);
     const int nb = (c->n + TPB - 1) / TPB;
-    if (c->prec == MFA_MIXED) k_vv_positions<float4><<<nb, TPB, 0, c->st>>>(a, fused_skin, zero_force);
-    else k_vv_positions<double4><<<nb, TPB, 0, c->st>>>(a, fused_skin, zero_force);
+    if (stage != VV_POSITIONS && nb > c->max_blocks) return MFA_ERR_ARGS;
+    memcpy(out, &a, sizeof(a));
+    *nblocks = nb;
+    return MFA_OK;
+}
+
+size_t vv_args_bytes() { return sizeof(VVArgs); }
+
+int launch_vv_grouped(int prec, int stage, const void* dargs, const int* doff, int nsys, int nblocks,
+                      cudaStream_t st) {
+    if (prec == MFA_MIXED) k_vv_grouped<float4><<<nblocks, TPB, 0, st>>>((const VVArgs*)dargs, doff, nsys, stage);
+    else k_vv_grouped<double4><<<nblocks, TPB, 0, st>>>((const VVArgs*)dargs, doff, nsys, stage);
+    MFA_CUDA_TRY(cudaGetLastError());
+    return MFA_OK;
+}
+
+int launch_vv_positions(mfa_ctx* c, int fused_skin, int zero_force) {
+    VVArgs a;
+    int nb;
+    TRY_(vv_stage_args(c, VV_POSITIONS, fused_skin, zero_force, 0, 0, &a, &nb));
+    if (c->prec == MFA_MIXED) k_vv_positions<float4><<<nb, TPB, 0, c->st>>>(a);
+    else k_vv_positions<double4><<<nb, TPB, 0, c->st>>>(a);
     MFA_CUDA_TRY(cudaGetLastError());
     note_launch(c, 1);
     return MFA_OK;
@@ -300,10 +347,9 @@ int launch_check_skin(mfa_ctx* c) {
 }
 
 int launch_vv_velocities(mfa_ctx* c, int fuse_bonds) {
-    VVArgs a = make_args(c);
-    set_bonds(c, a, fuse_bonds);
-    const int nb = (c->n + TPB - 1) / TPB;
-    if (nb > c->max_blocks) return MFA_ERR_ARGS;
+    VVArgs a;
+    int nb;
+    TRY_(vv_stage_args(c, VV_VELOCITIES, 0, 0, fuse_bonds, 0, &a, &nb));
     if (c->prec == MFA_MIXED) k_vv_velocities<float4><<<nb, TPB, 0, c->st>>>(a);
     else k_vv_velocities<double4><<<nb, TPB, 0, c->st>>>(a);
     MFA_CUDA_TRY(cudaGetLastError());
@@ -312,11 +358,9 @@ int launch_vv_velocities(mfa_ctx* c, int fuse_bonds) {
 }
 
 int launch_vv_fused(mfa_ctx* c, cudaGraphConditionalHandle rebuild_cond, int fuse_bonds) {
-    VVArgs a = make_args(c);
-    a.rebuild_cond = rebuild_cond;
-    set_bonds(c, a, fuse_bonds);
-    const int nb = (c->n + TPB - 1) / TPB;
-    if (nb > c->max_blocks) return MFA_ERR_ARGS;
+    VVArgs a;
+    int nb;
+    TRY_(vv_stage_args(c, VV_FUSED, 1, 1, fuse_bonds, rebuild_cond, &a, &nb));
     if (c->prec == MFA_MIXED) k_vv_fused<float4><<<nb, TPB, 0, c->st>>>(a);
     else k_vv_fused<double4><<<nb, TPB, 0, c->st>>>(a);
     MFA_CUDA_TRY(cudaGetLastError());

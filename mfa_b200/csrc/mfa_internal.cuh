@@ -119,18 +119,43 @@ struct mfa_ctx {
     double* h_stage;
 };
 
+#define TRY_(x)                          \
+    do {                                 \
+        int s__ = (x);                   \
+        if (s__ != MFA_OK) return s__;   \
+    } while (0)
+
+// stages of the integrator kernels
+enum { VV_POSITIONS = 0, VV_VELOCITIES = 1, VV_FUSED = 2 };
+
 // ---------- launchers (each file) ----------
 // integrate.cu
 int launch_vv_positions(mfa_ctx* c, int fused_skin, int zero_force);
 int launch_check_skin(mfa_ctx* c);
 int launch_vv_velocities(mfa_ctx* c, int fuse_bonds);
 int launch_vv_fused(mfa_ctx* c, cudaGraphConditionalHandle rebuild_cond, int fuse_bonds);
+// argument record of an integrator stage (for grouped launches) and the launch
+size_t vv_args_bytes();
+int vv_stage_args(mfa_ctx* c, int stage, int fused_skin, int zero_force, int fuse_bonds,
+                  cudaGraphConditionalHandle rebuild_cond, void* out, int* nblocks);
+int launch_vv_grouped(int prec, int stage, const void* dargs, const int* doff, int nsys, int nblocks,
+                      cudaStream_t st);
 // binning.cu
 int launch_rebuild(mfa_ctx* c, int rule, int conditional);
 int launch_rebuild_on(mfa_ctx* c, int rule, int conditional, cudaStream_t st, int in_cond_body);
+// the six rebuild stages as grouped launches
+constexpr int N_BIN_STAGES = 6;
+size_t bin_args_bytes();
+int bin_stage_args(mfa_ctx* c, int rule, int conditional, int in_cond_body, void* out, int nblocks[N_BIN_STAGES]);
+int launch_bin_grouped(int prec, int stage, const void* dargs, const int* doff, int nsys, int nblocks,
+                       cudaStream_t st, int* node_count);
 int launch_refresh_sorted(mfa_ctx* c);
 // pair.cu
 int launch_pair(mfa_ctx* c, int fuse_wall);   // adds to force
+size_t pair_args_bytes();
+int pair_stage_args(mfa_ctx* c, int fuse_wall, void* out, int* grid_out, size_t* smem_out, int* ft_out);
+int launch_pair_grouped(int prec, int k, int block, int ft, const void* dargs, const int* doff, int nsys, int grid,
+                        size_t smem, cudaStream_t st);
 int pair_set_shape(mfa_ctx* c, int tpp, int block, int tile_cap);
 int pair_tile_limit(const mfa_ctx* c);
 // bonds.cu
@@ -220,12 +245,36 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, const PhiloxKeys& key) {
 #define TAG_DPD 0x44504400u
 #define TAG_LGV 0x4C475600u
 
+// Position of a block in the launch it belongs to.  A plain launch uses
+// blockIdx/gridDim; a grouped launch (one kernel stage for several contexts,
+// see group_of) gives each block its index within its own context's share.
+struct Blk {
+    int id, n;
+};
+__device__ __forceinline__ Blk plain_blk() { return Blk{(int)blockIdx.x, (int)gridDim.x}; }
+
+// Grouped launch: off[0..nsys] are prefix sums of the contexts' block counts;
+// returns the context of block b.
+__device__ __forceinline__ int group_of(const int* __restrict__ off, int nsys, int b) {
+    int lo = 0, hi = nsys - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&off[mid]) <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+__device__ __forceinline__ Blk group_blk(const int* __restrict__ off, int s) {
+    const int o = __ldg(&off[s]);
+    return Blk{(int)blockIdx.x - o, __ldg(&off[s + 1]) - o};
+}
+
 // Block-wide FP64 sums of NQ values, committed deterministically: each block
 // writes its partials, the last block to finish adds them in block order and
 // stores the result in out[0..NQ).  Requires blockDim.x a multiple of 32, <= 1024.
 template <int NQ>
 __device__ __forceinline__ bool block_sum_commit(double (&v)[NQ], double* partials, int max_blocks,
-                                                 unsigned* counter, double* out) {
+                                                 unsigned* counter, double* out, Blk blk = plain_blk()) {
     __shared__ double sm[NQ][32];
     __shared__ bool am_last;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -241,18 +290,18 @@ __device__ __forceinline__ bool block_sum_commit(double (&v)[NQ], double* partia
         for (int q = 0; q < NQ; ++q) {
             double x = lane < nw ? sm[q][lane] : 0.0;
             for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-            if (lane == 0) partials[q * max_blocks + blockIdx.x] = x;
+            if (lane == 0) partials[q * max_blocks + blk.id] = x;
         }
     }
     __threadfence();
-    if (threadIdx.x == 0) am_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    if (threadIdx.x == 0) am_last = (atomicAdd(counter, 1u) == (unsigned)blk.n - 1);
     __syncthreads();
     if (!am_last) return false;
     __threadfence();
 #pragma unroll
     for (int q = 0; q < NQ; ++q) {
         double x = 0.0;
-        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+        for (int b = threadIdx.x; b < blk.n; b += blockDim.x)
             x += __ldcg(&partials[q * max_blocks + b]);
         for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
         __syncthreads();

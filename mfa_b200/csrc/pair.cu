@@ -36,6 +36,8 @@
 // terms summed in FP32, the grid-wide sums in FP64), double in FP64 mode.
 #include "mfa_internal.cuh"
 
+#include <string.h>
+
 namespace {
 
 struct PairArgs {
@@ -257,7 +259,7 @@ constexpr int MAXPC = 16;   // staged slot runs (at most 9 neighbouring rows)
 // 48 registers in FP32 (40 resident warps per SM: one wave for ~190k
 // particles), 128 in FP64, where the doubled operands would otherwise spill
 template <typename R, int K, int FT>
-__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 2) k_pair(PairArgs a) {
+__device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
     typedef typename Vec4<R>::T R4;
     constexpr int QC = qcap<K>();
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -281,7 +283,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 2) k_pair(PairArgs a
     const int nx = a.nb[0], ny = a.nb[1], nz = a.nb[2];
     int p0, p1;
     if (a.rowmode) {
-        const int row = blockIdx.x;
+        const int row = blk.id;
         p0 = a.cell_start[nx * row];
         p1 = a.cell_start[nx * row + nx];
         // staging: the neighbouring rows (in the order the list builder scans
@@ -324,7 +326,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 2) k_pair(PairArgs a
             }
         }
     } else {
-        p0 = blockIdx.x * blockDim.x;
+        p0 = blk.id * blockDim.x;
         p1 = min(p0 + (int)blockDim.x, a.n);
         if (threadIdx.x == 0) { s_mode = 0; s_npc = 0; }
     }
@@ -546,10 +548,10 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 2) k_pair(PairArgs a
     if (WALL) {
         double acc[4] = {a.lj_energy_factor * (double)e_lj, a.lj_energy_factor * (double)vir, (double)e_c,
                          (double)e_w};
-        block_sum_commit<4>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_VFF);
+        block_sum_commit<4>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_VFF, blk);
     } else {
         double acc[3] = {a.lj_energy_factor * (double)e_lj, a.lj_energy_factor * (double)vir, (double)e_c};
-        block_sum_commit<3>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_VFF);
+        block_sum_commit<3>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_VFF, blk);
     }
 }
 #undef Lx
@@ -565,39 +567,67 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 2) k_pair(PairArgs a
 #undef ALC
 #undef ISP
 
+template <typename R, int K, int FT>
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 2) k_pair(PairArgs a) {
+    pair_body<R, K, FT>(a, plain_blk());
+}
+// one launch for several contexts (argument records in device memory)
+template <typename R, int K, int FT>
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 2)
+    k_pair_grouped(const PairArgs* __restrict__ as, const int* __restrict__ off, int nsys) {
+    const int s = group_of(off, nsys, blockIdx.x);
+    pair_body<R, K, FT>(as[s], group_blk(off, s));
+}
+
 // the feature sets the time-step fast path and the subroutine entry points
 // use, each compiled on its own
 constexpr int FT_SETS[] = {0, FT_DPD, FT_DPD | FT_WALL, FT_WALL, FT_LGV, FT_LGV | FT_WALL, FT_LGV | FT_QSEP,
                            FT_LGV | FT_QLJ, FT_DPD | FT_QSEP, FT_DPD | FT_QLJ};
 constexpr int N_FT_SETS = sizeof(FT_SETS) / sizeof(int);
 
+// a grouped launch: argument records in device memory, block offsets per context
+struct Group {
+    const PairArgs* args;
+    const int* off;
+    int nsys;
+};
+
+template <typename R, int K, int F>
+void launch_one(const PairArgs& a, const Group* g, int grid, int block, size_t smem, cudaStream_t st) {
+    if (g) k_pair_grouped<R, K, F><<<grid, block, smem, st>>>(g->args, g->off, g->nsys);
+    else k_pair<R, K, F><<<grid, block, smem, st>>>(a);
+}
+template <typename R, int K, int F>
+int attr_one(size_t smem) {
+    if (cudaFuncSetAttribute(k_pair<R, K, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_pair_grouped<R, K, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+        return MFA_ERR_CUDA;
+    return MFA_OK;
+}
+
 template <typename R, int K, int I>
 struct Dispatch {
-    static void run(int ft, const PairArgs& a, int grid, int block, size_t smem, cudaStream_t st) {
+    static void run(int ft, const PairArgs& a, const Group* g, int grid, int block, size_t smem, cudaStream_t st) {
         if (ft == FT_SETS[I]) {
-            k_pair<R, K, FT_SETS[I]><<<grid, block, smem, st>>>(a);
+            launch_one<R, K, FT_SETS[I]>(a, g, grid, block, smem, st);
             return;
         }
-        Dispatch<R, K, I - 1>::run(ft, a, grid, block, smem, st);
+        Dispatch<R, K, I - 1>::run(ft, a, g, grid, block, smem, st);
     }
     static int attr(size_t smem) {
-        if (cudaFuncSetAttribute(k_pair<R, K, FT_SETS[I]>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem) != cudaSuccess)
-            return MFA_ERR_CUDA;
+        const int rc = attr_one<R, K, FT_SETS[I]>(smem);
+        if (rc != MFA_OK) return rc;
         return Dispatch<R, K, I - 1>::attr(smem);
     }
 };
 template <typename R, int K>
 struct Dispatch<R, K, -1> {
-    static void run(int, const PairArgs& a, int grid, int block, size_t smem, cudaStream_t st) {
-        k_pair<R, K, FT_GENERIC><<<grid, block, smem, st>>>(a);
+    static void run(int, const PairArgs& a, const Group* g, int grid, int block, size_t smem, cudaStream_t st) {
+        launch_one<R, K, FT_GENERIC>(a, g, grid, block, smem, st);
     }
-    static int attr(size_t smem) {
-        if (cudaFuncSetAttribute(k_pair<R, K, FT_GENERIC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem) != cudaSuccess)
-            return MFA_ERR_CUDA;
-        return MFA_OK;
-    }
+    static int attr(size_t smem) { return attr_one<R, K, FT_GENERIC>(smem); }
 };
 
 template <typename R>
@@ -608,10 +638,10 @@ size_t smem_bytes(int k, int block, int tile_cap) {
 }
 
 template <typename R>
-int launch_r(int k, int ft, const PairArgs& a, int grid, int block, size_t smem, cudaStream_t st) {
+int launch_r(int k, int ft, const PairArgs& a, const Group* g, int grid, int block, size_t smem, cudaStream_t st) {
     switch (k) {
-        case 2: Dispatch<R, 2, N_FT_SETS - 1>::run(ft, a, grid, block, smem, st); break;
-        case 4: Dispatch<R, 4, N_FT_SETS - 1>::run(ft, a, grid, block, smem, st); break;
+        case 2: Dispatch<R, 2, N_FT_SETS - 1>::run(ft, a, g, grid, block, smem, st); break;
+        case 4: Dispatch<R, 4, N_FT_SETS - 1>::run(ft, a, g, grid, block, smem, st); break;
         default: return MFA_ERR_ARGS;
     }
     return MFA_OK;
@@ -643,17 +673,24 @@ int pair_set_shape(mfa_ctx* c, int k, int block, int tile_cap) {
     if (block < 32 || block > 256 || block % 32) return MFA_ERR_ARGS;
     if (tile_cap < 0) tile_cap = 0;
     if (tile_cap > pair_tile_limit(c)) tile_cap = pair_tile_limit(c);
-    const size_t smem = c->prec == MFA_MIXED ? smem_bytes<float>(k, block, tile_cap)
-                                             : smem_bytes<double>(k, block, tile_cap);
-    const int rc = c->prec == MFA_MIXED ? attr_r<float>(k, smem) : attr_r<double>(k, smem);
-    if (rc != MFA_OK) return rc;
+    // every instantiation admits the largest dynamic shared memory any shape
+    // uses (the attribute is per function, shared by all contexts and batches)
+    static bool admitted[2][5];
+    bool& done = admitted[c->prec == MFA_MIXED ? 0 : 1][k];
+    if (!done) {
+        const int rc = c->prec == MFA_MIXED ? attr_r<float>(k, SMEM_LIMIT) : attr_r<double>(k, SMEM_LIMIT);
+        if (rc != MFA_OK) return rc;
+        done = true;
+    }
     c->pair_tpp = k;
     c->pair_block = block;
     c->tile_cap = tile_cap;
     return MFA_OK;
 }
 
-int launch_pair(mfa_ctx* c, int fuse_wall) {
+// The pair kernel's argument record, grid, dynamic shared memory and feature set
+// for a context.
+int pair_stage_args(mfa_ctx* c, int fuse_wall, void* out, int* grid_out, size_t* smem_out, int* ft_out) {
     if (!c->lists_valid) return MFA_ERR_STATE;
     PairArgs a;
     a.pos_s = c->pos_s; a.vel_s = c->vel_s; a.nbr = c->nbr; a.nnb = c->nnb;
@@ -704,8 +741,33 @@ int launch_pair(mfa_ctx* c, int fuse_wall) {
     if (p.charged) ft |= a.real_in_lj ? FT_QLJ : FT_QSEP;
     if (p.force_switch_on) ft |= FT_FSW;
     if (a.fuse_wall) ft |= FT_WALL;
-    const int rc = c->prec == MFA_MIXED ? launch_r<float>(c->pair_tpp, ft, a, grid, c->pair_block, smem, c->st)
-                                        : launch_r<double>(c->pair_tpp, ft, a, grid, c->pair_block, smem, c->st);
+    memcpy(out, &a, sizeof(a));
+    *grid_out = grid;
+    *smem_out = smem;
+    *ft_out = ft;
+    return MFA_OK;
+}
+
+size_t pair_args_bytes() { return sizeof(PairArgs); }
+
+int launch_pair_grouped(int prec, int k, int block, int ft, const void* dargs, const int* doff, int nsys, int grid,
+                        size_t smem, cudaStream_t st) {
+    Group g{(const PairArgs*)dargs, doff, nsys};
+    PairArgs dummy;
+    const int rc = prec == MFA_MIXED ? launch_r<float>(k, ft, dummy, &g, grid, block, smem, st)
+                                     : launch_r<double>(k, ft, dummy, &g, grid, block, smem, st);
+    if (rc != MFA_OK) return rc;
+    MFA_CUDA_TRY(cudaGetLastError());
+    return MFA_OK;
+}
+
+int launch_pair(mfa_ctx* c, int fuse_wall) {
+    PairArgs a;
+    int grid, ft;
+    size_t smem;
+    TRY_(pair_stage_args(c, fuse_wall, &a, &grid, &smem, &ft));
+    const int rc = c->prec == MFA_MIXED ? launch_r<float>(c->pair_tpp, ft, a, nullptr, grid, c->pair_block, smem, c->st)
+                                        : launch_r<double>(c->pair_tpp, ft, a, nullptr, grid, c->pair_block, smem, c->st);
     if (rc != MFA_OK) return rc;
     MFA_CUDA_TRY(cudaGetLastError());
     note_launch(c, 1);
