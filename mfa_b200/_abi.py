@@ -139,6 +139,8 @@ SIGNATURES = {
     "mfa_batch_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "mfa_batch_launches": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "mfa_batch_destroy": (C.c_int, [_P]),
+    "mfa_trajectory_observable": (C.c_int, [_P, C.c_int32, _DP]),
+    "mfa_adjoint": (C.c_int, [_P, C.c_int32, C.c_int32, _DP]),
 }
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libmfa_gpu.so")

@@ -176,6 +176,21 @@ class System:
         for d in range(3):
             self.params.n_bin[d] = int(n_bin[d])
 
+    # ---- trajectory sensitivities ----
+    GRAD_NAMES = ("eps_lj", "sigma", "k_fene", "r0", "gamma_dpd", "eps_wall")
+
+    def trajectory_observable(self, nsteps: int) -> float:
+        """J = time average over nsteps steps of <z> + <R_ee^2> (the state advances)."""
+        j = C.c_double(0.0)
+        check(self.lib.mfa_trajectory_observable(self.ctx, int(nsteps), C.byref(j)), "mfa_trajectory_observable")
+        return float(j.value)
+
+    def adjoint(self, nsteps: int, every: int = 20):
+        """(J, {parameter: dJ/dparameter}) by the hand-written adjoint (the state advances)."""
+        out = (C.c_double * 7)()
+        check(self.lib.mfa_adjoint(self.ctx, int(nsteps), int(every), out), "mfa_adjoint")
+        return float(out[0]), {k: float(out[1 + i]) for i, k in enumerate(self.GRAD_NAMES)}
+
     # ---- mirrors ----
     def stream_ptr(self) -> int:
         """cudaStream_t of the context (for event timing on the launching stream)."""

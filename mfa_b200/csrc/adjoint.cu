@@ -1,0 +1,580 @@
+// Adjoint of the time-step loop: gradients of a trajectory observable with
+// respect to the force-field parameters, by reverse-mode differentiation of
+// the discrete velocity-Verlet map that mfa_step runs.
+//
+// Forward step n -> n+1 (verlet_positions, forces, verlet_velocities):
+//   r' = r + dt v + dt^2/2 a          u = v + dt/2 a         (half-step velocity)
+//   F' = F(r', u; theta, noise of step n+1)                  (DPD uses u)
+//   a' = F'/m                          v' = u + dt/2 a'       (pinned heads: v' = a' = 0)
+// Observable J = 1/S sum_{s=1..S} O(r_s), O = <z> (all beads) + <R_ee^2> (chains).
+// Backward step n+1 -> n, with rho, nu, alpha the adjoints of r, v, a:
+//   lam_F = (alpha' + dt/2 nu') / m,  lam_u = nu'            (heads: 0)
+//   lam_r = rho' + (dF/dr')^T lam_F,  lam_u += (dF/du)^T lam_F,  g += (dF/dtheta)^T lam_F
+//   rho = lam_r + 1/S dO/dr (s >= 1),  nu = dt lam_r + lam_u,  alpha = dt^2/2 lam_r + dt/2 lam_u
+// The vector-Jacobian products are written out by hand for every force term
+// of the path: WCA/LJ and DPD pairs (half list, Newton's third law), FENE bonds
+// (with the clamp of intra_molec.f90:248) and the 9-3 walls.  The forward
+// states are recomputed segment by segment from checkpoints every K steps, with
+// the DPD noise replayed: Philox is keyed by (step, pair), so the recomputed
+// forces are those of the first pass.
+//
+// theta = (eps_LJ, sigma, k_FENE, R0, gamma_DPD, eps_wall), defined as:
+//   eps_LJ    all pair epsilons scale with it (epsil = 4 eps e_ij)
+//   sigma     all pair sigmas scale with it (sigma_2, range_2 = (2^(1/6) sigma)^2,
+//             hence the DPD range); the wall's sigma_wall is not changed
+//   k_FENE    k_chain = k R0^2;      R0: r_chain_2 = R0^2 (and k_chain = k R0^2)
+//   gamma     friction, and sig = sqrt(2 kT gamma / dt)
+//   eps_wall  a_wall of every particle type (and a_w)
+#include "mfa_internal.cuh"
+
+#include <math.h>
+#include <string.h>
+#include <vector>
+
+namespace {
+
+enum { G_EPS = 0, G_SIG = 1, G_K = 2, G_R0 = 3, G_GAM = 4, G_WALL = 5, G_N = 6 };
+
+struct AdjArgs {
+    const void* pos_s;            // sorted records of r' (w: id << 8 | type)
+    const void* vel_s;            // sorted records of u
+    const int32_t* __restrict__ nbr;
+    const int32_t* __restrict__ nnb;
+    const double* tabs;           // list radius, range_2, epsil, sigma_2, e_shift, inv_range_2
+    const double *fx, *fy, *fz;   // lam_F (particle order)
+    double *rx, *ry, *rz;         // lam_r accumulators
+    double *ux, *uy, *uz;         // lam_u accumulators
+    double* g;                    // G_N parameter gradient sums
+    int n, half, symmetry, dpd, dpd_weight, noise, wall;
+    double L[3], invL[3];
+    double sig, gam, eps_lj, sigma_lj;
+    long long step;
+    PhiloxKeys key;
+    double a_wall[T8], sigma_wall[T8], z_space_wall, wall_cut;
+};
+
+template <typename R> struct V4;
+template <> struct V4<float> { typedef float4 T; };
+template <> struct V4<double> { typedef double4 T; };
+
+__device__ __forceinline__ float rsq(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double rsq(double x) { return 1.0 / sqrt(x); }
+__device__ __forceinline__ float mi(float d, float L, float iL) { return fmaf(-L, truncf(2.0f * d * iL), d); }
+__device__ __forceinline__ double mi(double d, double L, double iL) { return d - L * (double)(int)(2.0 * d * iL); }
+
+// the DPD variate of a pair, exactly as the pair kernel draws it
+__device__ __forceinline__ float dpd_noise(uint32_t x0, uint32_t x1, int shape, float) {
+    if (shape == MFA_NOISE_UNIFORM) {
+        const float u = (float)(x0 >> 9) * 1.1920928955078125e-07f + 5.9604644775390625e-08f;
+        return 1.7320508075688772f * (2.0f * u - 1.0f);
+    }
+    const float u1 = fmaf((float)x0, 2.3283064365386963e-10f, 1.16415321826934814e-10f);
+    const float u2 = fmaf((float)x1, 2.3283064365386963e-10f, 1.16415321826934814e-10f);
+    const float s = -2.0f * __logf(u1);
+    const float r = s > 0.0f ? s * rsqrtf(s) : 0.0f;
+    return -r * __cosf(fmaf(6.283185307179586f, u2, -3.14159265358979f));
+}
+__device__ __forceinline__ double dpd_noise(uint32_t x0, uint32_t x1, int shape, double) {
+    if (shape == MFA_NOISE_UNIFORM) {
+        const float u = (float)(x0 >> 9) * 1.1920928955078125e-07f + 5.9604644775390625e-08f;
+        return (double)(1.7320508075688772f * (2.0f * u - 1.0f));
+    }
+    const double u1 = ((double)x0 + 0.5) * 2.3283064365386963e-10;
+    const double u2 = ((double)x1 + 0.5) * 2.3283064365386963e-10;
+    return sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+}
+
+__device__ __forceinline__ void warp_add_g(double* g, double (&gl)[G_N]) {
+#pragma unroll
+    for (int q = 0; q < G_N; ++q) {
+        double x = gl[q];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31) == 0 && x != 0.0) atomicAdd(&g[q], x);
+    }
+}
+
+// Pair and wall VJP: thread per owner slot, over its list row.
+template <typename R>
+__global__ void k_adj_pair(AdjArgs a) {
+    typedef typename V4<R>::T R4;
+    __shared__ double s_rc2[T8 * T8], s_eps[T8 * T8], s_sig2[T8 * T8], s_irc2[T8 * T8];
+    for (int k = threadIdx.x; k < T8 * T8; k += blockDim.x) {
+        s_rc2[k] = a.tabs[1 * T8 * T8 + k];
+        s_eps[k] = a.tabs[2 * T8 * T8 + k];
+        s_sig2[k] = a.tabs[3 * T8 * T8 + k];
+        s_irc2[k] = a.tabs[5 * T8 * T8 + k];
+    }
+    __syncthreads();
+    double gl[G_N] = {0, 0, 0, 0, 0, 0};
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < a.n) {
+        const R4* ps = (const R4*)a.pos_s;
+        const R4* vs = (const R4*)a.vel_s;
+        const R4 pi = ps[t], ui = vs[t];
+        const int wi = wbits(pi.w), ii = wi >> 8, ti = wi & 0xff;
+        const R lfx = (R)a.fx[ii], lfy = (R)a.fy[ii], lfz = (R)a.fz[ii];
+        R orx = 0, ory = 0, orz = 0, oux = 0, ouy = 0, ouz = 0;   // owner's lam_r, lam_u
+        const R Lx = (R)a.L[0], Ly = (R)a.L[1], Lz = (R)a.L[2];
+        const R iLx = (R)a.invL[0], iLy = (R)a.invL[1], iLz = (R)a.invL[2];
+        const R sg = (R)a.sig, gm = (R)a.gam;
+        const int m = a.nnb[t];
+        for (int k = 0; k < m; ++k) {
+            const int s = a.nbr[(size_t)k * a.n + t];
+            const R4 pj = ps[s];
+            R dx = mi(pi.x - pj.x, Lx, iLx), dy = mi(pi.y - pj.y, Ly, iLy), dz = pi.z - pj.z;
+            if (a.symmetry == 1) dz = mi(dz, Lz, iLz);
+            const R r2 = dx * dx + dy * dy + dz * dz;
+            const int wj = wbits(pj.w), jj = wj >> 8, ij = (ti - 1) * T8 + (wj & 0xff) - 1;
+            if (!(r2 < (R)s_rc2[ij])) continue;
+            // the pair force G acts on i (+G) and, with the half list, on j (-G):
+            // dl = lam_F_i - lam_F_j (half list) or lam_F_i (full list: j has its own row)
+            R dlx = lfx, dly = lfy, dlz = lfz;
+            if (a.half) { dlx -= (R)a.fx[jj]; dly -= (R)a.fy[jj]; dlz -= (R)a.fz[jj]; }
+            const R ddl = dx * dlx + dy * dly + dz * dlz;
+            // LJ: G = fs(r2) d, fs = eps (12 r12 - 6 r6) / r2
+            const R eps = (R)s_eps[ij], ir2 = (R)1 / r2;
+            const R r61 = (R)s_sig2[ij] * ir2, r6 = r61 * r61 * r61, r12 = r6 * r6;
+            const R fs = eps * ((R)12 * r12 - (R)6 * r6) * ir2;
+            const R dfs = eps * ((R)-84 * r12 + (R)24 * r6) * ir2 * ir2;   // d fs / d r2
+            R gx = fs * dlx + (R)2 * dfs * ddl * dx;
+            R gy = fs * dly + (R)2 * dfs * ddl * dy;
+            R gz = fs * dlz + (R)2 * dfs * ddl * dz;
+            gl[G_EPS] += (double)(fs * ddl) / a.eps_lj;
+            gl[G_SIG] += (double)(eps * ((R)144 * r12 - (R)36 * r6) * ir2 * ddl) / a.sigma_lj;
+            if (a.dpd) {
+                // DPD: G = P rhat, P = sig w_r g - gamma w_d (du . rhat), w_d = w_r^2
+                const R4 uj = vs[s];
+                const R dux = ui.x - uj.x, duy = ui.y - uj.y, duz = ui.z - uj.z;
+                const R ir = rsq(r2), r = r2 * ir;
+                const R hx = dx * ir, hy = dy * ir, hz = dz * ir;
+                const R sdu = dux * hx + duy * hy + duz * hz;
+                const R hdl = hx * dlx + hy * dly + hz * dlz;
+                const uint32_t lo = (uint32_t)min(ii, jj), hi = (uint32_t)max(ii, jj);
+                const uint4 ph = philox4x32_10(make_uint4(lo, hi, (uint32_t)a.step, TAG_DPD), a.key);
+                const R gn = dpd_noise(ph.x, ph.y, a.noise, R(0));
+                const R irc = sqrt((R)s_irc2[ij]);
+                R wr, wd, dwr, dwd;                  // weights and d/dr
+                if (a.dpd_weight == 1) { wr = 1; wd = 1; dwr = 0; dwd = 0; }
+                else { wr = (R)1 - r * irc; wd = wr * wr; dwr = -irc; dwd = (R)2 * wr * dwr; }
+                const R P = sg * wr * gn - gm * wd * sdu;
+                const R dP = sg * dwr * gn - gm * dwd * sdu;          // dP/dr at fixed du . rhat
+                // (dG/dd)^T dl = hdl [dP rhat - gamma w_d (du - sdu rhat) / r] + P/r (dl - hdl rhat)
+                const R c1 = hdl * dP, c2 = -hdl * gm * wd * ir, c3 = P * ir;
+                gx += c1 * hx + c2 * (dux - sdu * hx) + c3 * (dlx - hdl * hx);
+                gy += c1 * hy + c2 * (duy - sdu * hy) + c3 * (dly - hdl * hy);
+                gz += c1 * hz + c2 * (duz - sdu * hz) + c3 * (dlz - hdl * hz);
+                // (dG/d du)^T dl = -gamma w_d hdl rhat
+                const R cu = -gm * wd * hdl;
+                oux += cu * hx; ouy += cu * hy; ouz += cu * hz;
+                atomicAdd(&a.ux[jj], -(double)(cu * hx));
+                atomicAdd(&a.uy[jj], -(double)(cu * hy));
+                atomicAdd(&a.uz[jj], -(double)(cu * hz));
+                // gamma (friction and the noise amplitude sqrt(2 kT gamma / dt))
+                gl[G_GAM] += (double)((sg * (R)0.5 / gm * wr * gn - wd * sdu) * hdl);
+                // sigma through the DPD range: d w_r / d sigma = (r / rc) / sigma
+                if (a.dpd_weight != 1) {
+                    const R dws = r * irc / (R)a.sigma_lj;
+                    gl[G_SIG] += (double)((sg * dws * gn - gm * (R)2 * wr * dws * sdu) * hdl);
+                }
+            }
+            // G depends on d = r_i - r_j: both positions, whichever side it acts on
+            orx += gx; ory += gy; orz += gz;
+            atomicAdd(&a.rx[jj], -(double)gx);
+            atomicAdd(&a.ry[jj], -(double)gy);
+            atomicAdd(&a.rz[jj], -(double)gz);
+        }
+        if (a.wall == 2) {
+            // 9-3 walls (fluid_wall.f90:96-121): F_z += f(z) - f(Z - z), f = A phi(z)
+            const R sw = (R)a.sigma_wall[ti - 1], aw = (R)a.a_wall[ti - 1], cut = (R)a.wall_cut;
+            const R sw3 = sw * sw * sw, sw9 = sw3 * sw3 * sw3;
+            const R zb = pi.z, zt = (R)a.z_space_wall - pi.z;
+            R dfz = 0, phi = 0;
+            if (cut <= 0 || zb < cut) {
+                const R iz = (R)1 / zb, iz2 = iz * iz, iz4 = iz2 * iz2, iz5 = iz4 * iz, iz10 = iz5 * iz5;
+                phi += (R)9 * sw9 * iz10 - (R)3 * sw3 * iz4;
+                dfz += aw * ((R)-90 * sw9 * iz10 * iz + (R)12 * sw3 * iz5);
+            }
+            if (cut <= 0 || zt < cut) {
+                const R iz = (R)1 / zt, iz2 = iz * iz, iz4 = iz2 * iz2, iz5 = iz4 * iz, iz10 = iz5 * iz5;
+                phi -= (R)9 * sw9 * iz10 - (R)3 * sw3 * iz4;
+                dfz += aw * ((R)-90 * sw9 * iz10 * iz + (R)12 * sw3 * iz5);   // d/dz of -f(Z - z)
+            }
+            orz += dfz * lfz;
+            if (aw != (R)0) gl[G_WALL] += (double)(phi * lfz);
+        }
+        atomicAdd(&a.rx[ii], (double)orx);
+        atomicAdd(&a.ry[ii], (double)ory);
+        atomicAdd(&a.rz[ii], (double)orz);
+        if (a.dpd) {
+            atomicAdd(&a.ux[ii], (double)oux);
+            atomicAdd(&a.uy[ii], (double)ouy);
+            atomicAdd(&a.uz[ii], (double)ouz);
+        }
+    }
+    warp_add_g(a.g, gl);
+}
+
+struct AdjBondArgs {
+    const double *px, *py, *pz;   // r' (particle order)
+    const double *fx, *fy, *fz;   // lam_F
+    double *rx, *ry, *rz;         // lam_r accumulators
+    double* g;
+    int n_chain, n_mon, n_chain_d, n_mon_d, part_init_d, symmetry;
+    double L[3], invL[3];
+    double k_fene, r0, inv_r_chain_2, fene_clamp;
+};
+
+// FENE VJP, thread per bond (i, i+1): G = -fs d on i, +fs d on i+1, d = r_i - r_{i+1},
+// fs = k / (1 - x), x = min(r^2 / R0^2, clamp)
+template <typename R>
+__global__ void k_adj_fene(AdjBondArgs a) {
+    double gl[G_N] = {0, 0, 0, 0, 0, 0};
+    const int nb1 = a.n_chain * (a.n_mon - 1);
+    const int nb2 = a.n_mon_d >= 2 ? a.n_chain_d * (a.n_mon_d - 1) : 0;
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < nb1 + nb2) {
+        int i;
+        if (b < nb1) i = (b / (a.n_mon - 1)) * a.n_mon + b % (a.n_mon - 1);
+        else i = a.part_init_d + ((b - nb1) / (a.n_mon_d - 1)) * a.n_mon_d + (b - nb1) % (a.n_mon_d - 1);
+        const int j = i + 1;
+        const R dx = (R)mi(a.px[i] - a.px[j], a.L[0], a.invL[0]);
+        const R dy = (R)mi(a.py[i] - a.py[j], a.L[1], a.invL[1]);
+        const double dz64 = a.pz[i] - a.pz[j];
+        const R dz = (R)(a.symmetry == 1 ? mi(dz64, a.L[2], a.invL[2]) : dz64);
+        const R irc2 = (R)a.inv_r_chain_2;
+        R x = (dx * dx + dy * dy + dz * dz) * irc2;
+        const bool clamped = x >= (R)a.fene_clamp;
+        if (clamped) x = (R)a.fene_clamp;
+        const R k = (R)a.k_fene;
+        const R fs = k / ((R)1 - x);
+        const R fsx = clamped ? (R)0 : k / (((R)1 - x) * ((R)1 - x));       // d fs / d x
+        // coefficient of fs d: dl = lam_F_{i+1} - lam_F_i
+        const R dlx = (R)(a.fx[j] - a.fx[i]), dly = (R)(a.fy[j] - a.fy[i]), dlz = (R)(a.fz[j] - a.fz[i]);
+        const R ddl = dx * dlx + dy * dly + dz * dlz;
+        const R c = (R)2 * irc2 * fsx * ddl;
+        const R gx = fs * dlx + c * dx, gy = fs * dly + c * dy, gz = fs * dlz + c * dz;
+        atomicAdd(&a.rx[i], (double)gx); atomicAdd(&a.ry[i], (double)gy); atomicAdd(&a.rz[i], (double)gz);
+        atomicAdd(&a.rx[j], -(double)gx); atomicAdd(&a.ry[j], -(double)gy); atomicAdd(&a.rz[j], -(double)gz);
+        gl[G_K] += (double)(fs * ddl) / a.k_fene;
+        if (!clamped) gl[G_R0] += (double)(fsx * ((R)-2 * x / (R)a.r0) * ddl);
+    }
+    warp_add_g(a.g, gl);
+}
+
+// lam_F = (alpha' + dt/2 nu') / m, lam_u = nu', lam_r = rho' (pinned heads: 0)
+__global__ void k_adj_prep(int n, const double* __restrict__ rho, const double* __restrict__ nu,
+                           const double* __restrict__ alpha, const double* __restrict__ inv_mass, double hdt,
+                           int pin_heads, int n_head_span, int n_mon, double* lamF, double* lamU, double* lamR) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const bool head = pin_heads && i < n_head_span && (i % n_mon) == 0;
+    for (int d = 0; d < 3; ++d) {
+        const size_t k = (size_t)d * n + i;
+        lamF[k] = head ? 0.0 : (alpha[k] + hdt * nu[k]) * inv_mass[i];
+        lamU[k] = head ? 0.0 : nu[k];
+        lamR[k] = rho[k];
+    }
+}
+
+// rho = lam_r + w dO/dr(r), nu = dt lam_r + lam_u, alpha = dt^2/2 lam_r + dt/2 lam_u
+// dO/dr: <z> over all beads (1/n on z), <R_ee^2> over the chains (ends)
+__global__ void k_adj_combine(int n, const double* __restrict__ lamR, const double* __restrict__ lamU, double dt,
+                              double w_obs, const double* __restrict__ r, const int32_t* __restrict__ mic,
+                              double Lx, double Ly, double Lz, int n_chain, int n_mon, int pin_heads,
+                              double* rho, double* nu, double* alpha) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const bool head = pin_heads && i < n_chain * n_mon && (i % n_mon) == 0;
+    double o[3] = {0.0, 0.0, 0.0};
+    if (w_obs != 0.0) {
+        o[2] = w_obs / (double)n;
+        if (n_chain > 0 && n_mon > 1 && i < n_chain * n_mon) {
+            const int p = i % n_mon;
+            if (p == 0 || p == n_mon - 1) {
+                const int f = i - p, e = f + n_mon - 1;
+                const double L[3] = {Lx, Ly, Lz};
+                const double s = (p == 0 ? -2.0 : 2.0) * w_obs / (double)n_chain;
+                for (int d = 0; d < 3; ++d) {
+                    const double R = (r[(size_t)d * n + e] + L[d] * mic[(size_t)d * n + e]) -
+                                     (r[(size_t)d * n + f] + L[d] * mic[(size_t)d * n + f]);
+                    o[d] += s * R;
+                }
+            }
+        }
+    }
+    for (int d = 0; d < 3; ++d) {
+        const size_t k = (size_t)d * n + i;
+        const double lr = lamR[k], lu = lamU[k];
+        rho[k] = lr + o[d];
+        nu[k] = head ? 0.0 : dt * lr + lu;
+        alpha[k] = head ? 0.0 : 0.5 * dt * dt * lr + 0.5 * dt * lu;
+    }
+}
+
+// O(r) = <z> + <R_ee^2> of the current state, added (times w) to out[0]
+__global__ void k_observable(int n, const double* __restrict__ rx, const double* __restrict__ ry,
+                             const double* __restrict__ rz, const int32_t* __restrict__ mx,
+                             const int32_t* __restrict__ my, const int32_t* __restrict__ mz, double Lx, double Ly,
+                             double Lz, int n_chain, int n_mon, double w, double* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0.0;
+    if (i < n) v += rz[i] / (double)n;
+    if (i < n_chain && n_mon > 1) {
+        const int f = i * n_mon, e = f + n_mon - 1;
+        const double X = (rx[e] + Lx * mx[e]) - (rx[f] + Lx * mx[f]);
+        const double Y = (ry[e] + Ly * my[e]) - (ry[f] + Ly * my[f]);
+        const double Z = (rz[e] + Lz * mz[e]) - (rz[f] + Lz * mz[f]);
+        v += (X * X + Y * Y + Z * Z) / (double)n_chain;
+    }
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(out, w * v);
+}
+
+constexpr int T = 256;
+
+struct Work {
+    int n, S, K, nseg;
+    double* ck;          // checkpoints: nseg x (r, v, a) 9n doubles
+    int32_t* ckm;        // checkpoints: nseg x mic 3n
+    int64_t* ckstep;     // host copy of dstep per checkpoint
+    double* seg_r;       // K x 3n (r after the position half of each step)
+    double* seg_u;       // K x 3n (u)
+    int32_t* seg_m;      // K x 3n (mic)
+    double *rho, *nu, *alpha, *lamF, *lamU, *lamR;   // 3n each
+    double* dg;          // G_N + 1 (J)
+};
+
+int adj_forward_step(mfa_ctx* c, double* sr, double* su, int32_t* sm, double w, double* dJ) {
+    const int n = c->n;
+    TRY_(launch_vv_positions(c, 1, 1));
+    if (sr) {
+        MFA_CUDA_TRY(cudaMemcpyAsync(sr, c->rx, (size_t)3 * n * 8, cudaMemcpyDeviceToDevice, c->st));
+        MFA_CUDA_TRY(cudaMemcpyAsync(su, c->vx, (size_t)3 * n * 8, cudaMemcpyDeviceToDevice, c->st));
+        MFA_CUDA_TRY(cudaMemcpyAsync(sm, c->mx, (size_t)3 * n * 4, cudaMemcpyDeviceToDevice, c->st));
+    }
+    TRY_(launch_rebuild(c, c->bin_type, 1));
+    TRY_(launch_pair(c, c->p.symmetry == 0));
+    TRY_(launch_vv_velocities(c, 1));
+    if (dJ) {
+        const mfa_params& p = c->p;
+        k_observable<<<(n + T - 1) / T, T, 0, c->st>>>(n, c->rx, c->ry, c->rz, c->mx, c->my, c->mz,
+                                                         p.boundary[0], p.boundary[1], p.boundary[2], p.n_chain,
+                                                         p.n_mon, w, dJ);
+        MFA_CUDA_TRY(cudaGetLastError());
+    }
+    return MFA_OK;
+}
+
+int checkpoint_save(mfa_ctx* c, Work& w, int k) {
+    const size_t n3 = (size_t)3 * c->n;
+    MFA_CUDA_TRY(cudaMemcpyAsync(w.ck + k * 3 * n3, c->rx, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
+    MFA_CUDA_TRY(cudaMemcpyAsync(w.ck + k * 3 * n3 + n3, c->vx, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
+    MFA_CUDA_TRY(cudaMemcpyAsync(w.ck + k * 3 * n3 + 2 * n3, c->ax, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
+    MFA_CUDA_TRY(cudaMemcpyAsync(w.ckm + k * n3, c->mx, n3 * 4, cudaMemcpyDeviceToDevice, c->st));
+    MFA_CUDA_TRY(cudaMemcpyAsync(&w.ckstep[k], c->dstep, 8, cudaMemcpyDeviceToHost, c->st));
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    return MFA_OK;
+}
+
+int checkpoint_restore(mfa_ctx* c, Work& w, int k) {
+    const size_t n3 = (size_t)3 * c->n;
+    MFA_CUDA_TRY(cudaMemcpyAsync(c->rx, w.ck + k * 3 * n3, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
+    MFA_CUDA_TRY(cudaMemcpyAsync(c->vx, w.ck + k * 3 * n3 + n3, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
+    MFA_CUDA_TRY(cudaMemcpyAsync(c->ax, w.ck + k * 3 * n3 + 2 * n3, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
+    MFA_CUDA_TRY(cudaMemcpyAsync(c->mx, w.ckm + k * n3, n3 * 4, cudaMemcpyDeviceToDevice, c->st));
+    MFA_CUDA_TRY(cudaMemcpyAsync(c->dstep, &w.ckstep[k], 8, cudaMemcpyHostToDevice, c->st));
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    // lists for the restored positions
+    return mfa_binning(c);
+}
+
+AdjArgs pair_adj_args(mfa_ctx* c, Work& w, long long step) {
+    const mfa_params& p = c->p;
+    const int n = c->n;
+    AdjArgs a;
+    a.pos_s = c->pos_s; a.vel_s = c->vel_s; a.nbr = c->nbr; a.nnb = c->nnb; a.tabs = c->tabs;
+    a.fx = w.lamF; a.fy = w.lamF + n; a.fz = w.lamF + 2 * n;
+    a.rx = w.lamR; a.ry = w.lamR + n; a.rz = w.lamR + 2 * n;
+    a.ux = w.lamU; a.uy = w.lamU + n; a.uz = w.lamU + 2 * n;
+    a.g = w.dg;
+    a.n = n;
+    a.half = c->bin_type == 0;
+    a.symmetry = p.symmetry;
+    a.dpd = p.thermostat == MFA_THERMO_DPD;
+    a.dpd_weight = p.dpd_weight;
+    a.noise = p.noise;
+    a.wall = (p.symmetry == 0 && p.wall == 2) ? 2 : 0;
+    for (int d = 0; d < 3; ++d) { a.L[d] = p.boundary[d]; a.invL[d] = c->inv_boundary[d]; }
+    a.sig = p.sig; a.gam = p.friction;
+    // the physical eps and sigma the pair tables scale with: the largest pair's
+    double emax = 0.0, smax = 0.0;
+    for (int k = 0; k < T8 * T8; ++k)
+        if (p.range_2[k] > 0.0) { emax = fmax(emax, p.epsil[k] / 4.0); smax = fmax(smax, sqrt(p.sigma_2[k])); }
+    a.eps_lj = emax > 0.0 ? emax : 1.0;
+    a.sigma_lj = smax > 0.0 ? smax : 1.0;
+    a.step = step;
+    a.key = philox_round_keys((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
+    for (int k = 0; k < T8; ++k) { a.a_wall[k] = p.a_wall[k]; a.sigma_wall[k] = p.sigma_wall[k]; }
+    a.z_space_wall = p.z_space_wall;
+    a.wall_cut = p.wall_cut;
+    return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mfa_trajectory_observable(mfa_ctx* c, int32_t nsteps, double* J) {
+    if (!c || nsteps < 1 || !J) return MFA_ERR_ARGS;
+    if (!c->lists_valid) TRY_(mfa_binning(c));
+    double* dJ = nullptr;
+    if (cudaMalloc((void**)&dJ, 8) != cudaSuccess) return MFA_ERR_NOMEM;
+    int rc = MFA_OK;
+    if (cudaMemsetAsync(dJ, 0, 8, c->st) != cudaSuccess) rc = MFA_ERR_CUDA;
+    for (int s = 0; s < nsteps && rc == MFA_OK; ++s) rc = adj_forward_step(c, nullptr, nullptr, nullptr, 1.0 / nsteps, dJ);
+    if (rc == MFA_OK && (cudaMemcpyAsync(J, dJ, 8, cudaMemcpyDeviceToHost, c->st) != cudaSuccess ||
+                         cudaStreamSynchronize(c->st) != cudaSuccess))
+        rc = MFA_ERR_CUDA;
+    cudaFree(dJ);
+    if (rc == MFA_OK) c->i_time += nsteps;
+    if (rc != MFA_OK) return rc;
+    return mfa_sync(c);
+}
+
+int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
+    if (!c || nsteps < 1 || every < 1 || !out) return MFA_ERR_ARGS;
+    const mfa_params& p = c->p;
+    // the force terms differentiated here: pair (LJ/WCA, DPD), FENE, 9-3 walls
+    if (p.charged || p.thermostat == MFA_THERMO_LGV || p.bending || p.force_switch_on ||
+        (p.symmetry == 0 && (p.wall == 3 || p.wall == 4)) || (p.n_chain_d > 0 && p.n_mon_d >= 2))
+        return MFA_ERR_UNSUPPORTED;
+    if (!c->lists_valid) TRY_(mfa_binning(c));
+    const int n = c->n;
+    const size_t n3 = (size_t)3 * n;
+    Work w;
+    w.n = n; w.S = nsteps; w.K = every < nsteps ? every : nsteps;
+    w.nseg = (nsteps + w.K - 1) / w.K;
+    std::vector<int64_t> steps(w.nseg);
+    w.ckstep = steps.data();
+    void* bufs[9] = {nullptr};
+    size_t sizes[9] = {(size_t)w.nseg * 3 * n3 * 8, (size_t)w.nseg * n3 * 4, (size_t)w.K * n3 * 8,
+                       (size_t)w.K * n3 * 8, (size_t)w.K * n3 * 4, 6 * n3 * 8, (G_N + 1) * 8, 0, 0};
+    int rc = MFA_OK;
+    for (int k = 0; k < 7 && rc == MFA_OK; ++k)
+        if (cudaMalloc(&bufs[k], sizes[k]) != cudaSuccess) rc = MFA_ERR_NOMEM;
+    if (rc != MFA_OK) {
+        for (void* b : bufs) if (b) cudaFree(b);
+        return rc;
+    }
+    w.ck = (double*)bufs[0]; w.ckm = (int32_t*)bufs[1];
+    w.seg_r = (double*)bufs[2]; w.seg_u = (double*)bufs[3]; w.seg_m = (int32_t*)bufs[4];
+    double* adj = (double*)bufs[5];
+    w.rho = adj; w.nu = adj + n3; w.alpha = adj + 2 * n3; w.lamF = adj + 3 * n3; w.lamU = adj + 4 * n3;
+    w.lamR = adj + 5 * n3;
+    w.dg = (double*)bufs[6];
+    double* dJ = w.dg + G_N;
+    const double dt = p.dt, wobs = 1.0 / nsteps;
+    const int nb = (n + T - 1) / T;
+    auto run = [&]() -> int {
+        TRY_(mfa_sync(c));
+        MFA_CUDA_TRY(cudaMemsetAsync(w.dg, 0, (G_N + 1) * 8, c->st));
+        MFA_CUDA_TRY(cudaMemsetAsync(adj, 0, 6 * n3 * 8, c->st));
+        // forward pass with checkpoints and the observable
+        for (int s = 0; s < nsteps; ++s) {
+            if (s % w.K == 0) TRY_(checkpoint_save(c, w, s / w.K));
+            TRY_(adj_forward_step(c, nullptr, nullptr, nullptr, wobs, dJ));
+        }
+        TRY_(mfa_sync(c));
+        // rho_S = 1/S dO/dr_S (nu_S = alpha_S = 0)
+        k_adj_combine<<<nb, T, 0, c->st>>>(n, w.lamR, w.lamU, dt, wobs, c->rx, c->mx, p.boundary[0], p.boundary[1],
+                                           p.boundary[2], p.n_chain, p.n_mon, p.pin_heads, w.rho, w.nu, w.alpha);
+        MFA_CUDA_TRY(cudaGetLastError());
+        // the final state of the trajectory, restored at the end
+        std::vector<double> fin_rva(3 * n3);
+        std::vector<int32_t> fin_m(n3);
+        int64_t fin_step = 0;
+        MFA_CUDA_TRY(cudaMemcpyAsync(fin_rva.data(), c->rx, n3 * 8, cudaMemcpyDeviceToHost, c->st));
+        MFA_CUDA_TRY(cudaMemcpyAsync(fin_rva.data() + n3, c->vx, n3 * 8, cudaMemcpyDeviceToHost, c->st));
+        MFA_CUDA_TRY(cudaMemcpyAsync(fin_rva.data() + 2 * n3, c->ax, n3 * 8, cudaMemcpyDeviceToHost, c->st));
+        MFA_CUDA_TRY(cudaMemcpyAsync(fin_m.data(), c->mx, n3 * 4, cudaMemcpyDeviceToHost, c->st));
+        MFA_CUDA_TRY(cudaMemcpyAsync(&fin_step, c->dstep, 8, cudaMemcpyDeviceToHost, c->st));
+        MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+        // backward, segment by segment
+        for (int seg = w.nseg - 1; seg >= 0; --seg) {
+            const int s0 = seg * w.K, s1 = s0 + w.K < nsteps ? s0 + w.K : nsteps;
+            TRY_(checkpoint_restore(c, w, seg));
+            for (int s = s0; s < s1; ++s)
+                TRY_(adj_forward_step(c, w.seg_r + (s - s0) * n3, w.seg_u + (s - s0) * n3, w.seg_m + (s - s0) * n3,
+                                      0.0, nullptr));
+            for (int s = s1 - 1; s >= s0; --s) {
+                // the state after the position half of step s+1 (1-based step s0_step + s - s0 + 1)
+                const double* r1 = w.seg_r + (s - s0) * n3;
+                MFA_CUDA_TRY(cudaMemcpyAsync(c->rx, r1, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
+                MFA_CUDA_TRY(cudaMemcpyAsync(c->vx, w.seg_u + (s - s0) * n3, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
+                MFA_CUDA_TRY(cudaMemcpyAsync(c->mx, w.seg_m + (s - s0) * n3, n3 * 4, cudaMemcpyDeviceToDevice, c->st));
+                TRY_(launch_check_skin(c));
+                TRY_(launch_rebuild(c, c->bin_type, 1));
+                TRY_(launch_refresh_sorted(c));
+                k_adj_prep<<<nb, T, 0, c->st>>>(n, w.rho, w.nu, w.alpha, c->inv_mass, 0.5 * dt, p.pin_heads,
+                                                p.n_chain * p.n_mon, p.n_mon > 0 ? p.n_mon : 1, w.lamF, w.lamU,
+                                                w.lamR);
+                const long long step = (long long)w.ckstep[seg] + (s - s0) + 1;
+                AdjArgs aa = pair_adj_args(c, w, step);
+                if (c->prec == MFA_MIXED) k_adj_pair<float><<<nb, T, 0, c->st>>>(aa);
+                else k_adj_pair<double><<<nb, T, 0, c->st>>>(aa);
+                const int nbonds = p.n_chain * (p.n_mon > 0 ? p.n_mon - 1 : 0) +
+                                   (p.n_mon_d >= 2 ? p.n_chain_d * (p.n_mon_d - 1) : 0);
+                if (nbonds > 0) {
+                    AdjBondArgs ba;
+                    ba.px = r1; ba.py = r1 + n; ba.pz = r1 + 2 * n;
+                    ba.fx = w.lamF; ba.fy = w.lamF + n; ba.fz = w.lamF + 2 * n;
+                    ba.rx = w.lamR; ba.ry = w.lamR + n; ba.rz = w.lamR + 2 * n;
+                    ba.g = w.dg;
+                    ba.n_chain = p.n_chain; ba.n_mon = p.n_mon; ba.n_chain_d = p.n_chain_d; ba.n_mon_d = p.n_mon_d;
+                    ba.part_init_d = p.n_mon * p.n_chain; ba.symmetry = p.symmetry;
+                    for (int d = 0; d < 3; ++d) { ba.L[d] = p.boundary[d]; ba.invL[d] = c->inv_boundary[d]; }
+                    ba.k_fene = p.k_chain * p.inv_r_chain_2;
+                    ba.r0 = sqrt(p.r_chain_2);
+                    ba.inv_r_chain_2 = p.inv_r_chain_2;
+                    ba.fene_clamp = p.fene_clamp;
+                    const int bb = (nbonds + T - 1) / T;
+                    if (c->prec == MFA_MIXED) k_adj_fene<float><<<bb, T, 0, c->st>>>(ba);
+                    else k_adj_fene<double><<<bb, T, 0, c->st>>>(ba);
+                }
+                // back to the state before step s+1: the observable at r_s (s >= 1)
+                const double* r0 = s > s0 ? w.seg_r + (s - s0 - 1) * n3 : nullptr;
+                const int32_t* m0 = s > s0 ? w.seg_m + (s - s0 - 1) * n3 : nullptr;
+                if (s == s0 && s > 0) {
+                    // r_s is the segment's checkpoint
+                    r0 = w.ck + seg * 3 * n3;
+                    m0 = w.ckm + seg * n3;
+                }
+                k_adj_combine<<<nb, T, 0, c->st>>>(n, w.lamR, w.lamU, dt, r0 ? wobs : 0.0, r0 ? r0 : c->rx,
+                                                   m0 ? m0 : c->mx, p.boundary[0], p.boundary[1], p.boundary[2],
+                                                   p.n_chain, p.n_mon, p.pin_heads, w.rho, w.nu, w.alpha);
+                MFA_CUDA_TRY(cudaGetLastError());
+            }
+        }
+        // leave the context at the end of the trajectory, as mfa_step would
+        MFA_CUDA_TRY(cudaMemcpyAsync(c->rx, fin_rva.data(), n3 * 8, cudaMemcpyHostToDevice, c->st));
+        MFA_CUDA_TRY(cudaMemcpyAsync(c->vx, fin_rva.data() + n3, n3 * 8, cudaMemcpyHostToDevice, c->st));
+        MFA_CUDA_TRY(cudaMemcpyAsync(c->ax, fin_rva.data() + 2 * n3, n3 * 8, cudaMemcpyHostToDevice, c->st));
+        MFA_CUDA_TRY(cudaMemcpyAsync(c->mx, fin_m.data(), n3 * 4, cudaMemcpyHostToDevice, c->st));
+        MFA_CUDA_TRY(cudaMemcpyAsync(c->dstep, &fin_step, 8, cudaMemcpyHostToDevice, c->st));
+        MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+        TRY_(mfa_binning(c));
+        double h[G_N + 1];
+        MFA_CUDA_TRY(cudaMemcpyAsync(h, w.dg, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+        MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+        out[0] = h[G_N];
+        for (int q = 0; q < G_N; ++q) out[1 + q] = h[q];
+        c->i_time += nsteps;
+        return mfa_sync(c);
+    };
+    rc = run();
+    cudaStreamSynchronize(c->st);
+    for (void* b : bufs) if (b) cudaFree(b);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,141 @@
+"""Trajectory sensitivities (mfa_adjoint): the hand-written discrete adjoint of
+the velocity-Verlet loop against central finite differences with common
+random numbers (the DPD noise is keyed by step and pair, so the perturbed runs
+see the same noise), in FP64; the mixed-precision adjoint against the FP64 one.
+The adjoint is also wrapped here -- in the test harness only -- as a
+torch.autograd.Function, the way a Python optimiser would call it."""
+import math
+
+import numpy as np
+import pytest
+
+from mfa_b200 import _abi, configs
+from mfa_b200._abi import FP64, MIXED
+from mfa_b200.api import System
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ("eps_lj", "sigma", "k_fene", "r0", "gamma_dpd", "eps_wall")
+
+
+def perturbed(params, name, f):
+    """A copy of the derived parameters with one physical parameter scaled by f,
+    as mfa_adjoint defines them."""
+    p = params.copy()
+    act = [k for k in range(64) if p.range_2[k] > 0.0]
+    if name == "eps_lj":
+        for k in act:
+            p.epsil[k] *= f
+    elif name == "sigma":
+        for k in act:
+            p.sigma_2[k] *= f * f
+            p.range_2[k] *= f * f
+            p.inv_range_2[k] /= f * f
+    elif name == "k_fene":
+        p.k_chain *= f
+    elif name == "r0":
+        p.r_chain_2 *= f * f
+        p.inv_r_chain_2 /= f * f
+        p.k_chain *= f * f
+    elif name == "gamma_dpd":
+        p.friction *= f
+        p.sig *= math.sqrt(f)
+    elif name == "eps_wall":
+        for t in range(8):
+            p.a_wall[t] *= f
+        p.a_w *= f
+    return p
+
+
+def base_values(p):
+    act = [k for k in range(64) if p.range_2[k] > 0.0]
+    return {"eps_lj": max(p.epsil[k] for k in act) / 4.0, "sigma": max(math.sqrt(p.sigma_2[k]) for k in act),
+            "k_fene": p.k_chain * p.inv_r_chain_2, "r0": math.sqrt(p.r_chain_2), "gamma_dpd": p.friction,
+            "eps_wall": max(p.a_wall[t] for t in range(8))}
+
+
+@pytest.fixture(scope="module")
+def small_brush():
+    """4 x 4 chains of 16 beads, implicit solvent, 9-3 walls, DPD; relaxed a little."""
+    cfg = configs.brush(seed=21, nx=4, ny=4, n_mon=16, graft=0.3, z_wall=24.0, solvent=False, k_bend=0.0)
+    g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, precision=FP64)
+    g.init_forces()
+    g.step(400)
+    st = g.download()
+    g.close()
+    return cfg, st
+
+
+def run(cfg, st, params, prec, fn):
+    """A run from the stored state (r, v, a held fixed: the gradient is that of
+    the trajectory that starts from this state)."""
+    g = System(params, st["r0"], st["v"], cfg.a_type, cfg.mass, a=st["a"], mic=st["mic"], precision=prec)
+    g.binning()
+    out = fn(g)
+    g.close()
+    return out
+
+
+def test_adjoint_matches_central_differences(small_brush):
+    cfg, st = small_brush
+    nsteps, every, h = 40, 10, 1e-4
+    J, grad = run(cfg, st, cfg.params, FP64, lambda g: g.adjoint(nsteps, every))
+    J0 = run(cfg, st, cfg.params, FP64, lambda g: g.trajectory_observable(nsteps))
+    assert J == pytest.approx(J0, rel=1e-12)
+    base = base_values(cfg.params)
+    for name in NAMES:
+        jp = run(cfg, st, perturbed(cfg.params, name, 1 + h), FP64, lambda g: g.trajectory_observable(nsteps))
+        jm = run(cfg, st, perturbed(cfg.params, name, 1 - h), FP64, lambda g: g.trajectory_observable(nsteps))
+        fd = (jp - jm) / (2 * h * base[name])
+        assert grad[name] == pytest.approx(fd, rel=1e-3, abs=1e-6 * abs(J) / base[name]), (name, grad[name], fd)
+
+
+def test_adjoint_checkpoint_interval_does_not_change_the_gradient(small_brush):
+    cfg, st = small_brush
+    _, g1 = run(cfg, st, cfg.params, FP64, lambda g: g.adjoint(30, 30))
+    _, g2 = run(cfg, st, cfg.params, FP64, lambda g: g.adjoint(30, 7))
+    for name in NAMES:
+        assert g2[name] == pytest.approx(g1[name], rel=1e-9, abs=1e-12)
+
+
+def test_mixed_adjoint_close_to_fp64(small_brush):
+    cfg, st = small_brush
+    _, g64 = run(cfg, st, cfg.params, FP64, lambda g: g.adjoint(40, 10))
+    _, g32 = run(cfg, st, cfg.params, MIXED, lambda g: g.adjoint(40, 10))
+    scale = max(abs(v) for v in g64.values())
+    for name in NAMES:
+        assert abs(g32[name] - g64[name]) < 1e-2 * max(abs(g64[name]), 1e-3 * scale), (name, g32[name], g64[name])
+
+
+def test_torch_autograd_wrapper(small_brush):
+    torch = pytest.importorskip("torch")
+    cfg, st = small_brush
+    base = base_values(cfg.params)
+
+    class Observable(torch.autograd.Function):
+        """J(theta) of a 20-step run; backward returns the adjoint's gradient."""
+
+        @staticmethod
+        def forward(ctx, theta):
+            p = cfg.params
+            for name, val in zip(NAMES, theta.tolist()):
+                p = perturbed(p, name, val / base[name])
+            J, grad = run(cfg, st, p, FP64, lambda g: g.adjoint(20, 5))
+            ctx.save_for_backward(torch.tensor([grad[n] for n in NAMES], dtype=torch.float64))
+            return torch.tensor(J, dtype=torch.float64)
+
+        @staticmethod
+        def backward(ctx, gout):
+            (grad,) = ctx.saved_tensors
+            return gout * grad
+
+    theta = torch.tensor([base[n] for n in NAMES], dtype=torch.float64, requires_grad=True)
+    J = Observable.apply(theta)
+    J.backward()
+    # central differences of the wrapped function on two parameters
+    for i in (0, 4):
+        e = torch.zeros(6, dtype=torch.float64)
+        e[i] = 1e-4 * theta[i].item()
+        with torch.no_grad():
+            fd = (Observable.apply(theta + e) - Observable.apply(theta - e)) / (2 * e[i])
+        assert theta.grad[i].item() == pytest.approx(fd.item(), rel=1e-3, abs=1e-8)
