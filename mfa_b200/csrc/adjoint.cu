@@ -39,13 +39,13 @@ struct AdjArgs {
     const void* pos_s;            // sorted records of r' (w: id << 8 | type)
     const void* vel_s;            // sorted records of u
     const int32_t* __restrict__ nbr;
-    const int32_t* __restrict__ nnb;
+    const int32_t* __restrict__ ccount;   // entries per 32-slot chunk
     const double* tabs;           // list radius, range_2, epsil, sigma_2, e_shift, inv_range_2
     const double *fx, *fy, *fz;   // lam_F (particle order)
     double *rx, *ry, *rz;         // lam_r accumulators
     double *ux, *uy, *uz;         // lam_u accumulators
     double* g;                    // G_N parameter gradient sums
-    int n, half, symmetry, dpd, dpd_weight, noise, wall;
+    int n, maxnb, half, symmetry, dpd, dpd_weight, noise, wall;
     double L[3], invL[3];
     double sig, gam, eps_lj, sigma_lj;
     long long step;
@@ -93,7 +93,9 @@ __device__ __forceinline__ void warp_add_g(double* g, double (&gl)[G_N]) {
     }
 }
 
-// Pair and wall VJP: thread per owner slot, over its list row.
+// Pair and wall VJP: a warp per 32-slot chunk, its lanes over the chunk's list
+// entries (owner and partner both updated through atomics), then over the
+// chunk's slots for the walls.
 template <typename R>
 __global__ void k_adj_pair(AdjArgs a) {
     typedef typename V4<R>::T R4;
@@ -106,21 +108,21 @@ __global__ void k_adj_pair(AdjArgs a) {
     }
     __syncthreads();
     double gl[G_N] = {0, 0, 0, 0, 0, 0};
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < a.n) {
-        const R4* ps = (const R4*)a.pos_s;
-        const R4* vs = (const R4*)a.vel_s;
-        const R4 pi = ps[t], ui = vs[t];
-        const int wi = wbits(pi.w), ii = wi >> 8, ti = wi & 0xff;
-        const R lfx = (R)a.fx[ii], lfy = (R)a.fy[ii], lfz = (R)a.fz[ii];
-        R orx = 0, ory = 0, orz = 0, oux = 0, ouy = 0, ouz = 0;   // owner's lam_r, lam_u
-        const R Lx = (R)a.L[0], Ly = (R)a.L[1], Lz = (R)a.L[2];
-        const R iLx = (R)a.invL[0], iLy = (R)a.invL[1], iLz = (R)a.invL[2];
-        const R sg = (R)a.sig, gm = (R)a.gam;
-        const int m = a.nnb[t];
-        for (int k = 0; k < m; ++k) {
-            const int s = a.nbr[(size_t)k * a.n + t];
-            const R4 pj = ps[s];
+    const int lane = threadIdx.x & 31;
+    const int ch = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const R4* ps = (const R4*)a.pos_s;
+    const R4* vs = (const R4*)a.vel_s;
+    const R Lx = (R)a.L[0], Ly = (R)a.L[1], Lz = (R)a.L[2];
+    const R iLx = (R)a.invL[0], iLy = (R)a.invL[1], iLz = (R)a.invL[2];
+    const R sg = (R)a.sig, gm = (R)a.gam;
+    if (ch * 32 < a.n) {
+        const int cnt = a.ccount[ch];
+        const int32_t* crow = a.nbr + (size_t)ch * 32 * a.maxnb;
+        for (int e = lane; e < cnt; e += 32) {
+            const int ent = crow[e];
+            const int t = ch * 32 + (ent & 31), s = (int)((unsigned)ent >> 5);
+            const R4 pi = ps[t], pj = ps[s];
+            const int wi = wbits(pi.w), ii = wi >> 8, ti = wi & 0xff;
             R dx = mi(pi.x - pj.x, Lx, iLx), dy = mi(pi.y - pj.y, Ly, iLy), dz = pi.z - pj.z;
             if (a.symmetry == 1) dz = mi(dz, Lz, iLz);
             const R r2 = dx * dx + dy * dy + dz * dz;
@@ -128,7 +130,7 @@ __global__ void k_adj_pair(AdjArgs a) {
             if (!(r2 < (R)s_rc2[ij])) continue;
             // the pair force G acts on i (+G) and, with the half list, on j (-G):
             // dl = lam_F_i - lam_F_j (half list) or lam_F_i (full list: j has its own row)
-            R dlx = lfx, dly = lfy, dlz = lfz;
+            R dlx = (R)a.fx[ii], dly = (R)a.fy[ii], dlz = (R)a.fz[ii];
             if (a.half) { dlx -= (R)a.fx[jj]; dly -= (R)a.fy[jj]; dlz -= (R)a.fz[jj]; }
             const R ddl = dx * dlx + dy * dly + dz * dlz;
             // LJ: G = fs(r2) d, fs = eps (12 r12 - 6 r6) / r2
@@ -143,7 +145,7 @@ __global__ void k_adj_pair(AdjArgs a) {
             gl[G_SIG] += (double)(eps * ((R)144 * r12 - (R)36 * r6) * ir2 * ddl) / a.sigma_lj;
             if (a.dpd) {
                 // DPD: G = P rhat, P = sig w_r g - gamma w_d (du . rhat), w_d = w_r^2
-                const R4 uj = vs[s];
+                const R4 ui = vs[t], uj = vs[s];
                 const R dux = ui.x - uj.x, duy = ui.y - uj.y, duz = ui.z - uj.z;
                 const R ir = rsq(r2), r = r2 * ir;
                 const R hx = dx * ir, hy = dy * ir, hz = dz * ir;
@@ -163,9 +165,11 @@ __global__ void k_adj_pair(AdjArgs a) {
                 gx += c1 * hx + c2 * (dux - sdu * hx) + c3 * (dlx - hdl * hx);
                 gy += c1 * hy + c2 * (duy - sdu * hy) + c3 * (dly - hdl * hy);
                 gz += c1 * hz + c2 * (duz - sdu * hz) + c3 * (dlz - hdl * hz);
-                // (dG/d du)^T dl = -gamma w_d hdl rhat
+                // (dG/d du)^T dl = -gamma w_d hdl rhat, on u_i (+) and u_j (-)
                 const R cu = -gm * wd * hdl;
-                oux += cu * hx; ouy += cu * hy; ouz += cu * hz;
+                atomicAdd(&a.ux[ii], (double)(cu * hx));
+                atomicAdd(&a.uy[ii], (double)(cu * hy));
+                atomicAdd(&a.uz[ii], (double)(cu * hz));
                 atomicAdd(&a.ux[jj], -(double)(cu * hx));
                 atomicAdd(&a.uy[jj], -(double)(cu * hy));
                 atomicAdd(&a.uz[jj], -(double)(cu * hz));
@@ -178,13 +182,19 @@ __global__ void k_adj_pair(AdjArgs a) {
                 }
             }
             // G depends on d = r_i - r_j: both positions, whichever side it acts on
-            orx += gx; ory += gy; orz += gz;
+            atomicAdd(&a.rx[ii], (double)gx);
+            atomicAdd(&a.ry[ii], (double)gy);
+            atomicAdd(&a.rz[ii], (double)gz);
             atomicAdd(&a.rx[jj], -(double)gx);
             atomicAdd(&a.ry[jj], -(double)gy);
             atomicAdd(&a.rz[jj], -(double)gz);
         }
-        if (a.wall == 2) {
+        const int t = ch * 32 + lane;
+        if (a.wall == 2 && t < a.n) {
             // 9-3 walls (fluid_wall.f90:96-121): F_z += f(z) - f(Z - z), f = A phi(z)
+            const R4 pi = ps[t];
+            const int wi = wbits(pi.w), ii = wi >> 8, ti = wi & 0xff;
+            const R lfz = (R)a.fz[ii];
             const R sw = (R)a.sigma_wall[ti - 1], aw = (R)a.a_wall[ti - 1], cut = (R)a.wall_cut;
             const R sw3 = sw * sw * sw, sw9 = sw3 * sw3 * sw3;
             const R zb = pi.z, zt = (R)a.z_space_wall - pi.z;
@@ -199,16 +209,8 @@ __global__ void k_adj_pair(AdjArgs a) {
                 phi -= (R)9 * sw9 * iz10 - (R)3 * sw3 * iz4;
                 dfz += aw * ((R)-90 * sw9 * iz10 * iz + (R)12 * sw3 * iz5);   // d/dz of -f(Z - z)
             }
-            orz += dfz * lfz;
+            atomicAdd(&a.rz[ii], (double)(dfz * lfz));
             if (aw != (R)0) gl[G_WALL] += (double)(phi * lfz);
-        }
-        atomicAdd(&a.rx[ii], (double)orx);
-        atomicAdd(&a.ry[ii], (double)ory);
-        atomicAdd(&a.rz[ii], (double)orz);
-        if (a.dpd) {
-            atomicAdd(&a.ux[ii], (double)oux);
-            atomicAdd(&a.uy[ii], (double)ouy);
-            atomicAdd(&a.uz[ii], (double)ouz);
         }
     }
     warp_add_g(a.g, gl);
@@ -392,7 +394,8 @@ AdjArgs pair_adj_args(mfa_ctx* c, Work& w, long long step) {
     const mfa_params& p = c->p;
     const int n = c->n;
     AdjArgs a;
-    a.pos_s = c->pos_s; a.vel_s = c->vel_s; a.nbr = c->nbr; a.nnb = c->nnb; a.tabs = c->tabs;
+    a.pos_s = c->pos_s; a.vel_s = c->vel_s; a.nbr = c->nbr; a.ccount = c->ccount; a.tabs = c->tabs;
+    a.maxnb = c->maxnb;
     a.fx = w.lamF; a.fy = w.lamF + n; a.fz = w.lamF + 2 * n;
     a.rx = w.lamR; a.ry = w.lamR + n; a.rz = w.lamR + 2 * n;
     a.ux = w.lamU; a.uy = w.lamU + n; a.uz = w.lamU + 2 * n;
@@ -520,8 +523,9 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
                                                 w.lamR);
                 const long long step = (long long)w.ckstep[seg] + (s - s0) + 1;
                 AdjArgs aa = pair_adj_args(c, w, step);
-                if (c->prec == MFA_MIXED) k_adj_pair<float><<<nb, T, 0, c->st>>>(aa);
-                else k_adj_pair<double><<<nb, T, 0, c->st>>>(aa);
+                const int nbw = ((n + 31) / 32 * 32 + T - 1) / T;   // a warp per 32-slot chunk
+                if (c->prec == MFA_MIXED) k_adj_pair<float><<<nbw, T, 0, c->st>>>(aa);
+                else k_adj_pair<double><<<nbw, T, 0, c->st>>>(aa);
                 const int nbonds = p.n_chain * (p.n_mon > 0 ? p.n_mon - 1 : 0) +
                                    (p.n_mon_d >= 2 ? p.n_chain_d * (p.n_mon_d - 1) : 0);
                 if (nbonds > 0) {

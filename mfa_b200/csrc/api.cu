@@ -92,7 +92,7 @@ int alloc_list(mfa_ctx* c, int maxnb) {
     if (c->nbr) cudaFree(c->nbr);
     c->nbr = nullptr;
     c->maxnb = maxnb;
-    return dalloc(&c->nbr, (size_t)maxnb * c->n);
+    return dalloc(&c->nbr, (size_t)maxnb * 32 * ((c->n + 31) / 32));
 }
 
 int read_flags(mfa_ctx* c, int32_t* f) {
@@ -366,7 +366,8 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
     int maxnb = ((int)(2.0 * expect) + 32 + 31) / 32 * 32;
     if (maxnb > n) maxnb = ((n + 31) / 32) * 32;
     if (rc == MFA_OK) rc = alloc_list(c, maxnb);
-    A(dalloc(&c->nnb, n));
+    A(dalloc(&c->nnb, (size_t)n + (n + 31) / 32));
+    if (rc == MFA_OK) c->ccount = c->nnb + n;
     // partial-sum slots: enough for the largest grid of any reducing kernel
     // (particles / 32, cell rows, chains)
     c->max_blocks = (n + 31) / 32 + 64;
@@ -423,7 +424,7 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
     rc = MFA_OK;
     A(dzero(c, c->force, (size_t)4 * n * esz(c)));
     A(dzero(c, c->cell_count, ((size_t)3 * c->ncell + 2 + n + nrow) * 4));
-    A(dzero(c, c->nnb, (size_t)n * 4));
+    A(dzero(c, c->nnb, ((size_t)n + (n + 31) / 32) * 4));
     A(dzero(c, c->counters, R_N * sizeof(unsigned)));
     A(dzero(c, c->dscal, S_NSLOT * 8));
     A(dzero(c, c->dflags, F_NFLAG * 4));
@@ -825,23 +826,29 @@ int mfa_debug_lists(mfa_ctx* c, int32_t* cell_of, int32_t* nbr_count, int32_t* n
     if (!c->lists_valid) return MFA_ERR_STATE;
     const int n = c->n;
     MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
-    std::vector<int32_t> co(n), ids(n), cnt(n), lst((size_t)c->maxnb * n), cs(c->ncell + 1);
+    const int nchunk = (n + 31) / 32;
+    const size_t capc = (size_t)32 * c->maxnb;
+    std::vector<int32_t> co(n), ids(n), cnt(n), ccnt(nchunk), lst(capc * nchunk), cs(c->ncell + 1);
     MFA_CUDA_TRY(cudaMemcpy(co.data(), c->cell_of, (size_t)n * 4, cudaMemcpyDeviceToHost));
     MFA_CUDA_TRY(cudaMemcpy(ids.data(), c->ids, (size_t)n * 4, cudaMemcpyDeviceToHost));
     MFA_CUDA_TRY(cudaMemcpy(cnt.data(), c->nnb, (size_t)n * 4, cudaMemcpyDeviceToHost));
+    MFA_CUDA_TRY(cudaMemcpy(ccnt.data(), c->ccount, (size_t)nchunk * 4, cudaMemcpyDeviceToHost));
     MFA_CUDA_TRY(cudaMemcpy(lst.data(), c->nbr, lst.size() * 4, cudaMemcpyDeviceToHost));
     MFA_CUDA_TRY(cudaMemcpy(cs.data(), c->cell_start, cs.size() * 4, cudaMemcpyDeviceToHost));
     if (cell_of) memcpy(cell_of, co.data(), (size_t)n * 4);
-    for (int t = 0; t < n; ++t) {
-        const int i = ids[t];
-        const int m = cnt[t] < max_per ? cnt[t] : max_per;
-        if (nbr_count) nbr_count[i] = cnt[t];
-        if (!nbr) continue;
-        for (int k = 0; k < m; ++k) {
-            const int s = lst[(size_t)k * n + t];   // the partner's slot
-            nbr[(size_t)i * max_per + k] = (s >= 0 && s < n) ? ids[s] + 1 : 0;
-        }
-    }
+    std::vector<int> fill(n, 0);
+    for (int t = 0; t < n; ++t)
+        if (nbr_count) nbr_count[ids[t]] = cnt[t];
+    if (nbr)
+        for (int ch = 0; ch < nchunk; ++ch)
+            for (int k = 0; k < ccnt[ch]; ++k) {
+                const int e = lst[ch * capc + k];
+                const int t = ch * 32 + (e & 31), s = (int)((unsigned)e >> 5);   // owner slot, partner slot
+                if (t >= n) continue;
+                const int i = ids[t];
+                if (fill[t] < max_per) nbr[(size_t)i * max_per + fill[t]] = (s >= 0 && s < n) ? ids[s] + 1 : 0;
+                ++fill[t];
+            }
     return MFA_OK;
 }
 

@@ -12,13 +12,15 @@
 // a row is a contiguous range of slots.
 //   k_build_nbr     thread per slot: scans the neighbouring cells and keeps j with
 //                   r^2 < range_2(ti,tj) + skin_2, the reference's FP64
-//                   expression evaluated without contraction (bit-exact pair set).
+//                   expression evaluated without contraction (bit-exact pair set);
+//                   a warp (32 consecutive slots) writes its entries as one run.
 // binning.f90 keeps each pair once (i < j, binning.f90:81-104); here the pair is
 // kept in the row of its lower slot (the pair kernel applies Newton's third
 // law), so the set of unordered pairs -- with the reference's repeats when a
 // cell is scanned twice -- is the reference's.  my_binning.f90 keeps both
-// directions (a full list).  Column-major (entry k of slot t at nbr[k*n + t]);
-// an entry is the partner's slot.
+// directions (a full list).  Layout: the entries of the 32 slots of chunk c are
+// one run at nbr[c * 32 * maxnb ..] (ccount[c] of them, in no fixed order); an
+// entry is (partner slot << 5 | lane of the owning slot in the chunk).
 #include "mfa_internal.cuh"
 
 #include <string.h>
@@ -39,6 +41,7 @@ struct BinArgs {
     double4* pos64;
     float4* pos32;             // FP32 copy of pos64 for the list builder's prefilter
     int32_t *nbr, *nnb;
+    int32_t* ccount;           // entries per 32-slot chunk
     int32_t* flags;
     unsigned* counter;
     int n, ncell, nrow, maxnb;
@@ -249,7 +252,16 @@ __device__ __forceinline__ void build_nbr_body(const BinArgs& a, Blk blk) {
         scf[k] = (float)a.cut2[k] + a.prefilter_margin;
     }
     __syncthreads();
+    // the list of a 32-slot chunk (this warp) is one run of entries
+    // (partner slot << 5 | owner lane), appended through a shared cursor
+    __shared__ int wcur[32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int t = blk.id * blockDim.x + threadIdx.x;
+    const int chunk = t >> 5;
+    const long long capc = 32LL * a.maxnb;
+    int32_t* crow = a.nbr + (size_t)chunk * capc;
+    if (lane == 0) wcur[wib] = 0;
+    __syncwarp();
     if (t < a.n) {
         const double4 pi = a.pos64[t];
         const float4 pf = a.pos32[t];
@@ -298,17 +310,23 @@ __device__ __forceinline__ void build_nbr_body(const BinArgs& a, Blk blk) {
                     if (a.symmetry == 1) d2 = mimage64(d2, a.L[2], a.invL[2]);
                     const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
                     if (r2 < sc[trow + tj]) {
-                        if (cnt < a.maxnb) a.nbr[(size_t)cnt * a.n + t] = s;
+                        const int q = atomicAdd(&wcur[wib], 1);
+                        if (q < capc) crow[q] = (s << 5) | lane;
                         ++cnt;
                     }
                 }
             }
         }
-        a.nnb[t] = min(cnt, a.maxnb);
+        a.nnb[t] = cnt;
         atomicMax(&a.flags[F_MAXNB], cnt);
-        if (cnt > a.maxnb) {
+    }
+    __syncwarp();
+    if (lane == 0 && chunk * 32 < a.n) {
+        const int total = wcur[wib];
+        a.ccount[chunk] = (int)(total < capc ? total : capc);
+        if (total > capc) {
             set_err(a.flags, MFA_ERR_NEIGH_OVERFLOW);
-            atomicMax(&a.flags[F_NEEDNB], cnt);
+            atomicMax(&a.flags[F_NEEDNB], (total + 31) / 32);
         }
     }
     // the last block to finish closes the rebuild: f_skin = 0 (binning.f90:125)
@@ -365,7 +383,7 @@ BinArgs make_args(mfa_ctx* c, int rule, int conditional) {
     a.cell_count = c->cell_count; a.cell_start = c->cell_start; a.cell_cursor = c->cell_cursor;
     a.cell_of = c->cell_of; a.row_count = c->row_count; a.ids = c->ids; a.slot = c->slot;
     a.pos_s = c->pos_s; a.vel_s = c->vel_s; a.pos64 = c->pos64; a.pos32 = c->pos32;
-    a.nbr = c->nbr; a.nnb = c->nnb; a.flags = c->dflags;
+    a.nbr = c->nbr; a.nnb = c->nnb; a.ccount = c->ccount; a.flags = c->dflags;
     a.counter = c->counters + R_N - 1;
     a.n = c->n; a.ncell = c->ncell; a.nrow = c->nb[1] * c->nb[2]; a.maxnb = c->maxnb;
     for (int d = 0; d < 3; ++d) {

@@ -6,7 +6,8 @@
 //   vel_s:   cell-sorted copy of velocities, w = charge             (float4 / double4)
 //   ids:     slot -> particle, slot: particle -> slot (counting sort by cell)
 //   nbr:     Verlet list in slot space (half list for binning, full for
-//            my_binning), column k of row t at nbr[k*n + t], entries = slots
+//            my_binning): per chunk of 32 consecutive slots one run of entries
+//            (partner slot << 5 | owner lane), ccount[chunk] long
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -78,8 +79,9 @@ struct mfa_ctx {
     // pair tables on the device: range_2+skin_2, range_2, epsil, sigma_2, e_shift, inv_range_2
     double* tabs;                       // 6 x T8*T8
     // Verlet list
-    int maxnb;
+    int maxnb;                          // list capacity per slot (a chunk holds 32 x maxnb)
     int32_t *nbr, *nnb;
+    int32_t* ccount;                    // entries per 32-slot chunk (after nnb)
     // reductions / flags
     double* partials;                   // R_N regions x max_blocks x 4 quantities
     int max_blocks;

@@ -44,7 +44,7 @@ struct PairArgs {
     const void* pos_s;
     const void* vel_s;
     const int32_t* __restrict__ nbr;
-    const int32_t* __restrict__ nnb;
+    const int32_t* __restrict__ ccount;       // entries per 32-slot chunk
     const int32_t* __restrict__ cell_start;
     int32_t* flags;
     const double* mass;
@@ -54,7 +54,7 @@ struct PairArgs {
     double* partials;
     unsigned* counter;
     double* dscal;
-    int n, max_blocks;
+    int n, max_blocks, maxnb;
     int nb[3], rule, wy, nseg, tile_cap, rowmode;
     int half;                 // 1: half list (partner gets -f), 0: full list
     int symmetry, thermostat, dpd_weight, noise, charged, real_in_lj, fsw;
@@ -247,10 +247,10 @@ __device__ __forceinline__ bool has(const PairArgs& a, int bit) {
 template <int K> constexpr int qcap() { return 32 * K + 32; }
 
 // per-warp shared memory: queue (d, r^2), queue (j, id/type of j), owner
-// velocities, owner id/type, owner force accumulators
+// positions and velocities, owner id/type, owner force accumulators
 template <typename R, int K>
 constexpr size_t warp_bytes() {
-    return (size_t)qcap<K>() * (sizeof(typename Vec4<R>::T) + sizeof(int2)) + 32 * sizeof(typename Vec4<R>::T) +
+    return (size_t)qcap<K>() * (sizeof(typename Vec4<R>::T) + sizeof(int2)) + 64 * sizeof(typename Vec4<R>::T) +
            32 * sizeof(int) + 96 * sizeof(R);
 }
 
@@ -269,7 +269,8 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
     unsigned char* wmem = (unsigned char*)(tvel + a.tile_cap) + (size_t)warp * warp_bytes<R, K>();
     R4* qd = (R4*)wmem;                          // QC x (dx, dy, dz, r^2)
     R4* own_v = qd + QC;                         // 32 owner velocities (w = charge)
-    int2* qw = (int2*)(own_v + 32);              // QC x (owner << 23 | j index, id << 8 | type of j)
+    R4* own_p = own_v + 32;                      // 32 owner positions
+    int2* qw = (int2*)(own_p + 32);              // QC x (owner << 23 | j index, id << 8 | type of j)
     int* own_w = (int*)(qw + QC);                // 32 owner id << 8 | type
     R* facc = (R*)(own_w + 32);                  // 3 x 32 owner force accumulators
     __shared__ R s_rc2[T8 * T8], s_eps[T8 * T8], s_sig2[T8 * T8], s_esh[T8 * T8], s_irc2[T8 * T8];
@@ -447,38 +448,50 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
         if (a.half) red_add(&f4[wj >> 8], -fx, -fy, -fz);
     };
 
-    for (int base = p0 + 32 * warp; valid && base < p1; base += 32 * nwarp) {
-        const int t = base + lane;
-        const bool act = t < p1;
+    // chunks of 32 slots, each with its list as one run of entries (partner
+    // slot << 5 | owner lane): an untiled CTA owns blockDim/32 whole chunks; a
+    // tiled CTA (one cell row) takes the chunks overlapping its row and keeps
+    // the entries whose owner lies in the row.  The lanes walk the chunk's
+    // entries together, K per lane per round, whatever row they belong to.
+    const long long capc = 32LL * a.maxnb;
+    for (int ch = (p0 >> 5) + warp; valid && ch < ((p1 + 31) >> 5); ch += nwarp) {
+        const int t = (ch << 5) + lane;
+        const bool act = t >= p0 && t < p1;
         R4 pi;
-        int m = 0;
         if (act) {
             pi = ldg4(&gpos[t]);
-            m = a.nnb[t];
             if (need_v || LGV) own_v[lane] = ldg4(&gvel[t]);
         } else {
             pi.x = pi.y = pi.z = 0;
             pi.w = 0;
         }
-        const int wi = wbits(pi.w);
+        const int wi = act ? wbits(pi.w) : 0;
         own_w[lane] = wi;
+        own_p[lane] = pi;
         facc[lane] = 0;
         facc[32 + lane] = 0;
         facc[64 + lane] = 0;
-        const int rowi = act ? ((wi & 0xff) - 1) * T8 - 1 : 0;
-        const int mmax = __reduce_max_sync(0xffffffffu, m);
+        const int cnt = a.ccount[ch];
+        const int32_t* __restrict__ crow = a.nbr + (size_t)ch * capc;
         int qn = 0;
         __syncwarp();
-        for (int k0 = 0; k0 < mmax; k0 += K) {
-            int jx[K];
+        for (int e0 = 0; e0 < cnt; e0 += 32 * K) {
+            int jx[K], ol[K];
             R4 pj[K];
 #pragma unroll
             for (int u = 0; u < K; ++u) {
                 jx[u] = -1;
-                if (k0 + u < m) jx[u] = __ldg(&a.nbr[(size_t)(k0 + u) * a.n + t]);
+                ol[u] = 0;
+                const int e = e0 + 32 * u + lane;
+                if (e < cnt) {
+                    const int ent = __ldg(&crow[e]);
+                    ol[u] = ent & 31;
+                    jx[u] = (int)((unsigned)ent >> 5);
+                }
             }
 #pragma unroll
             for (int u = 0; u < K; ++u) {
+                if (jx[u] >= 0 && own_w[ol[u]] == 0) jx[u] = -1;   // owner outside this CTA's row
                 if (jx[u] >= 0) {
                     if (tile) {
                         // list entries are slots; find the staged run holding the slot
@@ -499,13 +512,15 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
                 R dx = 0, dy = 0, dz = 0, r2 = 0;
                 int wj = 0;
                 if (jx[u] >= 0) {
-                    dx = mimg(pi.x - pj[u].x, Lx, iLx);
-                    dy = mimg(pi.y - pj[u].y, Ly, iLy);
-                    dz = pi.z - pj[u].z;
+                    const R4 po = own_p[ol[u]];
+                    dx = mimg(po.x - pj[u].x, Lx, iLx);
+                    dy = mimg(po.y - pj[u].y, Ly, iLy);
+                    dz = po.z - pj[u].z;
                     if (a.symmetry == 1) dz = mimg(dz, Lz, iLz);
                     r2 = dx * dx + dy * dy + dz * dz;
                     wj = wbits(pj[u].w);
-                    keep = r2 < s_rc2[rowi + (wj & 0xff)] || (QSEP && r2 < ewrc2);
+                    const int rowo = ((own_w[ol[u]] & 0xff) - 1) * T8 - 1;
+                    keep = r2 < s_rc2[rowo + (wj & 0xff)] || (QSEP && r2 < ewrc2);
                 }
                 const unsigned mask = __ballot_sync(0xffffffffu, keep);
                 if (keep) {
@@ -513,7 +528,7 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
                     R4 e;
                     e.x = dx; e.y = dy; e.z = dz; e.w = r2;
                     qd[pos] = e;
-                    qw[pos] = make_int2((lane << 23) | jx[u], wj);
+                    qw[pos] = make_int2((ol[u] << 23) | jx[u], wj);
                 }
                 qn += __popc(mask);
             }
@@ -693,7 +708,7 @@ int pair_set_shape(mfa_ctx* c, int k, int block, int tile_cap) {
 int pair_stage_args(mfa_ctx* c, int fuse_wall, void* out, int* grid_out, size_t* smem_out, int* ft_out) {
     if (!c->lists_valid) return MFA_ERR_STATE;
     PairArgs a;
-    a.pos_s = c->pos_s; a.vel_s = c->vel_s; a.nbr = c->nbr; a.nnb = c->nnb;
+    a.pos_s = c->pos_s; a.vel_s = c->vel_s; a.nbr = c->nbr; a.ccount = c->ccount; a.maxnb = c->maxnb;
     a.cell_start = c->cell_start; a.flags = c->dflags;
     a.mass = c->mass; a.tabs = c->tabs; a.force = c->force; a.dstep = c->dstep;
     a.partials = c->partials + (size_t)R_PAIR * 4 * c->max_blocks;
