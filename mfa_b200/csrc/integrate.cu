@@ -218,7 +218,10 @@ __device__ __forceinline__ void vv_velocities_body(const VVArgs& a, Blk blk) {
 // verlet_velocities of step n followed by verlet_positions of step n+1 in one
 // pass over the state (the skin check of n+1 fused in); the force array is
 // reset for the force kernels of step n+1 (md_main.f90:88).
-template <typename R4>
+// COND: the kernel may open the rebuild's conditional graph node (a kernel
+// that can does not run under profilers that replay graph nodes one by one,
+// so the launches without a node use the variant that cannot)
+template <typename R4, bool COND>
 __device__ __forceinline__ void vv_fused_body(const VVArgs& a, Blk blk) {
     const int i = blk.id * blockDim.x + threadIdx.x;
     double ke = 0.0, eb[2] = {0.0, 0.0};
@@ -240,7 +243,7 @@ __device__ __forceinline__ void vv_fused_body(const VVArgs& a, Blk blk) {
             // taking its turn on the counter).  Only a rebuild that is due
             // opens the node (the condition starts at 0 every graph launch),
             // so that several contexts may share one node.
-            if (a.rebuild_cond && *(volatile int32_t*)&a.flags[F_SKIN] != 0)
+            if (COND && a.rebuild_cond && *(volatile int32_t*)&a.flags[F_SKIN] != 0)
                 cudaGraphSetConditional(a.rebuild_cond, 1u);
         }
     }
@@ -249,15 +252,24 @@ __device__ __forceinline__ void vv_fused_body(const VVArgs& a, Blk blk) {
 // plain launches (one context) and grouped launches (the same stage for
 // several contexts, argument records in device memory)
 template <typename R4> __global__ void k_vv_positions(VVArgs a) { vv_positions_body<R4>(a, plain_blk()); }
-template <typename R4> __global__ void k_vv_velocities(VVArgs a) { vv_velocities_body<R4>(a, plain_blk()); }
-template <typename R4> __global__ void k_vv_fused(VVArgs a) { vv_fused_body<R4>(a, plain_blk()); }
+// 64 registers in MIXED: four 256-thread blocks per SM (the bonded window of
+// the chain beads would otherwise take ~80 and leave one and a half waves);
+// FP64 keeps 85 (three blocks), where 64 would spill the doubled operands
+#define VV_BOUNDS __launch_bounds__(256, sizeof(R4) == 16 ? 4 : 3)
 template <typename R4>
-__global__ void k_vv_grouped(const VVArgs* __restrict__ as, const int* __restrict__ off, int nsys, int stage) {
+__global__ void VV_BOUNDS k_vv_velocities(VVArgs a) { vv_velocities_body<R4>(a, plain_blk()); }
+template <typename R4>
+__global__ void VV_BOUNDS k_vv_fused(VVArgs a) { vv_fused_body<R4, false>(a, plain_blk()); }
+template <typename R4>
+__global__ void VV_BOUNDS k_vv_fused_cond(VVArgs a) { vv_fused_body<R4, true>(a, plain_blk()); }
+template <typename R4>
+__global__ void VV_BOUNDS
+    k_vv_grouped(const VVArgs* __restrict__ as, const int* __restrict__ off, int nsys, int stage) {
     const int s = group_of(off, nsys, blockIdx.x);
     const Blk blk = group_blk(off, s);
     if (stage == VV_POSITIONS) vv_positions_body<R4>(as[s], blk);
     else if (stage == VV_VELOCITIES) vv_velocities_body<R4>(as[s], blk);
-    else vv_fused_body<R4>(as[s], blk);
+    else vv_fused_body<R4, true>(as[s], blk);
 }
 
 VVArgs make_args(mfa_ctx* c) {
@@ -361,8 +373,13 @@ int launch_vv_fused(mfa_ctx* c, cudaGraphConditionalHandle rebuild_cond, int fus
     VVArgs a;
     int nb;
     TRY_(vv_stage_args(c, VV_FUSED, 1, 1, fuse_bonds, rebuild_cond, &a, &nb));
-    if (c->prec == MFA_MIXED) k_vv_fused<float4><<<nb, TPB, 0, c->st>>>(a);
-    else k_vv_fused<double4><<<nb, TPB, 0, c->st>>>(a);
+    if (rebuild_cond) {
+        if (c->prec == MFA_MIXED) k_vv_fused_cond<float4><<<nb, TPB, 0, c->st>>>(a);
+        else k_vv_fused_cond<double4><<<nb, TPB, 0, c->st>>>(a);
+    } else {
+        if (c->prec == MFA_MIXED) k_vv_fused<float4><<<nb, TPB, 0, c->st>>>(a);
+        else k_vv_fused<double4><<<nb, TPB, 0, c->st>>>(a);
+    }
     MFA_CUDA_TRY(cudaGetLastError());
     note_launch(c, 1);
     return MFA_OK;

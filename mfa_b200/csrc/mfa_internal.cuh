@@ -300,11 +300,29 @@ __device__ __forceinline__ bool block_sum_commit(double (&v)[NQ], double* partia
     __syncthreads();
     if (!am_last) return false;
     __threadfence();
+    // every thread sums a fixed stripe of blocks (deterministic order); the
+    // loads of U blocks x NQ quantities are issued before any of them is used,
+    // so the last block waits for ~n/(U blockDim) L2 round trips, not n/blockDim
+    double xs[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) xs[q] = 0.0;
+    constexpr int U = NQ <= 2 ? 8 : 4;
+    for (int b0 = threadIdx.x; b0 < blk.n; b0 += U * blockDim.x) {
+        double v[U][NQ];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int b = b0 + u * blockDim.x;
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) v[u][q] = b < blk.n ? __ldcg(&partials[q * max_blocks + b]) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) xs[q] += v[u][q];
+    }
 #pragma unroll
     for (int q = 0; q < NQ; ++q) {
-        double x = 0.0;
-        for (int b = threadIdx.x; b < blk.n; b += blockDim.x)
-            x += __ldcg(&partials[q * max_blocks + b]);
+        double x = xs[q];
         for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
         __syncthreads();
         if (lane == 0) sm[q][wid] = x;
