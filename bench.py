@@ -256,7 +256,8 @@ def batch_bench(a):
     dev = local
     torch.cuda.set_device(dev)
     # whole systems are the unit of work: rank r takes every world-th system
-    cfgs = configs.uneven_brushes(seed=a.seed, n_sys=a.n_sys)[rank::world]
+    from mfa_b200.ranks import max_over_ranks, shard, sum_over_ranks
+    cfgs = shard(configs.uneven_brushes(seed=a.seed, n_sys=a.n_sys), rank, world)
     n = sum(c.n for c in cfgs)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
 
@@ -308,18 +309,11 @@ def batch_bench(a):
         return ms, launches, clocks, errs
 
     ms_mixed, launches, clocks, errs = timed_batch(_abi.MIXED, a.steps, a.warmup)
-    ms_max = ms_mixed
-    if dist is not None:
-        t = torch.tensor([ms_mixed], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-        nt = torch.tensor([n], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(nt)
-        n_all = int(nt.item())
-    else:
-        n_all = n
+    ms_max = max_over_ranks(ms_mixed, dist, f"cuda:{dev}")
+    n_all = int(sum_over_ranks(n, dist, f"cuda:{dev}"))
     value = n_all * a.steps / (ms_max * 1e-3)
     ms_fp64, _, _, _ = timed_batch(_abi.FP64, a.steps, a.warmup)
+    ms_fp64 = max_over_ranks(ms_fp64, dist, f"cuda:{dev}")
     # the same systems one after another (a launch sequence per system)
     ss = make(_abi.MIXED)
     st = torch.cuda.Stream(device=f"cuda:{dev}")
@@ -367,7 +361,7 @@ def batch_bench(a):
                        "l2": "flushed between timed iterations (256 MiB write); state is larger than L2",
                        "parallelism": f"whole systems over {world} GPU(s), no data exchange"},
             "fp64": {"value": n_all * a.steps / (ms_fp64 * 1e-3), "ms_per_step": ms_fp64 / a.steps},
-            "mixed_over_fp64": ms_fp64 / ms_mixed,
+            "mixed_over_fp64": ms_fp64 / ms_max,
             "one_system_at_a_time": {"value": n * seq_steps / t_seq,
                                      "note": "the same systems through mfa_step one after another (wall clock)"},
             "gpu_launches": int(launches),
@@ -578,11 +572,8 @@ def main():
     shape_mixed = g.tuned
     tuning_mixed = g.tuning
     skin_mixed, nbin_mixed, skin_tuning = g.params.skin, list(g.params.n_bin), g.skin_tuning
-    ms_max = ms_mixed
-    if dist is not None:
-        t = torch.tensor([ms_mixed], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+    from mfa_b200.ranks import max_over_ranks
+    ms_max = max_over_ranks(ms_mixed, dist, f"cuda:{dev}")
     value = world * n * a.steps / (ms_max * 1e-3)
 
     # steady state without flushes: captured 10-step graphs, L2-resident state
@@ -593,7 +584,7 @@ def main():
     g.step(a.steps)
     e1.record(ext)
     g.sync()
-    ms_resident = e0.elapsed_time(e1)
+    ms_resident = max_over_ranks(e0.elapsed_time(e1), dist, f"cuda:{dev}")
 
     # dominant kernel: the pair kernel, timed alone on the context's stream
     work = pair_work(g, cfg)
@@ -654,6 +645,7 @@ def main():
     # plain FP64 GPU path, same protocol
     g64, ms_fp64, _, _, _ = timed_run(_abi.FP64, a.steps, a.warmup)
     g64.close()
+    ms_fp64 = max_over_ranks(ms_fp64, dist, f"cuda:{dev}")
     value_fp64 = world * n * a.steps / (ms_fp64 * 1e-3)
 
     # end to end through the public API with host buffers
@@ -682,10 +674,7 @@ def main():
     out = ge.download(_abi.R0 | _abi.V)
     t_e2e = time.perf_counter() - t0
     ge.close()
-    if dist is not None:
-        t = torch.tensor([t_e2e], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+    t_e2e = max_over_ranks(t_e2e, dist, f"cuda:{dev}")
     e2e = world * n * a.steps / t_e2e
     scal_bytes = 16 * 8 + 8 * 4
     e2e_obj = {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": int(72 * n / a.steps),
