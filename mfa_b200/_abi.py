@@ -158,9 +158,12 @@ def load() -> C.CDLL:
     """Load libmfa_gpu.so (raises if it is absent: there is no CPU fallback)."""
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            raise ImportError(f"{LIB_PATH} is missing; build it with `make -C mfa_b200/csrc`")
-        lib = C.CDLL(LIB_PATH)
+        # MFA_LIB: another build of the same library (same ABI), e.g. one made
+        # with different compile-time options
+        path = os.environ.get("MFA_LIB", LIB_PATH)
+        if not os.path.exists(path):
+            raise ImportError(f"{path} is missing; build it with `make -C mfa_b200/csrc`")
+        lib = C.CDLL(path)
         for name, (res, args) in SIGNATURES.items():
             fn = getattr(lib, name)
             fn.restype = res

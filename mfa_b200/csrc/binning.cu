@@ -220,7 +220,7 @@ __device__ __forceinline__ int x_runs(const BinArgs& a, int cx, int nx, int wx, 
     for (int ix = 0; ix < wx; ++ix) {
         int kx;
         if (a.rule == 0) {
-            kx = (cx - 1 + ix + nx) % nx;        // binning.f90:71-76
+            kx = wrap_near(cx - 1 + ix, nx);     // binning.f90:71-76: mod(cx - 1 + ix, nx)
         } else {
             kx = cx + ix - 1;                    // my_binning.f90:70-72
             if (kx < 0) kx = nx - 1;

@@ -253,7 +253,8 @@ __device__ __forceinline__ void vv_fused_body(const VVArgs& a, Blk blk) {
 // several contexts, argument records in device memory)
 template <typename R4> __global__ void k_vv_positions(VVArgs a) { vv_positions_body<R4>(a, plain_blk()); }
 // 64 registers in MIXED: four 256-thread blocks per SM (the bonded window of
-// the chain beads would otherwise take ~80 and leave one and a half waves);
+// the chain beads would otherwise take ~80; at 48 registers it spills, and the
+// spills cost more than the extra wave: measured 58.3 vs 60.9 us per step);
 // FP64 keeps 85 (three blocks), where 64 would spill the doubled operands
 #define VV_BOUNDS __launch_bounds__(256, sizeof(R4) == 16 ? 4 : 3)
 template <typename R4>

@@ -362,11 +362,16 @@ __device__ __forceinline__ void wall93_term(R zz, R sw, R aw, R ae, R cut, R& f,
 // binning.f90:73-76 for rule 0 (j = c-1 .. c+delta_bin, mod n), my_binning.f90:74-80
 // for rule 1 (c-1 .. c+1 with a single wrap).  The pair kernel stages the rows
 // in this order and the list builder encodes entries with the same index.
+__host__ __device__ __forceinline__ int wrap_near(int k, int n) {
+    // k in [-n, 2n): the periodic index without a division (the stencil offsets
+    // are -1..+1, so (c - 1 + i + n) % n of binning.f90 never needs more)
+    return k < 0 ? k + n : (k >= n ? k - n : k);
+}
 __host__ __device__ __forceinline__ void neighbour_row(int rule, int cy, int cz, int iy, int iz, int ny, int nz,
                                                        int& ky, int& kz) {
     if (rule == 0) {
-        ky = (cy - 1 + iy + ny) % ny;
-        kz = (cz - 1 + iz + nz) % nz;
+        ky = wrap_near(cy - 1 + iy, ny);
+        kz = wrap_near(cz - 1 + iz, nz);
     } else {
         ky = cy + iy - 1;
         if (ky < 0) ky = ny - 1;
