@@ -377,7 +377,7 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
     A(dalloc(&c->counters, R_N));
     A(dalloc(&c->dscal, S_NSLOT));
     A(dalloc(&c->dflags, F_NFLAG));
-    A(dalloc(&c->dstep, 1));
+    A(dalloc(&c->dstep, 2));
     A(dalloc(&c->tabs, 6 * T8 * T8));
     if (rc == MFA_OK && cudaMallocHost((void**)&c->h_stage, (size_t)3 * n * sizeof(double)) != cudaSuccess)
         rc = MFA_ERR_NOMEM;
@@ -428,13 +428,14 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
     A(dzero(c, c->counters, R_N * sizeof(unsigned)));
     A(dzero(c, c->dscal, S_NSLOT * 8));
     A(dzero(c, c->dflags, F_NFLAG * 4));
-    A(dzero(c, c->dstep, 8));
+    A(dzero(c, c->dstep, 16));
     A(h2d(c, d12, soa.data(), soa.size() * 8));
     A(h2d(c, i7, mic.data(), mic.size() * 4));
     A(h2d(c, c->type, a_type, (size_t)n * 4));
     A(h2d(c, d3, m3.data(), m3.size() * 8));
     A(h2d(c, c->tabs, tabs.data(), tabs.size() * 8));
     if (rc == MFA_OK) rc = bonds_setup(c);
+    if (rc == MFA_OK) rc = set_energy_step(c, -1);
     if (rc == MFA_OK) {
         // pair kernel: 2 list entries per lane and round, 128-thread blocks
         // of consecutive slots; the tile (used when tiling is switched on) is
@@ -568,6 +569,8 @@ int mfa_step(mfa_ctx* c, int32_t nsteps) {
         c->i_time += 1;
         return MFA_OK;
     }
+    // energies of the last step only (and of the steps the energy log records)
+    TRY(set_energy_step(c, c->i_time + nsteps));
     // first step: positions (+ skin check, force reset), conditional rebuild
     TRY(launch_vv_positions(c, 1, 1));
     TRY(launch_rebuild(c, c->bin_type, 1));
@@ -583,6 +586,7 @@ int mfa_step(mfa_ctx* c, int32_t nsteps) {
     // last step: forces and the velocity half
     TRY(forces_fused(c));
     TRY(launch_vv_velocities(c, 1));
+    TRY(set_energy_step(c, -1));
     c->i_time += nsteps;
     return MFA_OK;
 }

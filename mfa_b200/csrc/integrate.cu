@@ -190,11 +190,14 @@ __device__ __forceinline__ void finish_energies(const VVArgs& a) {
     }
 }
 
-// the FENE bonds at the clamp counted by the warp, and the block sums of
-// m v^2, FENE (times k_chain, intra_molec.f90:272,300) and bending energy
-__device__ __forceinline__ bool vv_commit(const VVArgs& a, double ke, const double eb[2], int clamped, Blk blk) {
+// the FENE bonds at the clamp counted by the warp, and -- in the steps whose
+// energies are wanted (en) -- the block sums of m v^2, FENE (times k_chain,
+// intra_molec.f90:272,300) and bending energy; true in the last block
+__device__ __forceinline__ bool vv_commit(const VVArgs& a, double ke, const double eb[2], int clamped, Blk blk,
+                                          bool en) {
     for (int o = 16; o > 0; o >>= 1) clamped += __shfl_down_sync(0xffffffffu, clamped, o);
     if ((threadIdx.x & 31) == 0 && clamped) atomicAdd(&a.flags[F_FENE], clamped);
+    if (!en) return block_arrive_last(a.counter, blk);
     double acc[3] = {ke, a.bond.k_chain * eb[0], eb[1]};
     return block_sum_commit<3>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_TMP0, blk);
 }
@@ -210,8 +213,9 @@ __device__ __forceinline__ void vv_velocities_body(const VVArgs& a, Blk blk) {
         a.vx[i] = vx; a.vy[i] = vy; a.vz[i] = vz;
         a.ax[i] = ax; a.ay[i] = ay; a.az[i] = az;
     }
-    if (vv_commit(a, ke, eb, clamped, blk)) {
-        if (threadIdx.x == 0) finish_energies(a);
+    const bool en = energy_needed(a.dstep, a.elog ? a.elog_every : 0);
+    if (vv_commit(a, ke, eb, clamped, blk, en)) {
+        if (threadIdx.x == 0 && en) finish_energies(a);
     }
 }
 
@@ -235,9 +239,11 @@ __device__ __forceinline__ void vv_fused_body(const VVArgs& a, Blk blk) {
         // is written by the velocity half that closes a run of steps
         position_half<R4>(a, i, a.rx[i], a.ry[i], a.rz[i], vx, vy, vz, ax, ay, az, true);
     }
-    if (vv_commit(a, ke, eb, clamped, blk)) {
+    // every block reads the step before the last block advances it
+    const bool en = energy_needed(a.dstep, a.elog ? a.elog_every : 0);
+    if (vv_commit(a, ke, eb, clamped, blk, en)) {
         if (threadIdx.x == 0) {
-            finish_energies(a);
+            if (en) finish_energies(a);
             *a.dstep += 1;  // the next step has begun
             // every block's skin verdict is visible here (each fenced before
             // taking its turn on the counter).  Only a rebuild that is due
@@ -336,6 +342,15 @@ int launch_vv_grouped(int prec, int stage, const void* dargs, const int* doff, i
     if (prec == MFA_MIXED) k_vv_grouped<float4><<<nblocks, TPB, 0, st>>>((const VVArgs*)dargs, doff, nsys, stage);
     else k_vv_grouped<double4><<<nblocks, TPB, 0, st>>>((const VVArgs*)dargs, doff, nsys, stage);
     MFA_CUDA_TRY(cudaGetLastError());
+    return MFA_OK;
+}
+
+__global__ void k_set_i64(int64_t* p, long long v) { *p = v; }
+
+int set_energy_step(mfa_ctx* c, long long step) {
+    k_set_i64<<<1, 1, 0, c->st>>>(c->dstep + 1, step);
+    MFA_CUDA_TRY(cudaGetLastError());
+    note_launch(c, 1);
     return MFA_OK;
 }
 

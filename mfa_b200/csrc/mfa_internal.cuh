@@ -88,7 +88,8 @@ struct mfa_ctx {
     unsigned* counters;                 // R_N
     double* dscal;                      // S_NSLOT
     int32_t* dflags;                    // F_NFLAG
-    int64_t* dstep;                     // device copy of i_time
+    int64_t* dstep;                     // [0] device copy of i_time; [1] the step whose energies
+                                        // are wanted (-1: every step)
     // Ewald
     int nk;
     double4* kvec;                      // (kx, ky, kz, inv_k2*exp(-k2/(4 alpha_c)))
@@ -134,6 +135,8 @@ enum { VV_POSITIONS = 0, VV_VELOCITIES = 1, VV_FUSED = 2 };
 // integrate.cu
 int launch_vv_positions(mfa_ctx* c, int fused_skin, int zero_force);
 int launch_check_skin(mfa_ctx* c);
+// sets the step whose energies the kernels accumulate (-1: every step)
+int set_energy_step(mfa_ctx* c, long long step);
 int launch_vv_velocities(mfa_ctx* c, int fuse_bonds);
 int launch_vv_fused(mfa_ctx* c, cudaGraphConditionalHandle rebuild_cond, int fuse_bonds);
 // argument record of an integrator stage (for grouped launches) and the launch
@@ -195,6 +198,14 @@ __device__ __forceinline__ float mimage32(float d, float L, float invL) {
 
 __device__ __forceinline__ void set_err(int32_t* flags, int status) {
     atomicOr(&flags[F_ERR], 1 << status);
+}
+
+// Whether the kernels of the current step accumulate energies: always for the
+// subroutine entry points (dstep[1] = -1), else for the last step of an
+// mfa_step run (dstep[1]) and the steps the energy log records.
+__device__ __forceinline__ bool energy_needed(const int64_t* dstep, int elog_every) {
+    const long long st = dstep[0], want = dstep[1];
+    return want < 0 || st == want || (elog_every > 0 && st % elog_every == 0);
 }
 
 // Philox-4x32-10 (Salmon et al., SC'11), counter (c0..c3), key (k0, k1).
@@ -333,6 +344,21 @@ __device__ __forceinline__ bool block_sum_commit(double (&v)[NQ], double* partia
             if (lane == 0) out[q] = y;
         }
     }
+    if (threadIdx.x == 0) *counter = 0u;
+    return true;
+}
+
+// Arrival of a block that has no sums to commit: true in the last block to
+// arrive (which resets the counter); the writes of every block before its
+// arrival are visible to that block.
+__device__ __forceinline__ bool block_arrive_last(unsigned* counter, Blk blk) {
+    __shared__ bool arrive_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) arrive_last = (atomicAdd(counter, 1u) == (unsigned)blk.n - 1);
+    __syncthreads();
+    if (!arrive_last) return false;
+    __threadfence();
     if (threadIdx.x == 0) *counter = 0u;
     return true;
 }

@@ -62,6 +62,7 @@ struct PairArgs {
     double lj_energy_factor;  // 1 (half list) or 1/2 (full list: every pair seen twice)
     double L[3], invL[3];
     double sig, friction, dt;
+    int elog_every;           // energy log period (0: none): steps whose energies are wanted
     double r_2_min_init, r_2_min_time;
     long long s_time;
     double sqrt_alpha, alpha_c, inv_sqrt_pi, ewald_rc_2;
@@ -356,6 +357,7 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
     const R4* svel = tile ? tvel : gvel;
     R4* f4 = (R4*)a.force;
     const long long step = *a.dstep;
+    const bool EN = energy_needed(a.dstep, a.elog_every);   // uniform over the grid
     R r2min = 0;
     if (FSW) {
         // fluid_fluid.f90:42-49 force switch-on
@@ -398,10 +400,10 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
             const R r61 = s_sig2[ij] * inv_r2;
             const R r6 = r61 * r61 * r61;
             const R r12 = r6 * r6;
-            e_lj += eps * ((r12 - r6) - s_esh[ij]);
+            if (EN) e_lj += eps * ((r12 - r6) - s_esh[ij]);
             const R fs = eps * ((R)12 * r12 - (R)6 * r6) * inv_r2;   // force on i along d
             fsum = fs;
-            vir += fs * r2;
+            if (EN) vir += fs * r2;
             if (DPD || QLJ) {
                 const R inv_r = rsqrt_(r2c);
                 if (DPD) {
@@ -422,11 +424,11 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
                     const R qq = vq.w * vj.w;
                     const R r = r2c * inv_r;
                     const R ec = erfc_(SQA * r);
-                    e_c += qq * ec * inv_r;
+                    if (EN) e_c += qq * ec * inv_r;
                     const R fsc = qq * SQA * ISP * (R)2 * exp_(-ALC * r2c) * inv_r +
                                   qq * ec * inv_r * inv_r;
                     fsum += fsc * inv_r;
-                    vir += fsc * r2 * inv_r;
+                    if (EN) vir += fsc * r2 * inv_r;
                 }
             }
         }
@@ -435,11 +437,11 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
             const R ir = rsqrt_(r2);
             const R r = r2 * ir;
             const R ec = erfc_(SQA * r);
-            e_c += qq * ec * ir;
+            if (EN) e_c += qq * ec * ir;
             const R fsc = qq * SQA * ISP * (R)2 * exp_(-ALC * r2) * ir +
                           qq * ec * ir * ir;
             fsum += fsc * ir;
-            vir += fsc * r2 * ir;
+            if (EN) vir += fsc * r2 * ir;
         }
         const R fx = fsum * d.x, fy = fsum * d.y, fz = fsum * d.z;
         atomicAdd(&facc[ol], fx);
@@ -560,6 +562,7 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
         }
         __syncwarp();
     }
+    if (!EN) return;   // no energies this step: nothing to reduce
     if (WALL) {
         double acc[4] = {a.lj_energy_factor * (double)e_lj, a.lj_energy_factor * (double)vir, (double)e_c,
                          (double)e_w};
@@ -736,6 +739,7 @@ int pair_stage_args(mfa_ctx* c, int fuse_wall, void* out, int* grid_out, size_t*
     a.fuse_wall = fuse_wall && p.wall == 2;
     for (int d = 0; d < 3; ++d) { a.L[d] = p.boundary[d]; a.invL[d] = c->inv_boundary[d]; }
     a.sig = p.sig; a.friction = p.friction; a.dt = p.dt;
+    a.elog_every = c->elog ? c->elog_every : 0;
     a.r_2_min_init = p.r_2_min_init; a.r_2_min_time = p.r_2_min_time; a.s_time = p.s_time;
     a.sqrt_alpha = p.sqrt_alpha; a.alpha_c = p.alpha_c; a.inv_sqrt_pi = p.inv_sqrt_pi;
     a.ewald_rc_2 = p.ewald_rc_2;

@@ -315,6 +315,36 @@ def test_energy_log_and_dpd_temperature(melt_cfg):
     g.close()
 
 
+@pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg"])
+def test_energy_log_of_the_fast_path(name, request):
+    """Within a multi-step mfa_step run the kernels reduce energies only for the
+    steps the energy log records and for the last step; those entries equal the
+    energies the per-step path reports at the same steps (FP64, to rounding of
+    the differently fused reductions)."""
+    cfg = request.getfixturevalue(name)
+    g1 = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, precision=FP64)
+    g2 = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, precision=FP64)
+    g1.init_forces()
+    g2.init_forces()
+    want = []
+    for k in range(1, 48):
+        g1.md_step()
+        if k % 10 == 0:
+            s = g1.scalars()
+            want.append((k, s["e_total"], s["t_fluid"]))
+    g2.set_energy_log(10, 100)
+    g2.step(47)
+    log = g2.energy_log()
+    assert [int(x) for x in log[:, 0]] == [w[0] for w in want]
+    for row, (k, e_tot, t_kin) in zip(log, want):
+        assert row[1] == pytest.approx(e_tot, rel=1e-11)
+        assert row[3] == pytest.approx(t_kin, rel=1e-11)
+    s1, s2 = g1.scalars(), g2.scalars()
+    assert s2["i_time"] == 47 and s1["e_total"] == pytest.approx(s2["e_total"], rel=1e-11)
+    g1.close()
+    g2.close()
+
+
 @pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg", "charged_small_cfg"])
 @pytest.mark.parametrize("prec", [FP64, MIXED])
 def test_fused_forces_equal_the_subroutines(name, prec, request):
