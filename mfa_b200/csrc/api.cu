@@ -67,13 +67,14 @@ int check_params(const mfa_params* p, int precision) {
 }
 
 void invalidate_graph(mfa_ctx* c) {
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < 3 + N_CALL_GRAPHS; ++k) {
         if (c->gexec[k]) cudaGraphExecDestroy(c->gexec[k]);
         if (c->graph[k]) cudaGraphDestroy(c->graph[k]);
         c->gexec[k] = nullptr;
         c->graph[k] = nullptr;
         c->graph_kernels[k] = 0;
     }
+    for (int k = 0; k < N_CALL_GRAPHS; ++k) c->call_n[k] = 0;
 }
 
 void free_all(mfa_ctx* c) {
@@ -160,10 +161,12 @@ int launch_full_step(mfa_ctx* c) {
     return launch_vv_velocities(c, 1);
 }
 
-// The rebuild of a captured body step as a conditional graph node: the
-// integrator's last block sets the node's condition from the skin check, and
-// the six rebuild kernels run only when it tripped (no launches otherwise).
-int capture_vv_and_conditional_rebuild(mfa_ctx* c) {
+// The rebuild of a captured step as a conditional graph node: the kernel
+// captured before it (the integrator's last block in a body step, a one-thread
+// kernel after the first position half of a run) sets the node's condition
+// from the skin check, and the six rebuild kernels run only when it tripped
+// (no launches otherwise).  opener 0: the fused integrator; 1: positions only.
+int capture_conditional_rebuild(mfa_ctx* c, int opener) {
     cudaStreamCaptureStatus cs;
     cudaGraph_t g;
     const cudaGraphNode_t* deps = nullptr;
@@ -172,7 +175,8 @@ int capture_vv_and_conditional_rebuild(mfa_ctx* c) {
     if (cs != cudaStreamCaptureStatusActive) return MFA_ERR_STATE;
     cudaGraphConditionalHandle h;
     MFA_CUDA_TRY(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
-    TRY(launch_vv_fused(c, h, 1));
+    if (opener == 0) TRY(launch_vv_fused(c, h, 1));
+    else TRY(launch_open_rebuild(c, h));
     MFA_CUDA_TRY(cudaStreamGetCaptureInfo(c->st, &cs, nullptr, &g, &deps, &nd));
     cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
     np.conditional.handle = h;
@@ -196,21 +200,45 @@ int capture_vv_and_conditional_rebuild(mfa_ctx* c) {
 // with positions of n+1, then the rebuild of n+1 if due.
 int launch_body_step(mfa_ctx* c) {
     TRY(forces_fused(c));
-    if (c->capturing && c->cond_rebuild) return capture_vv_and_conditional_rebuild(c);
+    if (c->capturing && c->cond_rebuild) return capture_conditional_rebuild(c, 0);
     TRY(launch_vv_fused(c, 0, 1));
     return launch_rebuild(c, c->bin_type, 1);
 }
 
-// kind 0: one full step; 1: one body step; 2: GRAPH_BODY body steps
+// The first step of a run of nsteps >= 2 steps: positions (+ skin check, force
+// reset; the run's last step is the one whose energies are reduced), then the
+// rebuild if due.
+int launch_head_step(mfa_ctx* c, int nsteps) {
+    TRY(launch_vv_positions(c, 1, 1, nsteps));
+    if (c->capturing && c->cond_rebuild) return capture_conditional_rebuild(c, 1);
+    return launch_rebuild(c, c->bin_type, 1);
+}
+
+// The last step of a run: forces and the velocity half (energies reduced, and
+// every step's energies wanted again afterwards).
+int launch_tail_step(mfa_ctx* c) {
+    TRY(forces_fused(c));
+    return launch_vv_velocities(c, 1, 1);
+}
+
+// kind 0: one full step; 1: one body step; 2: GRAPH_BODY body steps;
+// 3 + k: a whole run of call_n[k] steps (head, body steps, tail)
 int capture(mfa_ctx* c, int kind) {
     cudaGraph_t g;
     MFA_CUDA_TRY(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
     c->capturing = 1;
     c->cap_count = 0;
     int rc = MFA_OK;
-    if (kind == 0) rc = launch_full_step(c);
-    else
+    if (kind == 0) {
+        rc = launch_full_step(c);
+    } else if (kind >= 3) {
+        const int n = c->call_n[kind - 3];
+        rc = launch_head_step(c, n);
+        for (int s = 1; s < n && rc == MFA_OK; ++s) rc = launch_body_step(c);
+        if (rc == MFA_OK) rc = launch_tail_step(c);
+    } else {
         for (int s = 0; s < (kind == 1 ? 1 : GRAPH_BODY) && rc == MFA_OK; ++s) rc = launch_body_step(c);
+    }
     c->capturing = 0;
     cudaError_t e = cudaStreamEndCapture(c->st, &g);
     if (rc != MFA_OK) return rc;
@@ -221,12 +249,17 @@ int capture(mfa_ctx* c, int kind) {
     return MFA_OK;
 }
 
-int replay(mfa_ctx* c, int kind) {
+// the captured graphs are dropped when what their arguments point to changed
+void check_graph_key(mfa_ctx* c) {
     const void* key[4] = {c->nbr, c->elog, c->kvec, (const void*)(intptr_t)(c->bin_type + 1)};
     if (memcmp(key, c->graph_key, sizeof(key)) != 0) {
         invalidate_graph(c);
         memcpy(c->graph_key, key, sizeof(key));
     }
+}
+
+int replay(mfa_ctx* c, int kind) {
+    check_graph_key(c);
     if (!c->gexec[kind]) {
         int rc = capture(c, kind);
         if (rc != MFA_OK && c->cond_rebuild) {
@@ -234,7 +267,10 @@ int replay(mfa_ctx* c, int kind) {
             // return at once when no rebuild is due
             cudaGetLastError();
             c->cond_rebuild = 0;
+            int keep[N_CALL_GRAPHS];
+            memcpy(keep, c->call_n, sizeof(keep));
             invalidate_graph(c);
+            memcpy(c->call_n, keep, sizeof(keep));
             rc = capture(c, kind);
         }
         TRY(rc);
@@ -242,6 +278,35 @@ int replay(mfa_ctx* c, int kind) {
     MFA_CUDA_TRY(cudaGraphLaunch(c->gexec[kind], c->st));
     c->launches += c->graph_kernels[kind];
     return MFA_OK;
+}
+
+// Runs of up to CALL_GRAPH_MAX steps replay one graph for the whole run (its
+// first step's rebuild in a conditional node too), captured once per step
+// count and kept for the N_CALL_GRAPHS counts used last.
+constexpr int CALL_GRAPH_MAX = 32;
+
+int call_graph_slot(const mfa_ctx* c, int nsteps) {
+    for (int k = 0; k < N_CALL_GRAPHS; ++k)
+        if (c->call_n[k] == nsteps) return k;
+    return -1;
+}
+
+int replay_call(mfa_ctx* c, int nsteps) {
+    check_graph_key(c);
+    int k = call_graph_slot(c, nsteps);
+    if (k < 0) {
+        k = 0;
+        for (int j = 1; j < N_CALL_GRAPHS; ++j)
+            if (c->call_used[j] < c->call_used[k]) k = j;
+        if (c->gexec[3 + k]) cudaGraphExecDestroy(c->gexec[3 + k]);
+        if (c->graph[3 + k]) cudaGraphDestroy(c->graph[3 + k]);
+        c->gexec[3 + k] = nullptr;
+        c->graph[3 + k] = nullptr;
+        c->graph_kernels[3 + k] = 0;
+        c->call_n[k] = nsteps;
+    }
+    c->call_used[k] = ++c->call_clock;
+    return replay(c, 3 + k);
 }
 
 }  // namespace
@@ -435,7 +500,8 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
     A(h2d(c, d3, m3.data(), m3.size() * 8));
     A(h2d(c, c->tabs, tabs.data(), tabs.size() * 8));
     if (rc == MFA_OK) rc = bonds_setup(c);
-    if (rc == MFA_OK) rc = set_energy_step(c, -1);
+    // the step whose energies are wanted: -1 (all bytes set), every step
+    if (rc == MFA_OK && cudaMemsetAsync(c->dstep + 1, 0xFF, 8, c->st) != cudaSuccess) rc = MFA_ERR_CUDA;
     if (rc == MFA_OK) {
         // pair kernel: 2 list entries per lane and round, 128-thread blocks
         // of consecutive slots; the tile (used when tiling is switched on) is
@@ -569,11 +635,21 @@ int mfa_step(mfa_ctx* c, int32_t nsteps) {
         c->i_time += 1;
         return MFA_OK;
     }
-    // energies of the last step only (and of the steps the energy log records)
-    TRY(set_energy_step(c, c->i_time + nsteps));
-    // first step: positions (+ skin check, force reset), conditional rebuild
-    TRY(launch_vv_positions(c, 1, 1));
-    TRY(launch_rebuild(c, c->bin_type, 1));
+    // energies are reduced for the last step only (and for the steps the
+    // energy log records).  A step count seen in the previous call (or
+    // captured before) replays one graph for the whole run; a new count runs
+    // the first and last step as plain launches around the body graphs, so
+    // that calls of ever-changing length capture nothing new.
+    const bool whole = nsteps <= CALL_GRAPH_MAX &&
+                       (nsteps == c->last_call_n || call_graph_slot(c, nsteps) >= 0);
+    c->last_call_n = nsteps;
+    if (whole) {
+        TRY(replay_call(c, nsteps));
+        c->i_time += nsteps;
+        return MFA_OK;
+    }
+    // first step: positions (+ skin check, force reset), rebuild if due
+    TRY(launch_head_step(c, nsteps));
     int body = nsteps - 1;
     while (body >= GRAPH_BODY) {
         TRY(replay(c, 2));
@@ -584,9 +660,7 @@ int mfa_step(mfa_ctx* c, int32_t nsteps) {
         --body;
     }
     // last step: forces and the velocity half
-    TRY(forces_fused(c));
-    TRY(launch_vv_velocities(c, 1));
-    TRY(set_energy_step(c, -1));
+    TRY(launch_tail_step(c));
     c->i_time += nsteps;
     return MFA_OK;
 }

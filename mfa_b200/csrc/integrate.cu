@@ -46,6 +46,11 @@ struct VVArgs {
     int fuse_bonds;
     BondParams bond;
     int fused_skin, zero_force;   // position half: skin check, force reset
+    // a run of steps on the fast path: its first position half sets the step
+    // whose energies are wanted to its last step (energy_span steps on), and
+    // its last velocity half resets it to -1 (every step) afterwards
+    long long energy_span;
+    int energy_reset;
 };
 
 // r += dt v + (0.5 dt^2) a ; v += (0.5 dt) a   (verlet_positions.f90:153,169)
@@ -109,7 +114,11 @@ __device__ __forceinline__ void position_half(const VVArgs& a, int i, double x, 
 template <typename R4>
 __device__ __forceinline__ void vv_positions_body(const VVArgs& a, Blk blk) {
     const int i = blk.id * blockDim.x + threadIdx.x;
-    if (i == 0) *a.dstep += 1;
+    if (i == 0) {
+        const long long st = a.dstep[0];
+        if (a.energy_span > 0) a.dstep[1] = st + a.energy_span;
+        a.dstep[0] = st + 1;
+    }
     if (i >= a.n) return;
     position_half<R4>(a, i, a.rx[i], a.ry[i], a.rz[i], a.vx[i], a.vy[i], a.vz[i],
                       a.ax[i], a.ay[i], a.az[i], a.fused_skin != 0);
@@ -215,7 +224,10 @@ __device__ __forceinline__ void vv_velocities_body(const VVArgs& a, Blk blk) {
     }
     const bool en = energy_needed(a.dstep, a.elog ? a.elog_every : 0);
     if (vv_commit(a, ke, eb, clamped, blk, en)) {
-        if (threadIdx.x == 0 && en) finish_energies(a);
+        if (threadIdx.x == 0) {
+            if (en) finish_energies(a);
+            if (a.energy_reset) a.dstep[1] = -1;   // every block has read it
+        }
     }
 }
 
@@ -308,6 +320,8 @@ VVArgs make_args(mfa_ctx* c) {
     a.bond = bond_params(c, 0, 0);
     a.fused_skin = 0;
     a.zero_force = 0;
+    a.energy_span = 0;
+    a.energy_reset = 0;
     return a;
 }
 
@@ -345,19 +359,24 @@ int launch_vv_grouped(int prec, int stage, const void* dargs, const int* doff, i
     return MFA_OK;
 }
 
-__global__ void k_set_i64(int64_t* p, long long v) { *p = v; }
+// Opens the conditional node that holds the rebuild when the skin check of the
+// position half before it tripped (the first step of a captured run).
+__global__ void k_open_rebuild(const int32_t* flags, cudaGraphConditionalHandle h) {
+    if (*(volatile const int32_t*)&flags[F_SKIN] != 0) cudaGraphSetConditional(h, 1u);
+}
 
-int set_energy_step(mfa_ctx* c, long long step) {
-    k_set_i64<<<1, 1, 0, c->st>>>(c->dstep + 1, step);
+int launch_open_rebuild(mfa_ctx* c, cudaGraphConditionalHandle h) {
+    k_open_rebuild<<<1, 1, 0, c->st>>>(c->dflags, h);
     MFA_CUDA_TRY(cudaGetLastError());
     note_launch(c, 1);
     return MFA_OK;
 }
 
-int launch_vv_positions(mfa_ctx* c, int fused_skin, int zero_force) {
+int launch_vv_positions(mfa_ctx* c, int fused_skin, int zero_force, long long energy_span) {
     VVArgs a;
     int nb;
     TRY_(vv_stage_args(c, VV_POSITIONS, fused_skin, zero_force, 0, 0, &a, &nb));
+    a.energy_span = energy_span;
     if (c->prec == MFA_MIXED) k_vv_positions<float4><<<nb, TPB, 0, c->st>>>(a);
     else k_vv_positions<double4><<<nb, TPB, 0, c->st>>>(a);
     MFA_CUDA_TRY(cudaGetLastError());
@@ -374,10 +393,11 @@ int launch_check_skin(mfa_ctx* c) {
     return MFA_OK;
 }
 
-int launch_vv_velocities(mfa_ctx* c, int fuse_bonds) {
+int launch_vv_velocities(mfa_ctx* c, int fuse_bonds, int energy_reset) {
     VVArgs a;
     int nb;
     TRY_(vv_stage_args(c, VV_VELOCITIES, 0, 0, fuse_bonds, 0, &a, &nb));
+    a.energy_reset = energy_reset;
     if (c->prec == MFA_MIXED) k_vv_velocities<float4><<<nb, TPB, 0, c->st>>>(a);
     else k_vv_velocities<double4><<<nb, TPB, 0, c->st>>>(a);
     MFA_CUDA_TRY(cudaGetLastError());

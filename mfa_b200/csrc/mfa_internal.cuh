@@ -49,6 +49,8 @@ enum {
 
 // reduction counters (last-block-done pattern), one per reducing kernel
 enum { R_PAIR = 0, R_BOND = 1, R_WALL = 2, R_VV = 3, R_EWALD = 4, R_N = 8 };
+// whole-run graphs kept per context (distinct step counts of mfa_step calls)
+constexpr int N_CALL_GRAPHS = 4;
 
 struct mfa_ctx {
     mfa_params p;
@@ -104,10 +106,15 @@ struct mfa_ctx {
     int lists_valid;
     int n_rebuilds_host;
     // fast path: captured graphs (0: one full step, 1: one fused body step,
-    // 2: GRAPH_BODY fused body steps) and the number of kernels in each
-    cudaGraphExec_t gexec[3];
-    cudaGraph_t graph[3];
-    int graph_kernels[3];
+    // 2: GRAPH_BODY fused body steps, 3..: whole runs of call_n[k - 3] steps)
+    // and the number of kernels in each
+    cudaGraphExec_t gexec[3 + N_CALL_GRAPHS];
+    cudaGraph_t graph[3 + N_CALL_GRAPHS];
+    int graph_kernels[3 + N_CALL_GRAPHS];
+    int call_n[N_CALL_GRAPHS];
+    long long call_used[N_CALL_GRAPHS];   // last use, for replacement
+    long long call_clock;
+    int last_call_n;                      // steps of the previous mfa_step call
     const void* graph_key[4];           // what the captured arguments depend on
     int cond_rebuild;                   // rebuilds in conditional graph nodes (1) or early-exit kernels (0)
     // kernel launch accounting
@@ -133,11 +140,13 @@ enum { VV_POSITIONS = 0, VV_VELOCITIES = 1, VV_FUSED = 2 };
 
 // ---------- launchers (each file) ----------
 // integrate.cu
-int launch_vv_positions(mfa_ctx* c, int fused_skin, int zero_force);
+// energy_span > 0: the first position half of a run of that many steps
+int launch_vv_positions(mfa_ctx* c, int fused_skin, int zero_force, long long energy_span = 0);
 int launch_check_skin(mfa_ctx* c);
-// sets the step whose energies the kernels accumulate (-1: every step)
-int set_energy_step(mfa_ctx* c, long long step);
-int launch_vv_velocities(mfa_ctx* c, int fuse_bonds);
+// energy_reset: the last velocity half of a run of steps
+int launch_vv_velocities(mfa_ctx* c, int fuse_bonds, int energy_reset = 0);
+// the one-thread kernel that opens a conditional rebuild node after a position half
+int launch_open_rebuild(mfa_ctx* c, cudaGraphConditionalHandle h);
 int launch_vv_fused(mfa_ctx* c, cudaGraphConditionalHandle rebuild_cond, int fuse_bonds);
 // argument record of an integrator stage (for grouped launches) and the launch
 size_t vv_args_bytes();
