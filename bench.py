@@ -54,7 +54,58 @@ def args_():
                     help="energy drift of FP64 vs mixed over --drift-steps NVE steps (not a throughput run)")
     ap.add_argument("--drift-steps", type=int, default=100000)
     ap.add_argument("--drift-equil", type=int, default=20000)
+    ap.add_argument("--kernel-times", action="store_true",
+                    help="device time of every kernel inside the time-step loop (CUPTI through the torch "
+                         "profiler, no serialisation), per step; not a throughput run")
     return ap.parse_args()
+
+
+def kernel_times(a):
+    """Per-kernel device times of the time-step loop as it runs (captured
+    graphs, conditional rebuild nodes, L2 warm): --steps steps in --chunk-step
+    mfa_step calls after the same relaxation and autotuning as the throughput
+    run.  The activity records of CUPTI time each kernel without replaying or
+    serialising it.  Prints one JSON line."""
+    import collections
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+    from mfa_b200 import _abi
+    from mfa_b200.api import System
+    from mfa_b200.tune import autotune
+    cfg, meta = make_config(a.workload, a.seed)
+    g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=_abi.MIXED, device=0)
+    if cfg.params.charged:
+        g.ewald_k(0)
+    g.init_forces()
+    if a.equil:
+        g.step(a.equil)
+    autotune(g)
+    for _ in range(max(3, a.warmup // a.chunk)):
+        g.step(a.chunk)
+    g.sync()
+    s0 = g.scalars()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        for _ in range(a.steps // a.chunk):
+            g.step(a.chunk)
+        g.sync()
+        torch.cuda.synchronize()
+    s1 = g.scalars()
+    steps = (a.steps // a.chunk) * a.chunk
+    agg = collections.defaultdict(lambda: [0, 0.0])
+    for ev in prof.events():
+        if ev.device_type == torch.autograd.DeviceType.CUDA:
+            agg[ev.name][0] += 1
+            agg[ev.name][1] += getattr(ev, "device_time_total", 0.0)
+    total = sum(t for _, t in agg.values())
+    rows = [{"kernel": k, "launches": n, "total_us": round(t, 1), "mean_us": round(t / n, 2),
+             "us_per_step": round(t / steps, 2), "share": round(t / total, 4)}
+            for k, (n, t) in sorted(agg.items(), key=lambda kv: -kv[1][1])]
+    print(json.dumps({"workload": meta["workload"], "beads": cfg.n, "steps": steps, "chunk": a.chunk,
+                      "skin": g.params.skin, "n_bin": list(g.params.n_bin),
+                      "list_rebuilds": s1["n_rebuilds"] - s0["n_rebuilds"],
+                      "kernel_us_per_step": round(total / steps, 2), "kernels": rows}))
+    g.close()
+    return 0
 
 
 def drift(a):
@@ -462,6 +513,8 @@ def main():
     a = args_()
     if a.drift:
         return drift(a)
+    if a.kernel_times:
+        return kernel_times(a)
     if a.workload == "adjoint" and a.impl != "reference":
         return adjoint_bench(a)
     if a.workload == "batch" and a.impl != "reference":

@@ -134,19 +134,17 @@ __global__ void k_check_skin(VVArgs a) {
     if (skin_tripped(a, i, a.rx[i], a.ry[i], a.rz[i], a.mx[i], a.my[i], a.mz[i])) a.flags[F_SKIN] = 1;
 }
 
-// velocity half of verlet_velocities.f90:174-185 and the head rules :269-282.
-// Returns the kinetic contribution m v^2 of particle i.
+// velocity half of verlet_velocities.f90:174-185 and the head rules :269-282,
+// with fb the bonded force of bead i (intra_molec + bending(2),
+// md_main.f90:106-111) when fuse_bonds.  Returns the kinetic contribution
+// m v^2 of particle i.
 template <typename R4>
 __device__ __forceinline__ double velocity_half(const VVArgs& a, int i, double& vx, double& vy, double& vz,
-                                                double& ax, double& ay, double& az, double eb[2], int& clamped,
-                                                bool store_force) {
+                                                double& ax, double& ay, double& az,
+                                                const decltype(R4::x) fb[3], bool store_force) {
     R4* f = (R4*)a.force;
     R4 fi = f[i];
     if (a.fuse_bonds) {
-        // intra_molec + bending(2) (md_main.f90:106-111) for bead i
-        typedef decltype(fi.x) R;
-        R fb[3] = {0, 0, 0};
-        bonded_on_bead<R>(a.bond, i, fb, eb[0], eb[1], clamped);
         fi.x += fb[0];
         fi.y += fb[1];
         fi.z += fb[2];
@@ -216,9 +214,13 @@ __device__ __forceinline__ void vv_velocities_body(const VVArgs& a, Blk blk) {
     const int i = blk.id * blockDim.x + threadIdx.x;
     double ke = 0.0, eb[2] = {0.0, 0.0};
     int clamped = 0;
+    // the bonded force first: its chain-window loads are in flight before the
+    // force record is read (fewer registers live across them)
+    decltype(R4::x) fb[3] = {0, 0, 0};
+    if (i < a.n && a.fuse_bonds) bonded_on_bead(a.bond, i, fb, eb[0], eb[1], clamped);
     if (i < a.n) {
         double vx = a.vx[i], vy = a.vy[i], vz = a.vz[i], ax, ay, az;
-        ke = velocity_half<R4>(a, i, vx, vy, vz, ax, ay, az, eb, clamped, true);
+        ke = velocity_half<R4>(a, i, vx, vy, vz, ax, ay, az, fb, true);
         a.vx[i] = vx; a.vy[i] = vy; a.vz[i] = vz;
         a.ax[i] = ax; a.ay[i] = ay; a.az[i] = az;
     }
@@ -242,9 +244,11 @@ __device__ __forceinline__ void vv_fused_body(const VVArgs& a, Blk blk) {
     const int i = blk.id * blockDim.x + threadIdx.x;
     double ke = 0.0, eb[2] = {0.0, 0.0};
     int clamped = 0;
+    decltype(R4::x) fb[3] = {0, 0, 0};
+    if (i < a.n && a.fuse_bonds) bonded_on_bead(a.bond, i, fb, eb[0], eb[1], clamped);
     if (i < a.n) {
         double vx = a.vx[i], vy = a.vy[i], vz = a.vz[i], ax, ay, az;
-        ke = velocity_half<R4>(a, i, vx, vy, vz, ax, ay, az, eb, clamped, false);
+        ke = velocity_half<R4>(a, i, vx, vy, vz, ax, ay, az, fb, false);
         R4 z4; z4.x = 0; z4.y = 0; z4.z = 0; z4.w = 0;
         ((R4*)a.force)[i] = z4;
         // a = F/m is used at once by the position half; the stored copy of a
@@ -393,30 +397,28 @@ int launch_check_skin(mfa_ctx* c) {
     return MFA_OK;
 }
 
+// an integrator kernel on the context's stream
+int launch_vv_kernel(mfa_ctx* c, void (*kernel)(VVArgs), int nb, const VVArgs& a) {
+    kernel<<<nb, TPB, 0, c->st>>>(a);
+    MFA_CUDA_TRY(cudaGetLastError());
+    note_launch(c, 1);
+    return MFA_OK;
+}
+
 int launch_vv_velocities(mfa_ctx* c, int fuse_bonds, int energy_reset) {
     VVArgs a;
     int nb;
     TRY_(vv_stage_args(c, VV_VELOCITIES, 0, 0, fuse_bonds, 0, &a, &nb));
     a.energy_reset = energy_reset;
-    if (c->prec == MFA_MIXED) k_vv_velocities<float4><<<nb, TPB, 0, c->st>>>(a);
-    else k_vv_velocities<double4><<<nb, TPB, 0, c->st>>>(a);
-    MFA_CUDA_TRY(cudaGetLastError());
-    note_launch(c, 1);
-    return MFA_OK;
+    return launch_vv_kernel(c, c->prec == MFA_MIXED ? k_vv_velocities<float4> : k_vv_velocities<double4>, nb, a);
 }
 
 int launch_vv_fused(mfa_ctx* c, cudaGraphConditionalHandle rebuild_cond, int fuse_bonds) {
     VVArgs a;
     int nb;
     TRY_(vv_stage_args(c, VV_FUSED, 1, 1, fuse_bonds, rebuild_cond, &a, &nb));
-    if (rebuild_cond) {
-        if (c->prec == MFA_MIXED) k_vv_fused_cond<float4><<<nb, TPB, 0, c->st>>>(a);
-        else k_vv_fused_cond<double4><<<nb, TPB, 0, c->st>>>(a);
-    } else {
-        if (c->prec == MFA_MIXED) k_vv_fused<float4><<<nb, TPB, 0, c->st>>>(a);
-        else k_vv_fused<double4><<<nb, TPB, 0, c->st>>>(a);
-    }
-    MFA_CUDA_TRY(cudaGetLastError());
-    note_launch(c, 1);
-    return MFA_OK;
+    void (*k)(VVArgs);
+    if (rebuild_cond) k = c->prec == MFA_MIXED ? k_vv_fused_cond<float4> : k_vv_fused_cond<double4>;
+    else k = c->prec == MFA_MIXED ? k_vv_fused<float4> : k_vv_fused<double4>;
+    return launch_vv_kernel(c, k, nb, a);
 }
