@@ -67,7 +67,7 @@ int check_params(const mfa_params* p, int precision) {
 }
 
 void invalidate_graph(mfa_ctx* c) {
-    for (int k = 0; k < 3 + N_CALL_GRAPHS; ++k) {
+    for (int k = 0; k < 2 + N_CALL_GRAPHS; ++k) {
         if (c->gexec[k]) cudaGraphExecDestroy(c->gexec[k]);
         if (c->graph[k]) cudaGraphDestroy(c->graph[k]);
         c->gexec[k] = nullptr;
@@ -81,10 +81,11 @@ void free_all(mfa_ctx* c) {
     invalidate_graph(c);
     void* ptrs[] = {c->rx, c->mx, c->type, c->mass, c->force, c->pos_s, c->vel_s, c->pos64, c->pos32,
                     c->ids, c->cell_count, c->nbr, c->nnb, c->partials, c->counters, c->dscal,
-                    c->dflags, c->dstep, c->kvec, c->rho, c->rho_part, c->elog, c->elog_n, c->tabs};
+                    c->dstep, c->kvec, c->rho, c->rho_part, c->elog, c->elog_n, c->tabs};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->h_stage) cudaFreeHost(c->h_stage);
+    if (c->h_scal) cudaFreeHost(c->h_scal);
     if (c->st) cudaStreamDestroy(c->st);
     if (c->st_body) cudaStreamDestroy(c->st_body);
 }
@@ -151,16 +152,6 @@ int forces_fused(mfa_ctx* c) {
 
 constexpr int GRAPH_BODY = 10;
 
-// One time step as the reference orders it (md_main.f90:73-147), with the
-// rebuild decided on the device: positions (+ skin check), rebuild if due,
-// forces, velocities.
-int launch_full_step(mfa_ctx* c) {
-    TRY(launch_vv_positions(c, 1, 1));
-    TRY(launch_rebuild(c, c->bin_type, 1));
-    TRY(forces_fused(c));
-    return launch_vv_velocities(c, 1);
-}
-
 // The rebuild of a captured step as a conditional graph node: the kernel
 // captured before it (the integrator's last block in a body step, a one-thread
 // kernel after the first position half of a run) sets the node's condition
@@ -205,9 +196,10 @@ int launch_body_step(mfa_ctx* c) {
     return launch_rebuild(c, c->bin_type, 1);
 }
 
-// The first step of a run of nsteps >= 2 steps: positions (+ skin check, force
+// The first step of a run of nsteps steps: positions (+ skin check, force
 // reset; the run's last step is the one whose energies are reduced), then the
-// rebuild if due.
+// rebuild if due.  A run of one step is one time step as the reference orders
+// it (md_main.f90:73-147): positions, rebuild if due, forces, velocities.
 int launch_head_step(mfa_ctx* c, int nsteps) {
     TRY(launch_vv_positions(c, 1, 1, nsteps));
     if (c->capturing && c->cond_rebuild) return capture_conditional_rebuild(c, 1);
@@ -221,23 +213,21 @@ int launch_tail_step(mfa_ctx* c) {
     return launch_vv_velocities(c, 1, 1);
 }
 
-// kind 0: one full step; 1: one body step; 2: GRAPH_BODY body steps;
-// 3 + k: a whole run of call_n[k] steps (head, body steps, tail)
+// kind 0: one body step; 1: GRAPH_BODY body steps; 2 + k: a whole run of
+// call_n[k] steps (head, body steps, tail)
 int capture(mfa_ctx* c, int kind) {
     cudaGraph_t g;
     MFA_CUDA_TRY(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
     c->capturing = 1;
     c->cap_count = 0;
     int rc = MFA_OK;
-    if (kind == 0) {
-        rc = launch_full_step(c);
-    } else if (kind >= 3) {
-        const int n = c->call_n[kind - 3];
+    if (kind >= 2) {
+        const int n = c->call_n[kind - 2];
         rc = launch_head_step(c, n);
         for (int s = 1; s < n && rc == MFA_OK; ++s) rc = launch_body_step(c);
         if (rc == MFA_OK) rc = launch_tail_step(c);
     } else {
-        for (int s = 0; s < (kind == 1 ? 1 : GRAPH_BODY) && rc == MFA_OK; ++s) rc = launch_body_step(c);
+        for (int s = 0; s < (kind == 0 ? 1 : GRAPH_BODY) && rc == MFA_OK; ++s) rc = launch_body_step(c);
     }
     c->capturing = 0;
     cudaError_t e = cudaStreamEndCapture(c->st, &g);
@@ -298,15 +288,15 @@ int replay_call(mfa_ctx* c, int nsteps) {
         k = 0;
         for (int j = 1; j < N_CALL_GRAPHS; ++j)
             if (c->call_used[j] < c->call_used[k]) k = j;
-        if (c->gexec[3 + k]) cudaGraphExecDestroy(c->gexec[3 + k]);
-        if (c->graph[3 + k]) cudaGraphDestroy(c->graph[3 + k]);
-        c->gexec[3 + k] = nullptr;
-        c->graph[3 + k] = nullptr;
-        c->graph_kernels[3 + k] = 0;
+        if (c->gexec[2 + k]) cudaGraphExecDestroy(c->gexec[2 + k]);
+        if (c->graph[2 + k]) cudaGraphDestroy(c->graph[2 + k]);
+        c->gexec[2 + k] = nullptr;
+        c->graph[2 + k] = nullptr;
+        c->graph_kernels[2 + k] = 0;
         c->call_n[k] = nsteps;
     }
     c->call_used[k] = ++c->call_clock;
-    return replay(c, 3 + k);
+    return replay(c, 2 + k);
 }
 
 }  // namespace
@@ -440,11 +430,14 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
     if (p->n_chain + p->n_chain_d + 64 > c->max_blocks) c->max_blocks = p->n_chain + p->n_chain_d + 64;
     A(dalloc(&c->partials, (size_t)R_N * 4 * c->max_blocks));
     A(dalloc(&c->counters, R_N));
-    A(dalloc(&c->dscal, S_NSLOT));
-    A(dalloc(&c->dflags, F_NFLAG));
+    static_assert(F_NFLAG % 2 == 0, "the flags fill whole doubles after the energies");
+    A(dalloc(&c->dscal, S_NSLOT + F_NFLAG / 2));
+    if (rc == MFA_OK) c->dflags = (int32_t*)(c->dscal + S_NSLOT);
     A(dalloc(&c->dstep, 2));
     A(dalloc(&c->tabs, 6 * T8 * T8));
     if (rc == MFA_OK && cudaMallocHost((void**)&c->h_stage, (size_t)3 * n * sizeof(double)) != cudaSuccess)
+        rc = MFA_ERR_NOMEM;
+    if (rc == MFA_OK && cudaMallocHost((void**)&c->h_scal, (S_NSLOT + F_NFLAG / 2) * sizeof(double)) != cudaSuccess)
         rc = MFA_ERR_NOMEM;
     if (rc != MFA_OK) { free_all(c); free(c); return rc; }
     // host-side staging
@@ -630,11 +623,6 @@ int mfa_step(mfa_ctx* c, int32_t nsteps) {
     if (nsteps == 0) return MFA_OK;
     if (c->p.charged && c->nk == 0) return MFA_ERR_STATE;
     if (!c->lists_valid) TRY(rebuild_abi(c, c->bin_type));
-    if (nsteps == 1) {
-        TRY(replay(c, 0));
-        c->i_time += 1;
-        return MFA_OK;
-    }
     // energies are reduced for the last step only (and for the steps the
     // energy log records).  A step count seen in the previous call (or
     // captured before) replays one graph for the whole run; a new count runs
@@ -652,11 +640,11 @@ int mfa_step(mfa_ctx* c, int32_t nsteps) {
     TRY(launch_head_step(c, nsteps));
     int body = nsteps - 1;
     while (body >= GRAPH_BODY) {
-        TRY(replay(c, 2));
+        TRY(replay(c, 1));
         body -= GRAPH_BODY;
     }
     while (body > 0) {
-        TRY(replay(c, 1));
+        TRY(replay(c, 0));
         --body;
     }
     // last step: forces and the velocity half
@@ -700,11 +688,12 @@ int mfa_read_energy_log(mfa_ctx* c, double* out, int32_t max_entries, int32_t* n
 
 int mfa_get_scalars(mfa_ctx* c, mfa_scalars* o) {
     if (!c || !o) return MFA_ERR_ARGS;
-    double s[S_NSLOT];
-    int32_t f[F_NFLAG];
-    MFA_CUDA_TRY(cudaMemcpyAsync(s, c->dscal, sizeof(s), cudaMemcpyDeviceToHost, c->st));
-    MFA_CUDA_TRY(cudaMemcpyAsync(f, c->dflags, sizeof(f), cudaMemcpyDeviceToHost, c->st));
+    // energies and flags are one device allocation: one copy into pinned memory
+    MFA_CUDA_TRY(cudaMemcpyAsync(c->h_scal, c->dscal, (S_NSLOT + F_NFLAG / 2) * sizeof(double),
+                                 cudaMemcpyDeviceToHost, c->st));
     MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    const double* s = c->h_scal;
+    const int32_t* f = (const int32_t*)(c->h_scal + S_NSLOT);
     memset(o, 0, sizeof(*o));
     o->v_fluid_fluid = s[S_VFF];
     o->v_fluid_wall = s[S_VFW];

@@ -88,8 +88,8 @@ struct mfa_ctx {
     double* partials;                   // R_N regions x max_blocks x 4 quantities
     int max_blocks;
     unsigned* counters;                 // R_N
-    double* dscal;                      // S_NSLOT
-    int32_t* dflags;                    // F_NFLAG
+    double* dscal;                      // S_NSLOT, followed by the flags in the same allocation
+    int32_t* dflags;                    // F_NFLAG (= dscal + S_NSLOT: one copy reads both)
     int64_t* dstep;                     // [0] device copy of i_time; [1] the step whose energies
                                         // are wanted (-1: every step)
     // Ewald
@@ -105,12 +105,12 @@ struct mfa_ctx {
     int bin_type;                       // 0 after binning, 1 after my_binning
     int lists_valid;
     int n_rebuilds_host;
-    // fast path: captured graphs (0: one full step, 1: one fused body step,
-    // 2: GRAPH_BODY fused body steps, 3..: whole runs of call_n[k - 3] steps)
-    // and the number of kernels in each
-    cudaGraphExec_t gexec[3 + N_CALL_GRAPHS];
-    cudaGraph_t graph[3 + N_CALL_GRAPHS];
-    int graph_kernels[3 + N_CALL_GRAPHS];
+    // fast path: captured graphs (0: one fused body step, 1: GRAPH_BODY fused
+    // body steps, 2..: whole runs of call_n[k - 2] steps) and the number of
+    // kernels in each
+    cudaGraphExec_t gexec[2 + N_CALL_GRAPHS];
+    cudaGraph_t graph[2 + N_CALL_GRAPHS];
+    int graph_kernels[2 + N_CALL_GRAPHS];
     int call_n[N_CALL_GRAPHS];
     long long call_used[N_CALL_GRAPHS];   // last use, for replacement
     long long call_clock;
@@ -127,6 +127,7 @@ struct mfa_ctx {
     int32_t* elog_n;
     // pinned host staging for uploads/downloads (3 x n doubles)
     double* h_stage;
+    double* h_scal;                     // pinned copy of dscal and dflags (mfa_get_scalars)
 };
 
 #define TRY_(x)                          \

@@ -407,8 +407,8 @@ def test_tiled_and_untiled_pair_kernels_agree(name, prec, request):
 @pytest.mark.parametrize("cond", ["1", "0"])
 def test_whole_run_graphs(name, cond, request, monkeypatch):
     """A step count repeated from the previous call replays one captured graph
-    for the whole run (first step's rebuild included; four counts kept, the
-    least recently used replaced).  Runs of changing length, whole-run graphs
+    for the whole run (first step's rebuild included, single steps too; four
+    counts kept, the least recently used replaced).  Runs of changing length, whole-run graphs
     and their replacement all follow the per-step path (FP64, to rounding of
     the differently fused reductions), with the energies of each run's last
     step, the step counter and the rebuild count."""
@@ -418,7 +418,7 @@ def test_whole_run_graphs(name, cond, request, monkeypatch):
     g2 = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, precision=FP64)
     g1.init_forces()
     g2.init_forces()
-    runs = [10, 10, 10, 10, 7, 7, 3, 3, 2, 2, 4, 4, 5, 5, 10, 10, 6, 7, 7]
+    runs = [10, 10, 10, 10, 7, 7, 3, 3, 2, 2, 1, 1, 1, 4, 4, 5, 5, 10, 10, 6, 7, 7]
     for n in runs:
         for _ in range(n):
             g1.md_step()
@@ -429,10 +429,10 @@ def test_whole_run_graphs(name, cond, request, monkeypatch):
         assert s2["t_fluid"] == pytest.approx(s1["t_fluid"], rel=1e-11)
     assert s1["n_rebuilds"] == s2["n_rebuilds"] and s2["n_rebuilds"] > 1
     a, b = g1.download(), g2.download()
-    # 109 steps: the pair kernel's reductions add in no fixed order, and the
+    # 125 steps: the pair kernel's reductions add in no fixed order, and the
     # dynamics amplify that rounding (as in the reproducibility test)
-    assert float(np.abs(a["r0"] - b["r0"]).max()) < 1e-11
-    assert float(np.abs(a["v"] - b["v"]).max()) < 1e-9
+    assert float(np.abs(a["r0"] - b["r0"]).max()) < 1e-10
+    assert float(np.abs(a["v"] - b["v"]).max()) < 1e-8
     assert (a["mic"] == b["mic"]).all()
     g1.close()
     g2.close()
