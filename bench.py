@@ -40,7 +40,7 @@ METRIC = "bead-steps/s"
 def args_():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--chunk", type=int, default=10, help="time steps per timed iteration (one mfa_step call)")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
