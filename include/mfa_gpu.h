@@ -222,13 +222,18 @@ int mfa_verlet_velocities(mfa_ctx* ctx);
 /* ---------------- fast path ---------------- */
 
 /* Runs nsteps complete time steps (md_main.f90:69-147) on the device: fused
- * kernels, rebuild decided on the device, each step replayed as a captured
- * CUDA graph.  No host synchronisation inside.  The rebuild of a captured
- * step sits in a conditional graph node that the integrator opens when the
- * skin check trips; with the environment variable MFA_GRAPH_CONDITIONAL=0 at
+ * kernels, rebuild decided on the device, steps replayed as captured CUDA
+ * graphs.  No host synchronisation inside.  The rebuild of a captured step
+ * sits in a conditional graph node that the integrator opens when the skin
+ * check trips; with the environment variable MFA_GRAPH_CONDITIONAL=0 at
  * mfa_init the rebuild kernels are launched every step instead and return at
  * once when no rebuild is due (for profilers that replay graph nodes one by
- * one, which do not handle conditional nodes). */
+ * one, which do not handle conditional nodes).  A call of at most 32 steps
+ * whose count equals the previous call's (or one of the four counts captured
+ * last) replays a single graph for the whole call; the first call with a new
+ * count captures nothing new.  Energies (mfa_get_scalars) are those of the
+ * call's last step; the steps in between reduce none, except the steps the
+ * energy log records. */
 int mfa_step(mfa_ctx* ctx, int32_t nsteps);
 /* Records e_total/v_total/t_fluid every `every` steps of mfa_step into a device
  * log of `capacity` entries (0 disables).  Read back with mfa_read_energy_log. */
