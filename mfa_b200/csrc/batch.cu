@@ -340,9 +340,11 @@ int mfa_batch_step(mfa_batch* b, int32_t nsteps) {
         TRY_(build_tables(b));
         b->key = current_key(b);
     }
-    // first step: positions (+ skin check, force reset), rebuild of the systems due
+    // first step: positions (+ skin check, force reset; every system reduces
+    // its energies on the last step of the run only, and on the steps its
+    // energy log records), rebuild of the systems due
     TRY_(launch_vv_grouped(b->prec, VV_POSITIONS, b->dargs + b->o_vvpos, b->doff + b->f_vv, b->nsys, b->nb_vv,
-                           b->st));
+                           b->st, nsteps));
     note(b, 1);
     TRY_(stage_rebuild(b, b->o_bin_first, b->st, false));
     int body = nsteps - 1;
@@ -357,7 +359,7 @@ int mfa_batch_step(mfa_batch* b, int32_t nsteps) {
     // last step: forces (chains' bonds in the integrator) and the velocity half
     TRY_(stage_pair(b));
     TRY_(launch_vv_grouped(b->prec, VV_VELOCITIES, b->dargs + b->o_vvvel, b->doff + b->f_vv, b->nsys, b->nb_vv,
-                           b->st));
+                           b->st, 0, 1));
     note(b, 1);
     for (mfa_ctx* c : b->ctx) c->i_time += nsteps;
     return MFA_OK;

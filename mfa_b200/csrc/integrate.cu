@@ -48,7 +48,8 @@ struct VVArgs {
     int fused_skin, zero_force;   // position half: skin check, force reset
     // a run of steps on the fast path: its first position half sets the step
     // whose energies are wanted to its last step (energy_span steps on), and
-    // its last velocity half resets it to -1 (every step) afterwards
+    // its last velocity half resets it to -1 (every step) afterwards (grouped
+    // launches pass both as kernel parameters instead)
     long long energy_span;
     int energy_reset;
 };
@@ -112,11 +113,11 @@ __device__ __forceinline__ void position_half(const VVArgs& a, int i, double x, 
 // zero_force: the fast path resets the force array here (md_main.f90:88), so
 // that the force kernels of the step only ever add to it
 template <typename R4>
-__device__ __forceinline__ void vv_positions_body(const VVArgs& a, Blk blk) {
+__device__ __forceinline__ void vv_positions_body(const VVArgs& a, Blk blk, long long energy_span) {
     const int i = blk.id * blockDim.x + threadIdx.x;
     if (i == 0) {
         const long long st = a.dstep[0];
-        if (a.energy_span > 0) a.dstep[1] = st + a.energy_span;
+        if (energy_span > 0) a.dstep[1] = st + energy_span;
         a.dstep[0] = st + 1;
     }
     if (i >= a.n) return;
@@ -210,7 +211,7 @@ __device__ __forceinline__ bool vv_commit(const VVArgs& a, double ke, const doub
 }
 
 template <typename R4>
-__device__ __forceinline__ void vv_velocities_body(const VVArgs& a, Blk blk) {
+__device__ __forceinline__ void vv_velocities_body(const VVArgs& a, Blk blk, int energy_reset) {
     const int i = blk.id * blockDim.x + threadIdx.x;
     double ke = 0.0, eb[2] = {0.0, 0.0};
     int clamped = 0;
@@ -228,7 +229,7 @@ __device__ __forceinline__ void vv_velocities_body(const VVArgs& a, Blk blk) {
     if (vv_commit(a, ke, eb, clamped, blk, en)) {
         if (threadIdx.x == 0) {
             if (en) finish_energies(a);
-            if (a.energy_reset) a.dstep[1] = -1;   // every block has read it
+            if (energy_reset) a.dstep[1] = -1;   // every block has read it
         }
     }
 }
@@ -273,25 +274,27 @@ __device__ __forceinline__ void vv_fused_body(const VVArgs& a, Blk blk) {
 
 // plain launches (one context) and grouped launches (the same stage for
 // several contexts, argument records in device memory)
-template <typename R4> __global__ void k_vv_positions(VVArgs a) { vv_positions_body<R4>(a, plain_blk()); }
+template <typename R4>
+__global__ void k_vv_positions(VVArgs a) { vv_positions_body<R4>(a, plain_blk(), a.energy_span); }
 // 64 registers in MIXED: four 256-thread blocks per SM (the bonded window of
 // the chain beads would otherwise take ~80; at 48 registers it spills, and the
 // spills cost more than the extra wave: measured 58.3 vs 60.9 us per step);
 // FP64 keeps 85 (three blocks), where 64 would spill the doubled operands
 #define VV_BOUNDS __launch_bounds__(256, sizeof(R4) == 16 ? 4 : 3)
 template <typename R4>
-__global__ void VV_BOUNDS k_vv_velocities(VVArgs a) { vv_velocities_body<R4>(a, plain_blk()); }
+__global__ void VV_BOUNDS k_vv_velocities(VVArgs a) { vv_velocities_body<R4>(a, plain_blk(), a.energy_reset); }
 template <typename R4>
 __global__ void VV_BOUNDS k_vv_fused(VVArgs a) { vv_fused_body<R4, false>(a, plain_blk()); }
 template <typename R4>
 __global__ void VV_BOUNDS k_vv_fused_cond(VVArgs a) { vv_fused_body<R4, true>(a, plain_blk()); }
 template <typename R4>
 __global__ void VV_BOUNDS
-    k_vv_grouped(const VVArgs* __restrict__ as, const int* __restrict__ off, int nsys, int stage) {
+    k_vv_grouped(const VVArgs* __restrict__ as, const int* __restrict__ off, int nsys, int stage,
+                 long long energy_span, int energy_reset) {
     const int s = group_of(off, nsys, blockIdx.x);
     const Blk blk = group_blk(off, s);
-    if (stage == VV_POSITIONS) vv_positions_body<R4>(as[s], blk);
-    else if (stage == VV_VELOCITIES) vv_velocities_body<R4>(as[s], blk);
+    if (stage == VV_POSITIONS) vv_positions_body<R4>(as[s], blk, energy_span);
+    else if (stage == VV_VELOCITIES) vv_velocities_body<R4>(as[s], blk, energy_reset);
     else vv_fused_body<R4, true>(as[s], blk);
 }
 
@@ -356,9 +359,11 @@ int vv_stage_args(mfa_ctx* c, int stage, int fused_skin, int zero_force, int fus
 size_t vv_args_bytes() { return sizeof(VVArgs); }
 
 int launch_vv_grouped(int prec, int stage, const void* dargs, const int* doff, int nsys, int nblocks,
-                      cudaStream_t st) {
-    if (prec == MFA_MIXED) k_vv_grouped<float4><<<nblocks, TPB, 0, st>>>((const VVArgs*)dargs, doff, nsys, stage);
-    else k_vv_grouped<double4><<<nblocks, TPB, 0, st>>>((const VVArgs*)dargs, doff, nsys, stage);
+                      cudaStream_t st, long long energy_span, int energy_reset) {
+    const VVArgs* as = (const VVArgs*)dargs;
+    if (prec == MFA_MIXED)
+        k_vv_grouped<float4><<<nblocks, TPB, 0, st>>>(as, doff, nsys, stage, energy_span, energy_reset);
+    else k_vv_grouped<double4><<<nblocks, TPB, 0, st>>>(as, doff, nsys, stage, energy_span, energy_reset);
     MFA_CUDA_TRY(cudaGetLastError());
     return MFA_OK;
 }

@@ -153,8 +153,10 @@ int launch_vv_fused(mfa_ctx* c, cudaGraphConditionalHandle rebuild_cond, int fus
 size_t vv_args_bytes();
 int vv_stage_args(mfa_ctx* c, int stage, int fused_skin, int zero_force, int fuse_bonds,
                   cudaGraphConditionalHandle rebuild_cond, void* out, int* nblocks);
+// energy_span / energy_reset: the first position half / last velocity half of
+// a run of steps (as launch_vv_positions / launch_vv_velocities)
 int launch_vv_grouped(int prec, int stage, const void* dargs, const int* doff, int nsys, int nblocks,
-                      cudaStream_t st);
+                      cudaStream_t st, long long energy_span = 0, int energy_reset = 0);
 // binning.cu
 int launch_rebuild(mfa_ctx* c, int rule, int conditional);
 int launch_rebuild_on(mfa_ctx* c, int rule, int conditional, cudaStream_t st, int in_cond_body);

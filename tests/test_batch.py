@@ -58,6 +58,15 @@ def test_batch_equals_systems_stepped_alone(prec):
         assert s2["e_total"] == pytest.approx(s1["e_total"], rel=1e-10 if prec == FP64 else 1e-5)
     # one launch per stage for all four systems: two per step plus the rebuilds
     assert b.launches() < 2 * 47 + 6 * 47
+    # further runs: the energies reduced are those of each run's last step
+    for n in (10, 10, 3):
+        for g in alone:
+            g.step(n)
+        b.step(n)
+        for g1, s2 in zip(alone, b.scalars()):
+            s1 = g1.scalars()
+            assert s2["i_time"] == s1["i_time"]
+            assert s2["e_total"] == pytest.approx(s1["e_total"], rel=1e-9 if prec == FP64 else 1e-4)
     b.close()
     for g in alone + grouped:
         g.close()
