@@ -204,9 +204,10 @@ int mfa_fluid_fluid(mfa_ctx* ctx);
  * mfa_fluid_wall.  Adds to force.  The pair kernel the time-step loop of
  * mfa_step runs. */
 int mfa_pair_forces(mfa_ctx* ctx);
-/* Every force of a step, md_main.f90:93-131: mfa_pair_forces, ewald_k(1) and
- * the chains' intra_molec + bending(2) (one pass, thread per bead).  Adds to
- * force (after mfa_zero_forces it replaces the six subroutine calls). */
+/* Every force of a step, md_main.f90:93-131: mfa_pair_forces, ewald_k(1),
+ * dipolar_correction (charged SYMMETRY 0) and the chains' intra_molec +
+ * bending(2) (one pass, thread per bead).  Adds to force (after
+ * mfa_zero_forces it replaces the seven subroutine calls). */
 int mfa_forces(mfa_ctx* ctx);
 /* fluid_wall.f90:2-204, inter_type 2, 3 or 4.  Adds to force (2,3), reflects v (3,4). */
 int mfa_fluid_wall(mfa_ctx* ctx, int32_t inter_type);
@@ -216,6 +217,12 @@ int mfa_intra_molec(mfa_ctx* ctx);
 int mfa_bending(mfa_ctx* ctx, int32_t mode);
 /* ewald_k.f90:1-211 (mode 0: build k-vectors, mode 1: k-space energy + force). */
 int mfa_ewald_k(mfa_ctx* ctx, int32_t mode);
+/* dipolar_correction.f90:17-39, called after ewald_k(1) for SYMMETRY 0
+ * (md_main.f90:128-131): the slab correction of Yeh and Berkowitz,
+ * M_z = sum q (z - Lz/2), F_z -= 4 pi q M_z / V, v_coul += 2 pi M_z^2 / V, with
+ * V the slab volume of ewald_k(0).  Adds to force; nothing for uncharged or
+ * SYMMETRY 1 systems; MFA_ERR_STATE before mfa_ewald_k(ctx, 0). */
+int mfa_dipolar_correction(mfa_ctx* ctx);
 /* verlet_velocities.f90:1-246: a = F/m, v += dt/2 a, heads pinned, energies. */
 int mfa_verlet_velocities(mfa_ctx* ctx);
 

@@ -118,6 +118,7 @@ SIGNATURES = {
     "mfa_intra_molec": (C.c_int, [_P]),
     "mfa_bending": (C.c_int, [_P, C.c_int32]),
     "mfa_ewald_k": (C.c_int, [_P, C.c_int32]),
+    "mfa_dipolar_correction": (C.c_int, [_P]),
     "mfa_verlet_velocities": (C.c_int, [_P]),
     "mfa_step": (C.c_int, [_P, C.c_int32]),
     "mfa_set_energy_log": (C.c_int, [_P, C.c_int32, C.c_int32]),

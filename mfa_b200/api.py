@@ -116,6 +116,9 @@ class System:
     def ewald_k(self, mode: int) -> None:
         check(self.lib.mfa_ewald_k(self.ctx, int(mode)), "ewald_k")
 
+    def dipolar_correction(self) -> None:
+        check(self.lib.mfa_dipolar_correction(self.ctx), "dipolar_correction")
+
     def verlet_velocities(self) -> None:
         check(self.lib.mfa_verlet_velocities(self.ctx), "verlet_velocities")
 
@@ -138,6 +141,8 @@ class System:
             self.bending(2)
         if full and p.charged:
             self.ewald_k(1)
+            if p.symmetry == 0:
+                self.dipolar_correction()
         f = self.download(_abi.F)["force"]
         self.upload(a=f / self.mass[:, None])
 
@@ -158,6 +163,8 @@ class System:
             self.bending(2)
         if p.charged:
             self.ewald_k(1)
+            if p.symmetry == 0:
+                self.dipolar_correction()     # md_main.f90:128-131
         self.verlet_velocities()
         return f_skin
 

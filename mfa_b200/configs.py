@@ -328,6 +328,47 @@ def charged(seed: int = 12345, n_chain: int = 200, n_mon: int = 50, density: flo
     return Config("charged", spec, p, r0, _maxwell(rng, mass, 1.0), a_type, mass, q)
 
 
+def charged_slab(seed: int = 12345, n_chain: int = 20, n_mon: int = 20, density: float = 0.5,
+                 z_wall: float = 12.0, alpha: float = 0.8, rc_real: float = 3.0, n_kmax: int = 4,
+                 skin: float = 0.3, friction: float = 0.5, thermostat: int = _abi.THERMO_LGV) -> Config:
+    """Polyelectrolyte chains (charge -1 on every second bead) and monovalent
+    counterions between two 9-3 walls at z = 0 and z = z_wall: the charged
+    channel (SYMMETRY 0, WALL 2) whose Ewald sum takes the slab k-set
+    (ewald_k.f90:41-46, an empty gap of twice the channel width in z) and the
+    dipolar correction of dipolar_correction.f90.
+
+    Types: 1 = neutral bead, 2 = charged bead (-1), 3 = counterion (+1)."""
+    rng = np.random.default_rng(seed)
+    n_poly = n_chain * n_mon
+    n_ci = n_poly // 2
+    n = n_poly + n_ci
+    lxy = math.sqrt(n / (density * z_wall))
+    box = np.array([lxy, lxy, z_wall])
+    periodic = np.array([True, True, False])
+    grid = _Grid(box, periodic, 0.8)
+    lo, hi = np.array([0.0, 0.0, 0.9]), np.array([lxy, lxy, z_wall - 0.9])
+    heads, hid = _place_free(rng, grid, n_chain, lo, hi)
+    chains = _grow_chains(rng, grid, heads, hid, n_mon, 0.97, box, periodic, zlim=(0.9, z_wall - 0.9))
+    ci, _ = _place_free(rng, grid, n_ci, lo, hi)
+    r0 = np.concatenate([chains.reshape(-1, 3), ci], axis=0)
+    a_type = np.ones(n, dtype=np.int32)
+    a_type[1:n_poly:2] = 2
+    a_type[n_poly:] = 3
+    charge = {1: 0.0, 2: -1.0, 3: 1.0}
+    q = np.array([charge[t] for t in a_type])
+    mass = np.ones(n)
+    spec = Spec(n_part=n, boundary=box, n_type=3, n_mon=n_mon, n_chain=n_chain, symmetry=0, wall=2,
+                thermostat=thermostat, friction=friction, charged=1, skin=skin, dt=0.005, temp=1.0,
+                k_chain_in=30.0, r_chain=1.5, alpha_c=alpha * alpha, n_kmax=n_kmax, ewald_rc=rc_real,
+                wall_cut=2.5, quirks=_abi.Q_WALL_ENERGY_AW, seed=seed)
+    p = derive(spec)
+    p.inv_sqrt_pi = 1.0 / math.sqrt(p.pi)
+    for d in range(3):
+        p.n_bin[d] = max(1, int(box[d] / (rc_real + skin)))
+        p.delta_bin[d] = 1 if p.n_bin[d] >= 3 else (0 if p.n_bin[d] == 2 else -1)
+    return Config("charged_slab", spec, p, r0, _maxwell(rng, mass, 1.0), a_type, mass, q)
+
+
 def brush_stretched(seed: int = 12345, nx: int = 16, ny: int = 16, n_mon: int = 64, graft: float = 0.3,
                     z_wall: Optional[float] = None, friction: float = 4.5, skin: float = 0.3,
                     z_head: float = 1.0, jitter: float = 0.15) -> Config:

@@ -146,7 +146,10 @@ int forces_fused(mfa_ctx* c) {
     // fluid_wall is called for SYMMETRY 0 only (md_main.f90:97)
     TRY(launch_pair(c, c->p.symmetry == 0));
     if (c->p.symmetry == 0 && (c->p.wall == 3 || c->p.wall == 4)) TRY(launch_wall(c, c->p.wall));
-    if (c->p.charged) TRY(launch_ewald(c));
+    if (c->p.charged) {
+        TRY(launch_ewald(c));
+        TRY(launch_dipolar(c));   // SYMMETRY 0 only (md_main.f90:128-131)
+    }
     return MFA_OK;
 }
 
@@ -558,14 +561,17 @@ int mfa_zero_forces(mfa_ctx* c) {
 
 int mfa_fluid_fluid(mfa_ctx* c) {
     if (!c) return MFA_ERR_ARGS;
-    // fluid_fluid.f90:17 resets v_coul; the k-space part is added by ewald_k
+    // fluid_fluid.f90:17 resets v_coul; the k-space part is added by ewald_k,
+    // the slab correction by dipolar_correction
     MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VCK, 0, 8, c->st));
+    MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VDIP, 0, 8, c->st));
     return launch_pair(c, 0);
 }
 
 int mfa_pair_forces(mfa_ctx* c) {
     if (!c) return MFA_ERR_ARGS;
     MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VCK, 0, 8, c->st));
+    MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VDIP, 0, 8, c->st));
     if (c->p.symmetry != 0 || (c->p.wall != 2 && c->p.wall != 3 && c->p.wall != 4))
         MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VFW, 0, 8, c->st));
     TRY(launch_pair(c, c->p.symmetry == 0));
@@ -611,6 +617,11 @@ int mfa_ewald_k(mfa_ctx* c, int32_t mode) {
     }
     if (mode != 1) return MFA_ERR_ARGS;
     return launch_ewald(c);
+}
+
+int mfa_dipolar_correction(mfa_ctx* c) {
+    if (!c) return MFA_ERR_ARGS;
+    return launch_dipolar(c);
 }
 
 int mfa_verlet_velocities(mfa_ctx* c) {
@@ -699,7 +710,7 @@ int mfa_get_scalars(mfa_ctx* c, mfa_scalars* o) {
     o->v_fluid_wall = s[S_VFW];
     o->v_intra_molec = s[S_VINTRA];
     o->v_bend = s[S_VBEND];
-    o->v_coul = c->p.charged ? (s[S_VCR] + c->v_coul_self) + s[S_VCK] : 0.0;
+    o->v_coul = c->p.charged ? ((s[S_VCR] + c->v_coul_self) + s[S_VCK]) + s[S_VDIP] : 0.0;
     o->t_fluid = s[S_TKIN];
     o->v_total = s[S_VTOT];
     o->e_total = s[S_ETOT];

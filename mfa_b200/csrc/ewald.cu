@@ -14,6 +14,10 @@
 //                    the energy 4 pi / V sum_k inv_k2 exp(-k2/4a) |rho|^2.
 //   k_ewald_force  - thread per particle, the same per-axis tables in shared
 //                    memory, F_i = -8 pi q_i / V sum_k k inv_k2 exp(..) (cos Im - sin Re).
+// Slab correction (dipolar_correction.f90, SYMMETRY 0):
+//   k_dipole_moment - M_z = sum_i q_i (z_i - Lz/2), a deterministic grid
+//                     reduction, and the energy 2 pi M_z^2 / V;
+//   k_dipole_force  - F_z,i -= 4 pi q_i M_z / V.
 #include "mfa_internal.cuh"
 
 #include <math.h>
@@ -258,6 +262,51 @@ int launch_ewald(mfa_ctx* c) {
     else k_ewald_force<double4><<<(c->n + FT - 1) / FT, FT, fsm, c->st>>>(a);
     MFA_CUDA_TRY(cudaGetLastError());
     note_launch(c, 3);
+    return MFA_OK;
+}
+
+namespace {
+
+// dipolar_correction.f90:20-24 (lz_half = boundary(3)/2, init_config.f90:246);
+// the moment is kept in the last staging slot for the force pass, the energy
+// (:32) in S_VDIP
+constexpr int S_DIPM = S_TMP0 + 3;
+
+__global__ void k_dipole_moment(EwArgs a, double lz_half) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[1] = {0.0};
+    if (i < a.n) acc[0] = a.q[i] * (a.rz[i] - lz_half);
+    if (block_sum_commit<1>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_DIPM) && threadIdx.x == 0) {
+        const double m = a.dscal[S_DIPM];
+        a.dscal[S_VDIP] = (((2.0 * a.pi) * m) * m) * a.inv_V;
+    }
+}
+
+// dipolar_correction.f90:26-30
+template <typename R4>
+__global__ void k_dipole_force(EwArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const double qi = a.q[i];
+    if (qi == 0.0) return;
+    const double m = a.dscal[S_DIPM];
+    R4* f4 = (R4*)a.force;
+    f4[i].z -= (((4.0 * a.pi) * qi) * m) * a.inv_V;
+}
+
+}  // namespace
+
+int launch_dipolar(mfa_ctx* c) {
+    if (!c->p.charged || c->p.symmetry != 0) return MFA_OK;
+    if (c->nk == 0) return MFA_ERR_STATE;   // V is the slab volume ewald_k(0) sets
+    EwArgs a = make_args(c);
+    const int T = 256, nb = (c->n + T - 1) / T;
+    if (nb > c->max_blocks) return MFA_ERR_ARGS;
+    k_dipole_moment<<<nb, T, 0, c->st>>>(a, c->p.boundary[2] / 2.0);
+    if (c->prec == MFA_MIXED) k_dipole_force<float4><<<nb, T, 0, c->st>>>(a);
+    else k_dipole_force<double4><<<nb, T, 0, c->st>>>(a);
+    MFA_CUDA_TRY(cudaGetLastError());
+    note_launch(c, 2);
     return MFA_OK;
 }
 

@@ -28,6 +28,7 @@ enum {
     S_VTOT = 8,
     S_ETOT = 9,
     S_VCOUL = 10,   // real + self + k
+    S_VDIP = 11,    // slab dipolar correction energy (SYMMETRY 0, charged)
     S_TMP0 = 12,    // 12..15: staging for kernels that publish a subset of slots
     S_NSLOT = 16
 };
@@ -183,6 +184,8 @@ int launch_wall(mfa_ctx* c, int inter_type);
 // ewald.cu
 int ewald_setup(mfa_ctx* c);
 int launch_ewald(mfa_ctx* c);
+// dipolar_correction.f90 (charged SYMMETRY 0; nothing otherwise)
+int launch_dipolar(mfa_ctx* c);
 
 // every kernel launch is recorded (graph captures count towards their graph)
 inline void note_launch(mfa_ctx* c, int k) {

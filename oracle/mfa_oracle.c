@@ -839,6 +839,22 @@ int orc_ewald_k(orc_state* s, int mode) {
     return MFA_OK;
 }
 
+/* dipolar_correction.f90:17-39 (Yeh-Berkowitz slab correction, called after
+ * ewald_k(1) for SYMMETRY 0, md_main.f90:128-131): M_z = sum q (z - Lz/2)
+ * (lz_half = boundary(3)/2, init_config.f90:246), F_z -= 4 pi q M_z / V,
+ * v_coul += 2 pi M_z^2 / V, with V the slab volume of ewald_k.f90:92 and pi
+ * the single-precision literal widened (twopi = 2*pi exactly). */
+void orc_dipolar_correction(orc_state* s) {
+    const mfa_params* p = &s->p;
+    if (!p->charged || p->symmetry != 0) return;
+    const double lz_half = p->boundary[2] / 2.0;
+    double m_z = 0.0;
+    for (int i = 0; i < s->n; ++i) m_z = m_z + s->q[i] * (s->r0[3 * i + 2] - lz_half);
+    for (int i = 0; i < s->n; ++i)
+        s->force[3 * i + 2] = s->force[3 * i + 2] - (((4.0 * p->pi) * s->q[i]) * m_z) * s->inv_V;
+    s->v_coul = s->v_coul + (((2.0 * p->pi) * m_z) * m_z) * s->inv_V;
+}
+
 /* verlet_velocities.f90:174-185 (kick), :262-294 (heads), :304-347 (energies) */
 void orc_verlet_velocities(orc_state* s) {
     const mfa_params* p = &s->p;
@@ -882,6 +898,7 @@ int orc_md_step(orc_state* s) {
     orc_intra_molec(s);
     if (p->bending) orc_bending(s, 2);
     if (p->charged) err = orc_ewald_k(s, 1);
+    if (p->charged && p->symmetry == 0) orc_dipolar_correction(s);
     orc_verlet_velocities(s);
     return err;
 }

@@ -44,6 +44,7 @@ void orc_fluid_wall(orc_state* s, int inter_type);
 void orc_intra_molec(orc_state* s);
 void orc_bending(orc_state* s, int mode);
 int  orc_ewald_k(orc_state* s, int mode);
+void orc_dipolar_correction(orc_state* s);
 void orc_verlet_velocities(orc_state* s);
 /* one md_main.f90:68-147 iteration in the reference's call order */
 int  orc_md_step(orc_state* s);

@@ -50,6 +50,7 @@ def load():
             "orc_intra_molec": (None, [P]),
             "orc_bending": (None, [P, C.c_int]),
             "orc_ewald_k": (C.c_int, [P, C.c_int]),
+            "orc_dipolar_correction": (None, [P]),
             "orc_verlet_velocities": (None, [P]),
             "orc_md_step": (C.c_int, [P]),
             "orc_check_fluid_fluid": (C.c_double, [P]),
@@ -142,6 +143,9 @@ class Oracle:
         rc = self.lib.orc_ewald_k(self.ptr, int(mode))
         if rc:
             raise RuntimeError(f"orc_ewald_k: {rc}")
+
+    def dipolar_correction(self):
+        self.lib.orc_dipolar_correction(self.ptr)
 
     def verlet_velocities(self):
         self.lib.orc_verlet_velocities(self.ptr)

@@ -43,3 +43,9 @@ def charged_small_cfg():
 def charged_ref_cfg():
     from mfa_b200 import configs
     return configs.charged(seed=14, n_chain=24, n_mon=20, density=0.5, reference_mode=True)
+
+
+@pytest.fixture(scope="session")
+def charged_slab_cfg():
+    from mfa_b200 import configs
+    return configs.charged_slab(seed=15, n_chain=20, n_mon=20, z_wall=12.0)

@@ -19,7 +19,7 @@ from oracle import Oracle, pair_multiset_full, pair_multiset_half, pair_multiset
 
 pytestmark = pytest.mark.gpu
 
-CFGS = ["melt_cfg", "brush_small_cfg", "charged_small_cfg", "charged_ref_cfg"]
+CFGS = ["melt_cfg", "brush_small_cfg", "charged_small_cfg", "charged_ref_cfg", "charged_slab_cfg"]
 
 
 def pair(cfg, prec, params=None, list_cap=512):
@@ -102,7 +102,7 @@ def run_both(o, g, nsteps):
     return fo, fg
 
 
-@pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg", "charged_small_cfg"])
+@pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg", "charged_small_cfg", "charged_slab_cfg"])
 @pytest.mark.parametrize("thermo", [_abi.THERMO_NONE, _abi.THERMO_DPD])
 def test_fp64_trajectory_100_steps(name, thermo, request):
     cfg = request.getfixturevalue(name)
@@ -122,7 +122,7 @@ def test_fp64_trajectory_100_steps(name, thermo, request):
     g.close()
 
 
-@pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg", "charged_small_cfg"])
+@pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg", "charged_small_cfg", "charged_slab_cfg"])
 def test_mixed_trajectory_100_steps(name, request):
     cfg = request.getfixturevalue(name)
     o, g = pair(cfg, MIXED)
@@ -138,7 +138,7 @@ def test_mixed_trajectory_100_steps(name, request):
     g.close()
 
 
-@pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg", "charged_small_cfg"])
+@pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg", "charged_small_cfg", "charged_slab_cfg"])
 @pytest.mark.parametrize("prec", [FP64, MIXED])
 def test_fast_path_equals_subroutine_path(name, prec, request):
     """mfa_step (fused kernels, captured graphs, device-side rebuild decision)
@@ -209,7 +209,7 @@ def test_regridding_keeps_the_forces(name, request):
     g.close()
 
 
-@pytest.mark.parametrize("name", ["charged_small_cfg", "charged_ref_cfg"])
+@pytest.mark.parametrize("name", ["charged_small_cfg", "charged_ref_cfg", "charged_slab_cfg"])
 def test_ewald_kspace(name, request):
     cfg = request.getfixturevalue(name)
     o, g = pair(cfg, FP64)
@@ -228,6 +228,36 @@ def test_ewald_kspace(name, request):
     g.ewald_k(1)
     assert relerr(g.download(_abi.F)["force"], o.state()["force"]) < 1e-10
     assert g.scalars()["v_coul"] == pytest.approx(o.scalars()["v_coul"], rel=1e-11)
+    g.close()
+
+
+@pytest.mark.parametrize("prec,tol", [(FP64, 1e-12), (MIXED, 1e-6)])
+def test_dipolar_correction(charged_slab_cfg, prec, tol):
+    """dipolar_correction (SYMMETRY 0): the slab correction's force and energy
+    equal the oracle's; the fast path's force pass includes it."""
+    cfg = charged_slab_cfg
+    o, g = pair(cfg, prec)
+    o.ewald_k(0)
+    g.ewald_k(0)
+    for x in (o, g):
+        x.zero_forces()
+    u0o, u0g = o.scalars()["v_coul"], g.scalars()["v_coul"]
+    o.dipolar_correction()
+    g.dipolar_correction()
+    fo, fg = o.state()["force"], g.download(_abi.F)["force"]
+    assert np.abs(fo[:, 2]).max() > 0.0
+    assert relerr(fg, fo) < tol
+    du_o = o.scalars()["v_coul"] - u0o
+    du_g = g.scalars()["v_coul"] - u0g
+    assert du_g == pytest.approx(du_o, rel=1e-10)
+    g.close()
+
+
+def test_dipolar_correction_needs_the_kspace_setup(charged_slab_cfg):
+    cfg = charged_slab_cfg
+    g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=FP64)
+    with pytest.raises(MfaError):
+        g.dipolar_correction()
     g.close()
 
 
@@ -345,11 +375,12 @@ def test_energy_log_of_the_fast_path(name, request):
     g2.close()
 
 
-@pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg", "charged_small_cfg"])
+@pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg", "charged_small_cfg", "charged_slab_cfg"])
 @pytest.mark.parametrize("prec", [FP64, MIXED])
 def test_fused_forces_equal_the_subroutines(name, prec, request):
-    """mfa_forces (pair pass with walls and bonds fused, then Ewald k-space) =
-    fluid_fluid; fluid_wall; intra_molec; bending(2); ewald_k(1)."""
+    """mfa_forces (pair pass with walls and bonds fused, then Ewald k-space and
+    the slab correction) = fluid_fluid; fluid_wall; intra_molec; bending(2);
+    ewald_k(1); dipolar_correction (SYMMETRY 0)."""
     cfg = request.getfixturevalue(name)
     g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=prec)
     p = g.params
@@ -364,6 +395,7 @@ def test_fused_forces_equal_the_subroutines(name, prec, request):
     g.bending(2)
     if p.charged:
         g.ewald_k(1)
+        g.dipolar_correction()          # nothing for SYMMETRY 1
     f1, s1 = g.download(_abi.F)["force"], g.scalars()
     g.zero_forces()
     g.forces()

@@ -169,6 +169,63 @@ def test_forces_are_minus_energy_gradient(brush_small_cfg):
             assert g == pytest.approx(f[i, d], rel=2e-5, abs=2e-4), (i, d)
 
 
+def test_dipolar_correction_formula(charged_slab_cfg):
+    """dipolar_correction.f90:17-39 against the slab correction it states
+    (Yeh and Berkowitz): M_z = sum q (z - Lz/2), F_z = -4 pi q M_z / V and
+    U = 2 pi M_z^2 / V, with V = Lx Ly Lz (1 + 2) the slab volume of
+    ewald_k.f90:92 and pi the widened single-precision literal."""
+    cfg = charged_slab_cfg
+    o = Oracle(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q)
+    o.ewald_k(0)
+    o.zero_forces()
+    u0 = o.scalars()["v_coul"]
+    o.dipolar_correction()
+    f = o.state()["force"]
+    L = np.asarray(cfg.params.boundary[:3], dtype=np.float64)
+    inv_v = 1.0 / (L[0] * L[1] * L[2] * 3.0)
+    m = float(np.sum(cfg.q * (cfg.r0[:, 2] - L[2] / 2.0)))
+    assert abs(m) > 1e-3
+    assert (f[:, :2] == 0.0).all()
+    np.testing.assert_allclose(f[:, 2], -4.0 * PI_F32 * cfg.q * m * inv_v, rtol=1e-12, atol=1e-15)
+    assert o.scalars()["v_coul"] - u0 == pytest.approx(2.0 * PI_F32 * m * m * inv_v, rel=1e-9)
+
+
+def slab_coulomb_energy(o):
+    """LJ + Ewald (real, k-space) + slab correction: energy and forces."""
+    o.zero_forces()
+    o.fluid_fluid()
+    o.ewald_k(1)
+    o.dipolar_correction()
+    s = o.scalars()
+    return s["v_fluid_fluid"] + s["v_coul"], o.state()["force"]
+
+
+def test_slab_coulomb_forces_are_minus_energy_gradient(charged_slab_cfg):
+    """Central differences of LJ + Ewald + dipolar energy against the summed
+    forces on the charged channel (thermostat off): the slab k-set, the
+    k-space forces and the dipolar term belong to one energy."""
+    cfg = charged_slab_cfg
+    p = cfg.params.copy()
+    p.thermostat = _abi.THERMO_NONE
+    o = Oracle(p, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, list_cap=512)
+    o.ewald_k(0)
+    o.binning()
+    _, f = slab_coulomb_energy(o)
+    rng = np.random.default_rng(2)
+    h = 1e-6
+    for i in rng.choice(cfg.n, 10, replace=False):
+        for d in range(3):
+            r = cfg.r0.copy()
+            r[i, d] += h
+            o.set_state(r0=r)
+            ep, _ = slab_coulomb_energy(o)
+            r[i, d] -= 2 * h
+            o.set_state(r0=r)
+            em, _ = slab_coulomb_energy(o)
+            g = -(ep - em) / (2 * h)
+            assert g == pytest.approx(f[i, d], rel=2e-5, abs=2e-4), (i, d)
+
+
 def test_list_energy_equals_all_pairs_energy(melt_cfg):
     """util.f90:283-322: the O(N^2) energy equals the Verlet-list energy."""
     cfg = melt_cfg
