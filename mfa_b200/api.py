@@ -52,6 +52,7 @@ class System:
                                 _ip(t), _dp(m), _dp(qq), _ip(mc), C.byref(ctx)), "mfa_init")
         self.ctx = ctx
         self.mass = m
+        self.a_type = t.copy()
 
     # ---- lifetime ----
     def close(self) -> None:
