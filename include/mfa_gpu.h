@@ -263,6 +263,35 @@ int mfa_set_pair_shape(mfa_ctx* ctx, int32_t entries_per_round, int32_t block, i
  * forces do not depend on either choice; the autotuner uses it. */
 int mfa_set_cells(mfa_ctx* ctx, const int32_t* n_bin, double skin);
 
+/* ---------------- observables on the device ---------------- */
+
+/* One observation of the current state (observation.f90:173-283), computed
+ * on the device; only these nine numbers come back (md_main.f90:159-165 reads
+ * the whole state for them).  Chains are unfolded bead by bead as the
+ * reference does (a bead moves by one box length when it lies more than half
+ * a box from the bead before it; brush chains in SYMMETRY 0 only, melt or
+ * droplet chains always).  r_g2_brush = r_g2(1,:), the per-axis mean square
+ * radius of gyration of the n_chain chains of n_mon beads; r_g2_melt =
+ * r_g2(2,:) over chains n_chain+1..n_chain+n_chain_d taken as ids
+ * (i_chain-1)*n_mon_d+1..i_chain*n_mon_d (the reference's indexing; NaN when
+ * there are none, its 0/0); momentum = sum m v (:279-283).  Synchronises.
+ * MFA_ERR_UNSUPPORTED when that melt indexing would run past the particles. */
+typedef struct mfa_observables {
+    double r_g2_brush[3];
+    double r_g2_melt[3];
+    double momentum[3];
+} mfa_observables;
+int mfa_observe(mfa_ctx* ctx, mfa_observables* out);
+/* histo(2) of functions.f90:157-185: adds the current z positions of the brush
+ * beads (ids 1..n_mon*n_chain) and the melt/droplet beads (the next
+ * n_mon_d*n_chain_d) to device-resident histograms of hist_dim bins
+ * (bin int(z / (Lz / hist_dim)) + 1, clamped), restarting them when reset is
+ * set or hist_dim changes.  counts (2 x hist_dim: brush, then melt) and n_obs
+ * (observations accumulated), when not NULL, receive the totals (then the
+ * call synchronises).  The normalisation of histo(1) -- counts * hist_dim /
+ * (Lz * n_obs * Lx * Ly) -- is the caller's. */
+int mfa_histogram_z(mfa_ctx* ctx, int32_t hist_dim, int32_t reset, double* counts, int32_t* n_obs);
+
 /* ---------------- host mirrors ---------------- */
 
 int mfa_get_scalars(mfa_ctx* ctx, mfa_scalars* out);

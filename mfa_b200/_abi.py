@@ -94,6 +94,12 @@ class MfaScalars(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class MfaObservables(C.Structure):
+    """struct mfa_observables."""
+
+    _fields_ = [("r_g2_brush", C.c_double * 3), ("r_g2_melt", C.c_double * 3), ("momentum", C.c_double * 3)]
+
+
 # every entry point declared in include/mfa_gpu.h: name -> (restype, argtypes)
 _P = C.c_void_p
 _DP = C.POINTER(C.c_double)
@@ -124,6 +130,8 @@ SIGNATURES = {
     "mfa_set_energy_log": (C.c_int, [_P, C.c_int32, C.c_int32]),
     "mfa_read_energy_log": (C.c_int, [_P, _DP, C.c_int32, _IP]),
     "mfa_get_scalars": (C.c_int, [_P, C.POINTER(MfaScalars)]),
+    "mfa_observe": (C.c_int, [_P, C.POINTER(MfaObservables)]),
+    "mfa_histogram_z": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "mfa_download": (C.c_int, [_P, C.c_uint32, _DP, _DP, _DP, _DP, _IP]),
     "mfa_upload": (C.c_int, [_P, C.c_uint32, _DP, _DP, _DP, _DP, _IP]),
     "mfa_sync": (C.c_int, [_P]),

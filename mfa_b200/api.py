@@ -252,6 +252,31 @@ class System:
         check(self.lib.mfa_debug_kvecs(self.ctx, C.byref(nk), _dp(out), max_k), "mfa_debug_kvecs")
         return out[: nk.value].copy()
 
+    def observe(self) -> dict:
+        """mfa_observe: radii of gyration (brush, melt) and total momentum."""
+        o = _abi.MfaObservables()
+        check(self.lib.mfa_observe(self.ctx, C.byref(o)), "mfa_observe")
+        return {"r_g2_brush": np.array(o.r_g2_brush[:]), "r_g2_melt": np.array(o.r_g2_melt[:]),
+                "momentum": np.array(o.momentum[:])}
+
+    def histogram_z(self, hist_dim: int, reset: bool = False):
+        """mfa_histogram_z: adds this state's z histograms; returns the
+        accumulated counts (2 x hist_dim: brush, melt) and observation count."""
+        out = np.zeros((2, hist_dim))
+        n = C.c_int32(0)
+        check(self.lib.mfa_histogram_z(self.ctx, int(hist_dim), int(bool(reset)), _dp(out), C.byref(n)),
+              "mfa_histogram_z")
+        return out, n.value
+
+    def density_profiles(self, counts, n_obs):
+        """histo(1) normalisation (functions.f90:137): counts * hist_dim /
+        (Lz * n_obs * Lx * Ly), with the bin centres."""
+        L = np.asarray(self.params.boundary[:3], dtype=np.float64)
+        hd = counts.shape[1]
+        dens = counts * hd * (1.0 / L[2]) / (n_obs * (L[0] * L[1]))
+        z = (np.arange(hd) + 0.5) * (L[2] / hd)
+        return z, dens
+
     def set_energy_log(self, every: int, capacity: int) -> None:
         check(self.lib.mfa_set_energy_log(self.ctx, every, capacity), "mfa_set_energy_log")
 

@@ -49,7 +49,7 @@ enum {
 };
 
 // reduction counters (last-block-done pattern), one per reducing kernel
-enum { R_PAIR = 0, R_BOND = 1, R_WALL = 2, R_VV = 3, R_EWALD = 4, R_N = 8 };
+enum { R_PAIR = 0, R_BOND = 1, R_WALL = 2, R_VV = 3, R_EWALD = 4, R_OBS = 5, R_N = 8 };
 // whole-run graphs kept per context (distinct step counts of mfa_step calls)
 constexpr int N_CALL_GRAPHS = 4;
 
@@ -129,6 +129,11 @@ struct mfa_ctx {
     // pinned host staging for uploads/downloads (3 x n doubles)
     double* h_stage;
     double* h_scal;                     // pinned copy of dscal and dflags (mfa_get_scalars)
+    // observables (observe.cu), allocated at their first use: unfolded
+    // coordinates (3 n) and 16 result slots; the z histogram and its count
+    double* obs_buf;
+    double* hist;
+    int hist_dim, hist_obs;
 };
 
 #define TRY_(x)                          \
