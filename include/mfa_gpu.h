@@ -223,8 +223,38 @@ int mfa_ewald_k(mfa_ctx* ctx, int32_t mode);
  * V the slab volume of ewald_k(0).  Adds to force; nothing for uncharged or
  * SYMMETRY 1 systems; MFA_ERR_STATE before mfa_ewald_k(ctx, 0). */
 int mfa_dipolar_correction(mfa_ctx* ctx);
-/* verlet_velocities.f90:1-246: a = F/m, v += dt/2 a, heads pinned, energies. */
+/* verlet_velocities.f90:1-246: a = F/m, v += dt/2 a, heads pinned, energies.
+ * With DPD_VV switched on (mfa_set_dpd_vv) only a = F/m and the kick
+ * (:23-35); the head rules and energies are compiled out there (:79-230). */
 int mfa_verlet_velocities(mfa_ctx* ctx);
+
+/* ---------------- optional terms behind cpp switches ---------------- */
+
+/* external_force.f90:1-20 (EXT_FORCE 1, md_main.f90:122-124): mode 1 adds
+ * -k_elastic (y - Ly/2) and -k_elastic (z - Lz/2) to every bead's force; other
+ * modes do nothing.  k_elastic is the commons variable read by init_params.f90:216. */
+int mfa_external_force(mfa_ctx* ctx, int32_t mode, double k_elastic);
+/* orientation.f90:3-185 (ORIENTATION, md_main.f90:114-121).  mode 1: angle
+ * term between a ghost bond at each grafted chain's head (one unit further
+ * from the mid-plane) and the chain's first bond, forces on the head and the
+ * second bead (x, y minimum-imaged); mode 2: the first and last bond against
+ * the x axis, as compiled with CHAIN_BC 2; modes 0 and 3 do nothing (mode 0's
+ * k_or = k_bend, alpha_or = 0 are the caller's arguments).  Adds to force.
+ * v_or may be NULL; otherwise the call synchronises and stores the
+ * orientation energy (v_or of the commons, not part of v_total).
+ * MFA_ERR_ARGS for chains of fewer than 2 beads. */
+int mfa_orientation(mfa_ctx* ctx, int32_t mode, double k_or, double alpha_or, double* v_or);
+/* The DPD_VV switch (control_simulation.h:51) as a runtime setting: on, it
+ * allocates force_d (zero, init_params.f90:839), makes mfa_verlet_velocities
+ * the kick alone and enables mfa_new_dpd_fd.  mfa_step, batches and the
+ * adjoint refuse a context with the switch on (MFA_ERR_UNSUPPORTED). */
+int mfa_set_dpd_vv(mfa_ctx* ctx, int32_t on);
+/* new_dpd_fd.f90:1-215 (md_main.f90:149-155): the dissipative force over the
+ * Verlet list with the current velocities (heads excluded, x and y
+ * minimum-imaged, no force switch-on); force += Fd_new - Fd_previous; then
+ * v += dt/2 F/m, a = F/m, t_fluid, v_total, e_total.  MFA_ERR_STATE unless
+ * DPD_VV is on and the lists are built. */
+int mfa_new_dpd_fd(mfa_ctx* ctx);
 
 /* ---------------- fast path ---------------- */
 

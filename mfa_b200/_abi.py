@@ -126,6 +126,10 @@ SIGNATURES = {
     "mfa_ewald_k": (C.c_int, [_P, C.c_int32]),
     "mfa_dipolar_correction": (C.c_int, [_P]),
     "mfa_verlet_velocities": (C.c_int, [_P]),
+    "mfa_external_force": (C.c_int, [_P, C.c_int32, C.c_double]),
+    "mfa_orientation": (C.c_int, [_P, C.c_int32, C.c_double, C.c_double, _DP]),
+    "mfa_set_dpd_vv": (C.c_int, [_P, C.c_int32]),
+    "mfa_new_dpd_fd": (C.c_int, [_P]),
     "mfa_step": (C.c_int, [_P, C.c_int32]),
     "mfa_set_energy_log": (C.c_int, [_P, C.c_int32, C.c_int32]),
     "mfa_read_energy_log": (C.c_int, [_P, _DP, C.c_int32, _IP]),

@@ -123,6 +123,26 @@ class System:
     def verlet_velocities(self) -> None:
         check(self.lib.mfa_verlet_velocities(self.ctx), "verlet_velocities")
 
+    # ---- optional terms behind the reference's cpp switches ----
+    def external_force(self, mode: int, k_elastic: float) -> None:
+        """external_force(mode) (EXT_FORCE 1): elastic pull towards y = Ly/2, z = Lz/2."""
+        check(self.lib.mfa_external_force(self.ctx, int(mode), float(k_elastic)), "external_force")
+
+    def orientation(self, mode: int, k_or: float, alpha_or: float = 0.0, energy: bool = False):
+        """orientation(mode) (ORIENTATION); returns v_or when energy=True (synchronises)."""
+        out = C.c_double(0.0)
+        check(self.lib.mfa_orientation(self.ctx, int(mode), float(k_or), float(alpha_or),
+                                       C.byref(out) if energy else None), "orientation")
+        return out.value if energy else None
+
+    def set_dpd_vv(self, on: bool = True) -> None:
+        """The DPD_VV switch: verlet_velocities becomes the kick alone, new_dpd_fd follows it."""
+        check(self.lib.mfa_set_dpd_vv(self.ctx, int(bool(on))), "set_dpd_vv")
+        self.dpd_vv = bool(on)
+
+    def new_dpd_fd(self) -> None:
+        check(self.lib.mfa_new_dpd_fd(self.ctx), "new_dpd_fd")
+
     # ---- compositions ----
     def init_forces(self, full: bool = False) -> None:
         """The start-up sequence of conf_default.f90:254-299: lists, the forces
@@ -167,6 +187,8 @@ class System:
             if p.symmetry == 0:
                 self.dipolar_correction()     # md_main.f90:128-131
         self.verlet_velocities()
+        if getattr(self, "dpd_vv", False):
+            self.new_dpd_fd()                 # md_main.f90:149-155
         return f_skin
 
     def step(self, nsteps: int) -> None:

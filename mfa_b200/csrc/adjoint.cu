@@ -448,7 +448,7 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
     if (!c || nsteps < 1 || every < 1 || !out) return MFA_ERR_ARGS;
     const mfa_params& p = c->p;
     // the force terms differentiated here: pair (LJ/WCA, DPD), FENE, 9-3 walls
-    if (p.charged || p.thermostat == MFA_THERMO_LGV || p.bending || p.force_switch_on ||
+    if (p.charged || p.thermostat == MFA_THERMO_LGV || p.bending || p.force_switch_on || c->dpd_vv ||
         (p.symmetry == 0 && (p.wall == 3 || p.wall == 4)) || (p.n_chain_d > 0 && p.n_mon_d >= 2))
         return MFA_ERR_UNSUPPORTED;
     if (!c->lists_valid) TRY_(mfa_binning(c));

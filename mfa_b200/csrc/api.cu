@@ -82,7 +82,7 @@ void free_all(mfa_ctx* c) {
     void* ptrs[] = {c->rx, c->mx, c->type, c->mass, c->force, c->pos_s, c->vel_s, c->pos64, c->pos32,
                     c->ids, c->cell_count, c->nbr, c->nnb, c->partials, c->counters, c->dscal,
                     c->dstep, c->kvec, c->rho, c->rho_part, c->elog, c->elog_n, c->tabs,
-                    c->obs_buf, c->hist};
+                    c->obs_buf, c->hist, c->fd, c->term_buf};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->h_stage) cudaFreeHost(c->h_stage);
@@ -627,12 +627,14 @@ int mfa_dipolar_correction(mfa_ctx* c) {
 
 int mfa_verlet_velocities(mfa_ctx* c) {
     if (!c) return MFA_ERR_ARGS;
+    if (c->dpd_vv) return launch_dpd_vv_kick(c);
     return launch_vv_velocities(c, 0);
 }
 
 int mfa_step(mfa_ctx* c, int32_t nsteps) {
     if (!c || nsteps < 0) return MFA_ERR_ARGS;
     if (nsteps == 0) return MFA_OK;
+    if (c->dpd_vv) return MFA_ERR_UNSUPPORTED;   // the fused step has no new_dpd_fd pass
     if (c->p.charged && c->nk == 0) return MFA_ERR_STATE;
     if (!c->lists_valid) TRY(rebuild_abi(c, c->bin_type));
     // energies are reduced for the last step only (and for the steps the

@@ -263,7 +263,7 @@ int mfa_batch_create(mfa_ctx* const* ctxs, int32_t n, mfa_batch** out) {
         if (!c) return MFA_ERR_ARGS;
         if (c->dev != ctxs[0]->dev || c->prec != ctxs[0]->prec) return MFA_ERR_UNSUPPORTED;
         // Ewald k-space and the hard walls of WALL 3/4 are not batched
-        if (c->p.charged || c->p.wall == 3 || c->p.wall == 4) return MFA_ERR_UNSUPPORTED;
+        if (c->p.charged || c->p.wall == 3 || c->p.wall == 4 || c->dpd_vv) return MFA_ERR_UNSUPPORTED;
         if (c->p.symmetry != ctxs[0]->p.symmetry || c->p.thermostat != ctxs[0]->p.thermostat ||
             c->p.force_switch_on != ctxs[0]->p.force_switch_on || c->p.wall != ctxs[0]->p.wall)
             return MFA_ERR_UNSUPPORTED;

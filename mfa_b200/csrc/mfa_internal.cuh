@@ -134,6 +134,11 @@ struct mfa_ctx {
     double* obs_buf;
     double* hist;
     int hist_dim, hist_obs;
+    // optional terms (terms.cu): DPD_VV switch and its two 3 x n FP64
+    // dissipative-force buffers (previous, current), and a small result buffer
+    int dpd_vv;
+    double* fd;
+    double* term_buf;
 };
 
 #define TRY_(x)                          \
@@ -191,6 +196,8 @@ int ewald_setup(mfa_ctx* c);
 int launch_ewald(mfa_ctx* c);
 // dipolar_correction.f90 (charged SYMMETRY 0; nothing otherwise)
 int launch_dipolar(mfa_ctx* c);
+// terms.cu: the velocity half of verlet_velocities under DPD_VV
+int launch_dpd_vv_kick(mfa_ctx* c);
 
 // every kernel launch is recorded (graph captures count towards their graph)
 inline void note_launch(mfa_ctx* c, int k) {

@@ -42,6 +42,9 @@ struct orc_state {
     double v_fluid_fluid, v_fluid_wall, v_intra_molec, v_bend, v_coul;
     double v_coul_self, t_fluid, v_total, e_total, virial;
     int fene_clamped;
+    /* DPD_VV (new_dpd_fd.f90): the dissipative force of the last re-evaluation */
+    int dpd_vv;
+    double* force_d;
     /* Ewald k-space (ewald_k.f90 saved variables) */
     int nk;
     double *k_vecs, *k_vecs_2, *inv_k_vecs_2, *re_rho_k, *im_rho_k, *cphase;
@@ -223,7 +226,7 @@ void orc_destroy(orc_state* s) {
     free(s->r0); free(s->v); free(s->a); free(s->force); free(s->r0_old);
     free(s->mic); free(s->mic_old); free(s->a_type); free(s->mass); free(s->inv_mass);
     free(s->q); free(s->cell_of); free(s->bin_fluid); free(s->ff_list);
-    free(s->binpnt); free(s->bin);
+    free(s->binpnt); free(s->bin); free(s->force_d);
     free(s->k_vecs); free(s->k_vecs_2); free(s->inv_k_vecs_2);
     free(s->re_rho_k); free(s->im_rho_k); free(s->cphase);
     free(s);
@@ -864,6 +867,9 @@ void orc_verlet_velocities(orc_state* s) {
             s->a[3 * i + d] = s->force[3 * i + d] * s->inv_mass[i];
             s->v[3 * i + d] = s->v[3 * i + d] + hdt * s->a[3 * i + d];
         }
+    /* verlet_velocities.f90:79-230 (head rules, kinetic and total energies)
+     * are compiled out under DPD_VV; new_dpd_fd computes the energies */
+    if (s->dpd_vv) return;
     if (p->pin_heads) {
         for (int c = 0; c < p->n_chain; ++c) {
             const int h = c * p->n_mon;
@@ -884,6 +890,199 @@ void orc_verlet_velocities(orc_state* s) {
     s->e_total = s->v_total + s->t_fluid;
 }
 
+/* ------------------------------------------------------------------ */
+/* Optional terms behind cpp switches                                  */
+/* ------------------------------------------------------------------ */
+
+/* external_force.f90:9-18, mode 1 (EXT_FORCE 1): an elastic pull of every
+ * bead towards the axis y = Ly/2, z = Lz/2.  No energy is kept. */
+void orc_external_force(orc_state* s, int mode, double k_elastic) {
+    if (mode != 1) return;
+    const mfa_params* p = &s->p;
+    for (int i = 0; i < s->n; ++i) {
+        s->force[3 * i + 1] = s->force[3 * i + 1] - k_elastic * (s->r0[3 * i + 1] - p->boundary[1] / 2.0);
+        s->force[3 * i + 2] = s->force[3 * i + 2] - k_elastic * (s->r0[3 * i + 2] - p->boundary[2] / 2.0);
+    }
+}
+
+/* orientation.f90:3-185.  mode 1 (SYMMETRY 0, :24-85): the angle between a
+ * ghost bond (head to a point one unit further from the mid-plane, :34-39)
+ * and the first bond; forces on the head and the second bead, x and y
+ * minimum-imaged (:43-48).  mode 2 (:89-175, as compiled with CHAIN_BC 2):
+ * the first and the last bond against the fixed unit vector x, every axis
+ * minimum-imaged.  Modes 0 and 3 do nothing.  Returns v_or. */
+double orc_orientation(orc_state* s, int mode, double k_or, double alpha_or) {
+    const mfa_params* p = &s->p;
+    const double* L = p->boundary;
+    const double* iL = s->inv_boundary;
+    const int nm = p->n_mon;
+    const double small1 = (double)0.0001f, small2 = (double)0.000001f;   /* default-REAL literals */
+    double v_or = 0.0;
+    if (mode != 1 && mode != 2) return 0.0;
+    for (int l = 0; l < p->n_chain; ++l) {
+        const int h = l * nm;
+        if (mode == 1) {
+            double g[3], rp[3], rn[3];
+            for (int j = 0; j < 3; ++j) g[j] = s->r0[3 * h + j];
+            if (s->r0[3 * h + 2] > L[2] / 2.0) g[2] = g[2] + 1.0;
+            else g[2] = g[2] - 1.0;
+            for (int j = 0; j < 3; ++j) {
+                rp[j] = s->r0[3 * h + j] - g[j];
+                rn[j] = s->r0[3 * (h + 1) + j] - s->r0[3 * h + j];
+            }
+            for (int j = 0; j < 2; ++j) {
+                rn[j] = mimage(rn[j], L[j], iL[j]);
+                rp[j] = mimage(rp[j], L[j], iL[j]);
+            }
+            double dot = 0.0, rp2 = 0.0, rn2 = 0.0, dn2 = 0.0, dn[3];
+            for (int j = 0; j < 3; ++j) {
+                dot = dot + rn[j] * rp[j];
+                rp2 = rp2 + rp[j] * rp[j];
+                rn2 = rn2 + rn[j] * rn[j];
+            }
+            const double cosa = dot / sqrt(rp2 * rn2);
+            for (int j = 0; j < 3; ++j) dn[j] = rp[j] * rn2 - rn[j] * dot;
+            for (int j = 0; j < 3; ++j) dn2 = dn2 + dn[j] * dn[j];
+            if (dn2 < small1) {
+                for (int j = 0; j < 3; ++j) dn[j] = dn[j] * 0.0;
+            } else {
+                const double den = sqrt(dn2 * rn2);
+                for (int j = 0; j < 3; ++j) dn[j] = dn[j] / den;
+            }
+            const double da = acos(cosa) - alpha_or;
+            const double fm = k_or * da;
+            v_or = v_or + 0.5 * fm * da;
+            for (int j = 0; j < 3; ++j) {
+                s->force[3 * h + j] = s->force[3 * h + j] - fm * dn[j];
+                s->force[3 * (h + 1) + j] = s->force[3 * (h + 1) + j] + fm * dn[j];
+            }
+        } else {
+            const int last = h + nm - 1;
+            for (int b = 1; b <= 2; ++b) {
+                double rp[3], rn[3], dn[3], dp[3];
+                if (b == 1) {
+                    rp[0] = 1.0; rp[1] = 0.0; rp[2] = 0.0;
+                    for (int j = 0; j < 3; ++j) rn[j] = s->r0[3 * (h + 1) + j] - s->r0[3 * h + j];
+                } else {
+                    for (int j = 0; j < 3; ++j) rp[j] = s->r0[3 * last + j] - s->r0[3 * (last - 1) + j];
+                    rn[0] = 1.0; rn[1] = 0.0; rn[2] = 0.0;
+                }
+                for (int j = 0; j < 3; ++j) {
+                    rn[j] = mimage(rn[j], L[j], iL[j]);
+                    rp[j] = mimage(rp[j], L[j], iL[j]);
+                }
+                double dot = 0.0, rp2 = 0.0, rn2 = 0.0, dn2 = 0.0, dp2 = 0.0;
+                for (int j = 0; j < 3; ++j) {
+                    dot = dot + rn[j] * rp[j];
+                    rp2 = rp2 + rp[j] * rp[j];
+                    rn2 = rn2 + rn[j] * rn[j];
+                }
+                const double cosa = dot / sqrt(rp2 * rn2);
+                for (int j = 0; j < 3; ++j) {
+                    dn[j] = rp[j] * rn2 - rn[j] * dot;
+                    dp[j] = -rn[j] * rp2 + rp[j] * dot;
+                }
+                for (int j = 0; j < 3; ++j) {
+                    dp2 = dp2 + dp[j] * dp[j];
+                    dn2 = dn2 + dn[j] * dn[j];
+                }
+                if (dn2 < small2) {
+                    for (int j = 0; j < 3; ++j) dn[j] = dn[j] * 0.0;
+                } else {
+                    const double den = sqrt(dn2 * rn2);
+                    for (int j = 0; j < 3; ++j) dn[j] = dn[j] / den;
+                }
+                if (dp2 < small2) {
+                    for (int j = 0; j < 3; ++j) dp[j] = dp[j] * 0.0;
+                } else {
+                    const double den = sqrt(dp2 * rp2);
+                    for (int j = 0; j < 3; ++j) dp[j] = dp[j] / den;
+                }
+                const double da = acos(cosa) - alpha_or;
+                const double fm = k_or * da;
+                v_or = v_or + 0.5 * fm * da;
+                double fb[6];
+                for (int j = 0; j < 3; ++j) { fb[j] = fm * dp[j]; fb[3 + j] = fm * dn[j]; }
+                const int i0 = b == 1 ? last : last - 1, i1 = b == 1 ? h : last, i2 = b == 1 ? h + 1 : h;
+                for (int j = 0; j < 3; ++j) {
+                    s->force[3 * i0 + j] = s->force[3 * i0 + j] + fb[j];
+                    s->force[3 * i1 + j] = s->force[3 * i1 + j] - fb[j] - fb[3 + j];
+                    s->force[3 * i2 + j] = s->force[3 * i2 + j] + fb[3 + j];
+                }
+            }
+        }
+    }
+    return v_or;
+}
+
+/* DPD_VV (control_simulation.h:51): force_d starts at zero (init_params.f90:839) */
+void orc_set_dpd_vv(orc_state* s, int on) {
+    s->dpd_vv = on != 0;
+    if (s->dpd_vv && !s->force_d) s->force_d = (double*)calloc((size_t)3 * s->n, sizeof(double));
+}
+
+/* new_dpd_fd.f90:17-112: the dissipative force re-evaluated over ff_list with
+ * the velocities after verlet_velocities, heads (type 1) excluded, x and y
+ * minimum-imaged only (:40-43), no force switch-on; the previous call's force_d
+ * is taken out of the force and the new one added (:17,:88); then a half kick
+ * with the corrected force, a = F/m, and the kinetic and total energies
+ * (:92-160; t_wall = 0, v_wall_wall = 0). */
+void orc_new_dpd_fd(orc_state* s) {
+    const mfa_params* p = &s->p;
+    const int n = s->n;
+    double* fd = s->force_d;
+    if (!fd) return;
+    for (int k = 0; k < 3 * n; ++k) s->force[k] = s->force[k] - fd[k];
+    for (int k = 0; k < 3 * n; ++k) fd[k] = 0.0;
+    const int row = s->list_cap + 1;
+    for (int i = 0; i < n; ++i) {
+        const int ti = s->a_type[i];
+        if (ti == 1) continue;
+        const int cnt = s->ff_list[(size_t)row * i];
+        for (int k = 1; k <= cnt; ++k) {
+            const int j = s->ff_list[(size_t)row * i + k] - 1;
+            const int tj = s->a_type[j];
+            if (tj == 1) continue;
+            double dr[3];
+            for (int d = 0; d < 3; ++d) dr[d] = s->r0[3 * i + d] - s->r0[3 * j + d];
+            for (int d = 0; d < 2; ++d) dr[d] = mimage(dr[d], p->boundary[d], s->inv_boundary[d]);
+            double r2 = 0.0;
+            for (int d = 0; d < 3; ++d) r2 = r2 + dr[d] * dr[d];
+            const double rr = p->range_2[(ti - 1) * MFA_MAX_TYPES + (tj - 1)];
+            if (!(r2 < rr)) continue;
+            double wd = 1.0;
+            if (p->dpd_weight == 0) {
+                const double u = 1.0 - sqrt(r2 / rr);
+                wd = u * u;
+            }
+            const double rs = sqrt(r2);
+            double rv[3], dv[3];
+            for (int d = 0; d < 3; ++d) {
+                rv[d] = dr[d] / rs;
+                dv[d] = s->v[3 * i + d] - s->v[3 * j + d];
+            }
+            const double rd = (dv[0] * rv[0] + dv[1] * rv[1]) + dv[2] * rv[2];
+            for (int d = 0; d < 3; ++d) {
+                const double f = -1.0 * p->friction * wd * rd * rv[d];
+                fd[3 * i + d] = fd[3 * i + d] + f;
+                fd[3 * j + d] = fd[3 * j + d] - f;
+            }
+        }
+    }
+    for (int k = 0; k < 3 * n; ++k) s->force[k] = s->force[k] + fd[k];
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d)
+            s->v[3 * i + d] = s->v[3 * i + d] + 0.5 * p->dt * s->force[3 * i + d] * s->inv_mass[i];
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) s->a[3 * i + d] = s->force[3 * i + d] * s->inv_mass[i];
+    double t = 0.0;
+    for (int d = 0; d < 3; ++d)
+        for (int i = 0; i < n; ++i) t = t + s->mass[i] * (s->v[3 * i + d] * s->v[3 * i + d]);
+    s->t_fluid = t / 2.0;
+    s->v_total = (s->v_fluid_wall + s->v_fluid_fluid) + s->v_intra_molec;
+    s->e_total = s->v_total + s->t_fluid;
+}
+
 /* md_main.f90:68-147 in order */
 int orc_md_step(orc_state* s) {
     const mfa_params* p = &s->p;
@@ -900,6 +1099,7 @@ int orc_md_step(orc_state* s) {
     if (p->charged) err = orc_ewald_k(s, 1);
     if (p->charged && p->symmetry == 0) orc_dipolar_correction(s);
     orc_verlet_velocities(s);
+    if (s->dpd_vv) orc_new_dpd_fd(s);   /* md_main.f90:149-155 */
     return err;
 }
 

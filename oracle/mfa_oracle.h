@@ -46,6 +46,13 @@ void orc_bending(orc_state* s, int mode);
 int  orc_ewald_k(orc_state* s, int mode);
 void orc_dipolar_correction(orc_state* s);
 void orc_verlet_velocities(orc_state* s);
+/* optional terms: external_force.f90 (EXT_FORCE), orientation.f90
+ * (ORIENTATION; returns v_or), and DPD_VV (new_dpd_fd.f90; orc_md_step calls
+ * it after verlet_velocities once switched on) */
+void orc_external_force(orc_state* s, int mode, double k_elastic);
+double orc_orientation(orc_state* s, int mode, double k_or, double alpha_or);
+void orc_set_dpd_vv(orc_state* s, int on);
+void orc_new_dpd_fd(orc_state* s);
 /* one md_main.f90:68-147 iteration in the reference's call order */
 int  orc_md_step(orc_state* s);
 

@@ -52,6 +52,10 @@ def load():
             "orc_ewald_k": (C.c_int, [P, C.c_int]),
             "orc_dipolar_correction": (None, [P]),
             "orc_verlet_velocities": (None, [P]),
+            "orc_external_force": (None, [P, C.c_int, C.c_double]),
+            "orc_orientation": (C.c_double, [P, C.c_int, C.c_double, C.c_double]),
+            "orc_set_dpd_vv": (None, [P, C.c_int]),
+            "orc_new_dpd_fd": (None, [P]),
             "orc_md_step": (C.c_int, [P]),
             "orc_check_fluid_fluid": (C.c_double, [P]),
             "orc_get_state": (None, [P, DP, DP, DP, DP, IP]),
@@ -149,6 +153,19 @@ class Oracle:
 
     def verlet_velocities(self):
         self.lib.orc_verlet_velocities(self.ptr)
+
+    def external_force(self, mode, k_elastic):
+        self.lib.orc_external_force(self.ptr, int(mode), float(k_elastic))
+
+    def orientation(self, mode, k_or, alpha_or=0.0):
+        """Adds the orientation forces; returns v_or."""
+        return float(self.lib.orc_orientation(self.ptr, int(mode), float(k_or), float(alpha_or)))
+
+    def set_dpd_vv(self, on=True):
+        self.lib.orc_set_dpd_vv(self.ptr, int(bool(on)))
+
+    def new_dpd_fd(self):
+        self.lib.orc_new_dpd_fd(self.ptr)
 
     def init_forces(self):
         p = self.params
