@@ -54,6 +54,9 @@ def args_():
                     help="energy drift of FP64 vs mixed over --drift-steps NVE steps (not a throughput run)")
     ap.add_argument("--drift-steps", type=int, default=100000)
     ap.add_argument("--drift-equil", type=int, default=20000)
+    ap.add_argument("--wall-cut", type=float, default=None,
+                    help="9-3 wall cutoff of the brush workload for --drift (default: the configuration's "
+                         "2.5; 0: no cutoff, the reference's uncut wall)")
     ap.add_argument("--kernel-times", action="store_true",
                     help="device time of every kernel inside the time-step loop (CUPTI through the torch "
                          "profiler, no serialisation), per step; not a throughput run")
@@ -116,7 +119,7 @@ def drift(a):
     import torch
     from mfa_b200 import _abi
     from mfa_b200.api import System
-    cfg, meta = make_config(a.workload, a.seed)
+    cfg, meta = make_config(a.workload, a.seed, wall_cut=a.wall_cut)
     g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=_abi.FP64)
     g.init_forces()
     g.step(a.drift_equil)
@@ -146,16 +149,37 @@ def drift(a):
                      "ms_per_step": e0.elapsed_time(e1) / a.drift_steps,
                      "bead_steps_per_s": cfg.n * a.drift_steps / (e0.elapsed_time(e1) * 1e-3)}
         h.close()
+        # e_total is the reference's sum (verlet_velocities.f90:336): it leaves
+        # out the bending and Coulomb energies, so with bending it is not a
+        # constant of the motion.  The same run again, read every `every`
+        # steps, with those terms added back.
+        h = System(p, st["r0"], st["v"], cfg.a_type, cfg.mass, q=cfg.q, mic=st["mic"], precision=prec)
+        h.init_forces(full=True)
+        ts, Ec = [], []
+        for _ in range(a.drift_steps // every):
+            h.step(every)
+            sc = h.scalars()
+            ts.append(sc["i_time"])
+            Ec.append(sc["e_total"] + sc["v_bend"] + (sc["v_coul"] if p.charged else 0.0))
+        h.close()
+        ts, Ec = np.asarray(ts, dtype=np.float64), np.asarray(Ec)
+        res[name]["conserved"] = {
+            "energy": "e_total + v_bend" + (" + v_coul" if p.charged else ""),
+            "drift_per_bead": float((Ec[-1] - Ec[0]) / cfg.n),
+            "fit_slope_per_bead_per_1e5_steps": float(np.polyfit(ts, Ec, 1)[0]) * 1e5 / cfg.n,
+            "fluct_rms_per_bead": float(np.std(Ec) / cfg.n)}
     print(json.dumps({"mode": "drift", "workload": meta["workload"], "beads": cfg.n, "nve_steps": a.drift_steps,
+                      "wall_cut": cfg.params.wall_cut if cfg.params.symmetry == 0 else None,
                       "dt": cfg.params.dt, "equilibration_steps_dpd": a.drift_equil, **res,
                       "mixed_over_fp64_speed": res["mixed"]["bead_steps_per_s"] / res["fp64"]["bead_steps_per_s"]}))
     return 0
 
 
-def make_config(name, seed):
+def make_config(name, seed, wall_cut=None):
     from mfa_b200 import configs
     if name == "brush":
-        return configs.brush(seed=seed), {
+        kw = {} if wall_cut is None else {"wall_cut": wall_cut}
+        return configs.brush(seed=seed, **kw), {
             "workload": "brush_explicit_solvent_32x32x64", "chains": "32x32", "n_mon": 64,
             "grafting_density": 0.3, "wall_gap": 60.0, "solvent_density": 0.85}
     if name == "melt":
