@@ -467,10 +467,11 @@ def adjoint_bench(a):
     from mfa_b200.api import System
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from test_adjoint import NAMES, base_values, perturbed
-    cfg = configs.brush(seed=a.seed, nx=16, ny=16, n_mon=64, graft=0.3, z_wall=60.0, solvent=False, k_bend=0.0)
+    # the brush of the throughput workload (bending k_b = 2 included), 16 x 16 chains, implicit solvent
+    cfg = configs.brush(seed=a.seed, nx=16, ny=16, n_mon=64, graft=0.3, z_wall=60.0, solvent=False, k_bend=2.0)
     S, K = 200, 20
     g0 = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, precision=_abi.FP64)
-    g0.init_forces()
+    g0.init_forces(full=True)
     g0.step(a.equil)
     st = g0.download()
     g0.close()
@@ -527,6 +528,7 @@ def adjoint_bench(a):
         "mode": "adjoint", "metric": "adjoint cost / forward cost", "value": res["mixed"]["adjoint_over_forward"],
         "unit": "ratio", "higher_is_better": False,
         "config": {"workload": "brush_implicit_16x16x64", "beads": cfg.n, "steps": S, "checkpoint_every": K,
+                   "k_bend": cfg.params.k_bend,
                    "observable": "time average of <z> + <R_ee^2>", "dt": cfg.params.dt},
         "fp64": res["fp64"], "mixed": res["mixed"], "central_differences_fp64": fd,
         "rel_err_fp64_adjoint_vs_fd": rel, "rel_err_mixed_vs_fp64_adjoint": rel32}))

@@ -382,15 +382,16 @@ int mfa_trajectory_observable(mfa_ctx* ctx, int32_t nsteps, double* J);
 /* The same run, differentiated: out[0] = J, out[1..6] = dJ/d(eps_LJ, sigma,
  * k_FENE, R0, gamma_DPD, eps_wall) by the discrete adjoint of the
  * velocity-Verlet map (hand-written vector-Jacobian products of the pair,
- * DPD, FENE and 9-3 wall forces), recomputing the forward states from
+ * DPD, FENE, bending and 9-3 wall forces), recomputing the forward states from
  * checkpoints every `every` steps with the DPD noise replayed.  Parameters:
  * eps_LJ and sigma scale every pair's epsil and sigma (range_2 with it);
  * k_FENE and R0 enter as k_chain = k R0^2 and r_chain_2 = R0^2; gamma_DPD as
  * friction and sig = sqrt(2 kT gamma / dt); eps_wall as every type's a_wall.
  * The run starts from the context's state (r, v and a = F/m as they are) and
  * that state is held fixed: the gradient is that of the trajectory from it.
- * Systems with Ewald, Langevin, bending, the force switch-on, WALL 3/4 or
- * melt chains return MFA_ERR_UNSUPPORTED.  The state advances by nsteps. */
+ * Systems with Ewald, Langevin, the force switch-on, WALL 3/4, melt chains or
+ * DPD_VV return MFA_ERR_UNSUPPORTED (bending is differentiated; k_bend is not
+ * one of the parameters).  The state advances by nsteps. */
 int mfa_adjoint(mfa_ctx* ctx, int32_t nsteps, int32_t every, double* out7);
 
 /* ---------------- binning without device allocation ---------------- */

@@ -13,7 +13,8 @@
 //   rho = lam_r + 1/S dO/dr (s >= 1),  nu = dt lam_r + lam_u,  alpha = dt^2/2 lam_r + dt/2 lam_u
 // The vector-Jacobian products are written out by hand for every force term
 // of the path: WCA/LJ and DPD pairs (half list, Newton's third law), FENE bonds
-// (with the clamp of intra_molec.f90:248) and the 9-3 walls.  The forward
+// (with the clamp of intra_molec.f90:248), the bending angles of bending.f90
+// (forward-mode derivative of the angle force) and the 9-3 walls.  The forward
 // states are recomputed segment by segment from checkpoints every K steps, with
 // the DPD noise replayed: Philox is keyed by (step, pair), so the recomputed
 // forces are those of the first pass.
@@ -263,6 +264,83 @@ __global__ void k_adj_fene(AdjBondArgs a) {
     warp_add_g(a.g, gl);
 }
 
+// Bending VJP (bending.f90 mode 2, the angle formula of bonded.cuh), thread
+// per angle centred on bead c of a grafted chain.  The bending force is
+// conservative, so its Jacobian is symmetric and (dF/dr)^T lam_F is the
+// derivative of the force along the displacement lam_F: the angle's force is
+// evaluated once more in forward mode (value, derivative) with the bond
+// vectors' tangents taken from lam_F.  The branches that zero a direction or
+// the angle have zero derivative, as the forward force is constant there.
+struct Dual {
+    double v, d;
+};
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a) { return {-a.v, -a.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+__device__ __forceinline__ Dual operator/(Dual a, Dual b) {
+    const double q = a.v / b.v;
+    return {q, (a.d - q * b.d) / b.v};
+}
+__device__ __forceinline__ Dual dsqrt(Dual a) {
+    const double r = sqrt(a.v);
+    return {r, a.d / (2.0 * r)};
+}
+__device__ __forceinline__ Dual dacos(Dual a) { return {acos(a.v), -a.d / sqrt(1.0 - a.v * a.v)}; }
+
+struct AdjBendArgs {
+    const double *px, *py, *pz;   // r' (particle order)
+    const double *fx, *fy, *fz;   // lam_F
+    double *rx, *ry, *rz;         // lam_r accumulators
+    int n_chain, n_mon;
+    double L[3], invL[3];
+    double k_bend, alpha_eq;
+};
+
+__global__ void k_adj_bend(AdjBendArgs a) {
+    const int na = a.n_mon - 2;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (na < 1 || t >= a.n_chain * na) return;
+    const int c = (t / na) * a.n_mon + t % na + 1;   // centre bead; c-1, c+1 on the same chain
+    const int id[3] = {c - 1, c, c + 1};
+    const double* P[3] = {a.px, a.py, a.pz};
+    const double* F[3] = {a.fx, a.fy, a.fz};
+    // bond vectors r(j+1) - r(j), imaged on every axis (bending.f90:34-57), as bonded.cuh forms them
+    Dual p[3], n[3];
+    for (int d = 0; d < 3; ++d) {
+        const double d0 = P[d][id[0]] - P[d][id[1]], d1 = P[d][id[1]] - P[d][id[2]];
+        p[d] = {-d0 + a.L[d] * (double)(int)(2.0 * d0 * a.invL[d]), F[d][id[1]] - F[d][id[0]]};
+        n[d] = {-d1 + a.L[d] * (double)(int)(2.0 * d1 * a.invL[d]), F[d][id[2]] - F[d][id[1]]};
+    }
+    const double tiny = 1.0000000116860974e-07;   // the forward's single-precision literal
+    const Dual dot = (n[0] * p[0] + n[1] * p[1]) + n[2] * p[2];
+    const Dual p2 = (p[0] * p[0] + p[1] * p[1]) + p[2] * p[2];
+    const Dual n2 = (n[0] * n[0] + n[1] * n[1]) + n[2] * n[2];
+    const Dual cosa = dot / dsqrt(p2 * n2);
+    Dual dn[3], dp[3];
+    for (int d = 0; d < 3; ++d) {
+        dn[d] = p[d] * n2 - n[d] * dot;
+        dp[d] = -n[d] * p2 + p[d] * dot;
+    }
+    const Dual dn2 = (dn[0] * dn[0] + dn[1] * dn[1]) + dn[2] * dn[2];
+    const Dual dp2 = (dp[0] * dp[0] + dp[1] * dp[1]) + dp[2] * dp[2];
+    const Dual zero = {0.0, 0.0};
+    if (dn2.v < tiny) { dn[0] = dn[1] = dn[2] = zero; }
+    else { const Dual s = Dual{1.0, 0.0} / dsqrt(dn2 * n2); for (int d = 0; d < 3; ++d) dn[d] = dn[d] * s; }
+    if (dp2.v < tiny) { dp[0] = dp[1] = dp[2] = zero; }
+    else { const Dual s = Dual{1.0, 0.0} / dsqrt(dp2 * p2); for (int d = 0; d < 3; ++d) dp[d] = dp[d] * s; }
+    const Dual da = cosa.v >= 1.0 ? zero : dacos(cosa) - Dual{a.alpha_eq, 0.0};
+    const Dual fm = Dual{a.k_bend, 0.0} * da;
+    double* R[3] = {a.rx, a.ry, a.rz};
+    for (int d = 0; d < 3; ++d) {
+        // forward: previous bead += fp, next bead += fn, centre -= fp + fn
+        const double gp = (fm * dp[d]).d, gn = (fm * dn[d]).d;
+        atomicAdd(&R[d][id[0]], gp);
+        atomicAdd(&R[d][id[2]], gn);
+        atomicAdd(&R[d][id[1]], -(gp + gn));
+    }
+}
+
 // lam_F = (alpha' + dt/2 nu') / m, lam_u = nu', lam_r = rho' (pinned heads: 0)
 __global__ void k_adj_prep(int n, const double* __restrict__ rho, const double* __restrict__ nu,
                            const double* __restrict__ alpha, const double* __restrict__ inv_mass, double hdt,
@@ -448,7 +526,7 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
     if (!c || nsteps < 1 || every < 1 || !out) return MFA_ERR_ARGS;
     const mfa_params& p = c->p;
     // the force terms differentiated here: pair (LJ/WCA, DPD), FENE, 9-3 walls
-    if (p.charged || p.thermostat == MFA_THERMO_LGV || p.bending || p.force_switch_on || c->dpd_vv ||
+    if (p.charged || p.thermostat == MFA_THERMO_LGV || p.force_switch_on || c->dpd_vv ||
         (p.symmetry == 0 && (p.wall == 3 || p.wall == 4)) || (p.n_chain_d > 0 && p.n_mon_d >= 2))
         return MFA_ERR_UNSUPPORTED;
     if (!c->lists_valid) TRY_(mfa_binning(c));
@@ -544,6 +622,17 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
                     const int bb = (nbonds + T - 1) / T;
                     if (c->prec == MFA_MIXED) k_adj_fene<float><<<bb, T, 0, c->st>>>(ba);
                     else k_adj_fene<double><<<bb, T, 0, c->st>>>(ba);
+                }
+                if (p.bending && p.n_mon >= 3 && p.n_chain > 0) {
+                    AdjBendArgs ka;
+                    ka.px = r1; ka.py = r1 + n; ka.pz = r1 + 2 * n;
+                    ka.fx = w.lamF; ka.fy = w.lamF + n; ka.fz = w.lamF + 2 * n;
+                    ka.rx = w.lamR; ka.ry = w.lamR + n; ka.rz = w.lamR + 2 * n;
+                    ka.n_chain = p.n_chain; ka.n_mon = p.n_mon;
+                    for (int d = 0; d < 3; ++d) { ka.L[d] = p.boundary[d]; ka.invL[d] = c->inv_boundary[d]; }
+                    ka.k_bend = p.k_bend; ka.alpha_eq = p.alpha_eq;
+                    const int nang = p.n_chain * (p.n_mon - 2);
+                    k_adj_bend<<<(nang + T - 1) / T, T, 0, c->st>>>(ka);
                 }
                 // back to the state before step s+1: the observable at r_s (s >= 1)
                 const double* r0 = s > s0 ? w.seg_r + (s - s0 - 1) * n3 : nullptr;
