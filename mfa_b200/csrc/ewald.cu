@@ -25,9 +25,10 @@
 
 namespace {
 
-constexpr int KM = 16;        // largest |n| per axis held in the tables
+constexpr int KM = 64;        // largest |n| per axis held in the tables
 constexpr int RHO_T = 512;    // threads per block in k_rho_partial
-constexpr int KPT = 8;        // k per thread  -> nk <= 4096
+constexpr int KPT = 8;        // k per thread: a block row covers KPT * RHO_T vectors
+constexpr int NK_MAX = 1 << 16;   // k-vectors of one context
 constexpr int CH = 32;        // particles per table batch
 constexpr int FT = 64;        // threads per block in k_ewald_force
 
@@ -44,6 +45,7 @@ struct EwArgs {
     int max_blocks;
     int n, nk, nblk, per_blk;
     int kmax[3];
+    int ts;                   // table stride: largest kmax + 1
     double dk[3];
     double pi, inv_V;
 };
@@ -52,7 +54,7 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// tables t[d*(KM+1) + n] = exp(i n dk_d r_d), n = 0..kmax_d
+// tables t[d*ts + n] = exp(i n dk_d r_d), n = 0..kmax_d (ts = largest kmax + 1)
 __device__ __forceinline__ void build_tables(double2* t, const EwArgs& a, double x, double y, double z) {
     const double r[3] = {x, y, z};
 #pragma unroll
@@ -61,33 +63,36 @@ __device__ __forceinline__ void build_tables(double2* t, const EwArgs& a, double
         sincos(a.dk[d] * r[d], &s, &c);
         const double2 e1 = make_double2(c, s);
         double2 e = make_double2(1.0, 0.0);
-        t[d * (KM + 1)] = e;
+        t[d * a.ts] = e;
         for (int n = 1; n <= a.kmax[d]; ++n) {
             e = cmul(e, e1);
-            t[d * (KM + 1) + n] = e;
+            t[d * a.ts + n] = e;
         }
     }
 }
 
-__device__ __forceinline__ double2 phase_from(const double2* t, int4 kn) {
+__device__ __forceinline__ double2 phase_from(const double2* t, int ts, int4 kn) {
     double2 ex = t[abs(kn.x)];
     if (kn.x < 0) ex.y = -ex.y;
-    double2 ey = t[(KM + 1) + abs(kn.y)];
+    double2 ey = t[ts + abs(kn.y)];
     if (kn.y < 0) ey.y = -ey.y;
-    const double2 ez = t[2 * (KM + 1) + kn.z];
+    const double2 ez = t[2 * ts + kn.z];
     return cmul(cmul(ex, ey), ez);
 }
 
+// blockIdx.x: a range of particles; blockIdx.y: a row of KPT * RHO_T k-vectors.
+// Dynamic shared memory: CH tables of 3 * ts phases, then CH charges.
 __global__ void __launch_bounds__(RHO_T) k_rho_partial(EwArgs a) {
-    __shared__ double2 tab[CH][3 * (KM + 1)];
-    __shared__ double sq[CH];
+    extern __shared__ double2 rtab[];
+    double* sq = (double*)(rtab + CH * 3 * a.ts);
     const int p0 = blockIdx.x * a.per_blk, p1 = min(a.n, p0 + a.per_blk);
+    const int kb = blockIdx.y * KPT * RHO_T;
     double2 acc[KPT];
     int4 kn[KPT];
 #pragma unroll
     for (int j = 0; j < KPT; ++j) {
         acc[j] = make_double2(0.0, 0.0);
-        const int k = threadIdx.x + j * RHO_T;
+        const int k = kb + threadIdx.x + j * RHO_T;
         kn[j] = k < a.nk ? a.kn[k] : make_int4(0, 0, 0, 0);
     }
     for (int b0 = p0; b0 < p1; b0 += CH) {
@@ -95,7 +100,7 @@ __global__ void __launch_bounds__(RHO_T) k_rho_partial(EwArgs a) {
         __syncthreads();
         if (threadIdx.x < nb) {
             const int i = b0 + threadIdx.x;
-            build_tables(tab[threadIdx.x], a, a.rx[i], a.ry[i], a.rz[i]);
+            build_tables(rtab + threadIdx.x * 3 * a.ts, a, a.rx[i], a.ry[i], a.rz[i]);
             sq[threadIdx.x] = a.q[i];
         }
         __syncthreads();
@@ -103,7 +108,7 @@ __global__ void __launch_bounds__(RHO_T) k_rho_partial(EwArgs a) {
             const double qi = sq[pp];
 #pragma unroll
             for (int j = 0; j < KPT; ++j) {
-                const double2 e = phase_from(tab[pp], kn[j]);
+                const double2 e = phase_from(rtab + pp * 3 * a.ts, a.ts, kn[j]);
                 acc[j].x += qi * e.x;
                 acc[j].y += qi * e.y;
             }
@@ -111,7 +116,7 @@ __global__ void __launch_bounds__(RHO_T) k_rho_partial(EwArgs a) {
     }
 #pragma unroll
     for (int j = 0; j < KPT; ++j) {
-        const int k = threadIdx.x + j * RHO_T;
+        const int k = kb + threadIdx.x + j * RHO_T;
         if (k < a.nk) a.rho_part[(size_t)blockIdx.x * a.nk + k] = acc[j];
     }
 }
@@ -136,7 +141,7 @@ __global__ void k_rho_reduce(EwArgs a) {
 template <typename R4>
 __global__ void __launch_bounds__(FT) k_ewald_force(EwArgs a) {
     extern __shared__ double2 ftab[];
-    double2* t = ftab + threadIdx.x * 3 * (KM + 1);
+    double2* t = ftab + threadIdx.x * 3 * a.ts;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const double qi = a.q[i];
@@ -144,7 +149,7 @@ __global__ void __launch_bounds__(FT) k_ewald_force(EwArgs a) {
     build_tables(t, a, a.rx[i], a.ry[i], a.rz[i]);
     double fx = 0.0, fy = 0.0, fz = 0.0;
     for (int k = 0; k < a.nk; ++k) {
-        const double2 e = phase_from(t, __ldg(&a.kn[k]));
+        const double2 e = phase_from(t, a.ts, __ldg(&a.kn[k]));
         const double2 r = __ldg(&a.rho[k]);
         const double4 kv = ldg4(&a.kvec[k]);
         const double sc = (e.x * r.y - e.y * r.x) * kv.w;   // (cos Im - sin Re) inv_k2 exp()
@@ -161,6 +166,15 @@ __global__ void __launch_bounds__(FT) k_ewald_force(EwArgs a) {
     f4[i] = o;
 }
 
+int table_stride(const mfa_ctx* c) {
+    int m = c->kmax[0];
+    if (c->kmax[1] > m) m = c->kmax[1];
+    if (c->kmax[2] > m) m = c->kmax[2];
+    return m + 1;
+}
+size_t rho_smem(const mfa_ctx* c) { return (size_t)CH * (3 * table_stride(c) * sizeof(double2) + sizeof(double)); }
+size_t force_smem(const mfa_ctx* c) { return (size_t)FT * 3 * table_stride(c) * sizeof(double2); }
+
 EwArgs make_args(mfa_ctx* c) {
     EwArgs a;
     a.rx = c->rx; a.ry = c->ry; a.rz = c->rz; a.q = c->q;
@@ -174,6 +188,7 @@ EwArgs make_args(mfa_ctx* c) {
     a.per_blk = (c->n + c->nblk_rho - 1) / c->nblk_rho;
     const mfa_params& p = c->p;
     for (int d = 0; d < 3; ++d) a.kmax[d] = c->kmax[d];
+    a.ts = table_stride(c);
     a.pi = p.pi;
     a.inv_V = c->inv_V;
     // the k components are n * delta_k (ewald_k.f90:117); the tables use delta_k
@@ -225,8 +240,8 @@ int ewald_setup(mfa_ctx* c) {
                 kv.push_back(make_double4(a0, a1, a2, inv * exp(-k2 * fac_alpha)));
                 kn.push_back(make_int4(x, y, z, 0));
             }
+    if (kv.size() > (size_t)NK_MAX) return MFA_ERR_UNSUPPORTED;
     c->nk = (int)kv.size();
-    if (c->nk > KPT * RHO_T) return MFA_ERR_UNSUPPORTED;
     c->kmax[0] = nkx; c->kmax[1] = nky; c->kmax[2] = nkz;
     c->inv_V = (c->inv_boundary[0] * c->inv_boundary[1]) / (p.boundary[2] * (1.0 + z_slab));
     if (c->kvec) cudaFree(c->kvec);
@@ -245,9 +260,13 @@ int ewald_setup(mfa_ctx* c) {
     c->nblk_rho = nblk;
     MFA_CUDA_TRY(cudaMalloc(&c->rho, (size_t)c->nk * sizeof(double2)));
     MFA_CUDA_TRY(cudaMalloc(&c->rho_part, (size_t)nblk * c->nk * sizeof(double2)));
+    // the attribute is per function and shared by every context: admit the
+    // largest tables any context can have (a launch passes its own size)
     const int fsm = FT * 3 * (KM + 1) * (int)sizeof(double2);
+    const int rsm = CH * (3 * (KM + 1) * (int)sizeof(double2) + (int)sizeof(double));
     MFA_CUDA_TRY(cudaFuncSetAttribute(k_ewald_force<float4>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
     MFA_CUDA_TRY(cudaFuncSetAttribute(k_ewald_force<double4>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+    MFA_CUDA_TRY(cudaFuncSetAttribute(k_rho_partial, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm));
     return MFA_OK;
 }
 
@@ -255,9 +274,10 @@ int launch_ewald(mfa_ctx* c) {
     if (!c->p.charged) return MFA_OK;
     if (c->nk == 0) return MFA_ERR_STATE;
     EwArgs a = make_args(c);
-    k_rho_partial<<<c->nblk_rho, RHO_T, 0, c->st>>>(a);
+    const dim3 rgrid(c->nblk_rho, (c->nk + KPT * RHO_T - 1) / (KPT * RHO_T));
+    k_rho_partial<<<rgrid, RHO_T, rho_smem(c), c->st>>>(a);
     k_rho_reduce<<<(c->nk + 255) / 256, 256, 0, c->st>>>(a);
-    const int fsm = FT * 3 * (KM + 1) * (int)sizeof(double2);
+    const size_t fsm = force_smem(c);
     if (c->prec == MFA_MIXED) k_ewald_force<float4><<<(c->n + FT - 1) / FT, FT, fsm, c->st>>>(a);
     else k_ewald_force<double4><<<(c->n + FT - 1) / FT, FT, fsm, c->st>>>(a);
     MFA_CUDA_TRY(cudaGetLastError());

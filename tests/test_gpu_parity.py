@@ -231,6 +231,29 @@ def test_ewald_kspace(name, request):
     g.close()
 
 
+def test_ewald_kspace_wide_slab():
+    """A slab channel at n_kmax = 10: the z spacing of the slab k-set is a third
+    of 2 pi / Lz, so |n_z| reaches 36 and the half-space holds more than 4096
+    vectors (tables sized by the largest |n|, vectors in several block rows)."""
+    cfg = configs.charged_slab(seed=16, n_kmax=10)
+    o, g = pair(cfg, FP64)
+    o.ewald_k(0)
+    g.ewald_k(0)
+    ko, kg = o.kvecs(), g.kvecs()
+    assert ko.shape == kg.shape and (ko == kg).all()
+    dkz = 2.0 * math.pi / (3.0 * cfg.params.boundary[2])
+    assert ko.shape[0] > 4096 and np.abs(ko[:, 2]).max() / dkz > 16.5
+    for x in (o, g):
+        x.binning()
+        x.zero_forces()
+        x.fluid_fluid()      # v_coul: real space and self term (fluid_fluid.f90:17)
+        x.zero_forces()
+        x.ewald_k(1)
+    assert relerr(g.download(_abi.F)["force"], o.state()["force"]) < 1e-10
+    assert g.scalars()["v_coul"] == pytest.approx(o.scalars()["v_coul"], rel=1e-11)
+    g.close()
+
+
 @pytest.mark.parametrize("prec,tol", [(FP64, 1e-12), (MIXED, 1e-6)])
 def test_dipolar_correction(charged_slab_cfg, prec, tol):
     """dipolar_correction (SYMMETRY 0): the slab correction's force and energy
