@@ -215,7 +215,9 @@ int mfa_fluid_wall(mfa_ctx* ctx, int32_t inter_type);
 int mfa_intra_molec(mfa_ctx* ctx);
 /* bending.f90:2-149 (mode 0: no-op, mode 2: angle forces).  Adds to force. */
 int mfa_bending(mfa_ctx* ctx, int32_t mode);
-/* ewald_k.f90:1-211 (mode 0: build k-vectors, mode 1: k-space energy + force). */
+/* ewald_k.f90:1-211 (mode 0: build k-vectors, mode 1: k-space energy + force).
+ * Mode 0 returns MFA_ERR_UNSUPPORTED beyond 64 multiples of delta_k on an axis
+ * or 65,536 vectors. */
 int mfa_ewald_k(mfa_ctx* ctx, int32_t mode);
 /* dipolar_correction.f90:17-39, called after ewald_k(1) for SYMMETRY 0
  * (md_main.f90:128-131): the slab correction of Yeh and Berkowitz,
