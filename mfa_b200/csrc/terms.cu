@@ -13,8 +13,6 @@
 // serial FP64 evaluation to rounding.
 #include "mfa_internal.cuh"
 
-#include <string.h>
-
 namespace {
 
 constexpr int TPB = 256;
