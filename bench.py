@@ -330,9 +330,11 @@ def batch_bench(a):
                                 device_id=torch.device("cuda", local))
     dev = local
     torch.cuda.set_device(dev)
-    # whole systems are the unit of work: rank r takes every world-th system
-    from mfa_b200.ranks import max_over_ranks, shard, sum_over_ranks
-    cfgs = shard(configs.uneven_brushes(seed=a.seed, n_sys=a.n_sys), rank, world)
+    # whole systems are the unit of work, shared out by bead count (greedy,
+    # largest first to the least-loaded rank; the same partition on every rank)
+    from mfa_b200.ranks import max_over_ranks, shard_by_weight, sum_over_ranks
+    every_sys = configs.uneven_brushes(seed=a.seed, n_sys=a.n_sys)
+    cfgs = shard_by_weight(every_sys, [c.n for c in every_sys], rank, world)
     n = sum(c.n for c in cfgs)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
 
@@ -434,7 +436,7 @@ def batch_bench(a):
                        "precision": "mixed", "dt": 0.005, "thermostat": "dpd",
                        "steps_per_timed_iteration": a.chunk,
                        "l2": "flushed between timed iterations (256 MiB write); state is larger than L2",
-                       "parallelism": f"whole systems over {world} GPU(s), no data exchange"},
+                       "parallelism": f"whole systems over {world} GPU(s) by bead count, no data exchange"},
             "fp64": {"value": n_all * a.steps / (ms_fp64 * 1e-3), "ms_per_step": ms_fp64 / a.steps},
             "mixed_over_fp64": ms_fp64 / ms_max,
             "one_system_at_a_time": {"value": n * seq_steps / t_seq,

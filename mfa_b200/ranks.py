@@ -24,6 +24,25 @@ def shard(items: Sequence[T], rank: int, world: int) -> list:
     return list(items[rank::world])
 
 
+def shard_by_weight(items: Sequence[T], weights: Sequence[float], rank: int, world: int) -> list:
+    """Whole systems for one rank, balanced by weight (bead count): greedy
+    longest-processing-time assignment -- systems in decreasing weight, each to
+    the rank with the least weight so far (ties to the lower rank, equal
+    weights in index order), so every rank computes the same partition with no
+    communication.  A rank's systems keep their original order; with one rank
+    it is the whole list."""
+    if len(items) != len(weights):
+        raise ValueError("one weight per item")
+    order = sorted(range(len(items)), key=lambda k: (-float(weights[k]), k))
+    load = [0.0] * world
+    owner = [0] * len(items)
+    for k in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        owner[k] = r
+        load[r] += float(weights[k])
+    return [items[k] for k in range(len(items)) if owner[k] == rank]
+
+
 def max_over_ranks(x: float, dist=None, device="cpu") -> float:
     """The largest value of x over the ranks (x itself without a process group)."""
     if dist is None:

@@ -8,7 +8,7 @@ import socket
 import pytest
 import torch.multiprocessing as mp
 
-from mfa_b200.ranks import max_over_ranks, shard, sum_over_ranks
+from mfa_b200.ranks import max_over_ranks, shard, shard_by_weight, sum_over_ranks
 
 
 def _free_port():
@@ -23,11 +23,12 @@ def _rank_main(rank, world, port, out):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     mine = shard(list(range(10)), rank, world)
+    mine_w = shard_by_weight(list(range(10)), [3, 9, 1, 7, 7, 2, 8, 5, 4, 6], rank, world)
     t = max_over_ranks(1.0 + rank, dist)            # each rank's own time
     n = sum_over_ranks(float(len(mine) * 100), dist)
     dist.barrier()
     dist.destroy_process_group()
-    out.put((rank, mine, t, n))
+    out.put((rank, mine, t, n, mine_w))
 
 
 def test_shard_covers_every_system_once():
@@ -35,6 +36,28 @@ def test_shard_covers_every_system_once():
     parts = [shard(items, r, 4) for r in range(4)]
     assert sorted(sum(parts, [])) == items
     assert max(len(p) for p in parts) - min(len(p) for p in parts) <= 1
+
+
+def test_shard_by_weight_balances_bead_counts():
+    # uneven systems in the bead-count range of the batch workload
+    import numpy as np
+    rng = np.random.default_rng(3)
+    w = [int(x) for x in rng.integers(1_000, 40_000, size=64)]
+    items = list(range(64))
+    for world in (1, 2, 3, 4, 8):
+        parts = [shard_by_weight(items, w, r, world) for r in range(world)]
+        assert sorted(sum(parts, [])) == items                      # every system once
+        assert all(p == sorted(p) for p in parts)                   # original order kept
+        loads = [sum(w[k] for k in p) for p in parts]
+        # greedy LPT: the largest load exceeds the mean by at most one system
+        assert max(loads) <= sum(w) / world + max(w)
+        rr = [sum(w[k] for k in shard(items, r, world)) for r in range(world)]
+        assert max(loads) <= max(rr)
+    assert shard_by_weight(items, w, 0, 1) == items
+    # a skewed case where every-world-th dealing is poor
+    w2 = [100, 1, 100, 1, 100, 1, 100, 1]
+    parts = [shard_by_weight(list(range(8)), w2, r, 2) for r in range(2)]
+    assert [sum(w2[k] for k in p) for p in parts] == [202, 202]
 
 
 def test_two_gloo_ranks_agree_on_time_and_size():
@@ -48,8 +71,10 @@ def test_two_gloo_ranks_agree_on_time_and_size():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    (r0, m0, t0, n0), (r1, m1, t1, n1) = res
+    (r0, m0, t0, n0, w0), (r1, m1, t1, n1, w1) = res
     assert m0 == [0, 2, 4, 6, 8] and m1 == [1, 3, 5, 7, 9]
+    # each rank computed the bead-count partition on its own: complementary, balanced
+    assert sorted(w0 + w1) == list(range(10)) and w0 == [1, 2, 4, 7, 8] and w1 == [0, 3, 5, 6, 9]
     assert t0 == t1 == 2.0                       # the slower rank's time for both
     assert n0 == n1 == 1000.0
 
