@@ -340,3 +340,22 @@ def test_gpu_dpd_vv_call_rules(brush_small_cfg):
     g.step(10)
     assert g.scalars()["i_time"] == 10
     g.close()
+
+
+def test_oracle_new_dpd_fd_full_list_applies_each_pair_twice(brush_small_cfg):
+    """new_dpd_fd.f90:33-84 adds each listed entry's force to both beads; with
+    my_binning's full list (every pair in both rows) a pair's dissipative force
+    is applied twice -- the reference's arithmetic, kept as it is."""
+    cfg = brush_small_cfg
+    fds = []
+    for rebuild in ("binning", "my_binning"):
+        o = _oracle(cfg)
+        o.init_forces()
+        getattr(o, rebuild)()
+        o.set_dpd_vv(True)
+        s1 = o.state()
+        o.new_dpd_fd()
+        fds.append(o.state()["force"] - s1["force"])
+    half, full = fds
+    assert np.abs(half).max() > 0.0
+    assert relerr(full, 2.0 * half) < 1e-12
