@@ -111,6 +111,34 @@ def kernel_times(a):
     return 0
 
 
+def loop_kernel_times(g, steps, chunk):
+    """Mean device time (us) and launch count of every kernel over `steps`
+    steps of the running loop (mfa_step calls of `chunk` steps, L2 warm),
+    from CUPTI's activity records through the torch profiler."""
+    import collections
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+    g.sync()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        for _ in range(max(1, steps // chunk)):
+            g.step(chunk)
+        g.sync()
+        torch.cuda.synchronize()
+    agg = collections.defaultdict(lambda: [0, 0.0])
+    for ev in prof.events():
+        if ev.device_type == torch.autograd.DeviceType.CUDA:
+            agg[ev.name][0] += 1
+            agg[ev.name][1] += getattr(ev, "device_time_total", 0.0)
+    return {k: {"launches": n, "mean_us": t / max(n, 1), "total_us": t} for k, (n, t) in agg.items()}
+
+
+def kernel_stat(kt, key):
+    """Launch count and mean time of the kernels whose name contains `key`."""
+    n = sum(v["launches"] for k, v in kt.items() if key in k)
+    t = sum(v["total_us"] for k, v in kt.items() if key in k)
+    return n, (t / n if n else None)
+
+
 def drift(a):
     """Equilibrate with the thermostat (FP64), then run the same state without
     thermostat (NVE) in FP64 and in mixed precision and report the energy
@@ -249,6 +277,13 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append((time.time(), line.strip()))
 
+    def wait_first(self, limit_s):
+        """Block until nvidia-smi has printed its first sample (or limit_s
+        passed), so that the sampler is running when the timed region opens."""
+        t0 = time.time()
+        while self.proc is not None and not self.lines and time.time() - t0 < limit_s:
+            time.sleep(0.02)
+
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
@@ -262,10 +297,15 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         b, e = self.window
         inside = [ln for ts, ln in self.lines if b <= ts <= e + 0.2]
+        where = "inside the timed region"
         if not inside and self.lines:
-            # a timed region shorter than the sampling period: the first sample after it began
-            later = [ln for ts, ln in self.lines if ts >= b]
-            inside = later[:1] if later else [self.lines[-1][1]]
+            # a timed region shorter than the sampling period (100 ms): the
+            # samples nearest to it, one on each side where there are two
+            before = [ln for ts, ln in self.lines if ts < b]
+            after = [ln for ts, ln in self.lines if ts > e]
+            inside = before[-1:] + after[:1]
+            where = (f"timed region of {1e3 * (e - b):.1f} ms is shorter than the 100 ms sampling "
+                     "period: the nearest sample on each side of it")
         for ln in inside:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 8:
@@ -280,7 +320,8 @@ class ClockSampler:
                     reasons.add(nm)
         sm.sort()
         med = sm[len(sm) // 2] if sm else None
-        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm),
+                "where": where if sm else "no sample arrived"}
 
 
 def pair_work(g, cfg):
@@ -354,12 +395,16 @@ def batch_bench(a):
         ext = torch.cuda.ExternalStream(b.stream_ptr(), device=f"cuda:{dev}")
         sampler = ClockSampler(dev)
         sampler.start()
-        for k in range(max(1, -(-warmup // a.chunk))):
+        chunks = [a.chunk] * (steps // a.chunk) + ([steps % a.chunk] if steps % a.chunk else [])
+        # at least three warm-up calls of each timed call length (graphs captured before timing)
+        warm_calls = [a.chunk] * max(3, -(-warmup // a.chunk))
+        warm_calls += [ln for ln in sorted(set(chunks)) if ln != a.chunk for _ in range(3)]
+        for k, ln in enumerate(warm_calls):
             with torch.cuda.stream(ext):
                 flush.fill_(k & 0xff)
-            b.step(a.chunk)
+            b.step(ln)
         b.sync()
-        chunks = [a.chunk] * (steps // a.chunk) + ([steps % a.chunk] if steps % a.chunk else [])
+        sampler.wait_first(5.0)
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in chunks]
         l0 = b.launches()
         if dist is not None:
@@ -467,8 +512,7 @@ def adjoint_bench(a):
     import torch
     from mfa_b200 import _abi, configs
     from mfa_b200.api import System
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from test_adjoint import NAMES, base_values, perturbed
+    from mfa_b200.sensitivity import NAMES, base_values, perturbed
     # the brush of the throughput workload (bending k_b = 2 included), 16 x 16 chains, implicit solvent
     cfg = configs.brush(seed=a.seed, nx=16, ny=16, n_mon=64, graft=0.3, z_wall=60.0, solvent=False, k_bend=2.0)
     S, K = 200, 20
@@ -616,11 +660,22 @@ def main():
         # nvidia-smi does not overlap the timed region
         sampler = ClockSampler(dev)
         sampler.start()
-        for k in range(max(1, -(-warmup // a.chunk))):
+        # warm-up: W steps rounded up to whole calls, and at least three calls
+        # of every length the timed loop uses.  mfa_step captures the graph of
+        # a whole call the second time it sees a step count, so three calls
+        # put the capture and instantiation before the first timed event.
+        lengths = sorted(set(chunks))
+        warm_calls = [a.chunk] * max(3, -(-warmup // a.chunk))
+        for ln in lengths:
+            if ln != a.chunk:
+                warm_calls += [ln] * 3
+        warm_calls.append(chunks[0])
+        for k, ln in enumerate(warm_calls):
             with torch.cuda.stream(ext):
                 flush.fill_(k & 0xff)
-            g.step(a.chunk)
+            g.step(ln)
         g.sync()
+        sampler.wait_first(5.0)
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in chunks]
         s0 = g.scalars()
         launches0 = s0["kernel_launches"]
@@ -643,9 +698,14 @@ def main():
         clocks = sampler.stop()
         if dist is not None:
             dist.barrier()
-        ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
+        per_call = [e0.elapsed_time(e1) for e0, e1 in ev]
+        ms = sum(per_call)
         s = g.scalars()
         s["rebuilds_timed"] = s["n_rebuilds"] - s0["n_rebuilds"]
+        srt = sorted(per_call)
+        s["per_call_ms"] = {"calls": len(per_call), "steps_per_call": a.chunk,
+                            "min": srt[0], "median": srt[len(srt) // 2], "max": srt[-1],
+                            "first": per_call[:8]}
         return g, ms, s["kernel_launches"] - launches0, clocks, s
 
     # headline: mixed precision
@@ -666,6 +726,10 @@ def main():
     e1.record(ext)
     g.sync()
     ms_resident = max_over_ranks(e0.elapsed_time(e1), dist, f"cuda:{dev}")
+
+    # device time of each kernel inside the running loop (CUPTI activity
+    # records: graph nodes as they run, nothing serialised or replayed)
+    loop_kt = loop_kernel_times(g, 200, a.chunk)
 
     # dominant kernel: the pair kernel, timed alone on the context's stream
     work = pair_work(g, cfg)
@@ -714,17 +778,34 @@ def main():
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = pair_bytes / (pair_ms * 1e-3) / 1e9
-    traffic = None
+    traffic, traffic_src = None, None
     try:
         prof = json.load(open(os.path.join(ROOT, "profiles", "pair_traffic.json")))
         if prof.get("workload") == meta["workload"]:
             traffic = prof.get("dram_bytes_per_launch")
+            traffic_src = ("stored ncu capture of the same kernel and workload (profiles/pair_traffic.json: "
+                           f"{prof.get('command', 'see file')}), not measured in this run")
     except (OSError, ValueError):
         pass
+    # integration: the fused velocity-Verlet kernel of the loop against the
+    # canonical 124 B per bead-step (mixed) of the integrator's streams
+    vv_n, vv_us = kernel_stat(loop_kt, "k_vv_fused")
+    pair_n, pair_us_loop = kernel_stat(loop_kt, "k_pair")
+    integ = None
+    if vv_us:
+        integ = {"bound": "hbm", "kernel": "k_vv_fused (verlet_velocities + verlet_positions + check_skin + "
+                                           "intra_molec + bending)",
+                 "launch_us": vv_us, "launches": vv_n, "algorithmic_bytes": 124 * n,
+                 "achieved_gbs": 124 * n / (vv_us * 1e-6) / 1e9,
+                 "frac": 124 * n / (vv_us * 1e-6) / 1e9 / hbm_peak,
+                 "source": "CUPTI activity records over 200 in-loop steps (L2 warm)"}
+    loop_total = sum(v["total_us"] for v in loop_kt.values())
+    loop_share = {k.split("(")[0].replace("void ", "")[:60]: round(v["total_us"] / loop_total, 4)
+                  for k, v in sorted(loop_kt.items(), key=lambda kv: -kv[1]["total_us"])[:8]} if loop_total else {}
     g.close()
 
     # plain FP64 GPU path, same protocol
-    g64, ms_fp64, _, _, _ = timed_run(_abi.FP64, a.steps, a.warmup)
+    g64, ms_fp64, _, _, s64 = timed_run(_abi.FP64, a.steps, a.warmup)
     g64.close()
     ms_fp64 = max_over_ranks(ms_fp64, dist, f"cuda:{dev}")
     value_fp64 = world * n * a.steps / (ms_fp64 * 1e-3)
@@ -739,6 +820,11 @@ def main():
         ge.ewald_k(0)
     ge.init_forces()
     ge.step(a.equil)
+    # the single-step call's graph is captured on its second call: three
+    # untimed single steps put that capture before the timed region
+    for _ in range(3):
+        ge.step(1)
+        ge.scalars()
     st = ge.download()
     pinned[0].copy_(torch.from_numpy(st["r0"]))
     pinned[1].copy_(torch.from_numpy(st["v"]))
@@ -784,15 +870,22 @@ def main():
                            l2=f"flushed between timed iterations of {a.chunk} steps "
                               "(256 MiB write on the context stream)",
                            parallelism=f"replicas x{world}"),
-            "fp64": {"value": value_fp64, "ms_per_step": ms_fp64 / a.steps},
+            "fp64": {"value": value_fp64, "ms_per_step": ms_fp64 / a.steps, "per_call_ms": s64["per_call_ms"]},
             "mixed_over_fp64": value / value_fp64,
             "value_l2_resident": world * n * a.steps / (ms_resident * 1e-3),
             "roofline": {"bound": "hbm", "kernel": "k_pair (fluid_fluid + dpd_forces + 9-3 walls)",
                          "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                         "traffic": traffic, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"
+                         "traffic": traffic, "traffic_source": traffic_src,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"
                          if "hbm_gbs" in peaks else "fallback 6650 GB/s",
                          "launch_ms": pair_ms, "algorithmic_bytes": pair_bytes,
+                         "timing": "CUDA events around the launch on the context stream, L2 flushed before each, "
+                                   f"mean of {reps}",
+                         "launch_us_in_loop": pair_us_loop,
                          "fp32_tflops": pair_flops / (pair_ms * 1e-3) / 1e12, **work},
+            "integration": integ,
+            "loop_kernel_share": loop_share,
+            "per_call_ms": s_mixed["per_call_ms"],
             "rebuild": {"bound": "hbm", "launch_ms": rebuild_ms, "algorithmic_bytes": 60 * n,
                         "achieved_gbs": 60 * n / (rebuild_ms * 1e-3) / 1e9,
                         "frac": 60 * n / (rebuild_ms * 1e-3) / 1e9 / hbm_peak,

@@ -413,9 +413,12 @@ int mfa_adjoint(mfa_ctx* ctx, int32_t nsteps, int32_t every, double* out7);
  * the process exits); larger grids return MFA_ERR_CAPACITY.  All calls share
  * that array: calls whose work overlaps on the GPU race and must be serialised
  * by the caller.  boundary and n_bin are host arrays of 3; stream is a
- * cudaStream_t (NULL for the default stream).  The first call on a device looks
- * the array's device address up (make it before any stream capture); every
- * call synchronises `stream` before returning and reports particles outside
+ * cudaStream_t (NULL for the default stream).  Every call looks the array's
+ * device address up on the current device (so it stays right after a
+ * cudaDeviceReset); the first call on a device also loads the library's device
+ * code there, so make it before any stream capture.  Any n_bin[d] or partial
+ * product above the capacity returns MFA_ERR_CAPACITY.  Every call synchronises
+ * `stream` before returning and reports particles outside
  * the grid (MFA_ERR_CELL_RANGE) or non-finite (MFA_ERR_NONFINITE). */
 int mfa_bin_cells_noalloc(const double* r0, int32_t n, const double* boundary,
                           const int32_t* n_bin, int32_t rule, int32_t* cell_of,

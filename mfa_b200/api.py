@@ -35,8 +35,14 @@ class System:
     """One simulated system resident on one GPU."""
 
     def __init__(self, params: MfaParams, r0, v, a_type, mass, q=None, a=None, mic=None,
-                 precision: int = _abi.MIXED, device: int = 0):
+                 precision: int = _abi.MIXED, device: int = 0, bin_type: int = 0):
+        if bin_type not in (0, 1):
+            raise ValueError("bin_type is 0 (binning) or 1 (my_binning)")
         self.lib = load()
+        # BIN_TYPE of control_simulation.h: the list rule of every rebuild this
+        # object starts (init_forces, md_step, restore); calling binning() or
+        # my_binning() directly switches it, as the library's context does
+        self.bin_type = bin_type
         self.params = params.copy()
         self.n = int(params.n_part)
         self.precision = precision
@@ -86,9 +92,18 @@ class System:
 
     def binning(self) -> None:
         check(self.lib.mfa_binning(self.ctx), "binning")
+        self.bin_type = 0
 
     def my_binning(self) -> None:
         check(self.lib.mfa_my_binning(self.ctx), "my_binning")
+        self.bin_type = 1
+
+    def rebuild(self) -> None:
+        """The list rebuild of md_main.f90:81-85 with this system's rule."""
+        if self.bin_type == 1:
+            self.my_binning()
+        else:
+            self.binning()
 
     def zero_forces(self) -> None:
         check(self.lib.mfa_zero_forces(self.ctx), "zero_forces")
@@ -152,7 +167,7 @@ class System:
         p = self.params
         if p.charged:
             self.ewald_k(0)
-        self.binning()
+        self.rebuild()
         self.zero_forces()
         self.fluid_fluid()
         if p.symmetry == 0 and p.wall in (2, 3, 4):
@@ -174,7 +189,7 @@ class System:
         self.verlet_positions()
         f_skin = self.check_skin()
         if f_skin == 1:
-            self.binning()
+            self.rebuild()
         self.zero_forces()
         self.fluid_fluid()
         if p.symmetry == 0 and p.wall in (2, 3, 4):

@@ -11,9 +11,11 @@ FP64 bit of the state for an exact resume (layout below).
 
 Binary side-car (little endian):
     8 bytes   magic ``b"MFASTATE"``
-    int32     version (1)
+    int32     version (2; version 1 files, without the next two fields, are read too)
     int32     n (particles)
     int64     i_time (the step counter)
+    int32     bin_type (the list rule: 0 binning, 1 my_binning)
+    int32     reserved (0)
     then      r0, v, a as n x 3 float64 (particle-major, xyz contiguous),
               mic as n x 3 int32 (periodic image counters), a_type as n int32.
 """
@@ -24,7 +26,7 @@ import struct
 import numpy as np
 
 MAGIC = b"MFASTATE"
-VERSION = 1
+VERSION = 2
 N_ORDER = 2          # mfa_common.f90:70 (predictor order kept for the top wall)
 
 
@@ -135,7 +137,7 @@ def read_conf(path: str, n_part: int, dt: float = 0.005) -> dict:
     return out
 
 
-def write_state(path: str, r0, v, a, mic, a_type, i_time: int) -> None:
+def write_state(path: str, r0, v, a, mic, a_type, i_time: int, bin_type: int = 0) -> None:
     """Every bit of the dynamic state (layout in the module docstring)."""
     r0 = np.ascontiguousarray(r0, dtype="<f8").reshape(-1, 3)
     n = r0.shape[0]
@@ -144,7 +146,7 @@ def write_state(path: str, r0, v, a, mic, a_type, i_time: int) -> None:
               np.ascontiguousarray(mic, dtype="<i4").reshape(n, 3),
               np.ascontiguousarray(a_type, dtype="<i4").reshape(n)]
     with open(path, "wb") as fh:
-        fh.write(MAGIC + struct.pack("<iiq", VERSION, n, int(i_time)))
+        fh.write(MAGIC + struct.pack("<iiqii", VERSION, n, int(i_time), int(bin_type), 0))
         for x in arrays:
             fh.write(x.tobytes())
 
@@ -155,8 +157,11 @@ def read_state(path: str) -> dict:
         if len(head) != 24 or head[:8] != MAGIC:
             raise ValueError(f"{path}: not a state file")
         version, n, i_time = struct.unpack("<iiq", head[8:])
-        if version != VERSION:
-            raise ValueError(f"{path}: version {version}, expected {VERSION}")
+        bin_type = None
+        if version == 2:
+            bin_type, _ = struct.unpack("<ii", fh.read(8))
+        elif version != 1:
+            raise ValueError(f"{path}: version {version}, expected 1 or {VERSION}")
         body = fh.read()
     sizes = [24 * n, 24 * n, 24 * n, 12 * n, 4 * n]
     if len(body) != sum(sizes):
@@ -168,6 +173,7 @@ def read_state(path: str) -> dict:
         out[name] = np.frombuffer(body[off:off + size], dtype=dt).reshape(shape).copy()
         off += size
     out["i_time"] = i_time
+    out["bin_type"] = bin_type
     return out
 
 
@@ -182,21 +188,26 @@ def save(system, conf_path: str | None = None, state_path: str | None = None, n_
                    p.n_chain_d, n_cell_w, dt=p.dt)
     if state_path:
         write_state(state_path, st["r0"], st["v"], st["a"], st["mic"], system.a_type,
-                    system.scalars()["i_time"])
+                    system.scalars()["i_time"], getattr(system, "bin_type", 0))
 
 
 def restore(system, state_path: str | None = None, conf_path: str | None = None) -> None:
     """Loads a saved state into a System with the same particles: every bit from
     the side-car (and its step counter), or the text file's 7 decimals (step
     counter left as it is).  Then rebuilds the cells and neighbour lists from
-    the loaded positions, as the reference's start-up does after reading
-    conf_old (init_config.f90:252)."""
+    the loaded positions with the system's own list rule (binning or
+    my_binning; a side-car written from a system of the other rule is
+    refused), as the reference's start-up does after reading conf_old with the
+    rule it was built with (init_config.f90:251-255)."""
     if (state_path is None) == (conf_path is None):
         raise ValueError("give exactly one of state_path and conf_path")
     if state_path:
         st = read_state(state_path)
         if st["r0"].shape[0] != system.n or (st["a_type"] != system.a_type).any():
             raise ValueError(f"{state_path}: particles differ from the system's")
+        rule = getattr(system, "bin_type", 0)
+        if st["bin_type"] is not None and st["bin_type"] != rule:
+            raise ValueError(f"{state_path}: saved with list rule {st['bin_type']}, the system uses {rule}")
         system.upload(r0=st["r0"], v=st["v"], a=st["a"], mic=st["mic"])
         system.set_step(st["i_time"])
     else:
@@ -204,4 +215,7 @@ def restore(system, state_path: str | None = None, conf_path: str | None = None)
         if (st["a_type"] != system.a_type).any():
             raise ValueError(f"{conf_path}: particle types differ from the system's")
         system.upload(r0=st["r0"], v=st["v"], a=st["a"])
-    system.binning()
+    if hasattr(system, "rebuild"):
+        system.rebuild()
+    else:
+        system.binning()

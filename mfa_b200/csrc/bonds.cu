@@ -3,7 +3,8 @@
 // Thread per chain bead (bonded.cuh): the bead's two bonds and the three angles
 // that move it, recomputed by each bead that needs them, so that every bead's
 // force is summed by one thread in a fixed order, without atomics.  The time-step
-// fast path folds the same computation into the pair kernel's epilogue.
+// fast path folds the same computation into the fused integrator (k_vv_fused in
+// integrate.cu), which adds it to the force record before a = F/m.
 #include "mfa_internal.cuh"
 
 #include <type_traits>

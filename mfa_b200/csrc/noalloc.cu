@@ -13,23 +13,20 @@
 // by the caller.  The counters are cleared at the start of every call, so
 // the contents a previous call left behind do not matter.
 //
-// The entry point looks the array's device address up with
-// cudaGetSymbolAddress once per device, on its first call with that device
-// current (host code cannot use the symbol itself as a device address); that
-// first call should therefore be made before any stream capture begins.
+// Host code cannot use the symbol itself as a device address, so every call
+// looks the array's device address up with cudaGetSymbolAddress, with the
+// caller's device current.  The lookup allocates nothing; doing it on every
+// call (rather than caching it per device) keeps the address right after a
+// cudaDeviceReset has re-created the context and reloaded this module.  The
+// first call on a device loads the module there, so it should be made before
+// any stream capture begins.
 #include "mfa_internal.cuh"
 
-#include <mutex>
-
 #define MFA_NOALLOC_MAX_CELLS (1 << 17)
-#define MFA_NOALLOC_MAX_DEVICES 64
 
 static __device__ __align__(256) int32_t g_noalloc_cells[2 * MFA_NOALLOC_MAX_CELLS + 32];
 
 namespace {
-
-std::mutex g_setup_mutex;
-int32_t* g_scratch_ptr[MFA_NOALLOC_MAX_DEVICES] = {nullptr};
 
 struct NaArgs {
     const double* r0;      // device, xyz interleaved per particle
@@ -129,18 +126,12 @@ __global__ void k_na_sort(NaArgs a) {
     }
 }
 
-// device address of the fixed scratch for the current device (looked up once)
+// device address of the fixed scratch on the current device
 int scratch_for_current_device(int32_t** out) {
-    int dev = -1;
-    MFA_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= MFA_NOALLOC_MAX_DEVICES) return MFA_ERR_UNSUPPORTED;
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
-        void* p = nullptr;
-        MFA_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_cells));
-        g_scratch_ptr[dev] = (int32_t*)p;
-    }
-    *out = g_scratch_ptr[dev];
+    void* p = nullptr;
+    MFA_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_cells));
+    if (!p) return MFA_ERR_CUDA;
+    *out = (int32_t*)p;
     return MFA_OK;
 }
 
@@ -156,7 +147,11 @@ extern "C" int mfa_bin_cells_noalloc(const double* r0, int32_t n, const double* 
     NaArgs a;
     for (int d = 0; d < 3; ++d) {
         if (n_bin[d] < 1 || !(boundary[d] > 0.0)) return MFA_ERR_ARGS;
+        // each factor and each partial product stays within the capacity, so
+        // the product cannot overflow whatever the three values are
+        if (n_bin[d] > MFA_NOALLOC_MAX_CELLS) return MFA_ERR_CAPACITY;
         ncell *= n_bin[d];
+        if (ncell > MFA_NOALLOC_MAX_CELLS) return MFA_ERR_CAPACITY;
         a.nb[d] = n_bin[d];
         a.rbin[d] = boundary[d] / (double)n_bin[d];   // make_binning_boxes.f90:188-195
         a.inv_rbin[d] = 1.0 / a.rbin[d];

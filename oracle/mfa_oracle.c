@@ -1089,7 +1089,9 @@ int orc_md_step(orc_state* s) {
     int err = 0;
     orc_verlet_positions(s);
     orc_check_skin(s);
-    if (s->f_skin == 1) err = orc_binning(s);
+    /* md_main.f90:81-85: the rule the program was built with (BIN_TYPE); here
+       the rule of the last list build */
+    if (s->f_skin == 1) err = s->bin_type == 1 ? orc_my_binning(s) : orc_binning(s);
     if (err) return err;
     orc_zero_forces(s);
     orc_fluid_fluid(s);

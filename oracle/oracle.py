@@ -84,8 +84,9 @@ class Oracle:
     """The reference's per-step routines on the CPU, same names as mfa_b200.System."""
 
     def __init__(self, params, r0, v, a_type, mass, q=None, a=None, mic=None,
-                 bin_cap: int = 300, list_cap: int = 256, rng_mode: int = 0):
+                 bin_cap: int = 300, list_cap: int = 256, rng_mode: int = 0, bin_type: int = 0):
         self.lib = load()
+        self.bin_type = bin_type      # BIN_TYPE: 0 binning, 1 my_binning
         self.params = params
         self.n = int(params.n_part)
         self._keep = [np.ascontiguousarray(x, dtype=dt).reshape(shape) if x is not None else None
@@ -171,7 +172,10 @@ class Oracle:
         p = self.params
         if p.charged:
             self.ewald_k(0)
-        self.binning()
+        if self.bin_type == 1:
+            self.my_binning()
+        else:
+            self.binning()
         self.zero_forces()
         self.fluid_fluid()
         if p.symmetry == 0 and p.wall in (2, 3, 4):

@@ -100,3 +100,21 @@ def test_product_package_does_not_reference_the_oracle():
             if f.endswith((".py", ".cu", ".cuh", ".h")):
                 txt = open(os.path.join(dirpath, f)).read()
                 assert "oracle" not in txt.lower(), f
+
+
+@pytest.mark.parametrize("n_bin", [(1 << 17 + 1, 1, 1), (1 << 16, 1 << 16, 1 << 16),
+                                   (2 ** 31 - 1, 2 ** 31 - 1, 2 ** 31 - 1), (64, 64, 64)])
+def test_noalloc_binning_rejects_grids_beyond_capacity_before_any_cuda_call(n_bin):
+    """Each n_bin factor and each partial product is checked against the fixed
+    131,072-cell capacity before the product is formed, so three large values
+    cannot wrap the cell count past the check.  The rejection comes before any
+    CUDA call (no GPU here: a call that got further would fail with
+    MFA_ERR_CUDA instead); the buffers are never touched."""
+    lib = _abi.load()
+    dummy = np.zeros(16, dtype=np.int32)
+    r0 = np.zeros((1, 3))
+    b = (C.c_double * 3)(10.0, 10.0, 10.0)
+    nb = (C.c_int32 * 3)(*n_bin)
+    ptr = C.c_void_p(dummy.ctypes.data)
+    rc = lib.mfa_bin_cells_noalloc(C.c_void_p(r0.ctypes.data), 1, b, nb, 0, ptr, ptr, ptr, None)
+    assert rc == _abi.ERR_CAPACITY

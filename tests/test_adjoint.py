@@ -4,7 +4,6 @@ random numbers (the DPD noise is keyed by step and pair, so the perturbed runs
 see the same noise), in FP64; the mixed-precision adjoint against the FP64 one.
 The adjoint is also wrapped here -- in the test harness only -- as a
 torch.autograd.Function, the way a Python optimiser would call it."""
-import math
 
 import numpy as np
 import pytest
@@ -12,46 +11,9 @@ import pytest
 from mfa_b200 import _abi, configs
 from mfa_b200._abi import FP64, MIXED
 from mfa_b200.api import System
+from mfa_b200.sensitivity import NAMES, base_values, perturbed
 
 pytestmark = pytest.mark.gpu
-
-NAMES = ("eps_lj", "sigma", "k_fene", "r0", "gamma_dpd", "eps_wall")
-
-
-def perturbed(params, name, f):
-    """A copy of the derived parameters with one physical parameter scaled by f,
-    as mfa_adjoint defines them."""
-    p = params.copy()
-    act = [k for k in range(64) if p.range_2[k] > 0.0]
-    if name == "eps_lj":
-        for k in act:
-            p.epsil[k] *= f
-    elif name == "sigma":
-        for k in act:
-            p.sigma_2[k] *= f * f
-            p.range_2[k] *= f * f
-            p.inv_range_2[k] /= f * f
-    elif name == "k_fene":
-        p.k_chain *= f
-    elif name == "r0":
-        p.r_chain_2 *= f * f
-        p.inv_r_chain_2 /= f * f
-        p.k_chain *= f * f
-    elif name == "gamma_dpd":
-        p.friction *= f
-        p.sig *= math.sqrt(f)
-    elif name == "eps_wall":
-        for t in range(8):
-            p.a_wall[t] *= f
-        p.a_w *= f
-    return p
-
-
-def base_values(p):
-    act = [k for k in range(64) if p.range_2[k] > 0.0]
-    return {"eps_lj": max(p.epsil[k] for k in act) / 4.0, "sigma": max(math.sqrt(p.sigma_2[k]) for k in act),
-            "k_fene": p.k_chain * p.inv_r_chain_2, "r0": math.sqrt(p.r_chain_2), "gamma_dpd": p.friction,
-            "eps_wall": max(p.a_wall[t] for t in range(8))}
 
 
 @pytest.fixture(scope="module")
