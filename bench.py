@@ -177,7 +177,7 @@ def drift(a):
                      "ms_per_step": e0.elapsed_time(e1) / a.drift_steps,
                      "bead_steps_per_s": cfg.n * a.drift_steps / (e0.elapsed_time(e1) * 1e-3)}
         h.close()
-        # e_total is the reference's sum (verlet_velocities.f90:336): it leaves
+        # e_total is the reference's sum (verlet_velocities.f90:187): it leaves
         # out the bending and Coulomb energies, so with bending it is not a
         # constant of the motion.  The same run again, read every `every`
         # steps, with those terms added back.

@@ -62,7 +62,7 @@ typedef enum mfa_precision {
 
 /* Noise shape for DPD / Langevin random forces */
 #define MFA_NOISE_GAUSS   0   /* Box-Muller on Philox-4x32-10 (stands in for rnor())   */
-#define MFA_NOISE_UNIFORM 1   /* sqrt(3)*(2u-1), the alternative of dpd_forces.f90:278 */
+#define MFA_NOISE_UNIFORM 1   /* sqrt(3)*(2u-1), the alternative of dpd_forces.f90:24 */
 
 /*
  * Run parameters.  These are the *derived* constants the reference computes in
@@ -86,13 +86,13 @@ typedef struct mfa_params {
     int32_t charged;         /* Ewald real + k-space (SYSTEM 2,3)                       */
     int32_t bending;         /* bending(2) over the grafted/bulk chains                 */
     int32_t force_switch_on; /* FORCE_SWITCH_ON clamp r^2 = max(r^2, r_2_min)           */
-    int32_t pin_heads;       /* brush heads pinned (verlet_velocities.f90:269-282)      */
+    int32_t pin_heads;       /* brush heads pinned (verlet_velocities.f90:113-145)      */
     int32_t quirks;          /* MFA_Q_* bits                                            */
     int32_t noise;           /* MFA_NOISE_*                                             */
     /* geometry and cell grid */
     double  boundary[3];
-    int32_t n_bin[3];        /* cells per axis (make_binning_boxes.f90:175-177)         */
-    int32_t delta_bin[3];    /* upper neighbour-cell offset (make_binning_boxes.f90:145-168) */
+    int32_t n_bin[3];        /* cells per axis (make_binning_boxes.f90:44-46)         */
+    int32_t delta_bin[3];    /* upper neighbour-cell offset (make_binning_boxes.f90:14-37) */
     int32_t pad0;
     /* pair tables [(ti-1)*MFA_MAX_TYPES + (tj-1)] */
     double  range_2[MFA_MAX_TYPES * MFA_MAX_TYPES];
@@ -107,7 +107,7 @@ typedef struct mfa_params {
     double  k_chain;         /* FENE k * R0^2 (init_params.f90:398), grafted chains     */
     double  k_ring;          /* FENE constant used for melt/droplet chains (intra_molec.f90:133) */
     double  r_chain_2, inv_r_chain_2;
-    double  fene_clamp;      /* 0.98 (single-precision literal, intra_molec.f90:248)    */
+    double  fene_clamp;      /* 0.98 (single-precision literal, intra_molec.f90:44)    */
     double  k_bend, alpha_eq;
     /* walls */
     double  a_wall[MFA_MAX_TYPES], sigma_wall[MFA_MAX_TYPES];
@@ -211,7 +211,7 @@ int mfa_pair_forces(mfa_ctx* ctx);
 int mfa_forces(mfa_ctx* ctx);
 /* fluid_wall.f90:2-204, inter_type 2, 3 or 4.  Adds to force (2,3), reflects v (3,4). */
 int mfa_fluid_wall(mfa_ctx* ctx, int32_t inter_type);
-/* intra_molec.f90:1-300: FENE bonds of grafted and melt chains.  Adds to force. */
+/* intra_molec.f90:1-539: FENE bonds of grafted and melt chains.  Adds to force. */
 int mfa_intra_molec(mfa_ctx* ctx);
 /* bending.f90:2-149 (mode 0: no-op, mode 2: angle forces).  Adds to force. */
 int mfa_bending(mfa_ctx* ctx, int32_t mode);

@@ -306,7 +306,7 @@ class System:
         return out, n.value
 
     def density_profiles(self, counts, n_obs):
-        """histo(1) normalisation (functions.f90:137): counts * hist_dim /
+        """histo(1) normalisation (functions.f90:139): counts * hist_dim /
         (Lz * n_obs * Lx * Ly), with the bin centres."""
         L = np.asarray(self.params.boundary[:3], dtype=np.float64)
         hd = counts.shape[1]

@@ -203,7 +203,7 @@ def melt(seed: int = 12345, n_chain: int = 100, n_mon: int = 32, density: float 
     """Bead-spring melt: n_chain x n_mon beads, cubic periodic box, WCA + FENE + DPD.
 
     Chains are stored in the grafted/bulk-chain segment (ids 1..n_mon*n_chain),
-    which the reference bonds with k_chain (intra_molec.f90:220-300)."""
+    which the reference bonds with k_chain (intra_molec.f90:16-96)."""
     rng = np.random.default_rng(seed)
     n = n_chain * n_mon
     L = (n / density) ** (1.0 / 3.0)

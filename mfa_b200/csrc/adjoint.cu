@@ -13,7 +13,7 @@
 //   rho = lam_r + 1/S dO/dr (s >= 1),  nu = dt lam_r + lam_u,  alpha = dt^2/2 lam_r + dt/2 lam_u
 // The vector-Jacobian products are written out by hand for every force term
 // of the path: WCA/LJ and DPD pairs (half list, Newton's third law), FENE bonds
-// (with the clamp of intra_molec.f90:248), the bending angles of bending.f90
+// (with the clamp of intra_molec.f90:44), the bending angles of bending.f90
 // (forward-mode derivative of the angle force) and the 9-3 walls.  The forward
 // states are recomputed segment by segment from checkpoints every K steps, with
 // the DPD noise replayed: Philox is keyed by (step, pair), so the recomputed

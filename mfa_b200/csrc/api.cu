@@ -393,7 +393,7 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
     int32_t* i2 = nullptr;
     A(dalloc(&i2, (size_t)2 * n));
     if (rc == MFA_OK) { c->ids = i2; c->slot = i2 + n; }
-    // cells (make_binning_boxes.f90:188-195)
+    // cells (make_binning_boxes.f90:57-64)
     c->ncell = 1;
     for (int d = 0; d < 3; ++d) {
         c->nb[d] = p->n_bin[d];

@@ -54,7 +54,7 @@ __device__ __forceinline__ double log1m_(double x) { return log(1.0 - x); }
 __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
 __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
 
-// image of r(k) - r(k+1) as intra_molec.f90:225-263 forms it (no z image in channels)
+// image of r(k) - r(k+1) as intra_molec.f90:21-59 forms it (no z image in channels)
 __device__ __forceinline__ double fene_image(double d, double L, double iL) {
     return d - L * (double)(int)(2.0 * d * iL);
 }
@@ -90,7 +90,7 @@ __device__ __forceinline__ double angle_forces(const BondParams& b, const R p[3]
 
 // Bonded force on bead i (adds to f); e_fene collects the bond potentials
 // -1/2 ln(1 - x) of the bond starting at i (to be multiplied by k_chain,
-// intra_molec.f90:272,300), e_bend the energy of the angle centred on i.
+// intra_molec.f90:96,270), e_bend the energy of the angle centred on i.
 // The chain window i-2 .. i+2 is walked once, bond by bond, so that only two
 // positions and two bond vectors are live at a time.
 template <typename R, typename E>
@@ -119,7 +119,7 @@ __device__ __forceinline__ void bonded_on_bead(const BondParams& b, int i, R f[3
         const double d0 = px - x, d1 = py - y, d2 = pz - z;    // r(j) - r(j+1), j = q-1
         const int j = q - 1;
         if (b.do_fene && (j == pos - 1 || j == pos)) {
-            // intra_molec.f90:225-263
+            // intra_molec.f90:21-59
             const R dx = (R)fene_image(d0, b.L[0], b.invL[0]);
             const R dy = (R)fene_image(d1, b.L[1], b.invL[1]);
             const R dz = (R)(b.symmetry == 1 ? fene_image(d2, b.L[2], b.invL[2]) : d2);

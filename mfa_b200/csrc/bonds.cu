@@ -42,7 +42,7 @@ __global__ void k_bonds(BondArgs a) {
     }
     for (int o = 16; o > 0; o >>= 1) clamped += __shfl_down_sync(0xffffffffu, clamped, o);
     if ((threadIdx.x & 31) == 0 && clamped) atomicAdd(&a.flags[F_FENE], clamped);
-    // intra_molec.f90:300 / :272: energies multiplied by k_chain
+    // intra_molec.f90:96 / :270: energies multiplied by k_chain
     double acc[2] = {a.b.k_chain * e_fene, e_bend};
     if (block_sum_commit<2>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_TMP0) && threadIdx.x == 0) {
         // publish only what this pass computed (intra_molec and bending are separate calls)

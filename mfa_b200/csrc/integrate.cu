@@ -173,7 +173,7 @@ __device__ __forceinline__ double velocity_half(const VVArgs& a, int i, double& 
 }
 
 __device__ __forceinline__ void finish_energies(const VVArgs& a) {
-    // verlet_velocities.f90:334-347 (v_wall_wall = 0, t_wall = 0); the block
+    // verlet_velocities.f90:155-198 (v_wall_wall = 0, t_wall = 0); the block
     // sums arrive in S_TMP0.. (kinetic, and FENE, bending when fused)
     double* s = a.dscal;
     s[S_TKIN] = 0.5 * s[S_TMP0];
@@ -200,7 +200,7 @@ __device__ __forceinline__ void finish_energies(const VVArgs& a) {
 
 // the FENE bonds at the clamp counted by the warp, and -- in the steps whose
 // energies are wanted (en) -- the block sums of m v^2, FENE (times k_chain,
-// intra_molec.f90:272,300) and bending energy; true in the last block
+// intra_molec.f90:96,270) and bending energy; true in the last block
 __device__ __forceinline__ bool vv_commit(const VVArgs& a, double ke, const double eb[2], int clamped, Blk blk,
                                           bool en) {
     for (int o = 16; o > 0; o >>= 1) clamped += __shfl_down_sync(0xffffffffu, clamped, o);

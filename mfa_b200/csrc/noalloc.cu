@@ -153,7 +153,7 @@ extern "C" int mfa_bin_cells_noalloc(const double* r0, int32_t n, const double* 
         ncell *= n_bin[d];
         if (ncell > MFA_NOALLOC_MAX_CELLS) return MFA_ERR_CAPACITY;
         a.nb[d] = n_bin[d];
-        a.rbin[d] = boundary[d] / (double)n_bin[d];   // make_binning_boxes.f90:188-195
+        a.rbin[d] = boundary[d] / (double)n_bin[d];   // make_binning_boxes.f90:57-64
         a.inv_rbin[d] = 1.0 / a.rbin[d];
     }
     if (ncell > MFA_NOALLOC_MAX_CELLS) return MFA_ERR_CAPACITY;

@@ -210,7 +210,7 @@ int mfa_histogram_z(mfa_ctx* c, int32_t hist_dim, int32_t reset, double* counts,
     }
     const int pd = p.n_mon * p.n_chain, pe = pd + p.n_mon_d * p.n_chain_d;
     if (pe > c->n) return MFA_ERR_ARGS;
-    // functions.f90:103-104 (z_step) and :160 (r_scaled = z * inv_z_step)
+    // functions.f90:124-125 (z_step) and :161 (r_scaled = z * inv_z_step)
     const double z_step = p.boundary[2] / (double)hist_dim;
     if (pe > 0) {
         k_obs_histo<<<blocks(pe), T, 0, c->st>>>(c->rz, pd, pe, 1.0 / z_step, hist_dim, c->hist);

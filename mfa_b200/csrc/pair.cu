@@ -407,7 +407,7 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
             if (DPD || QLJ) {
                 const R inv_r = rsqrt_(r2c);
                 if (DPD) {
-                    // dpd_forces.f90:273-348 with Philox noise keyed by the pair
+                    // dpd_forces.f90:19-94 with Philox noise keyed by the pair
                     const int ii = wi >> 8, jj = wj >> 8;
                     const uint32_t lo = (uint32_t)min(ii, jj), hi = (uint32_t)max(ii, jj);
                     const uint4 ph = philox4x32_10(make_uint4(lo, hi, (uint32_t)step, TAG_DPD), a.key);
@@ -420,7 +420,7 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
                     fsum += (sig * wr * g - gam * wd * rd) * inv_r;
                 }
                 if (QLJ) {
-                    // ewald_real.f90:411-428, inside the LJ range (reference behaviour)
+                    // ewald_real.f90:15-33, inside the LJ range (reference behaviour)
                     const R qq = vq.w * vj.w;
                     const R r = r2c * inv_r;
                     const R ec = erfc_(SQA * r);
@@ -547,7 +547,7 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
             R fx = facc[lane], fy = facc[32 + lane], fz = facc[64 + lane];
             const int ti = wi & 0xff, ii = wi >> 8;
             if (LGV) {
-                // lgv_forces.f90:377-393
+                // lgv_forces.f90:22-41
                 R g[3];
                 lgv_noise3<R>((uint32_t)ii, (uint32_t)step, a, g);
                 const double mi = a.mass[ii];

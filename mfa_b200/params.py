@@ -2,7 +2,7 @@
 
 The reference reads raw inputs (mfa_input, system_input) and derives the
 constants the hot path uses in init_params.f90:395-845, init_config.f90:217-246
-and make_binning_boxes.f90:145-195.  A Fortran shim passes those module
+and make_binning_boxes.f90:14-64.  A Fortran shim passes those module
 variables straight into ``mfa_params``; in Python, :func:`derive` plays the role
 of that init code.  Single-precision literals of the Fortran source (default
 REAL constants such as ``2.**(1./6.)``, ``0.4``, ``2.2``, ``0.98`` and
@@ -31,8 +31,8 @@ C_2_16 = float(np.float32(2.0) ** (np.float32(1.0) / np.float32(6.0)))
 C_2_2 = f32(2.2)          # init_params.f90:516
 PI_F32 = f32(3.1415926536)  # mfa_common.f90:332
 SKIN_REF = f32(0.4)       # init_params.f90:800
-BIN_SKIN = f32(0.4)       # make_binning_boxes.f90:174
-FENE_CLAMP = f32(0.98)    # intra_molec.f90:248
+BIN_SKIN = f32(0.4)       # make_binning_boxes.f90:43
+FENE_CLAMP = f32(0.98)    # intra_molec.f90:44
 
 
 @dataclass
@@ -155,7 +155,7 @@ def derive(spec: Spec) -> MfaParams:
     p.wall_cut = spec.wall_cut
     for d in range(3):
         p.va_spring_twall[d] = spec.va[d]
-    # make_binning_boxes.f90:145-177
+    # make_binning_boxes.f90:14-46
     for d in range(3):
         if spec.n_bin is None:
             p.n_bin[d] = int(spec.boundary[d] / (r_cut_max + BIN_SKIN))

@@ -169,7 +169,7 @@ static void particle_noise3(orc_state* s, int i, double g[3]) {
 static void* xcalloc(size_t n, size_t sz) { void* p = calloc(n ? n : 1, sz); return p; }
 
 static void setup_cells(orc_state* s) {
-    /* make_binning_boxes.f90:188-195 */
+    /* make_binning_boxes.f90:57-64 */
     for (int d = 0; d < 3; ++d) {
         s->nb[d] = s->p.n_bin[d];
         s->r_bin[d] = s->p.boundary[d] / (double)s->nb[d];
@@ -456,8 +456,8 @@ int orc_my_binning(orc_state* s) {
 void orc_zero_forces(orc_state* s) { memset(s->force, 0, 24 * (size_t)s->n); }
 
 /* ------------------------------------------------------------------ */
-/* fluid_fluid.f90:1-254 with dpd_forces.f90:256-352 (THERMOSTAT 0),     */
-/* lgv_forces.f90:358-396 (THERMOSTAT 1), ewald_real.f90:397-437         */
+/* fluid_fluid.f90:1-254 with dpd_forces.f90:1-98 (THERMOSTAT 0),     */
+/* lgv_forces.f90:1-44 (THERMOSTAT 1), ewald_real.f90:1-41         */
 /* ------------------------------------------------------------------ */
 void orc_fluid_fluid(orc_state* s) {
     const mfa_params* p = &s->p;
@@ -512,7 +512,7 @@ void orc_fluid_fluid(orc_state* s) {
                 s->force[3 * j + 2] += fl[2];
                 vir = vir - r_dummy * r_2_raw;
                 if (p->thermostat == MFA_THERMO_DPD) {
-                    /* dpd_forces.f90:273-348 */
+                    /* dpd_forces.f90:19-94 */
                     const double g_rand = pair_noise(s, i, j);
                     double w_d, w_r;
                     if (p->dpd_weight == 1) { w_d = 1.0; w_r = 1.0; }
@@ -535,7 +535,7 @@ void orc_fluid_fluid(orc_state* s) {
                     if (bt == 0) for (int d = 0; d < 3; ++d) s->force[3 * j + d] -= vd[d];
                 }
                 if (p->charged && real_in_lj) {
-                    /* ewald_real.f90:411-428 */
+                    /* ewald_real.f90:15-33 */
                     const double r = sqrt(r_2);
                     const double inv_r = 1.0 / r;
                     const double qq = s->q[i] * s->q[j];
@@ -574,7 +574,7 @@ void orc_fluid_fluid(orc_state* s) {
             s->force[3 * i + 2] += f_ipart[2];
         }
         if (p->thermostat == MFA_THERMO_LGV) {
-            /* lgv_forces.f90:377-393 */
+            /* lgv_forces.f90:22-41 */
             double g[3];
             particle_noise3(s, i, g);
             const double sm = sqrt(s->mass[i]);
@@ -648,7 +648,7 @@ void orc_fluid_wall(orc_state* s, int inter_type) {
     s->v_fluid_wall = vfw;
 }
 
-/* FENE term of intra_molec.f90:225-263; returns the pot_loc sum contribution */
+/* FENE term of intra_molec.f90:21-59; returns the pot_loc sum contribution */
 static double fene_bond(orc_state* s, int ip, int jp, double k, int pbc_z) {
     const mfa_params* p = &s->p;
     double dr[3];
@@ -670,7 +670,7 @@ static double fene_bond(orc_state* s, int ip, int jp, double k, int pbc_z) {
     return pot_loc;
 }
 
-/* intra_molec.f90:216-300 (grafted chains with k_chain; melt chains with k_ring) */
+/* intra_molec.f90:12-139,269-273,537 (grafted chains with k_chain; melt chains with k_ring) */
 void orc_intra_molec(orc_state* s) {
     const mfa_params* p = &s->p;
     s->fene_clamped = 0;
@@ -688,7 +688,7 @@ void orc_intra_molec(orc_state* s) {
             int ip = part_init_d + c * p->n_mon_d + m;
             vd = vd + fene_bond(s, ip, ip + 1, p->k_ring, p->symmetry == 1);
         }
-    /* intra_molec.f90:272 multiplies the melt sum by k_chain for SYSTEM != 4 */
+    /* intra_molec.f90:270 multiplies the melt sum by k_chain for SYSTEM != 4 */
     s->v_intra_molec = v_brush + p->k_chain * vd;
 }
 
@@ -1178,7 +1178,7 @@ int orc_get_kvecs(const orc_state* s, double* kv, int max_k) {
 }
 
 /* ------------------------------------------------------------------ */
-/* init_params.f90:395-845, make_binning_boxes.f90:145-195,             */
+/* init_params.f90:395-845, make_binning_boxes.f90:14-64,             */
 /* init_config.f90:228-239 derived constants                           */
 /* ------------------------------------------------------------------ */
 void orc_derive_params(const orc_inputs* in, mfa_params* o) {

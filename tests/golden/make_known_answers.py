@@ -3,7 +3,7 @@ force and energy expressions for single pairs, bonds, angles and wall
 distances, plus the rock-salt Madelung constant for the Ewald sums.
 
 These are computed here from the formulas as printed in the reference
-(fluid_fluid.f90:99-116, intra_molec.f90:248-251, bending.f90:64-96,
+(fluid_fluid.f90:99-116, intra_molec.f90:44-47, bending.f90:64-96,
 fluid_wall.f90:96-121) with Python floats, independently of the oracle, and
 serve as known-answer fixtures for it.  Run: python tests/golden/make_known_answers.py
 """

@@ -62,7 +62,7 @@ def test_my_binning_bit_exact(name, request):
 
 
 def test_binning_duplicate_cell_visits():
-    """n_bin = 2 with delta_bin = 1 (make_binning_boxes.f90:145-168): pairs in
+    """n_bin = 2 with delta_bin = 1 (make_binning_boxes.f90:14-37): pairs in
     the other cell are listed twice, as in the reference."""
     cfg = configs.melt(seed=5, n_chain=10, n_mon=8, density=0.5)
     p = cfg.params.copy()

@@ -265,7 +265,7 @@ def test_binning_and_my_binning_list_the_same_pairs(melt_cfg):
 
 
 def test_binning_small_grid_visits_cells_twice():
-    """make_binning_boxes.f90:145-168 takes delta_bin from the pre-binning n_bin;
+    """make_binning_boxes.f90:14-37 takes delta_bin from the pre-binning n_bin;
     with n_bin = 2 and delta_bin = 1 the other cell is scanned twice and pairs
     in it appear twice in the list (the reference's behaviour)."""
     spec = Spec(n_part=2, boundary=(3.2, 3.2, 3.2), n_type=1, thermostat=_abi.THERMO_NONE, skin=0.3,
@@ -315,9 +315,41 @@ def test_host_derivation_matches_oracle_derivation():
 
 
 def test_single_precision_literals():
-    # init_params.f90:502, mfa_common.f90:332, intra_molec.f90:248
+    # init_params.f90:502, mfa_common.f90:332, intra_molec.f90:44
     assert C_2_16 == 1.1224620342254639
     assert PI_F32 == 3.1415927410125732
     p = derive(Spec(n_part=1, boundary=(5.0, 5.0, 5.0)))
     assert p.fene_clamp == 0.9800000190734863
     assert p.range_2[0] == C_2_16 * C_2_16
+
+
+@pytest.mark.parametrize("r", [0.85, 1.0, 1.115])
+def test_force_switch_on_known_answer(r):
+    """fluid_fluid.f90:42-49,95-97 with init_force_switch_on.f90:15-22: inside
+    the cutoff, r^2 is replaced by max(r^2, r_2_min), r_2_min = (1 - t/t_on) *
+    (sigma_max / 0.9)^2 at time t = (s_time + i_time - 1) dt; the force keeps
+    the direction and length of the true separation (force_loc = r_dummy *
+    delta_r)."""
+    o = two_body(r)
+    p = o.params.copy()
+    p.force_switch_on = 1
+    p.r_2_min_time = 40.0
+    p.s_time = 1
+    o = Oracle(p, np.array([[5.0, 5.0, 5.0], [5.0 + r, 5.0, 5.0]]), np.zeros((2, 3)),
+               np.ones(2, dtype=np.int32), np.ones(2))
+    o.init_forces()
+    t = (p.s_time + o.scalars()["i_time"] - 1) * p.dt
+    r2_min = (1.0 - t / p.r_2_min_time) * (1.0 / float(np.float32(0.9))) ** 2
+    r2 = max(r * r, r2_min)
+    rc2 = C_2_16 ** 2
+    rd = (1.0 / rc2) ** 3
+    s6 = (1.0 / r2) ** 3
+    energy = 4.0 * ((s6 * s6 - s6) - rd * (rd - 1.0))
+    force = 4.0 * (12.0 * s6 * s6 - 6.0 * s6) / r2 * r      # on particle 2, along +x
+    s = o.scalars()
+    f = o.state()["force"]
+    assert s["v_fluid_fluid"] == pytest.approx(energy, rel=1e-12)
+    assert f[1, 0] == pytest.approx(force, rel=1e-12)
+    assert f[0, 0] == pytest.approx(-force, rel=1e-12)
+    if r * r < r2_min:
+        assert force < 4.0 * (12.0 / r ** 13 - 6.0 / r ** 7)   # softer than the true force
