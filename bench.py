@@ -54,6 +54,9 @@ def args_():
                     help="energy drift of FP64 vs mixed over --drift-steps NVE steps (not a throughput run)")
     ap.add_argument("--drift-steps", type=int, default=100000)
     ap.add_argument("--drift-equil", type=int, default=20000)
+    ap.add_argument("--dt", type=float, default=None,
+                    help="time step of the --drift runs (default: the configuration's 0.005); the DPD "
+                         "noise amplitude follows it (sig = sqrt(2 kT gamma / dt), init_params.f90:845)")
     ap.add_argument("--wall-cut", type=float, default=None,
                     help="9-3 wall cutoff of the brush workload for --drift (default: the configuration's "
                          "2.5; 0: no cutoff, the reference's uncut wall)")
@@ -147,7 +150,11 @@ def drift(a):
     import torch
     from mfa_b200 import _abi
     from mfa_b200.api import System
+    import math
     cfg, meta = make_config(a.workload, a.seed, wall_cut=a.wall_cut)
+    if a.dt is not None:
+        cfg.params.dt = a.dt
+        cfg.params.sig = math.sqrt(2.0 * cfg.params.temp * cfg.params.friction / a.dt)
     g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=_abi.FP64)
     g.init_forces()
     g.step(a.drift_equil)

@@ -73,6 +73,13 @@ __device__ __forceinline__ int cell_coord(const BinArgs& a, double x, int d, boo
     return ic;
 }
 
+// coordinate x moved by -L when binning.f90:27-29 wraps it into cell 0
+// (int(x / r_bin) = n_bin, i.e. x at the upper edge of the box)
+__device__ __forceinline__ double cell_image(const BinArgs& a, double x, int d) {
+    if (a.rule != 0) return x;
+    return (int)__dmul_rn(x, a.inv_rbin[d]) >= a.nb[d] ? __dsub_rn(x, a.L[d]) : x;
+}
+
 __device__ __forceinline__ void cell_assign_body(const BinArgs& a, Blk blk) {
     if (skip(a)) return;
     const int i = blk.id * blockDim.x + threadIdx.x;
@@ -205,8 +212,14 @@ __device__ __forceinline__ void gather_sorted_body(const BinArgs& a, Blk blk) {
         d.x = x; d.y = y; d.z = z;
         packw(d, i, ty);
         a.pos64[t] = d;
+        // the list builder's FP32 copy holds the image of the particle that
+        // lies in its cell: a coordinate equal to L (the wrap of
+        // verlet_positions.f90:243-248 keeps x <= L) is binned into cell 0 by
+        // binning.f90:27-29 and stored as x - L here.  z keeps its raw value
+        // in channels (no z image there).
         float4 f;
-        f.x = (float)x; f.y = (float)y; f.z = (float)z;
+        f.x = (float)(cell_image(a, x, 0)); f.y = (float)(cell_image(a, y, 1));
+        f.z = (float)(a.symmetry == 1 ? cell_image(a, z, 2) : z);
         packw(f, i, ty);
         a.pos32[t] = f;
     }
@@ -238,18 +251,25 @@ __device__ __forceinline__ int x_runs(const BinArgs& a, int cx, int nx, int wx, 
 }
 
 // Thread per slot: the neighbouring cells are visited as runs of consecutive
-// slots (one to three per neighbouring row).  A candidate is first tested in
-// FP32 against the list radius plus a margin far above FP32 rounding; only
-// those that pass get the reference's FP64 test, so the kept set is exactly
-// the FP64 criterion's.  Grids with fewer than 3 cells on an axis (where a
+// slots (one or two per neighbouring row).  On grids with at least 3 cells on
+// every axis (the prefilter path) a candidate is first tested in FP32 with the
+// periodic image of its run applied to the owner's position once per run (a
+// pair within the list radius lies in a neighbouring cell, so the cell
+// stencil's image is its minimum image), against the owner type's largest
+// list radius plus a margin far above FP32 rounding: about a dozen
+// instructions per candidate.  Only those that pass get the reference's FP64
+// test with the pair's own radius, so the kept set is exactly the FP64
+// criterion's.  Smaller grids (where the reference may scan a cell twice and a
 // pair's nearest image can be ambiguous in FP32) test every candidate in FP64.
 __device__ __forceinline__ void build_nbr_body(const BinArgs& a, Blk blk) {
     if (skip(a)) return;
     __shared__ double sc[T8 * T8];
-    __shared__ float scf[T8 * T8];
-    for (int k = threadIdx.x; k < T8 * T8; k += blockDim.x) {
-        sc[k] = a.cut2[k];
-        scf[k] = (float)a.cut2[k] + a.prefilter_margin;
+    __shared__ float scmax[T8];
+    for (int k = threadIdx.x; k < T8 * T8; k += blockDim.x) sc[k] = a.cut2[k];
+    if (threadIdx.x < T8) {
+        double m = 0.0;
+        for (int k = 0; k < T8; ++k) m = fmax(m, a.cut2[threadIdx.x * T8 + k]);
+        scmax[threadIdx.x] = (float)m + a.prefilter_margin;
     }
     __syncthreads();
     // the list of a 32-slot chunk (this warp) is one run of entries
@@ -264,56 +284,83 @@ __device__ __forceinline__ void build_nbr_body(const BinArgs& a, Blk blk) {
     __syncwarp();
     if (t < a.n) {
         const double4 pi = a.pos64[t];
-        const float4 pf = a.pos32[t];
         const int wi = wbits(pi.w);
-        const int ti = wi & 0xff, ii = wi >> 8;
-        const int c = a.cell_of[ii];
+        const int ti = wi & 0xff;
         const int nx = a.nb[0], ny = a.nb[1], nz = a.nb[2];
-        const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
-        int cnt = 0;
-        const int wx = a.rule == 0 ? a.dl[0] + 2 : 3;
-        const int wy = a.rule == 0 ? a.dl[1] + 2 : 3;
-        const int wz = a.rule == 0 ? a.dl[2] + 2 : 3;
-        int x0[3], x1[3];
-        const int nr = x_runs(a, cx, nx, wx, x0, x1);
-        const bool pre = a.prefilter != 0;
-        const float Lx = (float)a.L[0], Ly = (float)a.L[1], Lz = (float)a.L[2];
-        const float iLx = (float)a.invL[0], iLy = (float)a.invL[1], iLz = (float)a.invL[2];
+        // the owner's cell from its position, as cell_assign computes it
+        bool bad = false;
+        const int cx = cell_coord(a, pi.x, 0, bad), cy = cell_coord(a, pi.y, 1, bad),
+                  cz = cell_coord(a, pi.z, 2, bad);
         const int trow = (ti - 1) * T8 - 1;
-        for (int iz = 0; iz < wz; ++iz)
-        for (int iy = 0; iy < wy; ++iy) {
-            int ky, kz;
-            neighbour_row(a.rule, cy, cz, iy, iz, ny, nz, ky, kz);
-            const int rb = nx * (ky + ny * kz);
+        int cnt = 0;
+        // the reference's FP64 test of candidate slot s (binning.f90:89-104)
+        auto exact = [&](int s) {
+            const double4 pj = a.pos64[s];
+            const int tj = wbits(pj.w) & 0xff;
+            double d0 = __dsub_rn(pi.x, pj.x), d1 = __dsub_rn(pi.y, pj.y), d2 = __dsub_rn(pi.z, pj.z);
+            d0 = mimage64(d0, a.L[0], a.invL[0]);
+            d1 = mimage64(d1, a.L[1], a.invL[1]);
+            if (a.symmetry == 1) d2 = mimage64(d2, a.L[2], a.invL[2]);
+            const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
+            if (r2 < sc[trow + tj]) {
+                const int q = atomicAdd(&wcur[wib], 1);
+                if (q < capc) crow[q] = (s << 5) | lane;
+                ++cnt;
+            }
+        };
+        if (a.prefilter) {
+            // 3 x 3 x 3 stencil, nx, ny, nz >= 3: x runs [cx-1, cx+2) split where
+            // the periodic wrap breaks them, each with the owner's image shift
+            const float4 pf = a.pos32[t];
+            const float cut = scmax[ti - 1];
+            const float Lx = (float)a.L[0], Ly = (float)a.L[1], Lz = (float)a.L[2];
+            const int xa0 = cx == 0 ? nx - 1 : (cx == nx - 1 ? nx - 2 : cx - 1);
+            const int xa1 = cx == 0 ? nx : (cx == nx - 1 ? nx : cx + 2);
+            const float sxa = cx == 0 ? Lx : 0.0f;
+            const bool two = cx == 0 || cx == nx - 1;
+            const int xb1 = cx == 0 ? 2 : 1;
+            const float sxb = cx == 0 ? 0.0f : -Lx;
+            for (int iz = 0; iz < 3; ++iz)
+            for (int iy = 0; iy < 3; ++iy) {
+                int ky, kz;
+                neighbour_row(a.rule, cy, cz, iy, iz, ny, nz, ky, kz);
+                const int uy = cy - 1 + iy, uz = cz - 1 + iz;
+                const float oy = pf.y + (uy < 0 ? Ly : (uy >= ny ? -Ly : 0.0f));
+                const float oz = a.symmetry == 1 ? pf.z + (uz < 0 ? Lz : (uz >= nz ? -Lz : 0.0f)) : pf.z;
+                const int rb = nx * (ky + ny * kz);
 #pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                if (r >= nr) break;
-                int s0 = a.cell_start[rb + x0[r]];
-                const int s1 = a.cell_start[rb + x1[r]];
-                // half list: only partners at higher slots (the lower slot owns the pair)
-                if (a.rule == 0 && s0 <= t) s0 = t + 1;
-                for (int s = s0; s < s1; ++s) {
-                    if (s == t) continue;
-                    const float4 qf = a.pos32[s];
-                    const int tj = wbits(qf.w) & 0xff;
-                    if (pre) {
-                        float e0 = pf.x - qf.x, e1 = pf.y - qf.y, e2 = pf.z - qf.z;
-                        e0 = fmaf(-Lx, truncf(2.0f * e0 * iLx), e0);
-                        e1 = fmaf(-Ly, truncf(2.0f * e1 * iLy), e1);
-                        if (a.symmetry == 1) e2 = fmaf(-Lz, truncf(2.0f * e2 * iLz), e2);
-                        if (!(e0 * e0 + e1 * e1 + e2 * e2 < scf[trow + tj])) continue;
+                for (int r = 0; r < 2; ++r) {
+                    if (r == 1 && !two) break;
+                    int s0 = a.cell_start[rb + (r == 0 ? xa0 : 0)];
+                    const int s1 = a.cell_start[rb + (r == 0 ? xa1 : xb1)];
+                    const float ox = pf.x + (r == 0 ? sxa : sxb);
+                    // half list: only partners at higher slots (the lower slot owns the pair)
+                    if (a.rule == 0 && s0 <= t) s0 = t + 1;
+                    for (int s = s0; s < s1; ++s) {
+                        const float4 q = a.pos32[s];
+                        const float dx = ox - q.x, dy = oy - q.y, dz = oz - q.z;
+                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                        if (r2 < cut && s != t) exact(s);
                     }
-                    const double4 pj = a.pos64[s];
-                    double d0 = __dsub_rn(pi.x, pj.x), d1 = __dsub_rn(pi.y, pj.y), d2 = __dsub_rn(pi.z, pj.z);
-                    d0 = mimage64(d0, a.L[0], a.invL[0]);
-                    d1 = mimage64(d1, a.L[1], a.invL[1]);
-                    if (a.symmetry == 1) d2 = mimage64(d2, a.L[2], a.invL[2]);
-                    const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
-                    if (r2 < sc[trow + tj]) {
-                        const int q = atomicAdd(&wcur[wib], 1);
-                        if (q < capc) crow[q] = (s << 5) | lane;
-                        ++cnt;
-                    }
+                }
+            }
+        } else {
+            const int wx = a.rule == 0 ? a.dl[0] + 2 : 3;
+            const int wy = a.rule == 0 ? a.dl[1] + 2 : 3;
+            const int wz = a.rule == 0 ? a.dl[2] + 2 : 3;
+            int x0[3], x1[3];
+            const int nr = x_runs(a, cx, nx, wx, x0, x1);
+            for (int iz = 0; iz < wz; ++iz)
+            for (int iy = 0; iy < wy; ++iy) {
+                int ky, kz;
+                neighbour_row(a.rule, cy, cz, iy, iz, ny, nz, ky, kz);
+                const int rb = nx * (ky + ny * kz);
+                for (int r = 0; r < nr; ++r) {
+                    int s0 = a.cell_start[rb + x0[r]];
+                    const int s1 = a.cell_start[rb + x1[r]];
+                    if (a.rule == 0 && s0 <= t) s0 = t + 1;
+                    for (int s = s0; s < s1; ++s)
+                        if (s != t) exact(s);
                 }
             }
         }

@@ -12,17 +12,21 @@ SOLVENT 1, PARTICLE_4, BIN_TYPE 0, Langevin thermostat, dt = 2e-4,
             (verlet_velocities.f90:219-223, format i7,3g17.5), with
             V = v_wall_wall + v_fluid_wall + v_fluid_fluid + v_intra_molec
             (:187) and N = n_mon_tot = 102 (init_params.f90:478-480);
+  fort.41   every 5th observed step: i_time, v_fluid_fluid, v_intra_molec,
+            v_fluid_wall (observation.f90:304-307, format i7,3f15.5);
   mfa_output the inputs the run was made with (box, epsilon table, FENE
             constants, time step; the header of mfa_input echoed).
 
 The potential energy of a configuration does not depend on the thermostat's
 noise, so the oracle's v_fluid_fluid + v_intra_molec at conf_new's positions
-must equal fort.60's V/N of step 10000 to its five printed digits, and
-0.5 sum m v^2 / N of conf_new's velocities its KE/N.
+must equal fort.60's V/N of step 10000 to its five printed digits and each
+of fort.41's two terms at that step to the precision the 7-decimal positions
+of conf_new allow, and 0.5 sum m v^2 / N of conf_new's velocities fort.60's
+KE/N.
 
 This script copies conf_new as it is (tests/golden/reference_conf_new) and
-writes the fort.60 rows around step 10000 and the run's inputs, read from
-mfa_output and system_input, to tests/golden/reference_system4.json.
+writes the fort.60 and fort.41 rows around step 10000 and the run's inputs,
+read from mfa_output and system_input, to tests/golden/reference_system4.json.
 Run: python tests/golden/make_reference_system4.py [reference dir]
 """
 import json
@@ -41,6 +45,12 @@ def main(ref):
         if len(f) == 4 and 9950 <= int(f[0]) <= 10010:
             rows[f[0]] = {"v_per_n": float(f[1]), "e_per_n": float(f[2]), "t_per_n": float(f[3]),
                           "text": ln.rstrip("\n")}
+    terms = {}
+    for ln in open(os.path.join(ref, "fort.41")):
+        f = ln.split()
+        if len(f) == 4 and 9950 <= int(f[0]) <= 10010:
+            terms[f[0]] = {"v_fluid_fluid": float(f[1]), "v_intra_molec": float(f[2]),
+                           "v_fluid_wall": float(f[3]), "text": ln.rstrip("\n")}
     out = [ln.rstrip("\n") for ln in open(os.path.join(ref, "mfa_output"))]
 
     def value(label):
@@ -85,6 +95,7 @@ def main(ref):
         "k_elastic": value("Force constant of the external elastic field"),
         "conf_step": 10000,
         "fort60": rows,
+        "fort41": terms,
     }
     with open(os.path.join(HERE, "reference_system4.json"), "w") as fh:
         json.dump(fixture, fh, indent=1)

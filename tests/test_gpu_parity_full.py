@@ -167,3 +167,36 @@ def test_force_switch_on_clamps_pairs_fp64_and_mixed(melt_cfg):
     assert g.scalars()["e_total"] == pytest.approx(o.scalars()["e_total"], rel=1e-10)
     g.close()
     gm.close()
+
+
+@pytest.mark.parametrize("rule", [0, 1])
+def test_lists_bit_exact_with_particles_on_the_box_edge(melt_cfg, rule):
+    """verlet_positions.f90:243-248 keeps coordinates in [0, L], so a coordinate
+    can equal L exactly; binning.f90:27-29 then puts the particle in cell 0.
+    Particles moved onto x = L, y = L and x = 0 keep bit-exact lists (the
+    list builder's stencil images follow the cell the particle was binned in).
+    my_binning (rule 1) rejects a coordinate of L as outside its grid, as its
+    int(x / r_bin) indexing would overrun the reference's arrays."""
+    cfg = melt_cfg
+    r0 = cfg.r0.copy()
+    L = [cfg.params.boundary[d] for d in range(3)]
+    r0[0:200:7, 0] = L[0]
+    r0[1:200:7, 1] = L[1]
+    r0[2:200:7, 0] = 0.0
+    o = Oracle(cfg.params, r0, cfg.v, cfg.a_type, cfg.mass, list_cap=512)
+    g = System(cfg.params, r0, cfg.v, cfg.a_type, cfg.mass, precision=MIXED)
+    if rule == 1:
+        with pytest.raises(_abi.MfaError):
+            g.my_binning()
+        g.close()
+        return
+    o.binning()
+    g.binning()
+    cell_o, _, ff = o.lists()
+    cell_g, cnt, nbr = g.debug_lists(512)
+    g.close()
+    assert (cell_o == cell_g).all()
+    assert (cell_o[0:200:7] % cfg.params.n_bin[0] == 0).all()
+    ref = pair_multiset_half(ff)
+    got = pair_multiset_rows(cnt, nbr)
+    assert ref.shape == got.shape and (ref == got).all()

@@ -1,20 +1,22 @@
 """The oracle pinned to numbers the reference itself produced.
 
-The reference ships the restart file (conf_new) and the energy log (fort.60)
-of one of its own runs: SYSTEM 4 of control_simulation.h, one chain of 102
+The reference ships the restart file (conf_new) and the energy logs (fort.60,
+fort.41) of one of its own runs: SYSTEM 4 of control_simulation.h, one chain of 102
 beads in a periodic 70 x 90 x 90 box, WCA (SOLVENT 1) and FENE (k = 30,
 R0 = 1.5), written at step 10000.  tests/golden/make_reference_system4.py
 copied them here.  fort.60 prints V/N, (V + KE)/N and KE/N at that step
 (verlet_velocities.f90:223) with five significant digits, V = v_fluid_fluid +
 v_intra_molec (:187; no walls in a bulk box, bending and the external field are
-not part of it).  The potential energy does not depend on the Langevin noise
-of the run, so the oracle evaluated on conf_new's positions must reproduce the
-printed V/N, and conf_new's velocities the printed KE/N.
+not part of it); fort.41 prints v_fluid_fluid and v_intra_molec themselves
+with five decimals (observation.f90:304-307).  The potential energy does not
+depend on the Langevin noise of the run, so the oracle evaluated on conf_new's
+positions must reproduce each printed term and V/N, and conf_new's
+velocities the printed KE/N.
 
 conf_new keeps 7 decimals of each coordinate; the tolerance is half a unit of
 the last printed digit plus the largest change those rounded digits can make
-to V/N (sum of |dV/dx| over all coordinates times 5e-8, with the oracle's
-forces).  The CUDA path is then compared with the oracle on the same
+to the term (sum of |dV/dx| over all coordinates times 5e-8, with the oracle's
+force of that term alone).  The CUDA path is then compared with the oracle on the same
 configuration (FP64 to 1e-12, mixed to 1e-5) and with fort.60 directly.
 """
 import json
@@ -31,6 +33,7 @@ from mfa_b200.params import Spec, derive
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 FIX = json.load(open(os.path.join(GOLDEN, "reference_system4.json")))
 ROW = FIX["fort60"][str(FIX["conf_step"])]
+TERMS = FIX["fort41"][str(FIX["conf_step"])]
 N = FIX["n_part"]
 
 
@@ -66,6 +69,20 @@ def rounding_bound(force):
     return float(np.abs(force).sum()) * 5e-8 / N
 
 
+def term_forces():
+    """The oracle's force of fluid_fluid alone and of intra_molec alone."""
+    from oracle import Oracle
+    st = reference_state()
+    o = Oracle(reference_params(), st["r0"], st["v"], st["a_type"], np.ones(N))
+    o.binning()
+    out = {}
+    for name, call in (("v_fluid_fluid", o.fluid_fluid), ("v_intra_molec", o.intra_molec)):
+        o.zero_forces()
+        call()
+        out[name] = o.state()["force"]
+    return out
+
+
 def test_read_conf_parses_the_reference_restart_file():
     st = reference_state()
     assert (st["n_mon"], st["n_chain"], st["n_mon_d"], st["n_chain_d"]) == (102, 1, 11, 0)
@@ -93,6 +110,18 @@ def test_oracle_potential_energy_matches_the_reference_log():
     o = Oracle(reference_params(), st["r0"], st["v"], st["a_type"], np.ones(N))
     o.init_forces()
     assert abs(o.check_fluid_fluid() - s["v_fluid_fluid"]) <= 1e-12 * abs(s["v_fluid_fluid"])
+
+
+def test_oracle_energy_terms_match_the_reference_observation_log():
+    """Each term on its own, to its 5 printed decimals plus the rounding of
+    conf_new's positions (about 3e-6 of the LJ term)."""
+    s, _, _ = oracle_energies()
+    forces = term_forces()
+    for k in ("v_fluid_fluid", "v_intra_molec"):
+        tol = 5e-6 + float(np.abs(forces[k]).sum()) * 5e-8
+        assert tol < 1e-5 * abs(TERMS[k])
+        assert abs(s[k] - TERMS[k]) <= tol, (k, s[k], TERMS["text"], tol)
+    assert TERMS["v_fluid_wall"] == 0.0
 
 
 def test_kinetic_energy_of_the_restart_velocities_matches_the_reference_log():
@@ -132,3 +161,7 @@ def test_gpu_energies_on_the_reference_configuration(prec):
     assert float(np.abs(f - f_o).max()) <= tol * float(np.abs(f_o).max())
     v_per_n = (s["v_fluid_fluid"] + s["v_intra_molec"]) / N
     assert abs(v_per_n - ROW["v_per_n"]) <= 0.05 + rounding_bound(f_o), (v_per_n, ROW["text"])
+    if prec == _abi.FP64:
+        forces = term_forces()
+        for k in ("v_fluid_fluid", "v_intra_molec"):
+            assert abs(s[k] - TERMS[k]) <= 5e-6 + float(np.abs(forces[k]).sum()) * 5e-8, (k, s[k])
