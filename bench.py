@@ -135,6 +135,19 @@ def loop_kernel_times(g, steps, chunk):
     return {k: {"launches": n, "mean_us": t / max(n, 1), "total_us": t} for k, (n, t) in agg.items()}
 
 
+def short_name(k):
+    """A kernel's name without return type, namespace and argument list."""
+    k = k.replace("void ", "").replace("(anonymous namespace)::", "")
+    depth, out = 0, []
+    for ch in k:
+        if ch == "(" and depth == 0:
+            break
+        depth += ch == "<"
+        depth -= ch == ">"
+        out.append(ch)
+    return "".join(out)[:60]
+
+
 def kernel_stat(kt, key):
     """Launch count and mean time of the kernels whose name contains `key`."""
     n = sum(v["launches"] for k, v in kt.items() if key in k)
@@ -807,7 +820,7 @@ def main():
                  "frac": 124 * n / (vv_us * 1e-6) / 1e9 / hbm_peak,
                  "source": "CUPTI activity records over 200 in-loop steps (L2 warm)"}
     loop_total = sum(v["total_us"] for v in loop_kt.values())
-    loop_share = {k.split("(")[0].replace("void ", "")[:60]: round(v["total_us"] / loop_total, 4)
+    loop_share = {short_name(k): round(v["total_us"] / loop_total, 4)
                   for k, v in sorted(loop_kt.items(), key=lambda kv: -kv[1]["total_us"])[:8]} if loop_total else {}
     g.close()
 

@@ -376,10 +376,12 @@ int mfa_batch_destroy(mfa_batch* batch);
 
 /* No counterpart in the reference.  The observable of a run of nsteps time
  * steps from the current state, J = 1/S sum_{s=1..S} [<z>(s) + <R_ee^2>(s)]
- * (<z>: mean height of all beads; <R_ee^2>: mean squared end-to-end distance
- * of the grafted/bulk chains, unwrapped through mic_count), advancing the
- * state by nsteps along the subroutine-level step (verlet_positions, binning
- * when due, fluid_fluid + fluid_wall, intra_molec, verlet_velocities). */
+ * (<z>: mean height of all beads, unfolded through mic_count in a bulk box;
+ * <R_ee^2>: mean squared end-to-end distance of the grafted/bulk chains,
+ * unwrapped through mic_count), advancing the state by nsteps along the
+ * subroutine-level step (verlet_positions, binning when due, fluid_fluid +
+ * fluid_wall, intra_molec, bending, ewald_k(1) + dipolar_correction,
+ * verlet_velocities). */
 int mfa_trajectory_observable(mfa_ctx* ctx, int32_t nsteps, double* J);
 /* The same run, differentiated: out[0] = J, out[1..6] = dJ/d(eps_LJ, sigma,
  * k_FENE, R0, gamma_DPD, eps_wall) by the discrete adjoint of the
@@ -391,9 +393,13 @@ int mfa_trajectory_observable(mfa_ctx* ctx, int32_t nsteps, double* J);
  * friction and sig = sqrt(2 kT gamma / dt); eps_wall as every type's a_wall.
  * The run starts from the context's state (r, v and a = F/m as they are) and
  * that state is held fixed: the gradient is that of the trajectory from it.
- * Systems with Ewald, Langevin, the force switch-on, WALL 3/4, melt chains or
- * DPD_VV return MFA_ERR_UNSUPPORTED (bending is differentiated; k_bend is not
- * one of the parameters).  The state advances by nsteps. */
+ * Every force term of the step is differentiated: LJ/WCA, DPD or Langevin
+ * (gamma_DPD is then the Langevin friction, with its noise amplitude), Ewald
+ * real space (either form), k-space and the slab correction (charged systems
+ * need ewald_k(0) first, else MFA_ERR_STATE), FENE, bending and the 9-3 walls;
+ * the Ewald parameters and k_bend are not among the parameters.  Systems with
+ * the force switch-on, WALL 3/4, melt chains or DPD_VV return
+ * MFA_ERR_UNSUPPORTED.  The state advances by nsteps. */
 int mfa_adjoint(mfa_ctx* ctx, int32_t nsteps, int32_t every, double* out7);
 
 /* ---------------- binning without device allocation ---------------- */

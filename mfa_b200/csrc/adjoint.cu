@@ -6,7 +6,7 @@
 //   r' = r + dt v + dt^2/2 a          u = v + dt/2 a         (half-step velocity)
 //   F' = F(r', u; theta, noise of step n+1)                  (DPD uses u)
 //   a' = F'/m                          v' = u + dt/2 a'       (pinned heads: v' = a' = 0)
-// Observable J = 1/S sum_{s=1..S} O(r_s), O = <z> (all beads) + <R_ee^2> (chains).
+// Observable J = 1/S sum_{s=1..S} O(r_s), O = <z> (all beads, z unfolded) + <R_ee^2> (chains).
 // Backward step n+1 -> n, with rho, nu, alpha the adjoints of r, v, a:
 //   lam_F = (alpha' + dt/2 nu') / m,  lam_u = nu'            (heads: 0)
 //   lam_r = rho' + (dF/dr')^T lam_F,  lam_u += (dF/du)^T lam_F,  g += (dF/dtheta)^T lam_F
@@ -46,11 +46,16 @@ struct AdjArgs {
     double *rx, *ry, *rz;         // lam_r accumulators
     double *ux, *uy, *uz;         // lam_u accumulators
     double* g;                    // G_N parameter gradient sums
+    const double* mass;           // particle order (Langevin)
     int n, maxnb, half, symmetry, dpd, dpd_weight, noise, wall;
+    int lgv;                      // Langevin thermostat (lgv_forces.f90)
+    int charged, real_in_lj;      // Ewald real space: inside the LJ range, or to its own cutoff
     double L[3], invL[3];
     double sig, gam, eps_lj, sigma_lj;
+    double sqrt_alpha, alpha_c, inv_sqrt_pi, ewald_rc_2;
     long long step;
     PhiloxKeys key;
+    uint32_t seed0, seed1;
     double a_wall[T8], sigma_wall[T8], z_space_wall, wall_cut;
 };
 
@@ -128,20 +133,43 @@ __global__ void k_adj_pair(AdjArgs a) {
             if (a.symmetry == 1) dz = mi(dz, Lz, iLz);
             const R r2 = dx * dx + dy * dy + dz * dz;
             const int wj = wbits(pj.w), jj = wj >> 8, ij = (ti - 1) * T8 + (wj & 0xff) - 1;
-            if (!(r2 < (R)s_rc2[ij])) continue;
+            const bool in_lj = r2 < (R)s_rc2[ij];
+            // Ewald real space (ewald_real.f90:15-33): inside the LJ range in the
+            // reference's form (fluid_fluid.f90:94,166), else to its own cutoff
+            const bool in_q = a.charged && (a.real_in_lj ? in_lj : r2 < (R)a.ewald_rc_2);
+            if (!in_lj && !in_q) continue;
             // the pair force G acts on i (+G) and, with the half list, on j (-G):
             // dl = lam_F_i - lam_F_j (half list) or lam_F_i (full list: j has its own row)
             R dlx = (R)a.fx[ii], dly = (R)a.fy[ii], dlz = (R)a.fz[ii];
             if (a.half) { dlx -= (R)a.fx[jj]; dly -= (R)a.fy[jj]; dlz -= (R)a.fz[jj]; }
             const R ddl = dx * dlx + dy * dly + dz * dlz;
+            R gx = 0, gy = 0, gz = 0;
+            if (in_q) {
+                // G = h(r) d, h = qq (2 s c exp(-a r^2) / r^2 + erfc(s r) / r^3), s = sqrt(a),
+                // c the code's 1/sqrt(pi) constant; (dG/dd)^T dl = h dl + (h'(r) / r) (d . dl) d,
+                // with d erfc(s r)/dr = -(2/sqrt(pi)) s exp(-a r^2) (the function's own derivative)
+                const R4 ui = vs[t], uj = vs[s];
+                const R qq = ui.w * uj.w;
+                const R ir = rsq(r2), r = r2 * ir, ir2 = ir * ir, ir3 = ir2 * ir;
+                const R SQA = (R)a.sqrt_alpha, ALC = (R)a.alpha_c, ISP = (R)a.inv_sqrt_pi;
+                const R ex = exp(-ALC * r2), ec = erfc(SQA * r);
+                const R h = qq * ((R)2 * SQA * ISP * ex * ir2 + ec * ir3);
+                const R dh = qq * ((R)2 * SQA * ISP * ex * ((R)-2 * ALC * ir - (R)2 * ir3) -
+                                   (R)1.1283791670955126 * SQA * ex * ir3 - (R)3 * ec * ir3 * ir);
+                const R c = dh * ir * ddl;
+                gx += h * dlx + c * dx;
+                gy += h * dly + c * dy;
+                gz += h * dlz + c * dz;
+            }
+            if (in_lj) {
             // LJ: G = fs(r2) d, fs = eps (12 r12 - 6 r6) / r2
             const R eps = (R)s_eps[ij], ir2 = (R)1 / r2;
             const R r61 = (R)s_sig2[ij] * ir2, r6 = r61 * r61 * r61, r12 = r6 * r6;
             const R fs = eps * ((R)12 * r12 - (R)6 * r6) * ir2;
             const R dfs = eps * ((R)-84 * r12 + (R)24 * r6) * ir2 * ir2;   // d fs / d r2
-            R gx = fs * dlx + (R)2 * dfs * ddl * dx;
-            R gy = fs * dly + (R)2 * dfs * ddl * dy;
-            R gz = fs * dlz + (R)2 * dfs * ddl * dz;
+            gx += fs * dlx + (R)2 * dfs * ddl * dx;
+            gy += fs * dly + (R)2 * dfs * ddl * dy;
+            gz += fs * dlz + (R)2 * dfs * ddl * dz;
             gl[G_EPS] += (double)(fs * ddl) / a.eps_lj;
             gl[G_SIG] += (double)(eps * ((R)144 * r12 - (R)36 * r6) * ir2 * ddl) / a.sigma_lj;
             if (a.dpd) {
@@ -182,6 +210,7 @@ __global__ void k_adj_pair(AdjArgs a) {
                     gl[G_SIG] += (double)((sg * dws * gn - gm * (R)2 * wr * dws * sdu) * hdl);
                 }
             }
+            }
             // G depends on d = r_i - r_j: both positions, whichever side it acts on
             atomicAdd(&a.rx[ii], (double)gx);
             atomicAdd(&a.ry[ii], (double)gy);
@@ -212,6 +241,25 @@ __global__ void k_adj_pair(AdjArgs a) {
             }
             atomicAdd(&a.rz[ii], (double)(dfz * lfz));
             if (aw != (R)0) gl[G_WALL] += (double)(phi * lfz);
+        }
+        if (a.lgv && t < a.n) {
+            // Langevin (lgv_forces.f90:22-41): F += sig g sqrt(m) - gamma m u, the
+            // variates replayed (same Philox key as the pair kernel's)
+            const R4 pi = ps[t];
+            const int ii = wbits(pi.w) >> 8;
+            const R4 ui = vs[t];
+            const double m = a.mass[ii];
+            const double lx = a.fx[ii], ly = a.fy[ii], lz = a.fz[ii];
+            R g3[3];
+            lgv_noise3<R>((uint32_t)ii, (uint32_t)a.step, a.noise, a.seed0, a.seed1, g3);
+            const double cu = -a.gam * m;
+            atomicAdd(&a.ux[ii], cu * lx);
+            atomicAdd(&a.uy[ii], cu * ly);
+            atomicAdd(&a.uz[ii], cu * lz);
+            // d/d gamma: the friction and the amplitude sqrt(2 kT gamma / dt)
+            const double gdl = (double)g3[0] * lx + (double)g3[1] * ly + (double)g3[2] * lz;
+            const double udl = (double)ui.x * lx + (double)ui.y * ly + (double)ui.z * lz;
+            gl[G_GAM] += 0.5 * a.sig / a.gam * sqrt(m) * gdl - m * udl;
         }
     }
     warp_add_g(a.g, gl);
@@ -398,7 +446,9 @@ __global__ void k_observable(int n, const double* __restrict__ rx, const double*
                              double Lz, int n_chain, int n_mon, double w, double* out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double v = 0.0;
-    if (i < n) v += rz[i] / (double)n;
+    // z unfolded by the image counter (continuous across the periodic wrap of
+    // a bulk box; in channels z is never wrapped and the counter stays 0)
+    if (i < n) v += (rz[i] + Lz * mz[i]) / (double)n;
     if (i < n_chain && n_mon > 1) {
         const int f = i * n_mon, e = f + n_mon - 1;
         const double X = (rx[e] + Lx * mx[e]) - (rx[f] + Lx * mx[f]);
@@ -434,6 +484,10 @@ int adj_forward_step(mfa_ctx* c, double* sr, double* su, int32_t* sm, double w, 
     }
     TRY_(launch_rebuild(c, c->bin_type, 1));
     TRY_(launch_pair(c, c->p.symmetry == 0));
+    if (c->p.charged) {
+        TRY_(launch_ewald(c));      // md_main.f90:128-131
+        TRY_(launch_dipolar(c));    // SYMMETRY 0 only
+    }
     TRY_(launch_vv_velocities(c, 1));
     if (dJ) {
         const mfa_params& p = c->p;
@@ -482,6 +536,14 @@ AdjArgs pair_adj_args(mfa_ctx* c, Work& w, long long step) {
     a.half = c->bin_type == 0;
     a.symmetry = p.symmetry;
     a.dpd = p.thermostat == MFA_THERMO_DPD;
+    a.lgv = p.thermostat == MFA_THERMO_LGV;
+    a.mass = c->mass;
+    a.charged = p.charged;
+    a.real_in_lj = (p.quirks & MFA_Q_EWALD_REAL_IN_LJ) != 0;
+    a.sqrt_alpha = p.sqrt_alpha; a.alpha_c = p.alpha_c; a.inv_sqrt_pi = p.inv_sqrt_pi;
+    a.ewald_rc_2 = p.ewald_rc_2;
+    a.seed0 = (uint32_t)p.seed;
+    a.seed1 = (uint32_t)(p.seed >> 32);
     a.dpd_weight = p.dpd_weight;
     a.noise = p.noise;
     a.wall = (p.symmetry == 0 && p.wall == 2) ? 2 : 0;
@@ -525,10 +587,13 @@ int mfa_trajectory_observable(mfa_ctx* c, int32_t nsteps, double* J) {
 int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
     if (!c || nsteps < 1 || every < 1 || !out) return MFA_ERR_ARGS;
     const mfa_params& p = c->p;
-    // the force terms differentiated here: pair (LJ/WCA, DPD), FENE, 9-3 walls
-    if (p.charged || p.thermostat == MFA_THERMO_LGV || p.force_switch_on || c->dpd_vv ||
-        (p.symmetry == 0 && (p.wall == 3 || p.wall == 4)) || (p.n_chain_d > 0 && p.n_mon_d >= 2))
+    // the force terms differentiated here: pair (LJ/WCA, DPD, Ewald real
+    // space), Langevin, FENE, bending, 9-3 walls, Ewald k-space and the slab
+    // correction
+    if (p.force_switch_on || c->dpd_vv || (p.symmetry == 0 && (p.wall == 3 || p.wall == 4)) ||
+        (p.n_chain_d > 0 && p.n_mon_d >= 2))
         return MFA_ERR_UNSUPPORTED;
+    if (p.charged && c->nk == 0) return MFA_ERR_STATE;   // ewald_k(0) first
     if (!c->lists_valid) TRY_(mfa_binning(c));
     const int n = c->n;
     const size_t n3 = (size_t)3 * n;
@@ -539,10 +604,11 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
     w.ckstep = steps.data();
     void* bufs[9] = {nullptr};
     size_t sizes[9] = {(size_t)w.nseg * 3 * n3 * 8, (size_t)w.nseg * n3 * 4, (size_t)w.K * n3 * 8,
-                       (size_t)w.K * n3 * 8, (size_t)w.K * n3 * 4, 6 * n3 * 8, (G_N + 1) * 8, 0, 0};
+                       (size_t)w.K * n3 * 8, (size_t)w.K * n3 * 4, 6 * n3 * 8, (G_N + 1) * 8,
+                       p.charged ? ewald_adj_bytes(c) : 0, 0};
     int rc = MFA_OK;
-    for (int k = 0; k < 7 && rc == MFA_OK; ++k)
-        if (cudaMalloc(&bufs[k], sizes[k]) != cudaSuccess) rc = MFA_ERR_NOMEM;
+    for (int k = 0; k < 8 && rc == MFA_OK; ++k)
+        if (sizes[k] && cudaMalloc(&bufs[k], sizes[k]) != cudaSuccess) rc = MFA_ERR_NOMEM;
     if (rc != MFA_OK) {
         for (void* b : bufs) if (b) cudaFree(b);
         return rc;
@@ -634,6 +700,8 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
                     const int nang = p.n_chain * (p.n_mon - 2);
                     k_adj_bend<<<(nang + T - 1) / T, T, 0, c->st>>>(ka);
                 }
+                // Ewald k-space (and the slab correction) at r', c->rx holding r'
+                if (p.charged) TRY_(launch_ewald_adjoint(c, w.lamF, w.lamR, bufs[7]));
                 // back to the state before step s+1: the observable at r_s (s >= 1)
                 const double* r0 = s > s0 ? w.seg_r + (s - s0 - 1) * n3 : nullptr;
                 const int32_t* m0 = s > s0 ? w.seg_m + (s - s0 - 1) * n3 : nullptr;

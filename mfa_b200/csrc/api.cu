@@ -77,15 +77,30 @@ void invalidate_graph(mfa_ctx* c) {
     for (int k = 0; k < N_CALL_GRAPHS; ++k) c->call_n[k] = 0;
 }
 
+// r0(3,n) <-> three contiguous arrays (x[0..n), y[n..2n), z[2n..3n))
+__global__ void k_interleave3(const double* __restrict__ soa, double* __restrict__ aos, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    aos[3 * (size_t)i] = soa[i];
+    aos[3 * (size_t)i + 1] = soa[(size_t)n + i];
+    aos[3 * (size_t)i + 2] = soa[2 * (size_t)n + i];
+}
+__global__ void k_deinterleave3(const double* __restrict__ aos, double* __restrict__ soa, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    soa[i] = aos[3 * (size_t)i];
+    soa[(size_t)n + i] = aos[3 * (size_t)i + 1];
+    soa[2 * (size_t)n + i] = aos[3 * (size_t)i + 2];
+}
+
 void free_all(mfa_ctx* c) {
     invalidate_graph(c);
     void* ptrs[] = {c->rx, c->mx, c->type, c->mass, c->force, c->pos_s, c->vel_s, c->pos64, c->pos32,
                     c->ids, c->cell_count, c->nbr, c->nnb, c->partials, c->counters, c->dscal,
                     c->dstep, c->kvec, c->rho, c->rho_part, c->elog, c->elog_n, c->tabs,
-                    c->obs_buf, c->hist, c->fd, c->term_buf};
+                    c->obs_buf, c->hist, c->fd, c->term_buf, c->d_stage};
     for (void* p : ptrs)
         if (p) cudaFree(p);
-    if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->h_scal) cudaFreeHost(c->h_scal);
     if (c->st) cudaStreamDestroy(c->st);
     if (c->st_body) cudaStreamDestroy(c->st_body);
@@ -439,8 +454,7 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
     if (rc == MFA_OK) c->dflags = (int32_t*)(c->dscal + S_NSLOT);
     A(dalloc(&c->dstep, 2));
     A(dalloc(&c->tabs, 6 * T8 * T8));
-    if (rc == MFA_OK && cudaMallocHost((void**)&c->h_stage, (size_t)3 * n * sizeof(double)) != cudaSuccess)
-        rc = MFA_ERR_NOMEM;
+    A(dalloc(&c->d_stage, (size_t)3 * n));
     if (rc == MFA_OK && cudaMallocHost((void**)&c->h_scal, (S_NSLOT + F_NFLAG / 2) * sizeof(double)) != cudaSuccess)
         rc = MFA_ERR_NOMEM;
     if (rc != MFA_OK) { free_all(c); free(c); return rc; }
@@ -827,20 +841,19 @@ int mfa_sync(mfa_ctx* c) {
 int mfa_download(mfa_ctx* c, uint32_t mask, double* r0, double* v, double* a, double* force, int32_t* mic) {
     if (!c) return MFA_ERR_ARGS;
     const int n = c->n;
-    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
-    // x, y, z of one quantity are contiguous on the device: one copy through
-    // the pinned staging buffer, then the interleave into the r0(3,n) layout
-    double* buf = c->h_stage;
+    // x, y, z of one quantity are contiguous on the device: interleaved into the
+    // r0(3,n) layout by a kernel, then one copy per quantity (stream-ordered:
+    // the next interleave waits for the previous copy), one synchronisation
     auto get3 = [&](double* dst, const double* x) -> int {
-        MFA_CUDA_TRY(cudaMemcpyAsync(buf, x, (size_t)3 * n * 8, cudaMemcpyDeviceToHost, c->st));
-        MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
-        for (int i = 0; i < n; ++i)
-            for (int d = 0; d < 3; ++d) dst[3 * i + d] = buf[(size_t)d * n + i];
+        k_interleave3<<<(n + 255) / 256, 256, 0, c->st>>>(x, c->d_stage, n);
+        MFA_CUDA_TRY(cudaGetLastError());
+        MFA_CUDA_TRY(cudaMemcpyAsync(dst, c->d_stage, (size_t)3 * n * 8, cudaMemcpyDeviceToHost, c->st));
         return MFA_OK;
     };
     if ((mask & MFA_R0) && r0) TRY(get3(r0, c->rx));
     if ((mask & MFA_V) && v) TRY(get3(v, c->vx));
     if ((mask & MFA_A) && a) TRY(get3(a, c->ax));
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
     if ((mask & MFA_F) && force) {
         if (c->prec == MFA_MIXED) {
             std::vector<float> f4((size_t)4 * n);
@@ -867,18 +880,19 @@ int mfa_upload(mfa_ctx* c, uint32_t mask, const double* r0, const double* v, con
                const double* force, const int32_t* mic) {
     if (!c) return MFA_ERR_ARGS;
     const int n = c->n;
-    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
-    double* buf = c->h_stage;
+    // the r0(3,n) layout copied as it is, de-interleaved on the device; the
+    // copies and kernels are stream-ordered, and the call returns once they
+    // are done (the caller may reuse its buffers)
     auto put3 = [&](const double* src, double* x) -> int {
-        for (int i = 0; i < n; ++i)
-            for (int d = 0; d < 3; ++d) buf[(size_t)d * n + i] = src[3 * i + d];
-        MFA_CUDA_TRY(cudaMemcpyAsync(x, buf, (size_t)3 * n * 8, cudaMemcpyHostToDevice, c->st));
-        MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+        MFA_CUDA_TRY(cudaMemcpyAsync(c->d_stage, src, (size_t)3 * n * 8, cudaMemcpyHostToDevice, c->st));
+        k_deinterleave3<<<(n + 255) / 256, 256, 0, c->st>>>(c->d_stage, x, n);
+        MFA_CUDA_TRY(cudaGetLastError());
         return MFA_OK;
     };
     if ((mask & MFA_R0) && r0) TRY(put3(r0, c->rx));
     if ((mask & MFA_V) && v) TRY(put3(v, c->vx));
     if ((mask & MFA_A) && a) TRY(put3(a, c->ax));
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
     if ((mask & MFA_F) && force) {
         if (c->prec == MFA_MIXED) {
             std::vector<float> f4((size_t)4 * n, 0.0f);

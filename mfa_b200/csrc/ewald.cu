@@ -330,6 +330,153 @@ int launch_dipolar(mfa_ctx* c) {
     return MFA_OK;
 }
 
+namespace {
+
+// Adjoint of the k-space force.  F = -grad U_k, so its Jacobian is symmetric
+// and (dF/dr)^T lam = (dF/dr) lam, the change of the force when every particle
+// j moves along lam_j.  With theta_j = k.r_j, rho_k = sum_j q_j exp(i theta_j)
+// and sigma_k = sum_j q_j (k.lam_j) exp(i theta_j):
+//   dF_i = pre_i sum_k k A_k [cos theta_i Re sigma_k + sin theta_i Im sigma_k
+//                              - (k.lam_i)(cos theta_i Re rho_k + sin theta_i Im rho_k)],
+// pre_i = -8 pi q_i / V, A_k = inv_k2 exp(-k2 / 4 alpha) (the force of
+// ewald_k.f90:168-197 differentiated).  sigma_k is summed like rho_k (block
+// partials, then a block-ordered reduction).
+__global__ void __launch_bounds__(RHO_T) k_sig_partial(EwArgs a, const double* __restrict__ lam) {
+    extern __shared__ double2 rtab[];
+    double* sq = (double*)(rtab + CH * 3 * a.ts);
+    double* sl = sq + CH;                      // CH x 3 adjoint vectors
+    const int p0 = blockIdx.x * a.per_blk, p1 = min(a.n, p0 + a.per_blk);
+    const int kb = blockIdx.y * KPT * RHO_T;
+    double2 acc[KPT];
+    int4 kn[KPT];
+    double3 kv[KPT];
+#pragma unroll
+    for (int j = 0; j < KPT; ++j) {
+        acc[j] = make_double2(0.0, 0.0);
+        const int k = kb + threadIdx.x + j * RHO_T;
+        kn[j] = k < a.nk ? a.kn[k] : make_int4(0, 0, 0, 0);
+        const double4 v = k < a.nk ? a.kvec[k] : make_double4(0.0, 0.0, 0.0, 0.0);
+        kv[j] = make_double3(v.x, v.y, v.z);
+    }
+    for (int b0 = p0; b0 < p1; b0 += CH) {
+        const int nb = min(CH, p1 - b0);
+        __syncthreads();
+        if (threadIdx.x < nb) {
+            const int i = b0 + threadIdx.x;
+            build_tables(rtab + threadIdx.x * 3 * a.ts, a, a.rx[i], a.ry[i], a.rz[i]);
+            sq[threadIdx.x] = a.q[i];
+            sl[3 * threadIdx.x] = lam[i];
+            sl[3 * threadIdx.x + 1] = lam[a.n + i];
+            sl[3 * threadIdx.x + 2] = lam[2 * a.n + i];
+        }
+        __syncthreads();
+        for (int pp = 0; pp < nb; ++pp) {
+            const double qi = sq[pp], l0 = sl[3 * pp], l1 = sl[3 * pp + 1], l2 = sl[3 * pp + 2];
+#pragma unroll
+            for (int j = 0; j < KPT; ++j) {
+                const double w = qi * (kv[j].x * l0 + kv[j].y * l1 + kv[j].z * l2);
+                const double2 e = phase_from(rtab + pp * 3 * a.ts, a.ts, kn[j]);
+                acc[j].x += w * e.x;
+                acc[j].y += w * e.y;
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < KPT; ++j) {
+        const int k = kb + threadIdx.x + j * RHO_T;
+        if (k < a.nk) a.rho_part[(size_t)blockIdx.x * a.nk + k] = acc[j];
+    }
+}
+
+__global__ void k_sig_reduce(EwArgs a, double2* sig) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.nk) return;
+    double2 s = make_double2(0.0, 0.0);
+    for (int b = 0; b < a.nblk; ++b) {
+        const double2 v = a.rho_part[(size_t)b * a.nk + k];
+        s.x += v.x;
+        s.y += v.y;
+    }
+    sig[k] = s;
+}
+
+__global__ void __launch_bounds__(FT) k_ewald_adj(EwArgs a, const double2* __restrict__ sig,
+                                                  const double* __restrict__ lam, double* out) {
+    extern __shared__ double2 ftab[];
+    double2* t = ftab + threadIdx.x * 3 * a.ts;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const double qi = a.q[i];
+    if (qi == 0.0) return;
+    build_tables(t, a, a.rx[i], a.ry[i], a.rz[i]);
+    const double l0 = lam[i], l1 = lam[a.n + i], l2 = lam[2 * a.n + i];
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+    for (int k = 0; k < a.nk; ++k) {
+        const double2 e = phase_from(t, a.ts, __ldg(&a.kn[k]));
+        const double2 r = __ldg(&a.rho[k]);
+        const double2 sg = __ldg(&sig[k]);
+        const double4 kv = ldg4(&a.kvec[k]);
+        const double kl = kv.x * l0 + kv.y * l1 + kv.z * l2;
+        const double sc = ((e.x * sg.x + e.y * sg.y) - kl * (e.x * r.x + e.y * r.y)) * kv.w;
+        gx += kv.x * sc;
+        gy += kv.y * sc;
+        gz += kv.z * sc;
+    }
+    const double pre = ((-8.0 * a.pi) * qi) * a.inv_V;
+    out[i] += pre * gx;
+    out[a.n + i] += pre * gy;
+    out[2 * a.n + i] += pre * gz;
+}
+
+// Adjoint of the slab correction F_z,i = -4 pi q_i M_z / V, M_z = sum_j q_j
+// (z_j - Lz/2): J_{iz,jz} = -4 pi q_i q_j / V (symmetric), so the product is
+// -4 pi q_i / V sum_j q_j lam_z,j.
+__global__ void k_dipole_adj_sum(EwArgs a, const double* __restrict__ lam, double* sum) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v = i < a.n ? a.q[i] * lam[2 * a.n + i] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(sum, v);
+}
+
+__global__ void k_dipole_adj(EwArgs a, const double* __restrict__ sum, double* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    out[2 * a.n + i] += (((-4.0 * a.pi) * a.q[i]) * *sum) * a.inv_V;
+}
+
+}  // namespace
+
+size_t ewald_adj_bytes(const mfa_ctx* c) { return (size_t)(c->nk > 0 ? c->nk : 1) * sizeof(double2) + 64; }
+
+int launch_ewald_adjoint(mfa_ctx* c, const double* lam, double* out, void* scratch) {
+    if (!c->p.charged) return MFA_OK;
+    if (c->nk == 0) return MFA_ERR_STATE;
+    EwArgs a = make_args(c);
+    double2* sig = (double2*)scratch;
+    double* dsum = (double*)((char*)scratch + (size_t)c->nk * sizeof(double2));
+    const int fsm = FT * 3 * (KM + 1) * (int)sizeof(double2);
+    const int rsm = CH * (3 * (KM + 1) * (int)sizeof(double2) + (int)sizeof(double));
+    MFA_CUDA_TRY(cudaFuncSetAttribute(k_sig_partial, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      rsm + CH * 3 * (int)sizeof(double)));
+    MFA_CUDA_TRY(cudaFuncSetAttribute(k_ewald_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+    const dim3 rgrid(c->nblk_rho, (c->nk + KPT * RHO_T - 1) / (KPT * RHO_T));
+    // rho_k at the current positions, then sigma_k, then the product
+    k_rho_partial<<<rgrid, RHO_T, rho_smem(c), c->st>>>(a);
+    k_rho_reduce<<<(c->nk + 255) / 256, 256, 0, c->st>>>(a);
+    const size_t ssm = rho_smem(c) + (size_t)CH * 3 * sizeof(double);
+    k_sig_partial<<<rgrid, RHO_T, ssm, c->st>>>(a, lam);
+    k_sig_reduce<<<(c->nk + 255) / 256, 256, 0, c->st>>>(a, sig);
+    k_ewald_adj<<<(c->n + FT - 1) / FT, FT, force_smem(c), c->st>>>(a, sig, lam, out);
+    if (c->p.symmetry == 0) {
+        const int T = 256, nb = (c->n + T - 1) / T;
+        MFA_CUDA_TRY(cudaMemsetAsync(dsum, 0, sizeof(double), c->st));
+        k_dipole_adj_sum<<<nb, T, 0, c->st>>>(a, lam, dsum);
+        k_dipole_adj<<<nb, T, 0, c->st>>>(a, dsum, out);
+    }
+    MFA_CUDA_TRY(cudaGetLastError());
+    return MFA_OK;
+}
+
 int mfa_ewald_download_kvecs(mfa_ctx* c, double* out3, int max_k) {
     if (!c->kvec) return 0;
     std::vector<double4> kv(c->nk);

@@ -126,8 +126,9 @@ struct mfa_ctx {
     double* elog;
     int elog_every, elog_cap;
     int32_t* elog_n;
-    // pinned host staging for uploads/downloads (3 x n doubles)
-    double* h_stage;
+    // device staging for uploads/downloads (3 x n doubles): the host's r0(3,n)
+    // layout is copied as it is and (de)interleaved on the device
+    double* d_stage;
     double* h_scal;                     // pinned copy of dscal and dflags (mfa_get_scalars)
     // observables (observe.cu), allocated at their first use: unfolded
     // coordinates (3 n) and 16 result slots; the z histogram and its count
@@ -196,6 +197,10 @@ int ewald_setup(mfa_ctx* c);
 int launch_ewald(mfa_ctx* c);
 // dipolar_correction.f90 (charged SYMMETRY 0; nothing otherwise)
 int launch_dipolar(mfa_ctx* c);
+// adjoint of the k-space force and of the slab correction: out += (dF/dr)^T lam
+// (lam, out: 3 x n, particle order); scratch of ewald_adj_bytes(c) bytes
+size_t ewald_adj_bytes(const mfa_ctx* c);
+int launch_ewald_adjoint(mfa_ctx* c, const double* lam, double* out, void* scratch);
 // terms.cu: the velocity half of verlet_velocities under DPD_VV
 int launch_dpd_vv_kick(mfa_ctx* c);
 
@@ -284,6 +289,34 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, const PhiloxKeys& key) {
 }
 #define TAG_DPD 0x44504400u
 #define TAG_LGV 0x4C475600u
+
+// The three Langevin variates of particle `id` at `step` (lgv_forces.f90:25-27:
+// three rnor() per particle): one Philox-4x32-10 block keyed by (id, step),
+// Box-Muller on its four words (FP64 log/sincos), or the uniform alternative
+// sqrt(3)(2u - 1).  Shared by the pair kernel and its adjoint, which replays it.
+template <typename R>
+__device__ __forceinline__ void lgv_noise3(uint32_t id, uint32_t step, int noise, uint32_t seed0, uint32_t seed1,
+                                           R g[3]) {
+    const uint4 w = philox4x32_10(make_uint4(id, 0u, step, TAG_LGV), seed0, seed1);
+    if (noise == MFA_NOISE_UNIFORM) {
+        const uint32_t x[3] = {w.x, w.y, w.z};
+        for (int d = 0; d < 3; ++d) {
+            const float u = (float)(x[d] >> 9) * 1.1920928955078125e-07f + 5.9604644775390625e-08f;
+            g[d] = (R)(1.7320508075688772f * (2.0f * u - 1.0f));
+        }
+        return;
+    }
+    const double u0 = ((double)w.x + 0.5) * 2.3283064365386963e-10;
+    const double u1 = ((double)w.y + 0.5) * 2.3283064365386963e-10;
+    const double u2 = ((double)w.z + 0.5) * 2.3283064365386963e-10;
+    const double u3 = ((double)w.w + 0.5) * 2.3283064365386963e-10;
+    const R r1 = (R)sqrt(-2.0 * log(u0)), r2 = (R)sqrt(-2.0 * log(u2));
+    double s1, c1;
+    sincospi(2.0 * u1, &s1, &c1);
+    g[0] = r1 * (R)c1;
+    g[1] = r1 * (R)s1;
+    g[2] = r2 * (R)cospi(2.0 * u3);
+}
 
 // Position of a block in the launch it belongs to.  A plain launch uses
 // blockIdx/gridDim; a grouped launch (one kernel stage for several contexts,

@@ -125,25 +125,6 @@ __device__ __forceinline__ double noise1(uint32_t x0, uint32_t x1, int shape, do
     return sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
 }
 
-template <typename R>
-__device__ __forceinline__ void lgv_noise3(uint32_t id, uint32_t step, const PairArgs& a, R g[3]) {
-    const uint4 w = philox4x32_10(make_uint4(id, 0u, step, TAG_LGV), a.seed0, a.seed1);
-    if (a.noise == MFA_NOISE_UNIFORM) {
-        g[0] = noise1(w.x, 0u, 1, R(0)); g[1] = noise1(w.y, 0u, 1, R(0)); g[2] = noise1(w.z, 0u, 1, R(0));
-        return;
-    }
-    const double u0 = ((double)w.x + 0.5) * 2.3283064365386963e-10;
-    const double u1 = ((double)w.y + 0.5) * 2.3283064365386963e-10;
-    const double u2 = ((double)w.z + 0.5) * 2.3283064365386963e-10;
-    const double u3 = ((double)w.w + 0.5) * 2.3283064365386963e-10;
-    const R r1 = (R)sqrt(-2.0 * log(u0)), r2 = (R)sqrt(-2.0 * log(u2));
-    double s1, c1;
-    sincospi(2.0 * u1, &s1, &c1);
-    g[0] = r1 * (R)c1;
-    g[1] = r1 * (R)s1;
-    g[2] = r2 * (R)cospi(2.0 * u3);
-}
-
 // 9-3 wall (fluid_wall.f90:96-121) on one particle: returns F_z, adds energy.
 template <typename R, typename E>
 __device__ __forceinline__ R wall_force(const PairArgs& a, int t, R z, E& e) {
@@ -549,7 +530,7 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
             if (LGV) {
                 // lgv_forces.f90:22-41
                 R g[3];
-                lgv_noise3<R>((uint32_t)ii, (uint32_t)step, a, g);
+                lgv_noise3<R>((uint32_t)ii, (uint32_t)step, a.noise, a.seed0, a.seed1, g);
                 const double mi = a.mass[ii];
                 const R sm = (R)sqrt(mi), gm = (R)(a.friction * mi);
                 const R4 vi = own_v[lane];

@@ -134,3 +134,69 @@ def test_torch_autograd_wrapper(small_brush):
         with torch.no_grad():
             fd = (Observable.apply(theta + e) - Observable.apply(theta - e)) / (2 * e[i])
         assert theta.grad[i].item() == pytest.approx(fd.item(), rel=1e-3, abs=1e-8)
+
+
+def charged_start(cfg, steps=300):
+    """A charged configuration relaxed on the GPU (FP64), Ewald tables set up."""
+    g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=FP64)
+    g.init_forces(full=True)
+    g.step(steps)
+    st = g.download()
+    g.close()
+    return st
+
+
+def run_q(cfg, st, params, prec, fn):
+    g = System(params, st["r0"], st["v"], cfg.a_type, cfg.mass, q=cfg.q, a=st["a"], mic=st["mic"],
+               precision=prec)
+    g.ewald_k(0)
+    g.binning()
+    out = fn(g)
+    g.close()
+    return out
+
+
+def fd_check(cfg, st, nsteps=40, every=10, h=1e-4, mixed=False):
+    J, grad = run_q(cfg, st, cfg.params, FP64, lambda g: g.adjoint(nsteps, every))
+    J0 = run_q(cfg, st, cfg.params, FP64, lambda g: g.trajectory_observable(nsteps))
+    assert J == pytest.approx(J0, rel=1e-12)
+    base = base_values(cfg.params)
+    for name in NAMES:
+        jp = run_q(cfg, st, perturbed(cfg.params, name, 1 + h), FP64, lambda g: g.trajectory_observable(nsteps))
+        jm = run_q(cfg, st, perturbed(cfg.params, name, 1 - h), FP64, lambda g: g.trajectory_observable(nsteps))
+        fd = (jp - jm) / (2 * h * base[name])
+        assert grad[name] == pytest.approx(fd, rel=1e-3, abs=1e-6 * abs(J) / base[name]), (name, grad[name], fd)
+    if mixed:
+        _, g32 = run_q(cfg, st, cfg.params, MIXED, lambda g: g.adjoint(nsteps, every))
+        scale = max(abs(v) for v in grad.values())
+        for name in NAMES:
+            assert abs(g32[name] - grad[name]) < 2e-2 * max(abs(grad[name]), 1e-3 * scale), (name, g32[name])
+    return grad
+
+
+def test_adjoint_charged_bulk_langevin_matches_central_differences():
+    """Ewald real space with its own cutoff, the k-space sum (|n| <= 6) and the
+    Langevin thermostat (friction and noise amplitude through gamma): their
+    vector-Jacobian products enter every gradient through the state adjoint,
+    and the Langevin one also the gamma gradient directly."""
+    cfg = configs.charged(seed=41, n_chain=16, n_mon=10, density=0.5, n_kmax=6, rc_real=3.0)
+    assert cfg.params.thermostat == _abi.THERMO_LGV and cfg.params.charged
+    grad = fd_check(cfg, charged_start(cfg), mixed=True)
+    assert abs(grad["gamma_dpd"]) > 0.0
+
+
+def test_adjoint_charged_reference_mode_dpd_matches_central_differences():
+    """The reference's form of the Ewald real space (inside the LJ range, its
+    1/pi constant) with the DPD thermostat."""
+    cfg = configs.charged(seed=42, n_chain=16, n_mon=10, density=0.5, n_kmax=6, reference_mode=True,
+                          thermostat=_abi.THERMO_DPD, friction=4.5)
+    fd_check(cfg, charged_start(cfg))
+
+
+def test_adjoint_charged_slab_matches_central_differences():
+    """The charged channel: 9-3 walls, the slab k-set and the dipolar
+    correction (dipolar_correction.f90) with the Langevin thermostat."""
+    cfg = configs.charged_slab(seed=43, n_chain=12, n_mon=10, z_wall=8.0, n_kmax=4)
+    assert cfg.params.symmetry == 0
+    grad = fd_check(cfg, charged_start(cfg))
+    assert abs(grad["eps_wall"]) > 0.0

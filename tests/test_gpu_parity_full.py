@@ -53,7 +53,7 @@ def test_full_brush_lists_bit_exact(brush_full):
     assert (cell_o == cell_g).all()
     ref = pair_multiset_half(ff)
     got = pair_multiset_rows(cnt, nbr)
-    assert ref.shape[0] > 1_000_000
+    assert ref.shape[0] > 800_000                 # skin 0.3: about 4.8 listed pairs per bead
     assert ref.shape == got.shape and (ref == got).all()
 
 
