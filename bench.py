@@ -395,7 +395,8 @@ def batch_bench(a):
     # largest first to the least-loaded rank; the same partition on every rank)
     from mfa_b200.ranks import max_over_ranks, shard_by_weight, sum_over_ranks
     every_sys = configs.uneven_brushes(seed=a.seed, n_sys=a.n_sys)
-    cfgs = shard_by_weight(every_sys, [c.n for c in every_sys], rank, world)
+    my_ids = shard_by_weight(list(range(len(every_sys))), [c.n for c in every_sys], rank, world)
+    cfgs = [every_sys[k] for k in my_ids]
     n = sum(c.n for c in cfgs)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
 
@@ -448,13 +449,17 @@ def batch_bench(a):
         b.close()
         for g in ss:
             g.close()
-        return ms, launches, clocks, errs
+        return ms, launches, clocks, errs, sc
 
-    ms_mixed, launches, clocks, errs = timed_batch(_abi.MIXED, a.steps, a.warmup)
+    ms_mixed, launches, clocks, errs, sc_mixed = timed_batch(_abi.MIXED, a.steps, a.warmup)
+    # the per-system scalars of every rank in one table (one collective)
+    from mfa_b200.ranks import gather_system_values
+    table = gather_system_values([[x["e_total"], x["t_fluid"], float(x["error_bits"] != 0)] for x in sc_mixed],
+                                 my_ids, len(every_sys), dist, f"cuda:{dev}")
     ms_max = max_over_ranks(ms_mixed, dist, f"cuda:{dev}")
     n_all = int(sum_over_ranks(n, dist, f"cuda:{dev}"))
     value = n_all * a.steps / (ms_max * 1e-3)
-    ms_fp64, _, _, _ = timed_batch(_abi.FP64, a.steps, a.warmup)
+    ms_fp64, _, _, _, _ = timed_batch(_abi.FP64, a.steps, a.warmup)
     ms_fp64 = max_over_ranks(ms_fp64, dist, f"cuda:{dev}")
     # the same systems one after another (a launch sequence per system)
     ss = make(_abi.MIXED)
@@ -508,6 +513,10 @@ def batch_bench(a):
                                      "note": "the same systems through mfa_step one after another (wall clock)"},
             "gpu_launches": int(launches),
             "systems_with_errors": errs,
+            "gathered": {"systems": int(table.shape[0]), "systems_with_errors": int(table[:, 2].sum()),
+                         "kinetic_temperature_mean": float((2.0 * table[:, 1] / (3.0 * np.array(
+                             [c.n for c in every_sys]))).mean()),
+                         "note": "per-system e_total, t_fluid and error flag of every rank, one all-reduce"},
             "clocks": clocks,
         }
         if cpu is not None:

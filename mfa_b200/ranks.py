@@ -61,3 +61,32 @@ def sum_over_ranks(x: float, dist=None, device="cpu") -> float:
     t = torch.tensor([float(x)], dtype=torch.float64, device=device)
     dist.all_reduce(t)
     return float(t.item())
+
+
+def gather_system_values(values, index, n_total: int, dist=None, device="cpu"):
+    """The per-system values of every rank in one table: rank r holds rows
+    `values` (m_r x k) of the systems with global indices `index` (m_r); every
+    rank gets the n_total x k table, with one collective (a sum of disjoint
+    rows -- as an all-gather of the shards, without padding uneven shards).
+    A count column checks that every system was computed on exactly one rank.
+    Without a process group the local rows are the table."""
+    import numpy as np
+    vals = np.asarray(values, dtype=np.float64).reshape(len(index), -1)
+    k = vals.shape[1] if vals.size else 0
+    if dist is not None:
+        import torch
+        kk = torch.tensor([float(k)], dtype=torch.float64, device=device)
+        dist.all_reduce(kk, op=dist.ReduceOp.MAX)
+        k = int(kk.item())
+    table = np.zeros((n_total, k + 1))
+    for row, g in zip(vals, index):
+        table[g, :k] = row
+        table[g, k] += 1.0
+    if dist is not None:
+        import torch
+        t = torch.from_numpy(table).to(device)
+        dist.all_reduce(t)
+        table = t.cpu().numpy()
+    if not (table[:, k] == 1.0).all():
+        raise RuntimeError("a system was computed on no rank or on several")
+    return table[:, :k]

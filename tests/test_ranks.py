@@ -81,3 +81,68 @@ def test_two_gloo_ranks_agree_on_time_and_size():
 
 def test_without_process_group():
     assert max_over_ranks(3.5) == 3.5 and sum_over_ranks(2.0) == 2.0
+
+
+def _small_systems():
+    from mfa_b200 import configs
+    return [configs.melt(seed=60 + k, n_chain=4 + 2 * k, n_mon=8, density=0.7) for k in range(5)]
+
+
+def _step_with_oracle(cfg, steps=20):
+    """The CPU stand-in for one rank's GPU work: the oracle advances the system
+    and reports the per-system scalars a batch run gathers at its end."""
+    from oracle import Oracle
+    o = Oracle(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass)
+    o.init_forces()
+    for _ in range(steps):
+        o.md_step()
+    s = o.scalars()
+    return [s["e_total"], s["v_total"], s["t_fluid"], float(s["n_rebuilds"])]
+
+
+def _gather_main(rank, world, port, out):
+    import datetime
+    import sys
+    import torch.distributed as dist
+    from conftest import ROOT
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from mfa_b200.ranks import gather_system_values
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    systems = _small_systems()
+    ids = shard_by_weight(list(range(len(systems))), [c.n for c in systems], rank, world)
+    rows = [_step_with_oracle(systems[k]) for k in ids]
+    table = gather_system_values(rows, ids, len(systems), dist)
+    dist.barrier()
+    dist.destroy_process_group()
+    out.put((rank, ids, table.tolist()))
+
+
+def test_two_gloo_ranks_step_their_shards_and_gather_per_system_values():
+    """Each rank steps its bead-count share of a small uneven batch (CPU
+    stand-in: the oracle) and the per-system scalars are gathered into one
+    table on every rank; it equals the same systems stepped in one process."""
+    import numpy as np
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gather_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=300) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (_, ids0, t0), (_, ids1, t1) = res
+    assert sorted(ids0 + ids1) == list(range(5)) and ids0 and ids1
+    serial = np.array([_step_with_oracle(c) for c in _small_systems()])
+    assert np.array_equal(np.array(t0), np.array(t1))          # every rank holds the same table
+    assert np.array_equal(np.array(t0), serial)                # and it is the serial result, bit for bit
+
+
+def test_gather_without_process_group_and_ownership_check():
+    from mfa_b200.ranks import gather_system_values
+    t = gather_system_values([[1.0, 2.0], [3.0, 4.0]], [1, 0], 2)
+    assert t.tolist() == [[3.0, 4.0], [1.0, 2.0]]
+    with pytest.raises(RuntimeError):
+        gather_system_values([[1.0]], [0], 2)                   # system 1 computed nowhere
