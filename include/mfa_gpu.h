@@ -314,6 +314,21 @@ typedef struct mfa_observables {
     double momentum[3];
 } mfa_observables;
 int mfa_observe(mfa_ctx* ctx, mfa_observables* out);
+/* r_end_to_end_2v(2) of functions.f90:626-667 and the head forces of
+ * observation.f90:326-328, from the chains unfolded as for mfa_observe:
+ * r_ee9 = the mean end-to-end vector of the top brushes (chains
+ * 1..n_chain/2), the bottom brushes (n_chain/2+1..n_chain) and the melt
+ * (n_chain+1..n_chain+n_chain_d), x y z each; r_ee2_9 = the means of its
+ * squared components; every chain is read as n_mon beads from
+ * (i_chain-1)*n_mon+1, and the brush sums are divided by n_chain/2 in integer
+ * arithmetic, both as the reference does.  f_heads6 = minus the summed force
+ * on the grafted heads of the upper-wall chains (1..n_chain/2) and of the
+ * lower-wall chains, xyz each, as the last velocity half saw it before the pin
+ * (f_on_heads of verlet_velocities.f90:18; zeros when the heads are not
+ * pinned).  Any pointer may be NULL.  Synchronises.  The melt group is NaN
+ * when its chains are single beads (explicit solvent) or its indexing would
+ * run past the particles. */
+int mfa_observe_ends(mfa_ctx* ctx, double* r_ee9, double* r_ee2_9, double* f_heads6);
 /* histo(2) of functions.f90:157-185: adds the current z positions of the brush
  * beads (ids 1..n_mon*n_chain) and the melt/droplet beads (the next
  * n_mon_d*n_chain_d) to device-resident histograms of hist_dim bins

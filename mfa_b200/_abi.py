@@ -135,6 +135,7 @@ SIGNATURES = {
     "mfa_read_energy_log": (C.c_int, [_P, _DP, C.c_int32, _IP]),
     "mfa_get_scalars": (C.c_int, [_P, C.POINTER(MfaScalars)]),
     "mfa_observe": (C.c_int, [_P, C.POINTER(MfaObservables)]),
+    "mfa_observe_ends": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "mfa_histogram_z": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "mfa_download": (C.c_int, [_P, C.c_uint32, _DP, _DP, _DP, _DP, _IP]),
     "mfa_upload": (C.c_int, [_P, C.c_uint32, _DP, _DP, _DP, _DP, _IP]),

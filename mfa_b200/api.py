@@ -296,6 +296,14 @@ class System:
         return {"r_g2_brush": np.array(o.r_g2_brush[:]), "r_g2_melt": np.array(o.r_g2_melt[:]),
                 "momentum": np.array(o.momentum[:])}
 
+    def observe_ends(self) -> dict:
+        """mfa_observe_ends: mean end-to-end vectors and their squares for the
+        top brushes, bottom brushes and melt (3 x 3 each), and minus the
+        summed force on the heads of the upper- and lower-wall chains (2 x 3)."""
+        ree, ree2, fh = np.empty(9), np.empty(9), np.empty(6)
+        check(self.lib.mfa_observe_ends(self.ctx, _dp(ree), _dp(ree2), _dp(fh)), "mfa_observe_ends")
+        return {"r_ee": ree.reshape(3, 3), "r_ee2": ree2.reshape(3, 3), "head_force": fh.reshape(2, 3)}
+
     def histogram_z(self, hist_dim: int, reset: bool = False):
         """mfa_histogram_z: adds this state's z histograms; returns the
         accumulated counts (2 x hist_dim: brush, melt) and observation count."""

@@ -98,7 +98,7 @@ void free_all(mfa_ctx* c) {
     void* ptrs[] = {c->rx, c->mx, c->type, c->mass, c->force, c->pos_s, c->vel_s, c->pos64, c->pos32,
                     c->ids, c->cell_count, c->nbr, c->nnb, c->partials, c->counters, c->dscal,
                     c->dstep, c->kvec, c->rho, c->rho_part, c->elog, c->elog_n, c->tabs,
-                    c->obs_buf, c->hist, c->fd, c->term_buf, c->d_stage};
+                    c->obs_buf, c->hist, c->fd, c->term_buf, c->d_stage, c->f_heads};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->h_scal) cudaFreeHost(c->h_scal);
@@ -454,6 +454,11 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
     if (rc == MFA_OK) c->dflags = (int32_t*)(c->dscal + S_NSLOT);
     A(dalloc(&c->dstep, 2));
     A(dalloc(&c->tabs, 6 * T8 * T8));
+    if (p->pin_heads && p->n_chain > 0 && p->n_mon > 0) {
+        A(dalloc(&c->f_heads, (size_t)3 * p->n_chain));
+        if (rc == MFA_OK && dzero(c, c->f_heads, (size_t)3 * p->n_chain * sizeof(double)) != MFA_OK)
+            rc = MFA_ERR_CUDA;
+    }
     A(dalloc(&c->d_stage, (size_t)3 * n));
     if (rc == MFA_OK && cudaMallocHost((void**)&c->h_scal, (S_NSLOT + F_NFLAG / 2) * sizeof(double)) != cudaSuccess)
         rc = MFA_ERR_NOMEM;

@@ -35,6 +35,7 @@ struct VVArgs {
     int symmetry;
     int write_sorted;
     int pin_heads, n_chain, n_mon;
+    double* f_heads;              // force on each head before the pin (3 x n_chain), or null
     double L[3];
     double dt, skin_lim;
     double va[3];
@@ -160,6 +161,13 @@ __device__ __forceinline__ double velocity_half(const VVArgs& a, int i, double& 
     vy = __dadd_rn(vy, __dmul_rn(hdt, ay));
     vz = __dadd_rn(vz, __dmul_rn(hdt, az));
     if (a.pin_heads && i < a.n_chain * a.n_mon && (i % a.n_mon) == 0) {
+        if (a.f_heads) {
+            // f_on_heads(:,:) = force(:,1:part_init_d:n_mon) (verlet_velocities.f90:18)
+            double* fh = a.f_heads + 3 * (size_t)(i / a.n_mon);
+            fh[0] = (double)fi.x;
+            fh[1] = (double)fi.y;
+            fh[2] = (double)fi.z;
+        }
         const double sg = (i / a.n_mon < a.n_chain / 2) ? 1.0 : -1.0;
         vx = sg * a.va[0];
         vy = sg * a.va[1];
@@ -319,6 +327,7 @@ VVArgs make_args(mfa_ctx* c) {
     a.symmetry = c->p.symmetry;
     a.write_sorted = c->lists_valid;
     a.pin_heads = c->p.pin_heads; a.n_chain = c->p.n_chain; a.n_mon = c->p.n_mon;
+    a.f_heads = c->f_heads;
     for (int d = 0; d < 3; ++d) { a.L[d] = c->p.boundary[d]; a.va[d] = c->p.va_spring_twall[d]; }
     a.dt = c->p.dt;
     a.skin_lim = (c->p.skin / 2.0) * (c->p.skin / 2.0);

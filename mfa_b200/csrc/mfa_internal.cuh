@@ -133,6 +133,10 @@ struct mfa_ctx {
     // observables (observe.cu), allocated at their first use: unfolded
     // coordinates (3 n) and 16 result slots; the z histogram and its count
     double* obs_buf;
+    // the force on each grafted head before the pin zeroes it
+    // (verlet_velocities.f90:18, f_on_heads), 3 x n_chain chain-major; null
+    // unless the heads are pinned
+    double* f_heads;
     double* hist;
     int hist_dim, hist_obs;
     // optional terms (terms.cu): DPD_VV switch and its two 3 x n FP64

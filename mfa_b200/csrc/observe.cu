@@ -16,7 +16,13 @@
 //   k_obs_momentum      sum of m v over all particles (:279-283);
 //   k_obs_histo         z bins of the brush and melt beads, int(z / z_step) + 1
 //                       clamped to 1..hist_dim (functions.f90:157-185), counted
-//                       with FP64 atomics (exact for integers below 2^53).
+//                       with FP64 atomics (exact for integers below 2^53);
+//   k_obs_ends          one block: end-to-end vectors of the chains
+//                       (functions.f90:626-667) summed per group (top brushes,
+//                       bottom brushes, melt) and the force on the grafted
+//                       heads of the last step summed per wall
+//                       (observation.f90:326-328), each thread over a fixed
+//                       stride of chains, then a fixed reduction tree.
 #include "mfa_internal.cuh"
 
 namespace {
@@ -121,6 +127,59 @@ __global__ void k_obs_histo(const double* rz, int pd, int pe, double inv_z_step,
     atomicAdd(&hist[(i < pd ? 0 : hist_dim) + z - 1], 1.0);
 }
 
+// 24 sums: r_ee (3 groups x xyz), r_ee^2 (3 x xyz), head force (2 walls x xyz).
+// Chains 1..n_chain/2 are the top brushes, n_chain/2+1..n_chain the bottom
+// ones, n_chain+1..n_chain+nmelt the melt, every chain taken as n_mon beads
+// from (c-1) n_mon + 1 (the reference's indexing); the group sums are divided
+// by n_chain/2 (integer division, both brush groups) and n_chain_d, and the
+// head forces negated, as the reference writes them.  nmelt = 0 leaves the
+// melt group NaN.
+constexpr int NE = 24;
+__global__ void __launch_bounds__(1024) k_obs_ends(ObsArgs a, const double* __restrict__ f_heads, int nmelt) {
+    __shared__ double sm[NE][32];
+    double acc[NE];
+#pragma unroll
+    for (int q = 0; q < NE; ++q) acc[q] = 0.0;
+    const int nct = a.n_chain + nmelt, half = a.n_chain / 2;
+    for (int c = threadIdx.x; c < nct; c += blockDim.x) {
+        const int g = c < half ? 0 : (c < a.n_chain ? 1 : 2);
+        const int f = c * a.n_mon, e = f + a.n_mon - 1;
+        const double v[3] = {a.sx[e] - a.sx[f], a.sy[e] - a.sy[f], a.sz[e] - a.sz[f]};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            acc[3 * g + d] += v[d];
+            acc[9 + 3 * g + d] += v[d] * v[d];
+        }
+    }
+    if (f_heads)
+        for (int c = threadIdx.x; c < a.n_chain; c += blockDim.x) {
+            const int w = c < half ? 0 : 1;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) acc[18 + 3 * w + d] += f_heads[3 * (size_t)c + d];
+        }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NE; ++q) {
+        double x = acc[q];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sm[q][wid] = x;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        for (int q = 0; q < NE; ++q) {
+            double x = lane < nw ? sm[q][lane] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            if (lane == 0) {
+                const int grp = q < 18 ? (q % 9) / 3 : -1;
+                if (grp == 0 || grp == 1) x = x / (double)half;
+                else if (grp == 2) x = nmelt > 0 ? x / (double)a.n_chain_d : __longlong_as_double(0x7ff8000000000000LL);
+                else x = -x;
+                a.out[9 + q] = x;
+            }
+        }
+    }
+}
+
 constexpr int T = 256;
 
 ObsArgs make_args(mfa_ctx* c) {
@@ -151,7 +210,7 @@ int mfa_observe(mfa_ctx* c, mfa_observables* o) {
     // the melt indexing of observation.f90:256-259 must stay inside the particles
     if ((long long)(p.n_chain + p.n_chain_d) * p.n_mon_d > c->n) return MFA_ERR_UNSUPPORTED;
     if (blocks(c->n) > c->max_blocks) return MFA_ERR_ARGS;
-    if (!c->obs_buf) MFA_CUDA_TRY(cudaMalloc((void**)&c->obs_buf, (3 * (size_t)c->n + 16) * sizeof(double)));
+    if (!c->obs_buf) MFA_CUDA_TRY(cudaMalloc((void**)&c->obs_buf, (3 * (size_t)c->n + 40) * sizeof(double)));
     ObsArgs a = make_args(c);
     int launches = 0;
     k_obs_copy<<<blocks(c->n), T, 0, c->st>>>(a);
@@ -190,6 +249,45 @@ int mfa_observe(mfa_ctx* c, mfa_observables* o) {
         o->r_g2_melt[d] = p.n_chain_d > 0 && p.n_mon_d > 0 ? h[3 + d] : nan;
         o->momentum[d] = h[6 + d];
     }
+    return MFA_OK;
+}
+
+int mfa_observe_ends(mfa_ctx* c, double* r_ee9, double* r_ee2_9, double* f_heads6) {
+    if (!c) return MFA_ERR_ARGS;
+    const mfa_params& p = c->p;
+    // every chain, melt ones included, is read as n_mon beads (the reference's
+    // indexing); melt "chains" of single beads (explicit solvent), or an
+    // indexing that would run past the particles, leave the melt group NaN
+    if (p.n_mon < 1 || (long long)p.n_chain * p.n_mon > c->n) return MFA_ERR_UNSUPPORTED;
+    const int nmelt = (p.n_mon_d > 1 && (long long)(p.n_chain + p.n_chain_d) * p.n_mon <= c->n) ? p.n_chain_d : 0;
+    if (!c->obs_buf) MFA_CUDA_TRY(cudaMalloc((void**)&c->obs_buf, (3 * (size_t)c->n + 40) * sizeof(double)));
+    ObsArgs a = make_args(c);
+    int launches = 1;
+    // the chains refolded bead by bead, as for the radii of gyration
+    k_obs_copy<<<blocks(c->n), T, 0, c->st>>>(a);
+    if (p.symmetry == 0 && p.n_chain > 0 && p.n_mon > 1) {
+        k_obs_refold_brush<<<blocks(p.n_chain), T, 0, c->st>>>(a);
+        ++launches;
+    }
+    if (p.n_chain_d > 0 && p.n_mon_d > 1) {
+        const int pd = p.n_mon * p.n_chain, pe = pd + p.n_mon_d * p.n_chain_d;
+        const int first = pd / p.n_mon_d, last = (pe - 1) / p.n_mon_d;
+        k_obs_refold_melt<<<blocks(last - first + 1), T, 0, c->st>>>(a, first, last - first + 1);
+        ++launches;
+    }
+    k_obs_ends<<<1, 1024, 0, c->st>>>(a, c->f_heads, nmelt);
+    ++launches;
+    MFA_CUDA_TRY(cudaGetLastError());
+    note_launch(c, launches);
+    double h[NE];
+    MFA_CUDA_TRY(cudaMemcpyAsync(h, a.out + 9, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    for (int k = 0; k < 9; ++k) {
+        if (r_ee9) r_ee9[k] = h[k];
+        if (r_ee2_9) r_ee2_9[k] = h[9 + k];
+    }
+    for (int k = 0; k < 6; ++k)
+        if (f_heads6) f_heads6[k] = c->f_heads ? h[18 + k] : 0.0;
     return MFA_OK;
 }
 

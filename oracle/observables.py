@@ -14,6 +14,14 @@ product imports it.
   indexing (exact only when n_mon_d = n_mon or no brush precedes them);
   0/0 gives NaN when there are no such chains, as in the reference.
 - total momentum: observation.f90:279-283, sum over all particles of m v.
+- end-to-end vectors: functions.f90:626-667 (r_end_to_end_2v mode 2) -- chain
+  c (0-based, brush then melt) runs from bead c*n_mon to c*n_mon + n_mon - 1
+  of the unfolded coordinates (n_mon for the melt chains too, the
+  reference's indexing); groups top brushes (c < n_chain // 2), bottom
+  brushes, melt; sums divided by n_chain // 2 (both brush groups) and
+  n_chain_d.
+- head forces: observation.f90:326-328 -- minus the summed force on the
+  heads of chains c < n_chain // 2 (upper wall) and of the others.
 - z histogram: functions.f90:157-185 (histo mode 2) -- bin int(z / z_step) + 1
   clamped to 1..hist_dim, z_step = Lz / hist_dim, counted for the brush beads
   (column 0) and the melt/droplet beads (column 1).
@@ -82,3 +90,27 @@ def z_histogram(r0, boundary, hist_dim, n_mon, n_chain, n_mon_d, n_chain_d):
         idx = np.clip(idx, 1, hist_dim)
         np.add.at(out[col], idx - 1, 1.0)
     return out
+
+
+def end_to_end(spabs, n_mon, n_chain, n_chain_d):
+    """(r_ee, r_ee2), 3 groups x xyz each, as r_end_to_end_2v(2) forms them."""
+    r_ee = np.zeros((3, 3))
+    r_ee2 = np.zeros((3, 3))
+    half = n_chain // 2
+    for c in range(n_chain + n_chain_d):
+        g = 0 if c < half else (1 if c < n_chain else 2)
+        v = spabs[c * n_mon + n_mon - 1] - spabs[c * n_mon]
+        r_ee[g] += v
+        r_ee2[g] += v * v
+    with np.errstate(invalid="ignore", divide="ignore"):
+        for g, cnt in ((0, half), (1, half), (2, n_chain_d)):
+            r_ee[g] = r_ee[g] / float(cnt)
+            r_ee2[g] = r_ee2[g] / float(cnt)
+    return r_ee, r_ee2
+
+
+def head_forces(force_on_heads, n_chain):
+    """Minus the summed head force of the upper-wall and lower-wall chains."""
+    f = np.asarray(force_on_heads, dtype=np.float64).reshape(n_chain, 3)
+    half = n_chain // 2
+    return np.stack([-f[:half].sum(axis=0), -f[half:].sum(axis=0)])

@@ -107,3 +107,73 @@ def test_histogram_z_accumulates_exactly(brush_small_cfg):
     h3, n3 = g.histogram_z(40, reset=True)
     assert n3 == 1 and (h3 == ob.z_histogram(r_b, *args)).all()
     g.close()
+
+
+def test_end_to_end_of_straight_chains_closed_form():
+    """Three straight chains of 4 beads along x (spacing 1): top, bottom and a
+    melt chain; every end-to-end vector is (3, 0, 0)."""
+    s = np.zeros((12, 3))
+    for c in range(3):
+        s[4 * c:4 * c + 4, 0] = np.arange(4.0)
+    r_ee, r_ee2 = ob.end_to_end(s, 4, 2, 1)
+    np.testing.assert_allclose(r_ee, [[3, 0, 0]] * 3)
+    np.testing.assert_allclose(r_ee2, [[9, 0, 0]] * 3)
+    # n_chain = 1: the brush groups divide by n_chain // 2 = 0 (the reference's 0/0)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        r1, _ = ob.end_to_end(s[:4], 4, 1, 0)
+    assert np.isnan(r1[0]).all() and np.isinf(r1[1][0])
+    f = np.array([[1.0, 2.0, 3.0], [4.0, 5.0, 6.0], [7.0, 8.0, 9.0]])
+    np.testing.assert_allclose(ob.head_forces(f, 3), [[-1, -2, -3], [-11, -13, -15]])
+
+
+@pytest.mark.gpu
+def test_observe_ends_brush_against_restatement_and_oracle_head_forces(brush_small_cfg):
+    """End-to-end vectors of the brush (refolded chains) against the numpy
+    restatement, and the head forces of the last step against the oracle's
+    force on the heads at the same positions (every force term, before the
+    pin of verlet_velocities.f90:113-145 zeroes it)."""
+    from mfa_b200.api import System
+    from oracle import Oracle
+    cfg = brush_small_cfg
+    p = cfg.params.copy()
+    p.thermostat = _abi.THERMO_NONE
+    g = System(p, cfg.r0, cfg.v, cfg.a_type, cfg.mass, precision=FP64)
+    g.init_forces(full=True)
+    for _ in range(5):
+        g.md_step()
+    e = g.observe_ends()
+    st = g.download(_abi.R0 | _abi.V | _abi.A | _abi.MIC)
+    s = ob.refold(st["r0"], p.boundary, p.n_mon, p.n_chain, p.n_mon_d, p.n_chain_d, p.symmetry)
+    r_ee, r_ee2 = ob.end_to_end(s, p.n_mon, p.n_chain, 0)
+    np.testing.assert_allclose(e["r_ee"][:2], r_ee[:2], rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(e["r_ee2"][:2], r_ee2[:2], rtol=1e-12)
+    assert np.isnan(e["r_ee"][2]).all()              # solvent: single-bead "chains"
+    o = Oracle(p, st["r0"], st["v"], cfg.a_type, cfg.mass, a=st["a"], mic=st["mic"])
+    o.binning()
+    o.zero_forces()
+    o.fluid_fluid()
+    o.fluid_wall(p.wall)
+    o.intra_molec()
+    o.bending(2)
+    f = o.state()["force"][0:p.n_chain * p.n_mon:p.n_mon]
+    ref = ob.head_forces(f, p.n_chain)
+    assert np.abs(ref).max() > 0.0
+    np.testing.assert_allclose(e["head_force"], ref, rtol=1e-11, atol=1e-11 * np.abs(ref).max())
+    g.close()
+
+
+@pytest.mark.gpu
+def test_observe_ends_melt_chains(melt_cfg):
+    from mfa_b200.api import System
+    cfg = melt_cfg
+    p = cfg.params.copy()
+    half = p.n_chain // 2
+    p.n_chain_d, p.n_mon_d, p.n_chain = p.n_chain - half, p.n_mon, half
+    g = System(p, cfg.r0, cfg.v, cfg.a_type, cfg.mass, precision=FP64)
+    e = g.observe_ends()
+    s = ob.refold(cfg.r0, p.boundary, p.n_mon, p.n_chain, p.n_mon_d, p.n_chain_d, p.symmetry)
+    r_ee, r_ee2 = ob.end_to_end(s, p.n_mon, p.n_chain, p.n_chain_d)
+    np.testing.assert_allclose(e["r_ee"], r_ee, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(e["r_ee2"], r_ee2, rtol=1e-12)
+    assert (e["head_force"] == 0.0).all()            # no pinned heads in a melt
+    g.close()
