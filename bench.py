@@ -678,7 +678,8 @@ def main():
         tuned = autotune(g)
         shapes = tuned["pair_shape"]
         g.tuned = min(shapes, key=shapes.get)
-        g.tuning = {f"{k}x{b}{'-tiled' if t else ''}": round(1e3 * s / 300, 4) for (k, b, t), s in shapes.items()}
+        g.tuning = {f"{k}x{b}{'-tiled' if t else ''}{f'-queue{q}' if q else ''}": round(1e3 * s / 300, 4)
+                    for (k, b, t, q), s in shapes.items()}
         g.skin_tuning = {f"{s:g}": round(1e3 * v / 300, 4) for s, v in tuned["skin"].items()}
         ext = torch.cuda.ExternalStream(g.stream_ptr(), device=f"cuda:{dev}")
         # a timed iteration is `chunk` consecutive time steps (one mfa_step call:
@@ -892,7 +893,9 @@ def main():
             "config": dict(meta, beads=n, precision="mixed", dt=cfg.params.dt, skin=skin_mixed,
                            cells=nbin_mixed, autotune_skin_ms_per_step=skin_tuning,
                            pair_shape=f"{shape_mixed[0]} list entries per thread and round x {shape_mixed[1]}-thread blocks, "
-                                      f"{'tiled' if shape_mixed[2] else 'untiled'} (autotuned)",
+                                      f"{'tiled' if shape_mixed[2] else 'untiled'}"
+                                      f"{f', work queue of {shape_mixed[3]} CTAs per SM' if shape_mixed[3] else ''}"
+                                      " (autotuned)",
                            autotune_ms_per_step=tuning_mixed,
                            thermostat="dpd", replicas=world,
                            steps_per_timed_iteration=a.chunk,

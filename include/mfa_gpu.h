@@ -287,6 +287,15 @@ int mfa_read_energy_log(mfa_ctx* ctx, double* out3, int32_t max_entries, int32_t
  * (tiled = 0).  The forces do not depend on it beyond rounding; it is what the
  * autotuner (mfa_b200.tune) chooses. */
 int mfa_set_pair_shape(mfa_ctx* ctx, int32_t entries_per_round, int32_t block, int32_t tiled);
+/* No counterpart in the reference.  Untiled launches of the pair kernel with a
+ * work queue: a fixed grid of ctas_per_sm CTAs per multiprocessor whose warps
+ * take 32-particle chunks from a shared counter until none is left, so that
+ * warps that finish early take more work; 0 (the default) gives every block
+ * of consecutive particles its own CTA.  The forces do not depend on it beyond
+ * rounding; the autotuner chooses it.  Launches of one context must not
+ * overlap on the GPU (they share the counter), which a context's own stream
+ * guarantees. */
+int mfa_set_pair_queue(mfa_ctx* ctx, int32_t ctas_per_sm);
 
 /* Re-grids the cell list (n_bin cells per axis) and sets the Verlet skin
  * (skin_2 derived as init_params.f90:807-808 does).  Cells must be at least as

@@ -210,6 +210,11 @@ class System:
         """nsteps time steps on the device (fused kernels, captured graphs)."""
         check(self.lib.mfa_step(self.ctx, int(nsteps)), "mfa_step")
 
+    def set_pair_queue(self, ctas_per_sm: int) -> None:
+        """mfa_set_pair_queue: untiled pair launches with a work queue of
+        ctas_per_sm CTAs per multiprocessor (0: one CTA per block of slots)."""
+        check(self.lib.mfa_set_pair_queue(self.ctx, int(ctas_per_sm)), "mfa_set_pair_queue")
+
     def set_pair_shape(self, entries_per_round: int, block: int, tiled: bool = True) -> None:
         check(self.lib.mfa_set_pair_shape(self.ctx, int(entries_per_round), int(block), int(bool(tiled))),
               "mfa_set_pair_shape")

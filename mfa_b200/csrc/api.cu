@@ -98,7 +98,7 @@ void free_all(mfa_ctx* c) {
     void* ptrs[] = {c->rx, c->mx, c->type, c->mass, c->force, c->pos_s, c->vel_s, c->pos64, c->pos32,
                     c->ids, c->cell_count, c->nbr, c->nnb, c->partials, c->counters, c->dscal,
                     c->dstep, c->kvec, c->rho, c->rho_part, c->elog, c->elog_n, c->tabs,
-                    c->obs_buf, c->hist, c->fd, c->term_buf, c->d_stage, c->f_heads};
+                    c->obs_buf, c->hist, c->fd, c->term_buf, c->d_stage, c->f_heads, c->pair_qctr};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->h_scal) cudaFreeHost(c->h_scal);
@@ -449,6 +449,10 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
     if (p->n_chain + p->n_chain_d + 64 > c->max_blocks) c->max_blocks = p->n_chain + p->n_chain_d + 64;
     A(dalloc(&c->partials, (size_t)R_N * 4 * c->max_blocks));
     A(dalloc(&c->counters, R_N));
+    A(dalloc(&c->pair_qctr, 1));
+    if (rc == MFA_OK && dzero(c, c->pair_qctr, sizeof(unsigned long long)) != MFA_OK) rc = MFA_ERR_CUDA;
+    if (rc == MFA_OK && cudaDeviceGetAttribute(&c->n_sm, cudaDevAttrMultiProcessorCount, c->dev) != cudaSuccess)
+        rc = MFA_ERR_CUDA;
     static_assert(F_NFLAG % 2 == 0, "the flags fill whole doubles after the energies");
     A(dalloc(&c->dscal, S_NSLOT + F_NFLAG / 2));
     if (rc == MFA_OK) c->dflags = (int32_t*)(c->dscal + S_NSLOT);
@@ -825,6 +829,18 @@ int mfa_set_pair_shape(mfa_ctx* c, int32_t k, int32_t block, int32_t tiled) {
     MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
     c->pair_tiled = tiled;
     TRY(pair_set_shape(c, k, block, c->tile_cap));
+    TRY(dzero(c, c->pair_qctr, sizeof(unsigned long long)));   // the queue's grid may change
+    invalidate_graph(c);
+    return MFA_OK;
+}
+
+int mfa_set_pair_queue(mfa_ctx* c, int32_t ctas_per_sm) {
+    if (!c || ctas_per_sm < 0 || ctas_per_sm > 64) return MFA_ERR_ARGS;
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    c->pair_queue = ctas_per_sm;
+    // a new grid changes the tickets a launch draws: restart the counter
+    TRY(dzero(c, c->pair_qctr, sizeof(unsigned long long)));
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
     invalidate_graph(c);
     return MFA_OK;
 }

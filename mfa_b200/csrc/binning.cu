@@ -365,7 +365,12 @@ __device__ __forceinline__ void build_nbr_body(const BinArgs& a, Blk blk) {
             }
         }
         a.nnb[t] = cnt;
-        atomicMax(&a.flags[F_MAXNB], cnt);
+    }
+    // the longest row: one atomic per warp (a per-thread atomic on this one
+    // address would serialise every thread of the grid at one L2 slice)
+    {
+        const int mx = __reduce_max_sync(0xffffffffu, t < a.n ? a.nnb[t] : 0);
+        if (lane == 0 && mx > 0) atomicMax(&a.flags[F_MAXNB], mx);
     }
     __syncwarp();
     if (lane == 0 && chunk * 32 < a.n) {

@@ -132,6 +132,10 @@ struct mfa_ctx {
     double* h_scal;                     // pinned copy of dscal and dflags (mfa_get_scalars)
     // observables (observe.cu), allocated at their first use: unfolded
     // coordinates (3 n) and 16 result slots; the z histogram and its count
+    // pair-kernel work queue: CTAs per SM (0: one CTA per block of slots) and
+    // its 64-bit ticket counter; n_sm = multiprocessors of the device
+    int pair_queue, n_sm;
+    unsigned long long* pair_qctr;
     double* obs_buf;
     // the force on each grafted head before the pin zeroes it
     // (verlet_velocities.f90:18, f_on_heads), 3 x n_chain chain-major; null
@@ -190,6 +194,7 @@ int pair_stage_args(mfa_ctx* c, int fuse_wall, void* out, int* grid_out, size_t*
 int launch_pair_grouped(int prec, int k, int block, int ft, const void* dargs, const int* doff, int nsys, int grid,
                         size_t smem, cudaStream_t st);
 int pair_set_shape(mfa_ctx* c, int tpp, int block, int tile_cap);
+int pair_set_queue(mfa_ctx* c, int ctas_per_sm);
 int pair_tile_limit(const mfa_ctx* c);
 // bonds.cu
 int launch_bonds(mfa_ctx* c, int do_fene, int do_bend);

@@ -55,6 +55,8 @@ struct PairArgs {
     unsigned* counter;
     double* dscal;
     int n, max_blocks, maxnb;
+    unsigned long long* qctr;  // work-queue tickets (untiled launches with a queue), or null
+    int qmod;                  // tickets per launch: chunks + warps of the grid
     int nb[3], rule, wy, nseg, tile_cap, rowmode;
     int half;                 // 1: half list (partner gets -f), 0: full list
     int symmetry, thermostat, dpd_weight, noise, charged, real_in_lj, fsw;
@@ -308,6 +310,10 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
                 if (need_v) bulk_g2s(tvel + pc_base[lane], (const R4*)a.vel_s + pc_start[lane], bytes, &bar);
             }
         }
+    } else if (a.qctr) {
+        p0 = 0;                  // work queue: any chunk of the system
+        p1 = a.n;
+        if (threadIdx.x == 0) { s_mode = 0; s_npc = 0; }
     } else {
         p0 = blk.id * blockDim.x;
         p1 = min(p0 + (int)blockDim.x, a.n);
@@ -437,7 +443,19 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
     // the entries whose owner lies in the row.  The lanes walk the chunk's
     // entries together, K per lane per round, whatever row they belong to.
     const long long capc = 32LL * a.maxnb;
-    for (int ch = (p0 >> 5) + warp; valid && ch < ((p1 + 31) >> 5); ch += nwarp) {
+    // the chunks of this CTA: its own range (static), or -- with the work queue
+    // of an untiled launch -- tickets from a 64-bit counter shared by the
+    // grid.  Every launch draws exactly nchunk + (warps of the grid) tickets
+    // (each warp stops at its first ticket past the chunks), so a launch starts
+    // at a multiple of that number and ticket % qmod is its chunk.
+    const bool dyn = a.qctr != nullptr;
+    int ch = (p0 >> 5) + warp;
+    if (dyn) {
+        unsigned long long tk = 0;
+        if (lane == 0) tk = atomicAdd(a.qctr, 1ull);
+        ch = (int)(__shfl_sync(0xffffffffu, tk, 0) % (unsigned long long)a.qmod);
+    }
+    for (; valid && ch < ((p1 + 31) >> 5); ) {
         const int t = (ch << 5) + lane;
         const bool act = t >= p0 && t < p1;
         R4 pi;
@@ -542,6 +560,13 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
             red_add(&f4[ii], fx, fy, fz);
         }
         __syncwarp();
+        if (dyn) {
+            unsigned long long tk = 0;
+            if (lane == 0) tk = atomicAdd(a.qctr, 1ull);
+            ch = (int)(__shfl_sync(0xffffffffu, tk, 0) % (unsigned long long)a.qmod);
+        } else {
+            ch += nwarp;
+        }
     }
     if (!EN) return;   // no energies this step: nothing to reduce
     if (WALL) {
@@ -731,7 +756,17 @@ int pair_stage_args(mfa_ctx* c, int fuse_wall, void* out, int* grid_out, size_t*
     a.a_w = p.a_w; a.z_space_wall = p.z_space_wall; a.wall_cut = p.wall_cut;
     a.seed0 = (uint32_t)p.seed; a.seed1 = (uint32_t)(p.seed >> 32);
     a.key = philox_round_keys(a.seed0, a.seed1);
-    const int grid = c->pair_tiled ? c->nb[1] * c->nb[2] : (c->n + c->pair_block - 1) / c->pair_block;
+    int grid = c->pair_tiled ? c->nb[1] * c->nb[2] : (c->n + c->pair_block - 1) / c->pair_block;
+    a.qctr = nullptr;
+    a.qmod = 0;
+    if (!c->pair_tiled && c->pair_queue > 0 && c->pair_qctr) {
+        // a fixed grid of pair_queue CTAs per SM (at most the static grid)
+        // fetching 32-slot chunks from the queue
+        const int g2 = c->pair_queue * c->n_sm;
+        if (g2 < grid) grid = g2;
+        a.qctr = c->pair_qctr;
+        a.qmod = (c->n + 31) / 32 + grid * (c->pair_block / 32);
+    }
     if (grid > c->max_blocks) return MFA_ERR_ARGS;
     const size_t smem = c->prec == MFA_MIXED ? smem_bytes<float>(c->pair_tpp, c->pair_block, cap)
                                              : smem_bytes<double>(c->pair_tpp, c->pair_block, cap);

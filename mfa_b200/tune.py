@@ -2,7 +2,8 @@
 
 A larger skin lists more pairs per particle but rebuilds the lists less often;
 the pair kernel's best shape (list entries a thread tests per round, block
-size, shared-memory tiling or not) depends on the neighbour count.  Neither
+size, shared-memory tiling or not, a work queue of a fixed number of CTAs per
+multiprocessor or not) depends on the neighbour count.  Neither
 changes the forces, so both are measured rather than assumed: each candidate
 runs a few hundred real time steps of the system (the state advances; tuning
 doubles as equilibration) and the fastest is kept.
@@ -13,8 +14,10 @@ import time
 
 import math
 
-CANDIDATES = ((2, 128, True), (4, 64, True),
-              (2, 128, False), (4, 128, False), (2, 256, False), (4, 256, False))
+# (entries per lane and round, threads per block, tiled, work-queue CTAs per SM)
+CANDIDATES = ((2, 128, True, 0), (4, 64, True, 0),
+              (2, 128, False, 0), (4, 128, False, 0), (2, 256, False, 0), (4, 256, False, 0),
+              (2, 128, False, 6), (2, 128, False, 8), (2, 256, False, 3), (2, 256, False, 4))
 SKINS = (0.2, 0.3, 0.4, 0.5, 0.6)
 
 
@@ -70,9 +73,11 @@ def tune_pair_shape(system, steps: int = 300, candidates=CANDIDATES, repeats: in
     """Time `steps` fused time steps per candidate (best of `repeats`), set the
     fastest shape on `system` and return {shape: seconds}."""
     timings = {}
-    for k, block, tiled in candidates:
+    for k, block, tiled, queue in candidates:
         system.set_pair_shape(k, block, tiled)
-        timings[(k, block, tiled)] = _time(system, steps, repeats)
-    k, block, tiled = min(timings, key=timings.get)
+        system.set_pair_queue(0 if tiled else queue)
+        timings[(k, block, tiled, queue)] = _time(system, steps, repeats)
+    k, block, tiled, queue = min(timings, key=timings.get)
     system.set_pair_shape(k, block, tiled)
+    system.set_pair_queue(0 if tiled else queue)
     return timings
