@@ -155,6 +155,62 @@ def kernel_stat(kt, key):
     return n, (t / n if n else None)
 
 
+def accuracy_vs_fp64(cfg, st, dev, steps=2000, every=100):
+    """The mixed path's reported quantities against the plain FP64 path.
+
+    At one state (the mixed run's last): the force on every bead (max-norm
+    relative error), each energy term, and the pair pressure (2 KE + W)/(3 V)
+    with W the pair virial sum r_ij . f_ij.  Along a run of `steps` steps from
+    that state in both precisions (the same Philox noise, so the two stay
+    correlated until chaos separates them): the mean squared radius of
+    gyration of the grafted chains and the brush height (mean z of the chain
+    beads), sampled every `every` steps, with the difference of the two means
+    and the standard error of the FP64 mean (block averages)."""
+    import numpy as np
+    from mfa_b200 import _abi
+    from mfa_b200.api import System
+    p = cfg.params
+    V = p.boundary[0] * p.boundary[1] * p.boundary[2]
+    chain = np.arange(cfg.n) < p.n_chain * p.n_mon
+    out, traj = {}, {}
+    for name, prec in (("fp64", _abi.FP64), ("mixed", _abi.MIXED)):
+        g = System(p, st["r0"], st["v"], cfg.a_type, cfg.mass, q=cfg.q, a=st["a"], mic=st["mic"],
+                   precision=prec, device=dev)
+        g.init_forces(full=True)
+        f = g.download(_abi.F)["force"]
+        sc = g.scalars()
+        out[name] = {"force": f, "scalars": sc,
+                     "pressure": (2.0 * sc["t_fluid"] + sc["virial"]) / (3.0 * V)}
+        rg, hz = [], []
+        for _ in range(steps // every):
+            g.step(every)
+            rg.append(float(np.sum(g.observe()["r_g2_brush"])))
+            hz.append(float(g.download(_abi.R0)["r0"][chain, 2].mean()))
+        traj[name] = (np.array(rg), np.array(hz))
+        g.close()
+    f64, f32 = out["fp64"]["force"], out["mixed"]["force"]
+    s64, s32 = out["fp64"]["scalars"], out["mixed"]["scalars"]
+    res = {"force_max_rel": float(np.abs(f32 - f64).max() / np.abs(f64).max())}
+    for k in ("v_fluid_fluid", "v_fluid_wall", "v_intra_molec", "v_bend", "v_coul", "v_total"):
+        if s64[k] != 0.0:
+            res[k + "_rel"] = abs(s32[k] - s64[k]) / abs(s64[k])
+    res["pressure_pair"] = out["fp64"]["pressure"]
+    res["pressure_pair_rel"] = abs(out["mixed"]["pressure"] - out["fp64"]["pressure"]) / abs(out["fp64"]["pressure"])
+
+    def mean_sem(x):
+        b = x[: (len(x) // 5) * 5].reshape(5, -1).mean(axis=1)
+        return float(x.mean()), float(b.std(ddof=1) / np.sqrt(5))
+
+    for key, k in (("rg2", 0), ("brush_height_mean_z", 1)):
+        m64, e64 = mean_sem(traj["fp64"][k])
+        m32, _ = mean_sem(traj["mixed"][k])
+        res[key] = {"fp64": m64, "mixed": m32, "diff": m32 - m64, "sem_fp64": e64}
+    res["note"] = (f"forces, energies and pressure at one state; rg2 (sum of the per-axis mean square radii "
+                   f"of gyration of the grafted chains) and brush height averaged over {steps} steps from it, "
+                   f"every {every}")
+    return res
+
+
 def drift(a):
     """Equilibrate with the thermostat (FP64), then run the same state without
     thermostat (NVE) in FP64 and in mixed precision and report the energy
@@ -596,6 +652,17 @@ def adjoint_bench(a):
             js.append(g.trajectory_observable(S))
             g.close()
         fd[nm] = (js[0] - js[1]) / (2 * h * base[nm])
+    # step-size study for sigma: central differences against h (truncation
+    # error falls as h^2, rounding and the chaos of a 200-step trajectory grow
+    # as h falls), the adjoint beside them
+    fd_sigma = {}
+    for hh in (1e-3, 3e-4, 1e-4, 3e-5, 1e-5, 1e-6):
+        js = []
+        for f in (1 + hh, 1 - hh):
+            g = fresh(perturbed(cfg.params, "sigma", f), _abi.FP64)
+            js.append(g.trajectory_observable(S))
+            g.close()
+        fd_sigma[f"{hh:g}"] = (js[0] - js[1]) / (2 * hh * base["sigma"])
     g64 = res["fp64"]["grad"]
     rel = {nm: abs(g64[nm] - fd[nm]) / max(abs(fd[nm]), 1e-30) for nm in NAMES}
     rel32 = {nm: abs(res["mixed"]["grad"][nm] - g64[nm]) / max(abs(g64[nm]), 1e-30) for nm in NAMES}
@@ -606,7 +673,8 @@ def adjoint_bench(a):
                    "k_bend": cfg.params.k_bend,
                    "observable": "time average of <z> + <R_ee^2>", "dt": cfg.params.dt},
         "fp64": res["fp64"], "mixed": res["mixed"], "central_differences_fp64": fd,
-        "rel_err_fp64_adjoint_vs_fd": rel, "rel_err_mixed_vs_fp64_adjoint": rel32}))
+        "rel_err_fp64_adjoint_vs_fd": rel, "rel_err_mixed_vs_fp64_adjoint": rel32,
+        "fd_step_study_sigma": {"adjoint_fp64": g64["sigma"], "central_differences": fd_sigma}}))
     return 0
 
 
@@ -829,9 +897,26 @@ def main():
                  "achieved_gbs": 124 * n / (vv_us * 1e-6) / 1e9,
                  "frac": 124 * n / (vv_us * 1e-6) / 1e9 / hbm_peak,
                  "source": "CUPTI activity records over 200 in-loop steps (L2 warm)"}
+    # Ewald k-space (charged workloads): 12 FP64 flops per (particle, k) in each
+    # of the structure-factor and force passes (canonical count)
+    ewk = None
+    if cfg.params.charged:
+        nk = int(g.kvecs().shape[0])
+        n_rho, t_rho = kernel_stat(loop_kt, "k_rho_partial")
+        n_red, t_red = kernel_stat(loop_kt, "k_rho_reduce")
+        n_ef, t_ef = kernel_stat(loop_kt, "k_ewald_force")
+        if t_rho and t_ef:
+            us = t_rho + (t_red or 0.0) + t_ef
+            flops = 2 * 12 * n * nk
+            ewk = {"bound": "fp64 pipe", "k_vectors": nk, "flops_per_step": flops,
+                   "us_per_step": us, "tflops_fp64": flops / (us * 1e-6) / 1e12,
+                   "kernels_us": {"k_rho_partial": t_rho, "k_rho_reduce": t_red, "k_ewald_force": t_ef},
+                   "peak_note": "no FP64 peak in MEASURED_PEAKS.json; B200's nominal FP64 (non-tensor) rate is "
+                                "about 37 TFLOP/s"}
     loop_total = sum(v["total_us"] for v in loop_kt.values())
     loop_share = {short_name(k): round(v["total_us"] / loop_total, 4)
                   for k, v in sorted(loop_kt.items(), key=lambda kv: -kv[1]["total_us"])[:8]} if loop_total else {}
+    st_acc = g.download()
     g.close()
 
     # plain FP64 GPU path, same protocol
@@ -839,6 +924,9 @@ def main():
     g64.close()
     ms_fp64 = max_over_ranks(ms_fp64, dist, f"cuda:{dev}")
     value_fp64 = world * n * a.steps / (ms_fp64 * 1e-3)
+
+    # the mixed path's reported quantities against the FP64 path
+    acc = accuracy_vs_fp64(cfg, st_acc, dev) if rank == 0 and a.workload == "brush" else None
 
     # end to end through the public API with host buffers
     import ctypes as C
@@ -916,6 +1004,7 @@ def main():
                          "launch_us_in_loop": pair_us_loop,
                          "fp32_tflops": pair_flops / (pair_ms * 1e-3) / 1e12, **work},
             "integration": integ,
+            "ewald_k": ewk,
             "loop_kernel_share": loop_share,
             "per_call_ms": s_mixed["per_call_ms"],
             "rebuild": {"bound": "hbm", "launch_ms": rebuild_ms, "algorithmic_bytes": 60 * n,
@@ -924,6 +1013,7 @@ def main():
                         "note": "6 kernels (cell assign, row scan, scatter, per-cell sort, gather, list build); "
                                 "60 B per bead per rebuild"},
             "e2e": e2e_obj,
+            "accuracy_vs_fp64": acc,
             "gpu_launches": int(launches),
             "list_rebuilds_in_timed_steps": int(s_mixed["rebuilds_timed"]),
             "clocks": clocks,
