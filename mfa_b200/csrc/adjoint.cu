@@ -54,6 +54,7 @@ struct AdjArgs {
     double sig, gam, eps_lj, sigma_lj;
     double sqrt_alpha, alpha_c, inv_sqrt_pi, ewald_rc_2;
     long long step;
+    const int64_t* step_ptr;      // the step of the recomputed forward pass (device), or null: step
     PhiloxKeys key;
     uint32_t seed0, seed1;
     double a_wall[T8], sigma_wall[T8], z_space_wall, wall_cut;
@@ -116,6 +117,7 @@ __global__ void k_adj_pair(AdjArgs a) {
     double gl[G_N] = {0, 0, 0, 0, 0, 0};
     const int lane = threadIdx.x & 31;
     const int ch = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long step = a.step_ptr ? *a.step_ptr : a.step;
     const R4* ps = (const R4*)a.pos_s;
     const R4* vs = (const R4*)a.vel_s;
     const R Lx = (R)a.L[0], Ly = (R)a.L[1], Lz = (R)a.L[2];
@@ -181,7 +183,7 @@ __global__ void k_adj_pair(AdjArgs a) {
                 const R sdu = dux * hx + duy * hy + duz * hz;
                 const R hdl = hx * dlx + hy * dly + hz * dlz;
                 const uint32_t lo = (uint32_t)min(ii, jj), hi = (uint32_t)max(ii, jj);
-                const uint4 ph = philox4x32_10(make_uint4(lo, hi, (uint32_t)a.step, TAG_DPD), a.key);
+                const uint4 ph = philox4x32_10(make_uint4(lo, hi, (uint32_t)step, TAG_DPD), a.key);
                 const R gn = dpd_noise(ph.x, ph.y, a.noise, R(0));
                 const R irc = sqrt((R)s_irc2[ij]);
                 R wr, wd, dwr, dwd;                  // weights and d/dr
@@ -251,7 +253,7 @@ __global__ void k_adj_pair(AdjArgs a) {
             const double m = a.mass[ii];
             const double lx = a.fx[ii], ly = a.fy[ii], lz = a.fz[ii];
             R g3[3];
-            lgv_noise3<R>((uint32_t)ii, (uint32_t)a.step, a.noise, a.seed0, a.seed1, g3);
+            lgv_noise3<R>((uint32_t)ii, (uint32_t)step, a.noise, a.seed0, a.seed1, g3);
             const double cu = -a.gam * m;
             atomicAdd(&a.ux[ii], cu * lx);
             atomicAdd(&a.uy[ii], cu * ly);
@@ -466,17 +468,20 @@ struct Work {
     int n, S, K, nseg;
     double* ck;          // checkpoints: nseg x (r, v, a) 9n doubles
     int32_t* ckm;        // checkpoints: nseg x mic 3n
-    int64_t* ckstep;     // host copy of dstep per checkpoint
-    double* seg_r;       // K x 3n (r after the position half of each step)
+    int64_t* ckstep;     // dstep per checkpoint (device, nseg)
+    double* seg_r;       // (K + 1) x 3n: r after the position half of each step; slot K: the checkpoint's r
     double* seg_u;       // K x 3n (u)
-    int32_t* seg_m;      // K x 3n (mic)
+    int32_t* seg_m;      // (K + 1) x 3n (mic; slot K: the checkpoint's)
+    int64_t* seg_step;   // K: dstep as the forces of each recomputed step saw it
     double *rho, *nu, *alpha, *lamF, *lamU, *lamR;   // 3n each
     double* dg;          // G_N + 1 (J)
 };
 
-int adj_forward_step(mfa_ctx* c, double* sr, double* su, int32_t* sm, double w, double* dJ) {
+int adj_forward_step(mfa_ctx* c, double* sr, double* su, int32_t* sm, double w, double* dJ,
+                     int64_t* sstep = nullptr) {
     const int n = c->n;
     TRY_(launch_vv_positions(c, 1, 1));
+    if (sstep) MFA_CUDA_TRY(cudaMemcpyAsync(sstep, c->dstep, 8, cudaMemcpyDeviceToDevice, c->st));
     if (sr) {
         MFA_CUDA_TRY(cudaMemcpyAsync(sr, c->rx, (size_t)3 * n * 8, cudaMemcpyDeviceToDevice, c->st));
         MFA_CUDA_TRY(cudaMemcpyAsync(su, c->vx, (size_t)3 * n * 8, cudaMemcpyDeviceToDevice, c->st));
@@ -505,24 +510,29 @@ int checkpoint_save(mfa_ctx* c, Work& w, int k) {
     MFA_CUDA_TRY(cudaMemcpyAsync(w.ck + k * 3 * n3 + n3, c->vx, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
     MFA_CUDA_TRY(cudaMemcpyAsync(w.ck + k * 3 * n3 + 2 * n3, c->ax, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
     MFA_CUDA_TRY(cudaMemcpyAsync(w.ckm + k * n3, c->mx, n3 * 4, cudaMemcpyDeviceToDevice, c->st));
-    MFA_CUDA_TRY(cudaMemcpyAsync(&w.ckstep[k], c->dstep, 8, cudaMemcpyDeviceToHost, c->st));
-    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    MFA_CUDA_TRY(cudaMemcpyAsync(w.ckstep + k, c->dstep, 8, cudaMemcpyDeviceToDevice, c->st));
     return MFA_OK;
 }
 
+// The state of checkpoint k back in the context, and its r and mic in the
+// staging slot K of the segment buffers (the observable at the segment's
+// first state).  The lists are left as they are: the first position half
+// checks the skin against the last rebuild's positions and rebuilds when due.
 int checkpoint_restore(mfa_ctx* c, Work& w, int k) {
     const size_t n3 = (size_t)3 * c->n;
     MFA_CUDA_TRY(cudaMemcpyAsync(c->rx, w.ck + k * 3 * n3, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
     MFA_CUDA_TRY(cudaMemcpyAsync(c->vx, w.ck + k * 3 * n3 + n3, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
     MFA_CUDA_TRY(cudaMemcpyAsync(c->ax, w.ck + k * 3 * n3 + 2 * n3, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
     MFA_CUDA_TRY(cudaMemcpyAsync(c->mx, w.ckm + k * n3, n3 * 4, cudaMemcpyDeviceToDevice, c->st));
-    MFA_CUDA_TRY(cudaMemcpyAsync(c->dstep, &w.ckstep[k], 8, cudaMemcpyHostToDevice, c->st));
-    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
-    // lists for the restored positions
-    return mfa_binning(c);
+    MFA_CUDA_TRY(cudaMemcpyAsync(c->dstep, w.ckstep + k, 8, cudaMemcpyDeviceToDevice, c->st));
+    MFA_CUDA_TRY(cudaMemcpyAsync(w.seg_r + (size_t)w.K * n3, w.ck + k * 3 * n3, n3 * 8, cudaMemcpyDeviceToDevice,
+                                 c->st));
+    MFA_CUDA_TRY(cudaMemcpyAsync(w.seg_m + (size_t)w.K * n3, w.ckm + k * n3, n3 * 4, cudaMemcpyDeviceToDevice,
+                                 c->st));
+    return MFA_OK;
 }
 
-AdjArgs pair_adj_args(mfa_ctx* c, Work& w, long long step) {
+AdjArgs pair_adj_args(mfa_ctx* c, Work& w, const int64_t* step_ptr) {
     const mfa_params& p = c->p;
     const int n = c->n;
     AdjArgs a;
@@ -555,7 +565,8 @@ AdjArgs pair_adj_args(mfa_ctx* c, Work& w, long long step) {
         if (p.range_2[k] > 0.0) { emax = fmax(emax, p.epsil[k] / 4.0); smax = fmax(smax, sqrt(p.sigma_2[k])); }
     a.eps_lj = emax > 0.0 ? emax : 1.0;
     a.sigma_lj = smax > 0.0 ? smax : 1.0;
-    a.step = step;
+    a.step = 0;
+    a.step_ptr = step_ptr;
     a.key = philox_round_keys((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
     for (int k = 0; k < T8; ++k) { a.a_wall[k] = p.a_wall[k]; a.sigma_wall[k] = p.sigma_wall[k]; }
     a.z_space_wall = p.z_space_wall;
@@ -600,14 +611,12 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
     Work w;
     w.n = n; w.S = nsteps; w.K = every < nsteps ? every : nsteps;
     w.nseg = (nsteps + w.K - 1) / w.K;
-    std::vector<int64_t> steps(w.nseg);
-    w.ckstep = steps.data();
-    void* bufs[9] = {nullptr};
-    size_t sizes[9] = {(size_t)w.nseg * 3 * n3 * 8, (size_t)w.nseg * n3 * 4, (size_t)w.K * n3 * 8,
-                       (size_t)w.K * n3 * 8, (size_t)w.K * n3 * 4, 6 * n3 * 8, (G_N + 1) * 8,
-                       p.charged ? ewald_adj_bytes(c) : 0, 0};
+    void* bufs[10] = {nullptr};
+    size_t sizes[10] = {(size_t)w.nseg * 3 * n3 * 8, (size_t)w.nseg * n3 * 4, (size_t)(w.K + 1) * n3 * 8,
+                        (size_t)w.K * n3 * 8, (size_t)(w.K + 1) * n3 * 4, 6 * n3 * 8, (G_N + 1) * 8,
+                        p.charged ? ewald_adj_bytes(c) : 0, (size_t)w.nseg * 8, (size_t)w.K * 8};
     int rc = MFA_OK;
-    for (int k = 0; k < 8 && rc == MFA_OK; ++k)
+    for (int k = 0; k < 10 && rc == MFA_OK; ++k)
         if (sizes[k] && cudaMalloc(&bufs[k], sizes[k]) != cudaSuccess) rc = MFA_ERR_NOMEM;
     if (rc != MFA_OK) {
         for (void* b : bufs) if (b) cudaFree(b);
@@ -615,6 +624,7 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
     }
     w.ck = (double*)bufs[0]; w.ckm = (int32_t*)bufs[1];
     w.seg_r = (double*)bufs[2]; w.seg_u = (double*)bufs[3]; w.seg_m = (int32_t*)bufs[4];
+    w.ckstep = (int64_t*)bufs[8]; w.seg_step = (int64_t*)bufs[9];
     double* adj = (double*)bufs[5];
     w.rho = adj; w.nu = adj + n3; w.alpha = adj + 2 * n3; w.lamF = adj + 3 * n3; w.lamU = adj + 4 * n3;
     w.lamR = adj + 5 * n3;
@@ -622,16 +632,123 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
     double* dJ = w.dg + G_N;
     const double dt = p.dt, wobs = 1.0 / nsteps;
     const int nb = (n + T - 1) / T;
+    if (p.charged) TRY_(ewald_adjoint_prepare(c));
+    // forward steps with the observable (segment of len steps)
+    auto fwd = [&](int len) -> int {
+        for (int j = 0; j < len; ++j) TRY_(adj_forward_step(c, nullptr, nullptr, nullptr, wobs, dJ));
+        return MFA_OK;
+    };
+    // the segment recomputed from its checkpoint, each step's r', u, mic and step kept
+    auto rec = [&](int len) -> int {
+        for (int j = 0; j < len; ++j)
+            TRY_(adj_forward_step(c, w.seg_r + j * n3, w.seg_u + j * n3, w.seg_m + j * n3, 0.0, nullptr,
+                                  w.seg_step + j));
+        return MFA_OK;
+    };
+    // backward through the segment (steps len-1 .. 0); first_seg: the
+    // segment's first state is the trajectory's start, which the observable
+    // does not count
+    auto bwd = [&](int len, bool first_seg) -> int {
+        for (int j = len - 1; j >= 0; --j) {
+            const double* r1 = w.seg_r + j * n3;
+            MFA_CUDA_TRY(cudaMemcpyAsync(c->rx, r1, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
+            MFA_CUDA_TRY(cudaMemcpyAsync(c->vx, w.seg_u + j * n3, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
+            MFA_CUDA_TRY(cudaMemcpyAsync(c->mx, w.seg_m + j * n3, n3 * 4, cudaMemcpyDeviceToDevice, c->st));
+            TRY_(launch_check_skin(c));
+            TRY_(launch_rebuild(c, c->bin_type, 1));
+            TRY_(launch_refresh_sorted(c));
+            k_adj_prep<<<nb, T, 0, c->st>>>(n, w.rho, w.nu, w.alpha, c->inv_mass, 0.5 * dt, p.pin_heads,
+                                            p.n_chain * p.n_mon, p.n_mon > 0 ? p.n_mon : 1, w.lamF, w.lamU,
+                                            w.lamR);
+            AdjArgs aa = pair_adj_args(c, w, w.seg_step + j);
+            const int nbw = ((n + 31) / 32 * 32 + T - 1) / T;   // a warp per 32-slot chunk
+            if (c->prec == MFA_MIXED) k_adj_pair<float><<<nbw, T, 0, c->st>>>(aa);
+            else k_adj_pair<double><<<nbw, T, 0, c->st>>>(aa);
+            const int nbonds = p.n_chain * (p.n_mon > 0 ? p.n_mon - 1 : 0) +
+                               (p.n_mon_d >= 2 ? p.n_chain_d * (p.n_mon_d - 1) : 0);
+            if (nbonds > 0) {
+                AdjBondArgs ba;
+                ba.px = r1; ba.py = r1 + n; ba.pz = r1 + 2 * n;
+                ba.fx = w.lamF; ba.fy = w.lamF + n; ba.fz = w.lamF + 2 * n;
+                ba.rx = w.lamR; ba.ry = w.lamR + n; ba.rz = w.lamR + 2 * n;
+                ba.g = w.dg;
+                ba.n_chain = p.n_chain; ba.n_mon = p.n_mon; ba.n_chain_d = p.n_chain_d; ba.n_mon_d = p.n_mon_d;
+                ba.part_init_d = p.n_mon * p.n_chain; ba.symmetry = p.symmetry;
+                for (int d = 0; d < 3; ++d) { ba.L[d] = p.boundary[d]; ba.invL[d] = c->inv_boundary[d]; }
+                ba.k_fene = p.k_chain * p.inv_r_chain_2;
+                ba.r0 = sqrt(p.r_chain_2);
+                ba.inv_r_chain_2 = p.inv_r_chain_2;
+                ba.fene_clamp = p.fene_clamp;
+                const int bb = (nbonds + T - 1) / T;
+                if (c->prec == MFA_MIXED) k_adj_fene<float><<<bb, T, 0, c->st>>>(ba);
+                else k_adj_fene<double><<<bb, T, 0, c->st>>>(ba);
+            }
+            if (p.bending && p.n_mon >= 3 && p.n_chain > 0) {
+                AdjBendArgs ka;
+                ka.px = r1; ka.py = r1 + n; ka.pz = r1 + 2 * n;
+                ka.fx = w.lamF; ka.fy = w.lamF + n; ka.fz = w.lamF + 2 * n;
+                ka.rx = w.lamR; ka.ry = w.lamR + n; ka.rz = w.lamR + 2 * n;
+                ka.n_chain = p.n_chain; ka.n_mon = p.n_mon;
+                for (int d = 0; d < 3; ++d) { ka.L[d] = p.boundary[d]; ka.invL[d] = c->inv_boundary[d]; }
+                ka.k_bend = p.k_bend; ka.alpha_eq = p.alpha_eq;
+                const int nang = p.n_chain * (p.n_mon - 2);
+                k_adj_bend<<<(nang + T - 1) / T, T, 0, c->st>>>(ka);
+            }
+            // Ewald k-space (and the slab correction) at r', c->rx holding r'
+            if (p.charged) TRY_(launch_ewald_adjoint(c, w.lamF, w.lamR, bufs[7]));
+            // back to the state before this step: the observable at r_s (the
+            // previous slot, or the segment's checkpoint in staging slot K)
+            const bool at_start = j == 0 && first_seg;
+            const double* r0 = j > 0 ? w.seg_r + (j - 1) * n3 : w.seg_r + (size_t)w.K * n3;
+            const int32_t* m0 = j > 0 ? w.seg_m + (j - 1) * n3 : w.seg_m + (size_t)w.K * n3;
+            k_adj_combine<<<nb, T, 0, c->st>>>(n, w.lamR, w.lamU, dt, at_start ? 0.0 : wobs, r0, m0, p.boundary[0],
+                                               p.boundary[1], p.boundary[2], p.n_chain, p.n_mon, p.pin_heads,
+                                               w.rho, w.nu, w.alpha);
+            MFA_CUDA_TRY(cudaGetLastError());
+        }
+        return MFA_OK;
+    };
+    // Full segments replay captured graphs (one per sequence); a partial last
+    // segment, and any sequence whose capture fails, runs as plain launches.
+    cudaGraphExec_t gx[4] = {nullptr, nullptr, nullptr, nullptr};
+    auto capture = [&](int which, auto&& fn) -> void {
+        cudaGraph_t gr = nullptr;
+        if (cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return;
+        const int r = fn();
+        if (cudaStreamEndCapture(c->st, &gr) != cudaSuccess || r != MFA_OK || !gr) {
+            if (gr) cudaGraphDestroy(gr);
+            cudaGetLastError();
+            return;
+        }
+        if (cudaGraphInstantiate(&gx[which], gr, 0) != cudaSuccess) gx[which] = nullptr;
+        cudaGraphDestroy(gr);
+        cudaGetLastError();
+    };
+    auto replay = [&](int which, auto&& fn) -> int {
+        if (gx[which]) {
+            MFA_CUDA_TRY(cudaGraphLaunch(gx[which], c->st));
+            return MFA_OK;
+        }
+        return fn();
+    };
+    const bool full_last = nsteps % w.K == 0;
+    if (w.nseg > 1 || full_last) {
+        capture(0, [&] { return fwd(w.K); });
+        capture(1, [&] { return rec(w.K); });
+        capture(2, [&] { return bwd(w.K, false); });
+        capture(3, [&] { return bwd(w.K, true); });
+    }
     auto run = [&]() -> int {
         TRY_(mfa_sync(c));
         MFA_CUDA_TRY(cudaMemsetAsync(w.dg, 0, (G_N + 1) * 8, c->st));
         MFA_CUDA_TRY(cudaMemsetAsync(adj, 0, 6 * n3 * 8, c->st));
         // forward pass with checkpoints and the observable
-        for (int s = 0; s < nsteps; ++s) {
-            if (s % w.K == 0) TRY_(checkpoint_save(c, w, s / w.K));
-            TRY_(adj_forward_step(c, nullptr, nullptr, nullptr, wobs, dJ));
+        for (int seg = 0; seg < w.nseg; ++seg) {
+            const int len = seg * w.K + w.K <= nsteps ? w.K : nsteps - seg * w.K;
+            TRY_(checkpoint_save(c, w, seg));
+            if (len == w.K) TRY_(replay(0, [&] { return fwd(len); }));
+            else TRY_(fwd(len));
         }
-        TRY_(mfa_sync(c));
         // rho_S = 1/S dO/dr_S (nu_S = alpha_S = 0)
         k_adj_combine<<<nb, T, 0, c->st>>>(n, w.lamR, w.lamU, dt, wobs, c->rx, c->mx, p.boundary[0], p.boundary[1],
                                            p.boundary[2], p.n_chain, p.n_mon, p.pin_heads, w.rho, w.nu, w.alpha);
@@ -648,72 +765,14 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
         MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
         // backward, segment by segment
         for (int seg = w.nseg - 1; seg >= 0; --seg) {
-            const int s0 = seg * w.K, s1 = s0 + w.K < nsteps ? s0 + w.K : nsteps;
+            const int len = seg * w.K + w.K <= nsteps ? w.K : nsteps - seg * w.K;
             TRY_(checkpoint_restore(c, w, seg));
-            for (int s = s0; s < s1; ++s)
-                TRY_(adj_forward_step(c, w.seg_r + (s - s0) * n3, w.seg_u + (s - s0) * n3, w.seg_m + (s - s0) * n3,
-                                      0.0, nullptr));
-            for (int s = s1 - 1; s >= s0; --s) {
-                // the state after the position half of step s+1 (1-based step s0_step + s - s0 + 1)
-                const double* r1 = w.seg_r + (s - s0) * n3;
-                MFA_CUDA_TRY(cudaMemcpyAsync(c->rx, r1, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
-                MFA_CUDA_TRY(cudaMemcpyAsync(c->vx, w.seg_u + (s - s0) * n3, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
-                MFA_CUDA_TRY(cudaMemcpyAsync(c->mx, w.seg_m + (s - s0) * n3, n3 * 4, cudaMemcpyDeviceToDevice, c->st));
-                TRY_(launch_check_skin(c));
-                TRY_(launch_rebuild(c, c->bin_type, 1));
-                TRY_(launch_refresh_sorted(c));
-                k_adj_prep<<<nb, T, 0, c->st>>>(n, w.rho, w.nu, w.alpha, c->inv_mass, 0.5 * dt, p.pin_heads,
-                                                p.n_chain * p.n_mon, p.n_mon > 0 ? p.n_mon : 1, w.lamF, w.lamU,
-                                                w.lamR);
-                const long long step = (long long)w.ckstep[seg] + (s - s0) + 1;
-                AdjArgs aa = pair_adj_args(c, w, step);
-                const int nbw = ((n + 31) / 32 * 32 + T - 1) / T;   // a warp per 32-slot chunk
-                if (c->prec == MFA_MIXED) k_adj_pair<float><<<nbw, T, 0, c->st>>>(aa);
-                else k_adj_pair<double><<<nbw, T, 0, c->st>>>(aa);
-                const int nbonds = p.n_chain * (p.n_mon > 0 ? p.n_mon - 1 : 0) +
-                                   (p.n_mon_d >= 2 ? p.n_chain_d * (p.n_mon_d - 1) : 0);
-                if (nbonds > 0) {
-                    AdjBondArgs ba;
-                    ba.px = r1; ba.py = r1 + n; ba.pz = r1 + 2 * n;
-                    ba.fx = w.lamF; ba.fy = w.lamF + n; ba.fz = w.lamF + 2 * n;
-                    ba.rx = w.lamR; ba.ry = w.lamR + n; ba.rz = w.lamR + 2 * n;
-                    ba.g = w.dg;
-                    ba.n_chain = p.n_chain; ba.n_mon = p.n_mon; ba.n_chain_d = p.n_chain_d; ba.n_mon_d = p.n_mon_d;
-                    ba.part_init_d = p.n_mon * p.n_chain; ba.symmetry = p.symmetry;
-                    for (int d = 0; d < 3; ++d) { ba.L[d] = p.boundary[d]; ba.invL[d] = c->inv_boundary[d]; }
-                    ba.k_fene = p.k_chain * p.inv_r_chain_2;
-                    ba.r0 = sqrt(p.r_chain_2);
-                    ba.inv_r_chain_2 = p.inv_r_chain_2;
-                    ba.fene_clamp = p.fene_clamp;
-                    const int bb = (nbonds + T - 1) / T;
-                    if (c->prec == MFA_MIXED) k_adj_fene<float><<<bb, T, 0, c->st>>>(ba);
-                    else k_adj_fene<double><<<bb, T, 0, c->st>>>(ba);
-                }
-                if (p.bending && p.n_mon >= 3 && p.n_chain > 0) {
-                    AdjBendArgs ka;
-                    ka.px = r1; ka.py = r1 + n; ka.pz = r1 + 2 * n;
-                    ka.fx = w.lamF; ka.fy = w.lamF + n; ka.fz = w.lamF + 2 * n;
-                    ka.rx = w.lamR; ka.ry = w.lamR + n; ka.rz = w.lamR + 2 * n;
-                    ka.n_chain = p.n_chain; ka.n_mon = p.n_mon;
-                    for (int d = 0; d < 3; ++d) { ka.L[d] = p.boundary[d]; ka.invL[d] = c->inv_boundary[d]; }
-                    ka.k_bend = p.k_bend; ka.alpha_eq = p.alpha_eq;
-                    const int nang = p.n_chain * (p.n_mon - 2);
-                    k_adj_bend<<<(nang + T - 1) / T, T, 0, c->st>>>(ka);
-                }
-                // Ewald k-space (and the slab correction) at r', c->rx holding r'
-                if (p.charged) TRY_(launch_ewald_adjoint(c, w.lamF, w.lamR, bufs[7]));
-                // back to the state before step s+1: the observable at r_s (s >= 1)
-                const double* r0 = s > s0 ? w.seg_r + (s - s0 - 1) * n3 : nullptr;
-                const int32_t* m0 = s > s0 ? w.seg_m + (s - s0 - 1) * n3 : nullptr;
-                if (s == s0 && s > 0) {
-                    // r_s is the segment's checkpoint
-                    r0 = w.ck + seg * 3 * n3;
-                    m0 = w.ckm + seg * n3;
-                }
-                k_adj_combine<<<nb, T, 0, c->st>>>(n, w.lamR, w.lamU, dt, r0 ? wobs : 0.0, r0 ? r0 : c->rx,
-                                                   m0 ? m0 : c->mx, p.boundary[0], p.boundary[1], p.boundary[2],
-                                                   p.n_chain, p.n_mon, p.pin_heads, w.rho, w.nu, w.alpha);
-                MFA_CUDA_TRY(cudaGetLastError());
+            if (len == w.K) {
+                TRY_(replay(1, [&] { return rec(len); }));
+                TRY_(replay(seg == 0 ? 3 : 2, [&] { return bwd(len, seg == 0); }));
+            } else {
+                TRY_(rec(len));
+                TRY_(bwd(len, seg == 0));
             }
         }
         // leave the context at the end of the trajectory, as mfa_step would
@@ -734,6 +793,7 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
     };
     rc = run();
     cudaStreamSynchronize(c->st);
+    for (cudaGraphExec_t g : gx) if (g) cudaGraphExecDestroy(g);
     for (void* b : bufs) if (b) cudaFree(b);
     return rc;
 }

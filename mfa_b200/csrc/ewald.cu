@@ -446,6 +446,17 @@ __global__ void k_dipole_adj(EwArgs a, const double* __restrict__ sum, double* o
 
 }  // namespace
 
+// the adjoint kernels' shared-memory limits, set once before any launch or capture
+int ewald_adjoint_prepare(mfa_ctx* c) {
+    (void)c;
+    const int fsm = FT * 3 * (KM + 1) * (int)sizeof(double2);
+    const int rsm = CH * (3 * (KM + 1) * (int)sizeof(double2) + (int)sizeof(double));
+    MFA_CUDA_TRY(cudaFuncSetAttribute(k_sig_partial, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      rsm + CH * 3 * (int)sizeof(double)));
+    MFA_CUDA_TRY(cudaFuncSetAttribute(k_ewald_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+    return MFA_OK;
+}
+
 size_t ewald_adj_bytes(const mfa_ctx* c) { return (size_t)(c->nk > 0 ? c->nk : 1) * sizeof(double2) + 64; }
 
 int launch_ewald_adjoint(mfa_ctx* c, const double* lam, double* out, void* scratch) {
@@ -454,11 +465,7 @@ int launch_ewald_adjoint(mfa_ctx* c, const double* lam, double* out, void* scrat
     EwArgs a = make_args(c);
     double2* sig = (double2*)scratch;
     double* dsum = (double*)((char*)scratch + (size_t)c->nk * sizeof(double2));
-    const int fsm = FT * 3 * (KM + 1) * (int)sizeof(double2);
-    const int rsm = CH * (3 * (KM + 1) * (int)sizeof(double2) + (int)sizeof(double));
-    MFA_CUDA_TRY(cudaFuncSetAttribute(k_sig_partial, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      rsm + CH * 3 * (int)sizeof(double)));
-    MFA_CUDA_TRY(cudaFuncSetAttribute(k_ewald_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+
     const dim3 rgrid(c->nblk_rho, (c->nk + KPT * RHO_T - 1) / (KPT * RHO_T));
     // rho_k at the current positions, then sigma_k, then the product
     k_rho_partial<<<rgrid, RHO_T, rho_smem(c), c->st>>>(a);

@@ -209,6 +209,7 @@ int launch_dipolar(mfa_ctx* c);
 // adjoint of the k-space force and of the slab correction: out += (dF/dr)^T lam
 // (lam, out: 3 x n, particle order); scratch of ewald_adj_bytes(c) bytes
 size_t ewald_adj_bytes(const mfa_ctx* c);
+int ewald_adjoint_prepare(mfa_ctx* c);
 int launch_ewald_adjoint(mfa_ctx* c, const double* lam, double* out, void* scratch);
 // terms.cu: the velocity half of verlet_velocities under DPD_VV
 int launch_dpd_vv_kick(mfa_ctx* c);
