@@ -60,6 +60,8 @@ def args_():
     ap.add_argument("--wall-cut", type=float, default=None,
                     help="9-3 wall cutoff of the brush workload for --drift (default: the configuration's "
                          "2.5; 0: no cutoff, the reference's uncut wall)")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                    help="precision of the --kernel-times run")
     ap.add_argument("--kernel-times", action="store_true",
                     help="device time of every kernel inside the time-step loop (CUPTI through the torch "
                          "profiler, no serialisation), per step; not a throughput run")
@@ -79,7 +81,8 @@ def kernel_times(a):
     from mfa_b200.api import System
     from mfa_b200.tune import autotune
     cfg, meta = make_config(a.workload, a.seed)
-    g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=_abi.MIXED, device=0)
+    prec = _abi.FP64 if a.precision == "fp64" else _abi.MIXED
+    g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=prec, device=0)
     if cfg.params.charged:
         g.ewald_k(0)
     g.init_forces()
@@ -106,7 +109,8 @@ def kernel_times(a):
     rows = [{"kernel": k, "launches": n, "total_us": round(t, 1), "mean_us": round(t / n, 2),
              "us_per_step": round(t / steps, 2), "share": round(t / total, 4)}
             for k, (n, t) in sorted(agg.items(), key=lambda kv: -kv[1][1])]
-    print(json.dumps({"workload": meta["workload"], "beads": cfg.n, "steps": steps, "chunk": a.chunk,
+    print(json.dumps({"workload": meta["workload"], "precision": a.precision, "beads": cfg.n, "steps": steps,
+                      "chunk": a.chunk,
                       "skin": g.params.skin, "n_bin": list(g.params.n_bin),
                       "list_rebuilds": s1["n_rebuilds"] - s0["n_rebuilds"],
                       "kernel_us_per_step": round(total / steps, 2), "kernels": rows}))

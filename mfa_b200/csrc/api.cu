@@ -488,6 +488,11 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
         m3[2 * n + i] = q ? q[i] : 0.0;
         if (q) vself = vself - q[i] * q[i];
     }
+    c->uniform_mass = 1;
+    for (int i = 1; i < n; ++i)
+        if (mass[i] != mass[0]) { c->uniform_mass = 0; break; }
+    c->umass = n > 0 ? mass[0] : 1.0;
+    c->uinv_mass = 1.0 / c->umass;
     c->v_coul_self = p->charged ? vself * p->sqrt_alpha / sqrt(p->pi) : 0.0;   // init_config.f90:235-239
     std::vector<double> tabs((size_t)6 * T8 * T8);
     // list criterion: range_2 + skin_2 (binning.f90:104); with the real-space

@@ -19,6 +19,8 @@ struct VVArgs {
     const int32_t* type;
     const double* q;
     const double *mass, *inv_mass;
+    int uniform_mass;             // every particle has mass umass (no per-particle loads)
+    double umass, uinv_mass;
     void* pos_s;
     void* vel_s;
     void* force;
@@ -152,7 +154,7 @@ __device__ __forceinline__ double velocity_half(const VVArgs& a, int i, double& 
         fi.z += fb[2];
         if (store_force) f[i] = fi;
     }
-    const double im = a.inv_mass[i];
+    const double im = a.uniform_mass ? a.uinv_mass : a.inv_mass[i];
     const double hdt = 0.5 * a.dt;
     ax = __dmul_rn((double)fi.x, im);
     ay = __dmul_rn((double)fi.y, im);
@@ -176,7 +178,7 @@ __device__ __forceinline__ double velocity_half(const VVArgs& a, int i, double& 
         R4 z4; z4.x = 0; z4.y = 0; z4.z = 0; z4.w = 0;
         f[i] = z4;
     }
-    const double m = a.mass[i];
+    const double m = a.uniform_mass ? a.umass : a.mass[i];
     return __dmul_rn(m, __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz)));
 }
 
@@ -316,6 +318,7 @@ VVArgs make_args(mfa_ctx* c) {
     a.omx = c->omx; a.omy = c->omy; a.omz = c->omz;
     a.slot = c->slot; a.type = c->type; a.q = c->p.charged ? c->q : nullptr;
     a.mass = c->mass; a.inv_mass = c->inv_mass;
+    a.uniform_mass = c->uniform_mass; a.umass = c->umass; a.uinv_mass = c->uinv_mass;
     a.pos_s = c->pos_s; a.vel_s = c->vel_s; a.force = c->force;
     a.flags = c->dflags; a.dstep = c->dstep;
     a.partials = c->partials + (size_t)R_VV * 4 * c->max_blocks;

@@ -66,6 +66,10 @@ struct mfa_ctx {
     int32_t *mx, *my, *mz, *omx, *omy, *omz;
     int32_t* type;
     double *mass, *inv_mass, *q;
+    // every particle has the same mass (then the integrator takes it from its
+    // arguments instead of streaming two arrays): its value and inverse
+    int uniform_mass;
+    double umass, uinv_mass;
     void* force;                        // float4 / double4 [n]
     void* pos_s;                        // float4 / double4 [n]
     void* vel_s;                        // float4 / double4 [n]
