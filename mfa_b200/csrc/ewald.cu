@@ -10,10 +10,16 @@
 //                    axis by a complex power recurrence from one sincos per axis,
 //                    and every thread accumulates a fixed set of k in registers
 //                    (12 FP64 flops per (particle, k)).  Partials per block.
-//   k_rho_reduce   - sums the block partials in block order (deterministic) and
-//                    the energy 4 pi / V sum_k inv_k2 exp(-k2/4a) |rho|^2.
-//   k_ewald_force  - thread per particle, the same per-axis tables in shared
-//                    memory, F_i = -8 pi q_i / V sum_k k inv_k2 exp(..) (cos Im - sin Re).
+//   k_rho_reduce   - a warp per k sums the block partials (each lane a fixed
+//                    stride of blocks, then a fixed shuffle tree: deterministic)
+//                    and the energy 4 pi / V sum_k inv_k2 exp(-k2/4a) |rho|^2.
+//   k_ewald_force  - 32 particles per block, 8 threads per particle, each over
+//                    every 8th k-vector (the particles' per-axis tables in
+//                    shared memory), the 8 partial forces summed by a fixed
+//                    shuffle tree: F_i = -8 pi q_i / V sum_k k inv_k2 exp(..)
+//                    (cos Im - sin Re).
+// Both k-space passes visit the charged particles only (a list made once by
+// ewald_k(0)): the others contribute nothing to rho and feel no k-space force.
 // Slab correction (dipolar_correction.f90, SYMMETRY 0):
 //   k_dipole_moment - M_z = sum_i q_i (z_i - Lz/2), a deterministic grid
 //                     reduction, and the energy 2 pi M_z^2 / V;
@@ -30,10 +36,14 @@ constexpr int RHO_T = 512;    // threads per block in k_rho_partial
 constexpr int KPT = 8;        // k per thread: a block row covers KPT * RHO_T vectors
 constexpr int NK_MAX = 1 << 16;   // k-vectors of one context
 constexpr int CH = 32;        // particles per table batch
-constexpr int FT = 64;        // threads per block in k_ewald_force
+constexpr int FT = 64;        // threads per block in k_ewald_adj
+constexpr int FP = 32;        // particles per block in k_ewald_force
+constexpr int FS = 8;         // threads per particle in k_ewald_force (k-vector stride)
 
 struct EwArgs {
     const double *rx, *ry, *rz, *q;
+    const int* qidx;          // the charged particles
+    int nq;
     const double4* kvec;      // kx, ky, kz, inv_k2 * exp(-k2 fac_alpha)
     const int4* kn;           // nx, ny, nz
     double2* rho_part;
@@ -85,7 +95,7 @@ __device__ __forceinline__ double2 phase_from(const double2* t, int ts, int4 kn)
 __global__ void __launch_bounds__(RHO_T) k_rho_partial(EwArgs a) {
     extern __shared__ double2 rtab[];
     double* sq = (double*)(rtab + CH * 3 * a.ts);
-    const int p0 = blockIdx.x * a.per_blk, p1 = min(a.n, p0 + a.per_blk);
+    const int p0 = blockIdx.x * a.per_blk, p1 = min(a.nq, p0 + a.per_blk);
     const int kb = blockIdx.y * KPT * RHO_T;
     double2 acc[KPT];
     int4 kn[KPT];
@@ -99,7 +109,7 @@ __global__ void __launch_bounds__(RHO_T) k_rho_partial(EwArgs a) {
         const int nb = min(CH, p1 - b0);
         __syncthreads();
         if (threadIdx.x < nb) {
-            const int i = b0 + threadIdx.x;
+            const int i = a.qidx[b0 + threadIdx.x];
             build_tables(rtab + threadIdx.x * 3 * a.ts, a, a.rx[i], a.ry[i], a.rz[i]);
             sq[threadIdx.x] = a.q[i];
         }
@@ -121,43 +131,80 @@ __global__ void __launch_bounds__(RHO_T) k_rho_partial(EwArgs a) {
     }
 }
 
+// the partials of one k summed by a warp: lane l takes blocks l, l+32, ...,
+// then a fixed shuffle tree (the same order every call)
+__device__ __forceinline__ double2 warp_sum_partials(const double2* part, int nblk, int nk, int k, int lane) {
+    double2 s = make_double2(0.0, 0.0);
+    for (int b = lane; b < nblk; b += 32) {
+        const double2 v = part[(size_t)b * nk + k];
+        s.x += v.x;
+        s.y += v.y;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s.x += __shfl_down_sync(0xffffffffu, s.x, o);
+        s.y += __shfl_down_sync(0xffffffffu, s.y, o);
+    }
+    return s;
+}
+
+// warps over k with a grid stride (the grid is capped at the context's
+// partial-sum slots); each warp's energy terms summed in its lane 0
 __global__ void k_rho_reduce(EwArgs a) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
     double acc[1] = {0.0};
-    if (k < a.nk) {
-        double2 s = make_double2(0.0, 0.0);
-        for (int b = 0; b < a.nblk; ++b) {
-            const double2 v = a.rho_part[(size_t)b * a.nk + k];
-            s.x += v.x;
-            s.y += v.y;
+    for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < a.nk; k += nw) {
+        const double2 s = warp_sum_partials(a.rho_part, a.nblk, a.nk, k, lane);
+        if (lane == 0) {
+            a.rho[k] = s;
+            acc[0] += a.kvec[k].w * (s.x * s.x + s.y * s.y);   // ewald_k.f90:155-156
         }
-        a.rho[k] = s;
-        acc[0] = a.kvec[k].w * (s.x * s.x + s.y * s.y);   // ewald_k.f90:155-156
     }
     if (block_sum_commit<1>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_TMP0 + 2) && threadIdx.x == 0)
         a.dscal[S_VCK] = ((a.dscal[S_TMP0 + 2] * 4.0) * a.pi) * a.inv_V;   // :159
 }
 
 template <typename R4>
-__global__ void __launch_bounds__(FT) k_ewald_force(EwArgs a) {
+__global__ void __launch_bounds__(FP * FS) k_ewald_force(EwArgs a) {
     extern __shared__ double2 ftab[];
-    double2* t = ftab + threadIdx.x * 3 * a.ts;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
-    const double qi = a.q[i];
-    if (qi == 0.0) return;
-    build_tables(t, a, a.rx[i], a.ry[i], a.rz[i]);
-    double fx = 0.0, fy = 0.0, fz = 0.0;
-    for (int k = 0; k < a.nk; ++k) {
-        const double2 e = phase_from(t, a.ts, __ldg(&a.kn[k]));
-        const double2 r = __ldg(&a.rho[k]);
-        const double4 kv = ldg4(&a.kvec[k]);
-        const double sc = (e.x * r.y - e.y * r.x) * kv.w;   // (cos Im - sin Re) inv_k2 exp()
-        fx += kv.x * sc;
-        fy += kv.y * sc;
-        fz += kv.z * sc;
+    const int p = threadIdx.x / FS, sl = threadIdx.x % FS;
+    const int slot = blockIdx.x * FP + p;
+    const bool act = slot < a.nq;
+    const int i = act ? a.qidx[slot] : 0;
+    double2* t = ftab + p * 3 * a.ts;
+    // the particle's three per-axis tables, one axis per thread (sl < 3)
+    if (act && sl < 3) {
+        const double r = sl == 0 ? a.rx[i] : (sl == 1 ? a.ry[i] : a.rz[i]);
+        double s, c;
+        sincos(a.dk[sl] * r, &s, &c);
+        const double2 e1 = make_double2(c, s);
+        double2 e = make_double2(1.0, 0.0);
+        t[sl * a.ts] = e;
+        for (int n = 1; n <= a.kmax[sl]; ++n) {
+            e = cmul(e, e1);
+            t[sl * a.ts + n] = e;
+        }
     }
-    const double pre = ((-8.0 * a.pi) * qi) * a.inv_V;   // ewald_k.f90:194
+    __syncthreads();
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    if (act)
+        for (int k = sl; k < a.nk; k += FS) {
+            const double2 e = phase_from(t, a.ts, __ldg(&a.kn[k]));
+            const double2 r = __ldg(&a.rho[k]);
+            const double4 kv = ldg4(&a.kvec[k]);
+            const double sc = (e.x * r.y - e.y * r.x) * kv.w;   // (cos Im - sin Re) inv_k2 exp()
+            fx += kv.x * sc;
+            fy += kv.y * sc;
+            fz += kv.z * sc;
+        }
+    // the FS partial sums of a particle: adjacent lanes, fixed tree
+    for (int o = FS / 2; o > 0; o >>= 1) {
+        fx += __shfl_down_sync(0xffffffffu, fx, o, FS);
+        fy += __shfl_down_sync(0xffffffffu, fy, o, FS);
+        fz += __shfl_down_sync(0xffffffffu, fz, o, FS);
+    }
+    if (!act || sl != 0) return;
+    const double pre = ((-8.0 * a.pi) * a.q[i]) * a.inv_V;   // ewald_k.f90:194
     R4* f4 = (R4*)a.force;
     R4 o = f4[i];
     o.x += pre * fx;
@@ -173,19 +220,27 @@ int table_stride(const mfa_ctx* c) {
     return m + 1;
 }
 size_t rho_smem(const mfa_ctx* c) { return (size_t)CH * (3 * table_stride(c) * sizeof(double2) + sizeof(double)); }
-size_t force_smem(const mfa_ctx* c) { return (size_t)FT * 3 * table_stride(c) * sizeof(double2); }
+// blocks of 8 warps over the k-vectors, at most one per partial-sum slot
+int reduce_grid(const mfa_ctx* c) {
+    int g = (c->nk + 7) / 8;
+    if (g > c->max_blocks) g = c->max_blocks;
+    return g < 1 ? 1 : g;
+}
+size_t force_smem(const mfa_ctx* c) { return (size_t)FP * 3 * table_stride(c) * sizeof(double2); }
+size_t adj_smem(const mfa_ctx* c) { return (size_t)FT * 3 * table_stride(c) * sizeof(double2); }
 
 EwArgs make_args(mfa_ctx* c) {
     EwArgs a;
     a.rx = c->rx; a.ry = c->ry; a.rz = c->rz; a.q = c->q;
     a.kvec = c->kvec; a.kn = (const int4*)(c->kvec + c->nk);
     a.rho_part = c->rho_part; a.rho = c->rho; a.force = c->force;
+    a.qidx = c->qidx; a.nq = c->nq;
     a.partials = c->partials + (size_t)R_EWALD * 4 * c->max_blocks;
     a.counter = c->counters + R_EWALD;
     a.dscal = c->dscal;
     a.max_blocks = c->max_blocks;
     a.n = c->n; a.nk = c->nk; a.nblk = c->nblk_rho;
-    a.per_blk = (c->n + c->nblk_rho - 1) / c->nblk_rho;
+    a.per_blk = (c->nq + c->nblk_rho - 1) / c->nblk_rho;
     const mfa_params& p = c->p;
     for (int d = 0; d < 3; ++d) a.kmax[d] = c->kmax[d];
     a.ts = table_stride(c);
@@ -254,7 +309,23 @@ int ewald_setup(mfa_ctx* c) {
     MFA_CUDA_TRY(cudaMemcpyAsync(c->kvec, kv.data(), kv.size() * sizeof(double4), cudaMemcpyHostToDevice, c->st));
     MFA_CUDA_TRY(cudaMemcpyAsync(c->kvec + c->nk, kn.data(), kn.size() * sizeof(int4), cudaMemcpyHostToDevice, c->st));
     MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
-    int nblk = (c->n + CH - 1) / CH;
+    // the charged particles, in id order
+    {
+        std::vector<double> qh(c->n);
+        MFA_CUDA_TRY(cudaMemcpyAsync(qh.data(), c->q, (size_t)c->n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+        std::vector<int> idx;
+        for (int i = 0; i < c->n; ++i)
+            if (qh[i] != 0.0) idx.push_back(i);
+        if (c->qidx) cudaFree(c->qidx);
+        c->qidx = nullptr;
+        c->nq = (int)idx.size();
+        MFA_CUDA_TRY(cudaMalloc(&c->qidx, (idx.size() + 1) * sizeof(int)));
+        if (!idx.empty())
+            MFA_CUDA_TRY(cudaMemcpyAsync(c->qidx, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice, c->st));
+        MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    }
+    int nblk = (c->nq + CH - 1) / CH;
     if (nblk > 2 * 148) nblk = 2 * 148;
     if (nblk < 1) nblk = 1;
     c->nblk_rho = nblk;
@@ -262,7 +333,7 @@ int ewald_setup(mfa_ctx* c) {
     MFA_CUDA_TRY(cudaMalloc(&c->rho_part, (size_t)nblk * c->nk * sizeof(double2)));
     // the attribute is per function and shared by every context: admit the
     // largest tables any context can have (a launch passes its own size)
-    const int fsm = FT * 3 * (KM + 1) * (int)sizeof(double2);
+    const int fsm = FP * 3 * (KM + 1) * (int)sizeof(double2);
     const int rsm = CH * (3 * (KM + 1) * (int)sizeof(double2) + (int)sizeof(double));
     MFA_CUDA_TRY(cudaFuncSetAttribute(k_ewald_force<float4>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
     MFA_CUDA_TRY(cudaFuncSetAttribute(k_ewald_force<double4>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
@@ -276,10 +347,13 @@ int launch_ewald(mfa_ctx* c) {
     EwArgs a = make_args(c);
     const dim3 rgrid(c->nblk_rho, (c->nk + KPT * RHO_T - 1) / (KPT * RHO_T));
     k_rho_partial<<<rgrid, RHO_T, rho_smem(c), c->st>>>(a);
-    k_rho_reduce<<<(c->nk + 255) / 256, 256, 0, c->st>>>(a);
+    k_rho_reduce<<<reduce_grid(c), 256, 0, c->st>>>(a);
     const size_t fsm = force_smem(c);
-    if (c->prec == MFA_MIXED) k_ewald_force<float4><<<(c->n + FT - 1) / FT, FT, fsm, c->st>>>(a);
-    else k_ewald_force<double4><<<(c->n + FT - 1) / FT, FT, fsm, c->st>>>(a);
+    const int fgrid = (c->nq + FP - 1) / FP;
+    if (fgrid > 0) {
+        if (c->prec == MFA_MIXED) k_ewald_force<float4><<<fgrid, FP * FS, fsm, c->st>>>(a);
+        else k_ewald_force<double4><<<fgrid, FP * FS, fsm, c->st>>>(a);
+    }
     MFA_CUDA_TRY(cudaGetLastError());
     note_launch(c, 3);
     return MFA_OK;
@@ -345,7 +419,7 @@ __global__ void __launch_bounds__(RHO_T) k_sig_partial(EwArgs a, const double* _
     extern __shared__ double2 rtab[];
     double* sq = (double*)(rtab + CH * 3 * a.ts);
     double* sl = sq + CH;                      // CH x 3 adjoint vectors
-    const int p0 = blockIdx.x * a.per_blk, p1 = min(a.n, p0 + a.per_blk);
+    const int p0 = blockIdx.x * a.per_blk, p1 = min(a.nq, p0 + a.per_blk);
     const int kb = blockIdx.y * KPT * RHO_T;
     double2 acc[KPT];
     int4 kn[KPT];
@@ -362,7 +436,7 @@ __global__ void __launch_bounds__(RHO_T) k_sig_partial(EwArgs a, const double* _
         const int nb = min(CH, p1 - b0);
         __syncthreads();
         if (threadIdx.x < nb) {
-            const int i = b0 + threadIdx.x;
+            const int i = a.qidx[b0 + threadIdx.x];
             build_tables(rtab + threadIdx.x * 3 * a.ts, a, a.rx[i], a.ry[i], a.rz[i]);
             sq[threadIdx.x] = a.q[i];
             sl[3 * threadIdx.x] = lam[i];
@@ -389,15 +463,12 @@ __global__ void __launch_bounds__(RHO_T) k_sig_partial(EwArgs a, const double* _
 }
 
 __global__ void k_sig_reduce(EwArgs a, double2* sig) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= a.nk) return;
-    double2 s = make_double2(0.0, 0.0);
-    for (int b = 0; b < a.nblk; ++b) {
-        const double2 v = a.rho_part[(size_t)b * a.nk + k];
-        s.x += v.x;
-        s.y += v.y;
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < a.nk; k += nw) {
+        const double2 s = warp_sum_partials(a.rho_part, a.nblk, a.nk, k, lane);
+        if (lane == 0) sig[k] = s;
     }
-    sig[k] = s;
 }
 
 __global__ void __launch_bounds__(FT) k_ewald_adj(EwArgs a, const double2* __restrict__ sig,
@@ -469,11 +540,11 @@ int launch_ewald_adjoint(mfa_ctx* c, const double* lam, double* out, void* scrat
     const dim3 rgrid(c->nblk_rho, (c->nk + KPT * RHO_T - 1) / (KPT * RHO_T));
     // rho_k at the current positions, then sigma_k, then the product
     k_rho_partial<<<rgrid, RHO_T, rho_smem(c), c->st>>>(a);
-    k_rho_reduce<<<(c->nk + 255) / 256, 256, 0, c->st>>>(a);
+    k_rho_reduce<<<reduce_grid(c), 256, 0, c->st>>>(a);
     const size_t ssm = rho_smem(c) + (size_t)CH * 3 * sizeof(double);
     k_sig_partial<<<rgrid, RHO_T, ssm, c->st>>>(a, lam);
-    k_sig_reduce<<<(c->nk + 255) / 256, 256, 0, c->st>>>(a, sig);
-    k_ewald_adj<<<(c->n + FT - 1) / FT, FT, force_smem(c), c->st>>>(a, sig, lam, out);
+    k_sig_reduce<<<reduce_grid(c), 256, 0, c->st>>>(a, sig);
+    k_ewald_adj<<<(c->n + FT - 1) / FT, FT, adj_smem(c), c->st>>>(a, sig, lam, out);
     if (c->p.symmetry == 0) {
         const int T = 256, nb = (c->n + T - 1) / T;
         MFA_CUDA_TRY(cudaMemsetAsync(dsum, 0, sizeof(double), c->st));

@@ -103,6 +103,8 @@ struct mfa_ctx {
     double2* rho;                       // nk
     double2* rho_part;                  // nblk_rho x nk
     int nblk_rho;
+    int* qidx;                          // ids of the charged particles (k-space sums skip the rest)
+    int nq;
     int kmax[3];
     double inv_V, v_coul_self;
     // host-side bookkeeping
