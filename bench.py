@@ -62,6 +62,9 @@ def args_():
                          "2.5; 0: no cutoff, the reference's uncut wall)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="precision of the --kernel-times run")
+    ap.add_argument("--fixed-skin", type=float, default=None,
+                    help="--kernel-times: this skin (and the finest cells for it) after the autotuner, so that "
+                         "two builds are compared at equal list lengths")
     ap.add_argument("--kernel-times", action="store_true",
                     help="device time of every kernel inside the time-step loop (CUPTI through the torch "
                          "profiler, no serialisation), per step; not a throughput run")
@@ -89,6 +92,9 @@ def kernel_times(a):
     if a.equil:
         g.step(a.equil)
     autotune(g)
+    if a.fixed_skin is not None:
+        from mfa_b200.tune import cells_for
+        g.set_cells(cells_for(g.params, a.fixed_skin), a.fixed_skin)
     for _ in range(max(3, a.warmup // a.chunk)):
         g.step(a.chunk)
     g.sync()
