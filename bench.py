@@ -431,8 +431,11 @@ def pair_work(g, cfg):
     r2 = (d * d).sum(1)
     rc2 = np.array(p.range_2[:]).reshape(8, 8)[t[ii] - 1, t[jj] - 1]
     inside = int((r2 < rc2).sum())
-    return {"listed_half_pairs": int(cnt.sum()), "incut_half_pairs": inside,
-            "list_entries": int(cnt.sum())}
+    out = {"listed_half_pairs": int(cnt.sum()), "incut_half_pairs": inside, "list_entries": int(cnt.sum())}
+    if p.charged:
+        # Ewald real space: inside the LJ range (reference form) or to its own cutoff
+        out["ewald_real_pairs"] = inside if (p.quirks & _abi.Q_EWALD_REAL_IN_LJ) else int((r2 < p.ewald_rc_2).sum())
+    return out
 
 
 def batch_bench(a):
@@ -884,7 +887,15 @@ def main():
     # (4 B per entry)
     pair_bytes = n * (16 + 16 + 4 + 16 + 16) + 4 * work["list_entries"]
     # algorithmic flops (canonical counts): 17 per listed half-pair, 38 (LJ) + 29 (DPD) per in-cutoff half-pair
-    pair_flops = 17 * work["listed_half_pairs"] + (38 + 29) * work["incut_half_pairs"]
+    # canonical counts: 17 per listed half-pair; LJ 38 per in-cutoff pair; DPD
+    # 29 more with that thermostat; Ewald real 20 + erfc + exp (2 each) = 24
+    therm = cfg.params.thermostat
+    pair_flops = (17 * work["listed_half_pairs"] + (38 + (29 if therm == _abi.THERMO_DPD else 0)) *
+                  work["incut_half_pairs"] + 24 * work.get("ewald_real_pairs", 0))
+    pair_label = "k_pair (fluid_fluid" + (" + dpd_forces" if therm == _abi.THERMO_DPD else "") + \
+                 (" + lgv_forces" if therm == _abi.THERMO_LGV else "") + \
+                 (" + ewald_real" if cfg.params.charged else "") + \
+                 (" + 9-3 walls" if cfg.params.symmetry == 0 and cfg.params.wall == 2 else "") + ")"
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -1009,7 +1020,7 @@ def main():
             "fp64": {"value": value_fp64, "ms_per_step": ms_fp64 / a.steps, "per_call_ms": s64["per_call_ms"]},
             "mixed_over_fp64": value / value_fp64,
             "value_l2_resident": world * n * a.steps / (ms_resident * 1e-3),
-            "roofline": {"bound": "hbm", "kernel": "k_pair (fluid_fluid + dpd_forces + 9-3 walls)",
+            "roofline": {"bound": "hbm", "kernel": pair_label,
                          "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                          "traffic": traffic, "traffic_source": traffic_src,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"
