@@ -256,13 +256,26 @@ class System:
         check(self.lib.mfa_get_scalars(self.ctx, C.byref(s)), "mfa_get_scalars")
         return s.as_dict()
 
-    def download(self, mask: int = _abi.R0 | _abi.V | _abi.A | _abi.F | _abi.MIC) -> dict:
+    def download(self, mask: int = _abi.R0 | _abi.V | _abi.A | _abi.F | _abi.MIC, out: dict | None = None) -> dict:
+        """mfa_download of the quantities in mask.  `out` may hold the
+        destination arrays (n x 3, C-contiguous; float64, int32 for mic) by
+        name, e.g. pinned host buffers, which the device then writes directly."""
         n = self.n
-        r0 = np.empty((n, 3)) if mask & _abi.R0 else None
-        v = np.empty((n, 3)) if mask & _abi.V else None
-        a = np.empty((n, 3)) if mask & _abi.A else None
-        f = np.empty((n, 3)) if mask & _abi.F else None
-        mic = np.empty((n, 3), dtype=np.int32) if mask & _abi.MIC else None
+        out = out or {}
+
+        def dest(name, flag, dtype=np.float64):
+            if not mask & flag:
+                return None
+            x = out.get(name)
+            if x is None:
+                return np.empty((n, 3), dtype=dtype)
+            if x.shape != (n, 3) or x.dtype != dtype or not x.flags.c_contiguous:
+                raise ValueError(f"download: {name} must be a C-contiguous ({n}, 3) {np.dtype(dtype).name} array")
+            return x
+
+        r0, v, a = dest("r0", _abi.R0), dest("v", _abi.V), dest("a", _abi.A)
+        f = dest("force", _abi.F)
+        mic = dest("mic", _abi.MIC, np.int32)
         check(self.lib.mfa_download(self.ctx, mask, _dp(r0), _dp(v), _dp(a), _dp(f), _ip(mic)),
               "mfa_download")
         return {"r0": r0, "v": v, "a": a, "force": f, "mic": mic}
