@@ -29,6 +29,8 @@
 #include "mfa_internal.cuh"
 
 #include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 #include <vector>
 
@@ -711,16 +713,27 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
     // Full segments replay captured graphs (one per sequence); a partial last
     // segment, and any sequence whose capture fails, runs as plain launches.
     cudaGraphExec_t gx[4] = {nullptr, nullptr, nullptr, nullptr};
+    // MFA_DEBUG=1 in the environment reports a sequence that could not be
+    // captured (it then runs as plain launches)
+    const bool dbg = getenv("MFA_DEBUG") && getenv("MFA_DEBUG")[0] == '1';
     auto capture = [&](int which, auto&& fn) -> void {
         cudaGraph_t gr = nullptr;
         if (cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return;
         const int r = fn();
-        if (cudaStreamEndCapture(c->st, &gr) != cudaSuccess || r != MFA_OK || !gr) {
+        const cudaError_t ee = cudaStreamEndCapture(c->st, &gr);
+        if (ee != cudaSuccess || r != MFA_OK || !gr) {
+            if (dbg)
+                fprintf(stderr, "mfa_adjoint: sequence %d not captured (status %d, %s)\n", which, r,
+                        cudaGetErrorString(ee != cudaSuccess ? ee : cudaGetLastError()));
             if (gr) cudaGraphDestroy(gr);
             cudaGetLastError();
             return;
         }
-        if (cudaGraphInstantiate(&gx[which], gr, 0) != cudaSuccess) gx[which] = nullptr;
+        const cudaError_t ie = cudaGraphInstantiate(&gx[which], gr, 0);
+        if (ie != cudaSuccess) {
+            if (dbg) fprintf(stderr, "mfa_adjoint: sequence %d not instantiated (%s)\n", which, cudaGetErrorString(ie));
+            gx[which] = nullptr;
+        }
         cudaGraphDestroy(gr);
         cudaGetLastError();
     };

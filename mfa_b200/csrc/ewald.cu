@@ -37,8 +37,9 @@ constexpr int KPT = 8;        // k per thread: a block row covers KPT * RHO_T ve
 constexpr int NK_MAX = 1 << 16;   // k-vectors of one context
 constexpr int CH = 32;        // particles per table batch
 constexpr int FT = 64;        // threads per block in k_ewald_adj
-constexpr int FP = 32;        // particles per block in k_ewald_force
-constexpr int FS = 8;         // threads per particle in k_ewald_force (k-vector stride)
+constexpr int FP = 16;        // particles per block in k_ewald_force
+constexpr int FS = 16;        // threads per particle in k_ewald_force (k-vector stride)
+constexpr int TK = 256;       // k-vectors staged in shared memory at a time by k_ewald_force
 
 struct EwArgs {
     const double *rx, *ry, *rz, *q;
@@ -167,6 +168,10 @@ __global__ void k_rho_reduce(EwArgs a) {
 template <typename R4>
 __global__ void __launch_bounds__(FP * FS) k_ewald_force(EwArgs a) {
     extern __shared__ double2 ftab[];
+    // [FP x 3 x ts per-axis tables][TK k-vectors: index, rho, (k, A_k)]
+    int4* s_kn = (int4*)(ftab + FP * 3 * a.ts);
+    double2* s_rho = (double2*)(s_kn + TK);
+    double4* s_kv = (double4*)(s_rho + TK);
     const int p = threadIdx.x / FS, sl = threadIdx.x % FS;
     const int slot = blockIdx.x * FP + p;
     const bool act = slot < a.nq;
@@ -185,18 +190,27 @@ __global__ void __launch_bounds__(FP * FS) k_ewald_force(EwArgs a) {
             t[sl * a.ts + n] = e;
         }
     }
-    __syncthreads();
     double fx = 0.0, fy = 0.0, fz = 0.0;
-    if (act)
-        for (int k = sl; k < a.nk; k += FS) {
-            const double2 e = phase_from(t, a.ts, __ldg(&a.kn[k]));
-            const double2 r = __ldg(&a.rho[k]);
-            const double4 kv = ldg4(&a.kvec[k]);
-            const double sc = (e.x * r.y - e.y * r.x) * kv.w;   // (cos Im - sin Re) inv_k2 exp()
-            fx += kv.x * sc;
-            fy += kv.y * sc;
-            fz += kv.z * sc;
+    for (int k0 = 0; k0 < a.nk; k0 += TK) {
+        const int nt = min(TK, a.nk - k0);
+        __syncthreads();   // the tables are written / the previous tile is consumed
+        for (int j = threadIdx.x; j < nt; j += blockDim.x) {
+            s_kn[j] = a.kn[k0 + j];
+            s_rho[j] = a.rho[k0 + j];
+            s_kv[j] = a.kvec[k0 + j];
         }
+        __syncthreads();
+        if (act)
+            for (int j = sl; j < nt; j += FS) {
+                const double2 e = phase_from(t, a.ts, s_kn[j]);
+                const double2 r = s_rho[j];
+                const double4 kv = s_kv[j];
+                const double sc = (e.x * r.y - e.y * r.x) * kv.w;   // (cos Im - sin Re) inv_k2 exp()
+                fx += kv.x * sc;
+                fy += kv.y * sc;
+                fz += kv.z * sc;
+            }
+    }
     // the FS partial sums of a particle: adjacent lanes, fixed tree
     for (int o = FS / 2; o > 0; o >>= 1) {
         fx += __shfl_down_sync(0xffffffffu, fx, o, FS);
@@ -226,7 +240,9 @@ int reduce_grid(const mfa_ctx* c) {
     if (g > c->max_blocks) g = c->max_blocks;
     return g < 1 ? 1 : g;
 }
-size_t force_smem(const mfa_ctx* c) { return (size_t)FP * 3 * table_stride(c) * sizeof(double2); }
+size_t force_smem(const mfa_ctx* c) {
+    return (size_t)FP * 3 * table_stride(c) * sizeof(double2) + (size_t)TK * (sizeof(int4) + sizeof(double2) + sizeof(double4));
+}
 size_t adj_smem(const mfa_ctx* c) { return (size_t)FT * 3 * table_stride(c) * sizeof(double2); }
 
 EwArgs make_args(mfa_ctx* c) {
@@ -333,7 +349,7 @@ int ewald_setup(mfa_ctx* c) {
     MFA_CUDA_TRY(cudaMalloc(&c->rho_part, (size_t)nblk * c->nk * sizeof(double2)));
     // the attribute is per function and shared by every context: admit the
     // largest tables any context can have (a launch passes its own size)
-    const int fsm = FP * 3 * (KM + 1) * (int)sizeof(double2);
+    const int fsm = FP * 3 * (KM + 1) * (int)sizeof(double2) + TK * (int)(sizeof(int4) + sizeof(double2) + sizeof(double4));
     const int rsm = CH * (3 * (KM + 1) * (int)sizeof(double2) + (int)sizeof(double));
     MFA_CUDA_TRY(cudaFuncSetAttribute(k_ewald_force<float4>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
     MFA_CUDA_TRY(cudaFuncSetAttribute(k_ewald_force<double4>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));

@@ -476,21 +476,19 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
         const int32_t* __restrict__ crow = a.nbr + (size_t)ch * capc;
         int qn = 0;
         __syncwarp();
-        // the list entries of the next round are loaded while this round's
-        // partner records are gathered and tested (-1: no entry)
-        int nxt[K];
-#pragma unroll
-        for (int u = 0; u < K; ++u) nxt[u] = 32 * u + lane < cnt ? __ldg(&crow[32 * u + lane]) : -1;
         for (int e0 = 0; e0 < cnt; e0 += 32 * K) {
             int jx[K], ol[K];
             R4 pj[K];
 #pragma unroll
             for (int u = 0; u < K; ++u) {
-                const int ent = nxt[u];
-                ol[u] = ent >= 0 ? ent & 31 : 0;
-                jx[u] = ent >= 0 ? (int)((unsigned)ent >> 5) : -1;
-                const int e = e0 + 32 * K + 32 * u + lane;
-                nxt[u] = e < cnt ? __ldg(&crow[e]) : -1;
+                jx[u] = -1;
+                ol[u] = 0;
+                const int e = e0 + 32 * u + lane;
+                if (e < cnt) {
+                    const int ent = __ldg(&crow[e]);
+                    ol[u] = ent & 31;
+                    jx[u] = (int)((unsigned)ent >> 5);
+                }
             }
 #pragma unroll
             for (int u = 0; u < K; ++u) {
