@@ -320,16 +320,6 @@ int replay_call(mfa_ctx* c, int nsteps) {
 
 }  // namespace
 
-// The list rebuild after a skin check (positions half or launch_check_skin):
-// inside a stream capture a conditional graph node (no rebuild launches when
-// none is due), else the rebuild kernels that return at once when none is due.
-int rebuild_if_due(mfa_ctx* c) {
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    MFA_CUDA_TRY(cudaStreamIsCapturing(c->st, &cs));
-    if (cs == cudaStreamCaptureStatusActive && c->cond_rebuild) return capture_conditional_rebuild(c, 1);
-    return launch_rebuild(c, c->bin_type, 1);
-}
-
 extern "C" {
 
 int mfa_abi_version(void) { return MFA_ABI_VERSION; }

@@ -185,7 +185,6 @@ int launch_vv_grouped(int prec, int stage, const void* dargs, const int* doff, i
                       cudaStream_t st, long long energy_span = 0, int energy_reset = 0);
 // binning.cu
 int launch_rebuild(mfa_ctx* c, int rule, int conditional);
-int rebuild_if_due(mfa_ctx* c);
 int launch_rebuild_on(mfa_ctx* c, int rule, int conditional, cudaStream_t st, int in_cond_body);
 // the six rebuild stages as grouped launches
 constexpr int N_BIN_STAGES = 6;

@@ -97,10 +97,24 @@ __device__ __forceinline__ double rcp_(double x) { return 1.0 / x; }
 __device__ __forceinline__ double rsqrt_(double x) { return sqrt(1.0 / x); }
 __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
 __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
-__device__ __forceinline__ float erfc_(float x) { return erfcf(x); }
-__device__ __forceinline__ double erfc_(double x) { return erfc(x); }
-__device__ __forceinline__ float exp_(float x) { return expf(x); }
-__device__ __forceinline__ double exp_(double x) { return exp(x); }
+
+// erfc(x) and exp(-x^2) of the Ewald real-space term (x = sqrt(alpha) r,
+// x2 = alpha r^2).  FP64: the library functions.  FP32 (mixed): exp(-x^2)
+// once, and erfc(x) from it by the rational approximation of Abramowitz and
+// Stegun, Handbook of Mathematical Functions, eq. 7.1.26 (absolute error below
+// 1.5e-7 for x >= 0), so the pair costs one exponential instead of an erfc and
+// an exponential.
+__device__ __forceinline__ void ewald_erfc_exp(float x, float x2, float& ec, float& ex) {
+    ex = expf(-x2);
+    const float t = __frcp_rn(fmaf(0.3275911f, x, 1.0f));
+    const float poly = fmaf(fmaf(fmaf(fmaf(1.061405429f, t, -1.453152027f), t, 1.421413741f), t, -0.284496736f), t,
+                            0.254829592f);
+    ec = t * poly * ex;
+}
+__device__ __forceinline__ void ewald_erfc_exp(double x, double x2, double& ec, double& ex) {
+    ec = erfc(x);
+    ex = exp(-x2);
+}
 
 // Gaussian (Box-Muller) or uniform variate from two Philox words.
 __device__ __forceinline__ float noise1(uint32_t x0, uint32_t x1, int shape, float) {
@@ -410,10 +424,10 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
                     // ewald_real.f90:15-33, inside the LJ range (reference behaviour)
                     const R qq = vq.w * vj.w;
                     const R r = r2c * inv_r;
-                    const R ec = erfc_(SQA * r);
+                    R ec, ex;
+                    ewald_erfc_exp(SQA * r, ALC * r2c, ec, ex);
                     if (EN) e_c += qq * ec * inv_r;
-                    const R fsc = qq * SQA * ISP * (R)2 * exp_(-ALC * r2c) * inv_r +
-                                  qq * ec * inv_r * inv_r;
+                    const R fsc = qq * SQA * ISP * (R)2 * ex * inv_r + qq * ec * inv_r * inv_r;
                     fsum += fsc * inv_r;
                     if (EN) vir += fsc * r2 * inv_r;
                 }
@@ -423,10 +437,10 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
             const R qq = vq.w * vj.w;
             const R ir = rsqrt_(r2);
             const R r = r2 * ir;
-            const R ec = erfc_(SQA * r);
+            R ec, ex;
+            ewald_erfc_exp(SQA * r, ALC * r2, ec, ex);
             if (EN) e_c += qq * ec * ir;
-            const R fsc = qq * SQA * ISP * (R)2 * exp_(-ALC * r2) * ir +
-                          qq * ec * ir * ir;
+            const R fsc = qq * SQA * ISP * (R)2 * ex * ir + qq * ec * ir * ir;
             fsum += fsc * ir;
             if (EN) vir += fsc * r2 * ir;
         }
