@@ -107,19 +107,36 @@ def kernel_times(a):
     s1 = g.scalars()
     steps = (a.steps // a.chunk) * a.chunk
     agg = collections.defaultdict(lambda: [0, 0.0])
+    spans = []
     for ev in prof.events():
         if ev.device_type == torch.autograd.DeviceType.CUDA:
             agg[ev.name][0] += 1
             agg[ev.name][1] += getattr(ev, "device_time_total", 0.0)
+            spans.append((ev.time_range.start, ev.time_range.end, short_name(ev.name)))
     total = sum(t for _, t in agg.values())
     rows = [{"kernel": k, "launches": n, "total_us": round(t, 1), "mean_us": round(t / n, 2),
              "us_per_step": round(t / steps, 2), "share": round(t / total, 4)}
             for k, (n, t) in sorted(agg.items(), key=lambda kv: -kv[1][1])]
+    # idle device time between consecutive kernels of the loop (graph-node
+    # and conditional-node latency), by (previous -> next) kernel
+    spans.sort()
+    gaps = collections.defaultdict(lambda: [0, 0.0])
+    for (s0_, e0, n0), (s1_, e1, n1) in zip(spans, spans[1:]):
+        gap = s1_ - e0
+        if 0.0 <= gap < 200.0:    # a larger gap is the host between mfa_step calls
+            gaps[n0 + " -> " + n1][0] += 1
+            gaps[n0 + " -> " + n1][1] += gap
+    gap_total = sum(t for _, t in gaps.values())
+    span_us = (spans[-1][1] - spans[0][0]) if spans else 0.0
+    gap_rows = [{"between": k, "count": n, "mean_us": round(t / n, 2), "us_per_step": round(t / steps, 2)}
+                for k, (n, t) in sorted(gaps.items(), key=lambda kv: -kv[1][1])]
     print(json.dumps({"workload": meta["workload"], "precision": a.precision, "beads": cfg.n, "steps": steps,
                       "chunk": a.chunk,
                       "skin": g.params.skin, "n_bin": list(g.params.n_bin),
                       "list_rebuilds": s1["n_rebuilds"] - s0["n_rebuilds"],
-                      "kernel_us_per_step": round(total / steps, 2), "kernels": rows}))
+                      "kernel_us_per_step": round(total / steps, 2),
+                      "first_to_last_kernel_us_per_step": round(span_us / steps, 2),
+                      "gap_us_per_step": round(gap_total / steps, 2), "kernels": rows, "gaps": gap_rows[:12]}))
     g.close()
     return 0
 
@@ -759,9 +776,10 @@ def main():
         tuned = autotune(g)
         shapes = tuned["pair_shape"]
         g.tuned = min(shapes, key=shapes.get)
-        g.tuning = {f"{k}x{b}{'-tiled' if t else ''}{f'-queue{q}' if q else ''}": round(1e3 * s / 300, 4)
-                    for (k, b, t, q), s in shapes.items()}
-        g.skin_tuning = {f"{s:g}": round(1e3 * v / 300, 4) for s, v in tuned["skin"].items()}
+        g.tuning = {f"{k}x{b}{'-tiled' if t else ''}{f'-queue{q}' if q else ''}{f'-split{p}' if p > 1 else ''}":
+                    round(1e3 * s / 300, 4) for (k, b, t, q, p), s in shapes.items()}
+        g.skin_tuning = {f"{s:g}": round(1e3 * v / 300, 4) for s, v in tuned["skin_for_shape"].items()}
+        g.skin_tuning_first = {f"{s:g}": round(1e3 * v / 300, 4) for s, v in tuned["skin"].items()}
         ext = torch.cuda.ExternalStream(g.stream_ptr(), device=f"cuda:{dev}")
         # a timed iteration is `chunk` consecutive time steps (one mfa_step call:
         # fused velocity/position kernels, captured graphs); L2 is flushed
@@ -1012,9 +1030,11 @@ def main():
                            pair_shape=f"{shape_mixed[0]} list entries per thread and round x {shape_mixed[1]}-thread blocks, "
                                       f"{'tiled' if shape_mixed[2] else 'untiled'}"
                                       f"{f', work queue of {shape_mixed[3]} CTAs per SM' if shape_mixed[3] else ''}"
+                                      f"{f', each chunk list cut into {shape_mixed[4]} pieces' if shape_mixed[4] > 1 else ''}"
                                       " (autotuned)",
                            autotune_ms_per_step=tuning_mixed,
-                           thermostat="dpd", replicas=world,
+                           thermostat={_abi.THERMO_DPD: "dpd", _abi.THERMO_LGV: "langevin"}.get(
+                               cfg.params.thermostat, "none"), replicas=world,
                            steps_per_timed_iteration=a.chunk,
                            l2=f"flushed between timed iterations of {a.chunk} steps "
                               "(256 MiB write on the context stream)",

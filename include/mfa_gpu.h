@@ -296,6 +296,17 @@ int mfa_set_pair_shape(mfa_ctx* ctx, int32_t entries_per_round, int32_t block, i
  * overlap on the GPU (they share the counter), which a context's own stream
  * guarantees. */
 int mfa_set_pair_queue(mfa_ctx* ctx, int32_t ctas_per_sm);
+/* No counterpart in the reference.  Untiled launches of the pair kernel cut
+ * the list of every 32-particle chunk into `pieces` runs of equal length (1 to
+ * 64), each taken by its own warp, so that a small system with long lists
+ * (few chunks, many entries each) still occupies every multiprocessor; the
+ * owners' forces of the pieces are summed by atomic adds.  The default is set
+ * at mfa_init from the expected neighbour count and the device's
+ * multiprocessor count; tiled launches use 1.  The forces do not depend on it
+ * beyond rounding; the autotuner chooses it. */
+int mfa_set_pair_split(mfa_ctx* ctx, int32_t pieces);
+/* The current pieces per chunk (mfa_set_pair_split). */
+int mfa_get_pair_split(mfa_ctx* ctx, int32_t* pieces);
 
 /* Re-grids the cell list (n_bin cells per axis) and sets the Verlet skin
  * (skin_2 derived as init_params.f90:807-808 does).  Cells must be at least as

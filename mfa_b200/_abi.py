@@ -142,6 +142,8 @@ SIGNATURES = {
     "mfa_sync": (C.c_int, [_P]),
     "mfa_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "mfa_set_pair_queue": (C.c_int, [_P, C.c_int32]),
+    "mfa_set_pair_split": (C.c_int, [_P, C.c_int32]),
+    "mfa_get_pair_split": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "mfa_set_pair_shape": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32]),
     "mfa_set_cells": (C.c_int, [_P, _IP, C.c_double]),
     "mfa_bin_cells_noalloc": (C.c_int, [C.c_void_p, C.c_int32, _DP, _IP, C.c_int32, C.c_void_p, C.c_void_p,

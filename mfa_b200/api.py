@@ -215,6 +215,17 @@ class System:
         ctas_per_sm CTAs per multiprocessor (0: one CTA per block of slots)."""
         check(self.lib.mfa_set_pair_queue(self.ctx, int(ctas_per_sm)), "mfa_set_pair_queue")
 
+    def set_pair_split(self, pieces: int) -> None:
+        """mfa_set_pair_split: untiled pair launches cut each 32-particle
+        chunk's list into `pieces` runs, one warp each."""
+        check(self.lib.mfa_set_pair_split(self.ctx, int(pieces)), "mfa_set_pair_split")
+
+    def pair_split(self) -> int:
+        """mfa_get_pair_split: the current pieces per chunk."""
+        v = C.c_int32(0)
+        check(self.lib.mfa_get_pair_split(self.ctx, C.byref(v)), "mfa_get_pair_split")
+        return int(v.value)
+
     def set_pair_shape(self, entries_per_round: int, block: int, tiled: bool = True) -> None:
         check(self.lib.mfa_set_pair_shape(self.ctx, int(entries_per_round), int(block), int(bool(tiled))),
               "mfa_set_pair_shape")

@@ -442,17 +442,30 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
     if (rc == MFA_OK) rc = alloc_list(c, maxnb);
     A(dalloc(&c->nnb, (size_t)n + (n + 31) / 32));
     if (rc == MFA_OK) c->ccount = c->nnb + n;
+    if (rc == MFA_OK && cudaDeviceGetAttribute(&c->n_sm, cudaDevAttrMultiProcessorCount, c->dev) != cudaSuccess)
+        rc = MFA_ERR_CUDA;
     // partial-sum slots: enough for the largest grid of any reducing kernel
-    // (particles / 32, cell rows, chains)
+    // (particles / 32, cell rows, chains; 16 CTAs per SM for the pair kernel
+    // of a small system whose chunks are cut into pieces)
     c->max_blocks = (n + 31) / 32 + 64;
     if (nrow + 64 > c->max_blocks) c->max_blocks = nrow + 64;
     if (p->n_chain + p->n_chain_d + 64 > c->max_blocks) c->max_blocks = p->n_chain + p->n_chain_d + 64;
+    if (16 * c->n_sm > c->max_blocks) c->max_blocks = 16 * c->n_sm;
     A(dalloc(&c->partials, (size_t)R_N * 4 * c->max_blocks));
     A(dalloc(&c->counters, R_N));
     A(dalloc(&c->pair_qctr, 1));
     if (rc == MFA_OK && dzero(c, c->pair_qctr, sizeof(unsigned long long)) != MFA_OK) rc = MFA_ERR_CUDA;
-    if (rc == MFA_OK && cudaDeviceGetAttribute(&c->n_sm, cudaDevAttrMultiProcessorCount, c->dev) != cudaSuccess)
-        rc = MFA_ERR_CUDA;
+    // pieces per chunk of the pair kernel's list: double while the warps
+    // still fit the device twice over (32 per SM) and a piece keeps at least
+    // two rounds of 64 entries (a half list: 32 owners x expect / 2 entries)
+    {
+        const long long nchunk = (n + 31) / 32;
+        const double per_chunk = 16.0 * expect;
+        c->pair_split = 1;
+        while (c->pair_split < 16 && nchunk * c->pair_split * 2 <= 32LL * c->n_sm &&
+               per_chunk / (2.0 * c->pair_split) >= 128.0)
+            c->pair_split *= 2;
+    }
     static_assert(F_NFLAG % 2 == 0, "the flags fill whole doubles after the energies");
     A(dalloc(&c->dscal, S_NSLOT + F_NFLAG / 2));
     if (rc == MFA_OK) c->dflags = (int32_t*)(c->dscal + S_NSLOT);
@@ -836,6 +849,23 @@ int mfa_set_pair_shape(mfa_ctx* c, int32_t k, int32_t block, int32_t tiled) {
     TRY(pair_set_shape(c, k, block, c->tile_cap));
     TRY(dzero(c, c->pair_qctr, sizeof(unsigned long long)));   // the queue's grid may change
     invalidate_graph(c);
+    return MFA_OK;
+}
+
+int mfa_set_pair_split(mfa_ctx* c, int32_t pieces) {
+    if (!c || pieces < 1 || pieces > 64) return MFA_ERR_ARGS;
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    c->pair_split = pieces;
+    // the queue's ticket count per launch follows the number of pieces
+    TRY(dzero(c, c->pair_qctr, sizeof(unsigned long long)));
+    MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    invalidate_graph(c);
+    return MFA_OK;
+}
+
+int mfa_get_pair_split(mfa_ctx* c, int32_t* pieces) {
+    if (!c || !pieces) return MFA_ERR_ARGS;
+    *pieces = c->pair_split;
     return MFA_OK;
 }
 

@@ -92,6 +92,7 @@ std::vector<const void*> current_key(const mfa_batch* b) {
         k.push_back((const void*)(intptr_t)(c->maxnb * 4 + c->bin_type));
         k.push_back((const void*)(intptr_t)c->tile_cap);
         k.push_back((const void*)(intptr_t)(c->pair_tiled * 1000 + c->pair_tpp * 100 + c->pair_block / 32));
+        k.push_back((const void*)(intptr_t)c->pair_split);
     }
     return k;
 }
@@ -117,8 +118,12 @@ int build_tables(mfa_batch* b) {
     b->f_vv = n + 1;
     b->f_bin = 2 * (n + 1);
     b->hoff.assign((2 + N_BIN_STAGES) * (size_t)(n + 1), 0);
-    // one pair-kernel shape for all systems (the batch's), set before the records are made
-    for (mfa_ctx* c : b->ctx) TRY_(pair_set_shape(c, b->k, b->block, c->tile_cap));
+    // one pair-kernel shape for all systems (the batch's), set before the
+    // records are made; whole chunk lists (the systems together fill the GPU)
+    for (mfa_ctx* c : b->ctx) {
+        TRY_(pair_set_shape(c, b->k, b->block, c->tile_cap));
+        c->pair_split = 1;
+    }
     b->pair_smem = 0;
     b->nb_pair = b->nb_vv = 0;
     for (int s = 0; s < N_BIN_STAGES; ++s) b->nb_bin[s] = 0;

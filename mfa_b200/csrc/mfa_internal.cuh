@@ -136,12 +136,13 @@ struct mfa_ctx {
     // layout is copied as it is and (de)interleaved on the device
     double* d_stage;
     double* h_scal;                     // pinned copy of dscal and dflags (mfa_get_scalars)
+    // pair-kernel work queue: CTAs per SM (0: one CTA per block of slots) and
+    // its 64-bit ticket counter; n_sm = multiprocessors of the device;
+    // pair_split = pieces each 32-slot chunk's list is cut into (untiled)
+    int pair_queue, n_sm, pair_split;
+    unsigned long long* pair_qctr;
     // observables (observe.cu), allocated at their first use: unfolded
     // coordinates (3 n) and 16 result slots; the z histogram and its count
-    // pair-kernel work queue: CTAs per SM (0: one CTA per block of slots) and
-    // its 64-bit ticket counter; n_sm = multiprocessors of the device
-    int pair_queue, n_sm;
-    unsigned long long* pair_qctr;
     double* obs_buf;
     // the force on each grafted head before the pin zeroes it
     // (verlet_velocities.f90:18, f_on_heads), 3 x n_chain chain-major; null

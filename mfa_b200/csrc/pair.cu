@@ -56,7 +56,8 @@ struct PairArgs {
     double* dscal;
     int n, max_blocks, maxnb;
     unsigned long long* qctr;  // work-queue tickets (untiled launches with a queue), or null
-    int qmod;                  // tickets per launch: chunks + warps of the grid
+    int qmod;                  // tickets per launch: pieces + warps of the grid
+    int split;                 // pieces per chunk (untiled): warps that share one chunk's entries
     int nb[3], rule, wy, nseg, tile_cap, rowmode;
     int half;                 // 1: half list (partner gets -f), 0: full list
     int symmetry, thermostat, dpd_weight, noise, charged, real_in_lj, fsw;
@@ -329,8 +330,8 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
         p1 = a.n;
         if (threadIdx.x == 0) { s_mode = 0; s_npc = 0; }
     } else {
-        p0 = blk.id * blockDim.x;
-        p1 = min(p0 + (int)blockDim.x, a.n);
+        p0 = 0;                  // static: warp w of the grid takes pieces w, w + warps, ...
+        p1 = a.n;
         if (threadIdx.x == 0) { s_mode = 0; s_npc = 0; }
     }
     for (int k = threadIdx.x; k < T8 * T8; k += blockDim.x) {
@@ -452,24 +453,31 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
     };
 
     // chunks of 32 slots, each with its list as one run of entries (partner
-    // slot << 5 | owner lane): an untiled CTA owns blockDim/32 whole chunks; a
-    // tiled CTA (one cell row) takes the chunks overlapping its row and keeps
-    // the entries whose owner lies in the row.  The lanes walk the chunk's
-    // entries together, K per lane per round, whatever row they belong to.
+    // slot << 5 | owner lane).  An untiled launch cuts every chunk's run into
+    // `split` pieces of equal length (a piece: chunk * split + part), so that a
+    // small system with long lists still spreads over every SM; warp w of the
+    // grid takes pieces w, w + (warps of the grid), ...  A tiled CTA (one cell
+    // row, split 1) takes the chunks overlapping its row and keeps the entries
+    // whose owner lies in the row.  The lanes walk a piece's entries together,
+    // K per lane per round, whatever row they belong to.
     const long long capc = 32LL * a.maxnb;
-    // the chunks of this CTA: its own range (static), or -- with the work queue
-    // of an untiled launch -- tickets from a 64-bit counter shared by the
-    // grid.  Every launch draws exactly nchunk + (warps of the grid) tickets
-    // (each warp stops at its first ticket past the chunks), so a launch starts
-    // at a multiple of that number and ticket % qmod is its chunk.
+    // with the work queue of an untiled launch, pieces are tickets from a
+    // 64-bit counter shared by the grid.  Every launch draws exactly
+    // npiece + (warps of the grid) tickets (each warp stops at its first ticket
+    // past the pieces), so a launch starts at a multiple of that number and
+    // ticket % qmod is its piece.
     const bool dyn = a.qctr != nullptr;
-    int ch = (p0 >> 5) + warp;
+    const int S = a.rowmode ? 1 : a.split;
+    const int pc_end = ((p1 + 31) >> 5) * S;
+    int pc = a.rowmode ? (p0 >> 5) + warp : blk.id * nwarp + warp;
+    const int pc_step = a.rowmode ? nwarp : blk.n * nwarp;
     if (dyn) {
         unsigned long long tk = 0;
         if (lane == 0) tk = atomicAdd(a.qctr, 1ull);
-        ch = (int)(__shfl_sync(0xffffffffu, tk, 0) % (unsigned long long)a.qmod);
+        pc = (int)(__shfl_sync(0xffffffffu, tk, 0) % (unsigned long long)a.qmod);
     }
-    for (; valid && ch < ((p1 + 31) >> 5); ) {
+    for (; valid && pc < pc_end; ) {
+        const int ch = S == 1 ? pc : pc / S;
         const int t = (ch << 5) + lane;
         const bool act = t >= p0 && t < p1;
         R4 pi;
@@ -487,10 +495,12 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
         facc[32 + lane] = 0;
         facc[64 + lane] = 0;
         const int cnt = a.ccount[ch];
+        const int eb = S == 1 ? 0 : (int)(((long long)cnt * (pc - ch * S)) / S);
+        const int ee = S == 1 ? cnt : (int)(((long long)cnt * (pc - ch * S + 1)) / S);
         const int32_t* __restrict__ crow = a.nbr + (size_t)ch * capc;
         int qn = 0;
         __syncwarp();
-        for (int e0 = 0; e0 < cnt; e0 += 32 * K) {
+        for (int e0 = eb; e0 < ee; e0 += 32 * K) {
             int jx[K], ol[K];
             R4 pj[K];
 #pragma unroll
@@ -498,7 +508,7 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
                 jx[u] = -1;
                 ol[u] = 0;
                 const int e = e0 + 32 * u + lane;
-                if (e < cnt) {
+                if (e < ee) {
                     const int ent = __ldg(&crow[e]);
                     ol[u] = ent & 31;
                     jx[u] = (int)((unsigned)ent >> 5);
@@ -557,9 +567,12 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
         if (lane < qn) evaluate(lane);
         __syncwarp();
         if (act) {
+            // the piece's part of its chunk, recomputed here rather than held
+            // through the entry loop
+            const int part = S == 1 ? 0 : pc % S;
             R fx = facc[lane], fy = facc[32 + lane], fz = facc[64 + lane];
             const int ti = wi & 0xff, ii = wi >> 8;
-            if (LGV) {
+            if (LGV && part == 0) {
                 // lgv_forces.f90:22-41
                 R g[3];
                 lgv_noise3<R>((uint32_t)ii, (uint32_t)step, a.noise, a.seed0, a.seed1, g);
@@ -570,16 +583,16 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
                 fy += sig * g[1] * sm - gm * vi.y;
                 fz += sig * g[2] * sm - gm * vi.z;
             }
-            if (WALL) fz += wall_force<R>(a, ti, pi.z, e_w);
-            red_add(&f4[ii], fx, fy, fz);
+            if (WALL && part == 0) fz += wall_force<R>(a, ti, pi.z, e_w);
+            if (part == 0 || fx != (R)0 || fy != (R)0 || fz != (R)0) red_add(&f4[ii], fx, fy, fz);
         }
         __syncwarp();
         if (dyn) {
             unsigned long long tk = 0;
             if (lane == 0) tk = atomicAdd(a.qctr, 1ull);
-            ch = (int)(__shfl_sync(0xffffffffu, tk, 0) % (unsigned long long)a.qmod);
+            pc = (int)(__shfl_sync(0xffffffffu, tk, 0) % (unsigned long long)a.qmod);
         } else {
-            ch += nwarp;
+            pc += pc_step;
         }
     }
     if (!EN) return;   // no energies this step: nothing to reduce
@@ -770,16 +783,22 @@ int pair_stage_args(mfa_ctx* c, int fuse_wall, void* out, int* grid_out, size_t*
     a.a_w = p.a_w; a.z_space_wall = p.z_space_wall; a.wall_cut = p.wall_cut;
     a.seed0 = (uint32_t)p.seed; a.seed1 = (uint32_t)(p.seed >> 32);
     a.key = philox_round_keys(a.seed0, a.seed1);
-    int grid = c->pair_tiled ? c->nb[1] * c->nb[2] : (c->n + c->pair_block - 1) / c->pair_block;
+    // untiled: one warp per piece (a chunk's entries cut into `split` pieces),
+    // at most max_blocks CTAs (the warps then take several pieces each)
+    a.split = c->pair_tiled ? 1 : c->pair_split;
+    const long long npiece = (long long)((c->n + 31) / 32) * a.split;
+    const int nwarp = c->pair_block / 32;
+    int grid = c->pair_tiled ? c->nb[1] * c->nb[2] : (int)((npiece + nwarp - 1) / nwarp);
+    if (!c->pair_tiled && grid > c->max_blocks) grid = c->max_blocks;
     a.qctr = nullptr;
     a.qmod = 0;
     if (!c->pair_tiled && c->pair_queue > 0 && c->pair_qctr) {
         // a fixed grid of pair_queue CTAs per SM (at most the static grid)
-        // fetching 32-slot chunks from the queue
+        // fetching pieces from the queue
         const int g2 = c->pair_queue * c->n_sm;
         if (g2 < grid) grid = g2;
         a.qctr = c->pair_qctr;
-        a.qmod = (c->n + 31) / 32 + grid * (c->pair_block / 32);
+        a.qmod = (int)npiece + grid * nwarp;
     }
     if (grid > c->max_blocks) return MFA_ERR_ARGS;
     const size_t smem = c->prec == MFA_MIXED ? smem_bytes<float>(c->pair_tpp, c->pair_block, cap)

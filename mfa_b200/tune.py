@@ -3,10 +3,11 @@
 A larger skin lists more pairs per particle but rebuilds the lists less often;
 the pair kernel's best shape (list entries a thread tests per round, block
 size, shared-memory tiling or not, a work queue of a fixed number of CTAs per
-multiprocessor or not) depends on the neighbour count.  Neither
-changes the forces, so both are measured rather than assumed: each candidate
-runs a few hundred real time steps of the system (the state advances; tuning
-doubles as equilibration) and the fastest is kept.
+multiprocessor or not, the pieces each chunk's list is cut into) depends on
+the neighbour count and the system size.  None of them changes the forces, so
+all are measured rather than assumed: each candidate runs a few hundred real
+time steps of the system (the state advances; tuning doubles as
+equilibration) and the fastest is kept.
 """
 from __future__ import annotations
 
@@ -19,6 +20,8 @@ CANDIDATES = ((2, 128, True, 0), (4, 64, True, 0),
               (2, 128, False, 0), (4, 128, False, 0), (2, 256, False, 0), (4, 256, False, 0),
               (2, 128, False, 6), (2, 128, False, 8), (2, 256, False, 3), (2, 256, False, 4))
 SKINS = (0.2, 0.3, 0.4, 0.5, 0.6)
+# pieces per chunk tried for the best untiled shape
+SPLITS = (1, 2, 4, 8, 16, 32)
 
 
 def list_radius(params, skin: float) -> float:
@@ -63,21 +66,36 @@ def tune_cells(system, steps: int = 300, skins=SKINS, repeats: int = 2) -> dict:
 
 
 def autotune(system, steps: int = 300) -> dict:
-    """Cell size and skin first, then the pair kernel's launch shape."""
+    """Cell size and skin, then the pair kernel's launch shape, then the skin
+    again for that shape (a cheaper pair kernel moves the skin's optimum)."""
     cells = tune_cells(system, steps)
     shape = tune_pair_shape(system, steps)
-    return {"skin": cells, "pair_shape": shape}
+    cells2 = tune_cells(system, steps)
+    return {"skin": cells, "pair_shape": shape, "skin_for_shape": cells2}
 
 
-def tune_pair_shape(system, steps: int = 300, candidates=CANDIDATES, repeats: int = 2) -> dict:
-    """Time `steps` fused time steps per candidate (best of `repeats`), set the
-    fastest shape on `system` and return {shape: seconds}."""
-    timings = {}
-    for k, block, tiled, queue in candidates:
-        system.set_pair_shape(k, block, tiled)
-        system.set_pair_queue(0 if tiled else queue)
-        timings[(k, block, tiled, queue)] = _time(system, steps, repeats)
-    k, block, tiled, queue = min(timings, key=timings.get)
+def _set_shape(system, k, block, tiled, queue, split):
     system.set_pair_shape(k, block, tiled)
     system.set_pair_queue(0 if tiled else queue)
+    system.set_pair_split(1 if tiled else split)
+
+
+def tune_pair_shape(system, steps: int = 300, candidates=CANDIDATES, splits=SPLITS, repeats: int = 2) -> dict:
+    """Time `steps` fused time steps per candidate (best of `repeats`), set the
+    fastest shape on `system` and return {shape: seconds}.  The candidates run
+    with the context's default pieces per chunk; the best untiled one is then
+    timed with each count in `splits`."""
+    split0 = system.pair_split()
+    timings = {}
+    for k, block, tiled, queue in candidates:
+        _set_shape(system, k, block, tiled, queue, split0)
+        timings[(k, block, tiled, queue, 1 if tiled else split0)] = _time(system, steps, repeats)
+    untiled = [c for c in timings if not c[2]]
+    if untiled:
+        k, block, _, queue, _ = min(untiled, key=timings.get)
+        for split in splits:
+            if (k, block, False, queue, split) not in timings:
+                _set_shape(system, k, block, False, queue, split)
+                timings[(k, block, False, queue, split)] = _time(system, steps, repeats)
+    _set_shape(system, *min(timings, key=timings.get))
     return timings

@@ -436,16 +436,19 @@ def test_tiled_and_untiled_pair_kernels_agree(name, prec, request):
     """The pair kernel reads neighbour records from its shared-memory tile (one
     block per cell row) or through the caches (blocks of consecutive particles,
     or a fixed grid of 1 or 8 CTAs per SM taking chunks from the work queue,
-    where one CTA per SM makes every warp take many chunks); the forces agree to
-    the rounding of the reductions' order, and so do 40 steps of the fast path
-    (repeated launches reuse the queue's ticket counter)."""
+    where one CTA per SM makes every warp take many chunks), with each chunk's
+    list whole or cut into 2 to 64 pieces (static or queued); the forces agree
+    to the rounding of the reductions' order, and so do 40 steps of the fast
+    path (repeated launches reuse the queue's ticket counter)."""
     cfg = request.getfixturevalue(name)
     out = []
-    for k, block, tiled, queue in ((2, 128, True, 0), (4, 64, True, 0), (2, 64, False, 0), (4, 256, False, 0),
-                                   (2, 128, False, 1), (2, 128, False, 8)):
+    for k, block, tiled, queue, split in ((2, 128, True, 0, 1), (4, 64, True, 0, 1), (2, 64, False, 0, 1),
+                                          (4, 256, False, 0, 1), (2, 128, False, 1, 1), (2, 128, False, 8, 1),
+                                          (2, 128, False, 0, 4), (4, 64, False, 0, 64), (2, 256, False, 3, 8)):
         g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=prec)
         g.set_pair_shape(k, block, tiled)
         g.set_pair_queue(queue)
+        g.set_pair_split(split)
         if cfg.params.charged:
             g.ewald_k(0)
         g.binning()
