@@ -671,6 +671,27 @@ def adjoint_bench(a):
         res[name] = {"J": J, "grad": grad, "adjoint_ms": t_adj, "forward_observable_ms": t_obs,
                      "forward_fast_path_ms": t_fast, "adjoint_over_forward": t_adj / t_obs,
                      "adjoint_over_fast_path": t_adj / t_fast}
+    # where the mixed adjoint's device time goes: CUPTI activity records of one
+    # more adjoint call (after the timed ones: its graphs are captured)
+    import collections
+    from torch.profiler import ProfilerActivity, profile
+    g = fresh(cfg.params, _abi.MIXED)
+    g.adjoint(S, K)
+    g.sync()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        g.adjoint(S, K)
+        g.sync()
+        torch.cuda.synchronize()
+    g.close()
+    agg = collections.defaultdict(lambda: [0, 0.0])
+    for ev in prof.events():
+        if ev.device_type == torch.autograd.DeviceType.CUDA:
+            agg[short_name(ev.name)][0] += 1
+            agg[short_name(ev.name)][1] += getattr(ev, "device_time_total", 0.0)
+    adj_total = sum(t for _, t in agg.values())
+    adj_kernels = {"kernel_ms": round(adj_total / 1e3, 3),
+                   "top": [{"kernel": k, "launches": n, "ms": round(t / 1e3, 3), "share": round(t / adj_total, 4)}
+                           for k, (n, t) in sorted(agg.items(), key=lambda kv: -kv[1][1])[:10]]}
     # central differences (FP64) for every parameter
     base = base_values(cfg.params)
     h = 1e-4
@@ -704,7 +725,8 @@ def adjoint_bench(a):
                    "observable": "time average of <z> + <R_ee^2>", "dt": cfg.params.dt},
         "fp64": res["fp64"], "mixed": res["mixed"], "central_differences_fp64": fd,
         "rel_err_fp64_adjoint_vs_fd": rel, "rel_err_mixed_vs_fp64_adjoint": rel32,
-        "fd_step_study_sigma": {"adjoint_fp64": g64["sigma"], "central_differences": fd_sigma}}))
+        "fd_step_study_sigma": {"adjoint_fp64": g64["sigma"], "central_differences": fd_sigma},
+        "mixed_adjoint_kernels": adj_kernels}))
     return 0
 
 

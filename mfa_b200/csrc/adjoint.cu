@@ -51,6 +51,7 @@ struct AdjArgs {
     const double* mass;           // particle order (Langevin)
     int n, maxnb, half, symmetry, dpd, dpd_weight, noise, wall;
     int lgv;                      // Langevin thermostat (lgv_forces.f90)
+    int split;                    // pieces per chunk list (a warp each)
     int charged, real_in_lj;      // Ewald real space: inside the LJ range, or to its own cutoff
     double L[3], invL[3];
     double sig, gam, eps_lj, sigma_lj;
@@ -102,9 +103,10 @@ __device__ __forceinline__ void warp_add_g(double* g, double (&gl)[G_N]) {
     }
 }
 
-// Pair and wall VJP: a warp per 32-slot chunk, its lanes over the chunk's list
-// entries (owner and partner both updated through atomics), then over the
-// chunk's slots for the walls.
+// Pair and wall VJP: a warp per piece of a 32-slot chunk's list (the list cut
+// into `split` runs of equal length), its lanes over the piece's entries
+// (owner and partner both updated through atomics); the warp of a chunk's
+// first piece then goes over the chunk's slots for the walls and Langevin.
 template <typename R>
 __global__ void k_adj_pair(AdjArgs a) {
     typedef typename V4<R>::T R4;
@@ -118,7 +120,8 @@ __global__ void k_adj_pair(AdjArgs a) {
     __syncthreads();
     double gl[G_N] = {0, 0, 0, 0, 0, 0};
     const int lane = threadIdx.x & 31;
-    const int ch = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int piece = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int ch = piece / a.split, part = piece - ch * a.split;
     const long long step = a.step_ptr ? *a.step_ptr : a.step;
     const R4* ps = (const R4*)a.pos_s;
     const R4* vs = (const R4*)a.vel_s;
@@ -127,8 +130,10 @@ __global__ void k_adj_pair(AdjArgs a) {
     const R sg = (R)a.sig, gm = (R)a.gam;
     if (ch * 32 < a.n) {
         const int cnt = a.ccount[ch];
+        const int eb = (int)(((long long)cnt * part) / a.split);
+        const int ee = (int)(((long long)cnt * (part + 1)) / a.split);
         const int32_t* crow = a.nbr + (size_t)ch * 32 * a.maxnb;
-        for (int e = lane; e < cnt; e += 32) {
+        for (int e = eb + lane; e < ee; e += 32) {
             const int ent = crow[e];
             const int t = ch * 32 + (ent & 31), s = (int)((unsigned)ent >> 5);
             const R4 pi = ps[t], pj = ps[s];
@@ -224,7 +229,7 @@ __global__ void k_adj_pair(AdjArgs a) {
             atomicAdd(&a.rz[jj], -(double)gz);
         }
         const int t = ch * 32 + lane;
-        if (a.wall == 2 && t < a.n) {
+        if (part == 0 && a.wall == 2 && t < a.n) {
             // 9-3 walls (fluid_wall.f90:96-121): F_z += f(z) - f(Z - z), f = A phi(z)
             const R4 pi = ps[t];
             const int wi = wbits(pi.w), ii = wi >> 8, ti = wi & 0xff;
@@ -246,7 +251,7 @@ __global__ void k_adj_pair(AdjArgs a) {
             atomicAdd(&a.rz[ii], (double)(dfz * lfz));
             if (aw != (R)0) gl[G_WALL] += (double)(phi * lfz);
         }
-        if (a.lgv && t < a.n) {
+        if (part == 0 && a.lgv && t < a.n) {
             // Langevin (lgv_forces.f90:22-41): F += sig g sqrt(m) - gamma m u, the
             // variates replayed (same Philox key as the pair kernel's)
             const R4 pi = ps[t];
@@ -569,6 +574,11 @@ AdjArgs pair_adj_args(mfa_ctx* c, Work& w, const int64_t* step_ptr) {
     a.sigma_lj = smax > 0.0 ? smax : 1.0;
     a.step = 0;
     a.step_ptr = step_ptr;
+    // pieces per chunk: double while the warps fit 16 per SM (a small
+    // system's few chunks would leave most SMs idle), at most 8
+    const long long nchunk = (n + 31) / 32;
+    a.split = 1;
+    while (a.split < 8 && nchunk * a.split * 2 <= 16LL * c->n_sm) a.split *= 2;
     a.key = philox_round_keys((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
     for (int k = 0; k < T8; ++k) { a.a_wall[k] = p.a_wall[k]; a.sigma_wall[k] = p.sigma_wall[k]; }
     a.z_space_wall = p.z_space_wall;
@@ -663,7 +673,7 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
                                             p.n_chain * p.n_mon, p.n_mon > 0 ? p.n_mon : 1, w.lamF, w.lamU,
                                             w.lamR);
             AdjArgs aa = pair_adj_args(c, w, w.seg_step + j);
-            const int nbw = ((n + 31) / 32 * 32 + T - 1) / T;   // a warp per 32-slot chunk
+            const int nbw = (int)(((long long)(n + 31) / 32 * aa.split * 32 + T - 1) / T);   // a warp per piece
             if (c->prec == MFA_MIXED) k_adj_pair<float><<<nbw, T, 0, c->st>>>(aa);
             else k_adj_pair<double><<<nbw, T, 0, c->st>>>(aa);
             const int nbonds = p.n_chain * (p.n_mon > 0 ? p.n_mon - 1 : 0) +
