@@ -494,7 +494,7 @@ int adj_forward_step(mfa_ctx* c, double* sr, double* su, int32_t* sm, double w, 
         MFA_CUDA_TRY(cudaMemcpyAsync(su, c->vx, (size_t)3 * n * 8, cudaMemcpyDeviceToDevice, c->st));
         MFA_CUDA_TRY(cudaMemcpyAsync(sm, c->mx, (size_t)3 * n * 4, cudaMemcpyDeviceToDevice, c->st));
     }
-    TRY_(launch_rebuild(c, c->bin_type, 1));
+    TRY_(c->coop_rebuild ? launch_rebuild_coop(c, c->bin_type) : launch_rebuild(c, c->bin_type, 1));
     TRY_(launch_pair(c, c->p.symmetry == 0));
     if (c->p.charged) {
         TRY_(launch_ewald(c));      // md_main.f90:128-131
@@ -667,7 +667,7 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
             MFA_CUDA_TRY(cudaMemcpyAsync(c->vx, w.seg_u + j * n3, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
             MFA_CUDA_TRY(cudaMemcpyAsync(c->mx, w.seg_m + j * n3, n3 * 4, cudaMemcpyDeviceToDevice, c->st));
             TRY_(launch_check_skin(c));
-            TRY_(launch_rebuild(c, c->bin_type, 1));
+            TRY_(c->coop_rebuild ? launch_rebuild_coop(c, c->bin_type) : launch_rebuild(c, c->bin_type, 1));
             TRY_(launch_refresh_sorted(c));
             k_adj_prep<<<nb, T, 0, c->st>>>(n, w.rho, w.nu, w.alpha, c->inv_mass, 0.5 * dt, p.pin_heads,
                                             p.n_chain * p.n_mon, p.n_mon > 0 ? p.n_mon : 1, w.lamF, w.lamU,

@@ -210,6 +210,10 @@ int capture_conditional_rebuild(mfa_ctx* c, int opener) {
 // with positions of n+1, then the rebuild of n+1 if due.
 int launch_body_step(mfa_ctx* c) {
     TRY(forces_fused(c));
+    if (c->coop_rebuild) {
+        TRY(launch_vv_fused(c, 0, 1));
+        return launch_rebuild_coop(c, c->bin_type);
+    }
     if (c->capturing && c->cond_rebuild) return capture_conditional_rebuild(c, 0);
     TRY(launch_vv_fused(c, 0, 1));
     return launch_rebuild(c, c->bin_type, 1);
@@ -221,6 +225,7 @@ int launch_body_step(mfa_ctx* c) {
 // it (md_main.f90:73-147): positions, rebuild if due, forces, velocities.
 int launch_head_step(mfa_ctx* c, int nsteps) {
     TRY(launch_vv_positions(c, 1, 1, nsteps));
+    if (c->coop_rebuild) return launch_rebuild_coop(c, c->bin_type);
     if (c->capturing && c->cond_rebuild) return capture_conditional_rebuild(c, 1);
     return launch_rebuild(c, c->bin_type, 1);
 }
@@ -271,6 +276,17 @@ int replay(mfa_ctx* c, int kind) {
     check_graph_key(c);
     if (!c->gexec[kind]) {
         int rc = capture(c, kind);
+        if (rc != MFA_OK && c->coop_rebuild) {
+            // a runtime or device without captured cooperative launches: the
+            // rebuild in conditional graph nodes
+            cudaGetLastError();
+            c->coop_rebuild = 0;
+            int keep[N_CALL_GRAPHS];
+            memcpy(keep, c->call_n, sizeof(keep));
+            invalidate_graph(c);
+            memcpy(c->call_n, keep, sizeof(keep));
+            rc = capture(c, kind);
+        }
         if (rc != MFA_OK && c->cond_rebuild) {
             // a runtime without conditional graph nodes: rebuild kernels that
             // return at once when no rebuild is due
@@ -380,6 +396,13 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
     {
         const char* e = getenv("MFA_GRAPH_CONDITIONAL");
         c->cond_rebuild = (e && e[0] == '0') ? 0 : 1;
+        // MFA_REBUILD_COOP=0: no cooperative rebuild kernel (the rebuild as
+        // above); on by default where the device runs cooperative launches
+        const char* k = getenv("MFA_REBUILD_COOP");
+        int coop = 0;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->dev);
+        c->coop_rebuild = (k && k[0] == '0') ? 0 : (coop ? 1 : 0);
+        c->coop_grid = 0;
     }
     int rc = MFA_OK;
 #define A(x) do { if (rc == MFA_OK) rc = (x); } while (0)
@@ -444,6 +467,10 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
     if (rc == MFA_OK) c->ccount = c->nnb + n;
     if (rc == MFA_OK && cudaDeviceGetAttribute(&c->n_sm, cudaDevAttrMultiProcessorCount, c->dev) != cudaSuccess)
         rc = MFA_ERR_CUDA;
+    if (rc == MFA_OK && c->coop_rebuild && rebuild_coop_setup(c) != MFA_OK) {
+        cudaGetLastError();
+        c->coop_rebuild = 0;
+    }
     // partial-sum slots: enough for the largest grid of any reducing kernel
     // (particles / 32, cell rows, chains; 16 CTAs per SM for the pair kernel
     // of a small system whose chunks are cut into pieces)

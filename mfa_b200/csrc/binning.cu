@@ -55,6 +55,8 @@ struct BinArgs {
     int in_cond_body;    // launched from a conditional graph node: count the rebuild there
     int with_pos64;      // the gather also writes the list builder's FP64/FP32 copies
     const double* cut2;  // list criterion range_2 + skin_2 (T8 x T8)
+    int vnb[N_BIN_STAGES];   // cooperative rebuild: blocks of each stage at COOP_T threads
+    unsigned* bar;           // cooperative rebuild: grid barrier (arrivals, generation)
 };
 
 __device__ __forceinline__ bool skip(const BinArgs& a) {
@@ -422,6 +424,79 @@ __global__ void k_bin_grouped(const BinArgs* __restrict__ as, const int* __restr
     }
 }
 
+// One cooperative launch for the whole rebuild, used by the captured time-step
+// graphs: the six stages above, each a grid-stride loop over the blocks it
+// would have as a launch of its own, with a grid-wide barrier between stages.
+// When no rebuild is due every CTA returns after one flag read -- a launch of
+// a few microseconds in place of a conditional graph node, whose evaluation
+// costs the step more.  The grid is co-resident (cooperative launch), so the
+// barrier's waits end; each is bounded all the same (2 s), after which the
+// CTA reports MFA_ERR_TIMEOUT and returns.
+constexpr int COOP_T = 128;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// arrivals in bar[0], generation in bar[1]; the last CTA to arrive resets the
+// count and advances the generation.  Every CTA's writes before the barrier
+// are visible to every CTA after it (fences on both sides, as a cooperative
+// group's grid sync does).
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int32_t* flags) {
+    __shared__ int ok_s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vgen = bar + 1;
+        const unsigned g = *vgen;
+        int ok = 1;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            bar[0] = 0u;
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            const unsigned long long t0 = global_ns();
+            while (*vgen == g) {
+                if (global_ns() - t0 > 2000000000ull) {
+                    set_err(flags, MFA_ERR_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        ok_s = ok;
+    }
+    __syncthreads();
+    return ok_s != 0;
+}
+
+template <typename R4>
+__global__ void __launch_bounds__(COOP_T, 8) k_rebuild_coop(BinArgs a) {
+    // the flag is set before this launch and cleared only by the last stage,
+    // after every CTA has passed the barriers: all CTAs read the same value
+    if (*(volatile const int32_t*)&a.flags[F_SKIN] == 0) return;
+    for (int st = 0; st < N_BIN_STAGES; ++st) {
+        const int nv = a.vnb[st];
+        for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
+            const Blk blk{vb, nv};
+            switch (st) {
+                case 0: cell_assign_body(a, blk); break;
+                case 1: scan_rows_body(a, blk); break;
+                case 2: cell_scatter_body(a, blk); break;
+                case 3: cell_sort_body(a, blk); break;
+                case 4: gather_sorted_body<R4>(a, blk); break;
+                default: build_nbr_body(a, blk); break;
+            }
+            __syncthreads();
+        }
+        if (st + 1 < N_BIN_STAGES && !grid_barrier(a.bar, a.flags)) return;
+    }
+}
+
 // block size of each rebuild stage (assign, row scan, scatter, sort, gather, build)
 constexpr int BIN_T[N_BIN_STAGES] = {256, 256, 256, 128, 256, 128};
 
@@ -436,7 +511,7 @@ BinArgs make_args(mfa_ctx* c, int rule, int conditional) {
     a.cell_of = c->cell_of; a.row_count = c->row_count; a.ids = c->ids; a.slot = c->slot;
     a.pos_s = c->pos_s; a.vel_s = c->vel_s; a.pos64 = c->pos64; a.pos32 = c->pos32;
     a.nbr = c->nbr; a.nnb = c->nnb; a.ccount = c->ccount; a.flags = c->dflags;
-    a.counter = c->counters + R_N - 1;
+    a.counter = c->counters + R_BIN;
     a.n = c->n; a.ncell = c->ncell; a.nrow = c->nb[1] * c->nb[2]; a.maxnb = c->maxnb;
     for (int d = 0; d < 3; ++d) {
         a.nb[d] = c->nb[d]; a.dl[d] = c->p.delta_bin[d];
@@ -465,6 +540,8 @@ int bin_stage_args(mfa_ctx* c, int rule, int conditional, int in_cond_body, void
         for (int d = 0; d < 3; ++d)
             if (c->p.delta_bin[d] < -1 || c->p.delta_bin[d] > 1) return MFA_ERR_ARGS;
     BinArgs a = make_args(c, rule, conditional);
+    for (int s = 0; s < N_BIN_STAGES; ++s) a.vnb[s] = 0;
+    a.bar = nullptr;
     a.in_cond_body = in_cond_body;
     a.with_pos64 = 1;
     a.cut2 = c->tabs;
@@ -508,6 +585,48 @@ int launch_rebuild_on(mfa_ctx* c, int rule, int conditional, cudaStream_t st, in
     MFA_CUDA_TRY(cudaGetLastError());
     if (!in_cond_body) note_launch(c, N_BIN_STAGES);
     return MFA_OK;
+}
+
+int launch_rebuild_coop(mfa_ctx* c, int rule) {
+    BinArgs a;
+    int nb[N_BIN_STAGES];
+    TRY_(bin_stage_args(c, rule, 0, 0, &a, nb));
+    const int nrow = c->nb[1] * c->nb[2];
+    a.vnb[0] = (c->n + COOP_T - 1) / COOP_T;
+    a.vnb[1] = (nrow + COOP_T / 32 - 1) / (COOP_T / 32);
+    a.vnb[2] = (c->n + COOP_T - 1) / COOP_T;
+    a.vnb[3] = (c->ncell + COOP_T - 1) / COOP_T;
+    a.vnb[4] = (c->n + COOP_T - 1) / COOP_T;
+    a.vnb[5] = (c->n + COOP_T - 1) / COOP_T;
+    a.bar = c->counters + R_GRID;
+    const void* fn = c->prec == MFA_MIXED ? (const void*)k_rebuild_coop<float4> : (const void*)k_rebuild_coop<double4>;
+    if (c->coop_grid < 1) return MFA_ERR_STATE;
+    int vmax = 1;
+    for (int s = 0; s < N_BIN_STAGES; ++s) vmax = a.vnb[s] > vmax ? a.vnb[s] : vmax;
+    const int grid = c->coop_grid < vmax ? c->coop_grid : vmax;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(COOP_T);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = c->st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    void* argv[] = {&a};
+    MFA_CUDA_TRY(cudaLaunchKernelExC(&cfg, fn, argv));
+    note_launch(c, 1);
+    return MFA_OK;
+}
+
+// the cooperative rebuild's grid: the CTAs that fit the device at once
+int rebuild_coop_setup(mfa_ctx* c) {
+    const void* fn = c->prec == MFA_MIXED ? (const void*)k_rebuild_coop<float4> : (const void*)k_rebuild_coop<double4>;
+    int per_sm = 0;
+    MFA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, COOP_T, 0));
+    c->coop_grid = per_sm * c->n_sm;
+    return per_sm >= 1 ? MFA_OK : MFA_ERR_UNSUPPORTED;
 }
 
 int launch_refresh_sorted(mfa_ctx* c) {

@@ -49,7 +49,9 @@ enum {
 };
 
 // reduction counters (last-block-done pattern), one per reducing kernel
-enum { R_PAIR = 0, R_BOND = 1, R_WALL = 2, R_VV = 3, R_EWALD = 4, R_OBS = 5, R_N = 8 };
+// reduction counters (and partial-sum regions); R_GRID: the two words (arrivals,
+// generation) of the cooperative rebuild's grid barrier
+enum { R_PAIR = 0, R_BOND = 1, R_WALL = 2, R_VV = 3, R_EWALD = 4, R_OBS = 5, R_BIN = 7, R_GRID = 8, R_N = 10 };
 // whole-run graphs kept per context (distinct step counts of mfa_step calls)
 constexpr int N_CALL_GRAPHS = 4;
 
@@ -124,6 +126,8 @@ struct mfa_ctx {
     int last_call_n;                      // steps of the previous mfa_step call
     const void* graph_key[4];           // what the captured arguments depend on
     int cond_rebuild;                   // rebuilds in conditional graph nodes (1) or early-exit kernels (0)
+    int coop_rebuild;                   // captured steps rebuild in one cooperative kernel (1) or as above (0)
+    int coop_grid;                      // its grid (co-resident CTAs), 0 until first computed
     // kernel launch accounting
     long long launches;
     long long cap_count;
@@ -194,6 +198,8 @@ int bin_stage_args(mfa_ctx* c, int rule, int conditional, int in_cond_body, void
 int launch_bin_grouped(int prec, int stage, const void* dargs, const int* doff, int nsys, int nblocks,
                        cudaStream_t st, int* node_count);
 int launch_refresh_sorted(mfa_ctx* c);
+int launch_rebuild_coop(mfa_ctx* c, int rule);
+int rebuild_coop_setup(mfa_ctx* c);
 // pair.cu
 int launch_pair(mfa_ctx* c, int fuse_wall);   // adds to force
 size_t pair_args_bytes();

@@ -465,16 +465,29 @@ def test_tiled_and_untiled_pair_kernels_agree(name, prec, request):
         assert float(np.abs(r - out[0][1]).max()) < (1e-12 if prec == FP64 else 1e-4)
 
 
+# how the captured steps hold the rebuild: one cooperative kernel (default),
+# conditional graph nodes, or six kernels that return at once when no rebuild
+# is due -- (MFA_REBUILD_COOP, MFA_GRAPH_CONDITIONAL)
+REBUILD_MODES = {"coop": ("1", "1"), "cond": ("0", "1"), "kernels": ("0", "0")}
+
+
+def set_rebuild_mode(monkeypatch, mode):
+    coop, cond = REBUILD_MODES[mode]
+    monkeypatch.setenv("MFA_REBUILD_COOP", coop)
+    monkeypatch.setenv("MFA_GRAPH_CONDITIONAL", cond)
+
+
 @pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg"])
-@pytest.mark.parametrize("cond", ["1", "0"])
-def test_whole_run_graphs(name, cond, request, monkeypatch):
+@pytest.mark.parametrize("mode", ["coop", "cond", "kernels"])
+def test_whole_run_graphs(name, mode, request, monkeypatch):
     """A step count repeated from the previous call replays one captured graph
     for the whole run (first step's rebuild included, single steps too; four
     counts kept, the least recently used replaced).  Runs of changing length, whole-run graphs
     and their replacement all follow the per-step path (FP64, to rounding of
     the differently fused reductions), with the energies of each run's last
-    step, the step counter and the rebuild count."""
-    monkeypatch.setenv("MFA_GRAPH_CONDITIONAL", cond)
+    step, the step counter and the rebuild count, whichever way the captured
+    steps hold the rebuild."""
+    set_rebuild_mode(monkeypatch, mode)
     cfg = request.getfixturevalue(name)
     g1 = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, precision=FP64)
     g2 = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, precision=FP64)
@@ -500,29 +513,37 @@ def test_whole_run_graphs(name, cond, request, monkeypatch):
     g2.close()
 
 
+@pytest.mark.parametrize("name", ["brush_small_cfg", "melt_cfg"])
 @pytest.mark.parametrize("prec", [FP64, MIXED])
-def test_rebuild_in_conditional_nodes_or_early_exit_kernels(brush_small_cfg, prec, monkeypatch):
-    """The captured steps hold the rebuild in conditional graph nodes; with
-    MFA_GRAPH_CONDITIONAL=0 the rebuild kernels launch every step and return
-    at once when none is due.  Same physics, same rebuild count; the launch
-    count differs by the six skipped kernels of every step without a rebuild."""
-    cfg = brush_small_cfg
-    out = []
-    for mode in ("1", "0"):
-        monkeypatch.setenv("MFA_GRAPH_CONDITIONAL", mode)
+def test_rebuild_coop_conditional_or_early_exit(name, prec, monkeypatch, request):
+    """The captured steps hold the rebuild in one cooperative kernel (six stages
+    with grid barriers between them, a return after one flag read when none is
+    due), in conditional graph nodes, or as six kernels launched every step
+    that return at once when none is due.  Same physics, same rebuild count,
+    no error flag; the launch counts differ by the kernels of every step: one
+    cooperative launch, six early-exit launches, or six only when due."""
+    cfg = request.getfixturevalue(name)
+    out = {}
+    for mode in ("coop", "cond", "kernels"):
+        set_rebuild_mode(monkeypatch, mode)
         g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, precision=prec)
         g.init_forces()
         s0 = g.scalars()
         g.step(64)
         s1 = g.scalars()
-        out.append((g.download(_abi.R0)["r0"], s1["n_rebuilds"] - s0["n_rebuilds"],
-                    s1["kernel_launches"] - s0["kernel_launches"]))
+        assert s1["error_bits"] == 0
+        out[mode] = (g.download(_abi.R0)["r0"], s1["n_rebuilds"] - s0["n_rebuilds"],
+                     s1["kernel_launches"] - s0["kernel_launches"])
         g.close()
-    (r1, nr1, l1), (r0, nr0, l0) = out
-    assert nr1 == nr0 and nr1 > 0
-    assert float(np.abs(r1 - r0).max()) < (1e-12 if prec == FP64 else 1e-4)
+    (rc, nrc, lc), (r1, nr1, l1), (r0, nr0, l0) = out["coop"], out["cond"], out["kernels"]
+    assert nr1 == nr0 == nrc and nr1 > 0
+    tol = 1e-12 if prec == FP64 else 1e-4
+    assert float(np.abs(r1 - r0).max()) < tol
+    assert float(np.abs(rc - r0).max()) < tol
     # 63 captured steps, each launching the rebuild chain only when due
     assert l0 - l1 == 6 * (63 - (nr1 - 1)) or l0 - l1 == 6 * (63 - nr1)
+    # one cooperative launch in place of six early-exit ones, every step
+    assert l0 - lc == 5 * 64
 
 
 @pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg"])
