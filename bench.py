@@ -15,9 +15,11 @@ GPU (weak scaling, no data exchange between ranks).
 Timing: W untimed warm-up steps; K timed steps, each bracketed by CUDA events on
 the context's stream, with L2 flushed (a 256 MiB write on the same stream)
 between timed steps; barrier + synchronize around the loop; max over ranks.
-`e2e` is the same metric through the public API with host buffers: the initial
-state uploaded from pinned host memory, every step followed by a device->host
-read of the step's energies, the final state downloaded into pinned host memory.
+`e2e` is the same metric through the public API with host buffers, on the wall
+clock: the initial state uploaded from pinned host memory, mfa_step calls of
+--chunk steps with each call's scalars read back, every step's energies (the
+device energy log) read back, the final state downloaded into pinned host
+memory.
 
 --impl reference runs the CPU restatement of the reference's loop (serial, one
 core, like the Fortran program) on the same workload.
@@ -107,15 +109,22 @@ def kernel_times(a):
     s1 = g.scalars()
     steps = (a.steps // a.chunk) * a.chunk
     agg = collections.defaultdict(lambda: [0, 0.0])
+    durs = collections.defaultdict(list)
     spans = []
     for ev in prof.events():
         if ev.device_type == torch.autograd.DeviceType.CUDA:
             agg[ev.name][0] += 1
             agg[ev.name][1] += getattr(ev, "device_time_total", 0.0)
+            durs[ev.name].append(ev.time_range.end - ev.time_range.start)
             spans.append((ev.time_range.start, ev.time_range.end, short_name(ev.name)))
     total = sum(t for _, t in agg.values())
+
+    def pct(x, q):
+        x = sorted(x)
+        return round(x[min(len(x) - 1, int(q * len(x)))], 2)
     rows = [{"kernel": k, "launches": n, "total_us": round(t, 1), "mean_us": round(t / n, 2),
-             "us_per_step": round(t / steps, 2), "share": round(t / total, 4)}
+             "us_per_step": round(t / steps, 2), "share": round(t / total, 4),
+             "p10_p50_p90_max_us": [pct(durs[k], 0.1), pct(durs[k], 0.5), pct(durs[k], 0.9), pct(durs[k], 1.0)]}
             for k, (n, t) in sorted(agg.items(), key=lambda kv: -kv[1][1])]
     # idle device time between consecutive kernels of the loop (graph-node
     # and conditional-node latency), by (previous -> next) kernel
@@ -887,6 +896,9 @@ def main():
     # L2 flushed before every `chunk`-th launch, as the timed loop flushes it
     # before every call of `chunk` steps (the launch-average of that loop);
     # and, for reference, flushed before every launch (cold)
+    # A spin of ~0.5 ms on the stream after each flush lets the host enqueue
+    # the launches that follow before the device reaches them, so the events
+    # time the device work and not the host's enqueue rate.
     reps = 2 * a.chunk
     pk, pk_cold = [], []
     torch.cuda.nvtx.range_push("pair_alone")
@@ -895,6 +907,7 @@ def main():
         if cold or k % a.chunk == 0:
             with torch.cuda.stream(ext):
                 flush.fill_(k & 0xff)
+                torch.cuda._sleep(1_000_000)
         g.zero_forces()
         p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         p0.record(ext)
@@ -913,6 +926,7 @@ def main():
     for k in range(5):
         with torch.cuda.stream(ext):
             flush.fill_(k & 0xff)
+            torch.cuda._sleep(1_000_000)
         b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         b0.record(ext)
         g.binning()
@@ -1005,11 +1019,17 @@ def main():
         ge.ewald_k(0)
     ge.init_forces()
     ge.step(a.equil)
-    # the single-step call's graph is captured on its second call: three
-    # untimed single steps put that capture before the timed region
-    for _ in range(3):
-        ge.step(1)
-        ge.scalars()
+    # every step's energies (e_total, v_total, t_fluid: the quantities of
+    # fort.60) recorded on the device and read back by the host
+    e2e_calls = [a.chunk] * (a.steps // a.chunk) + ([a.steps % a.chunk] if a.steps % a.chunk else [])
+    log_cap = a.steps + 4 * a.chunk + 16
+    ge.set_energy_log(1, log_cap)
+    # a call's graph is captured on its second call of that length: three
+    # untimed calls of each length put the capture before the timed region
+    for ln in sorted(set(e2e_calls)):
+        for _ in range(3):
+            ge.step(ln)
+            ge.scalars()
     st = ge.download()
     pinned[0].copy_(torch.from_numpy(st["r0"]))
     pinned[1].copy_(torch.from_numpy(st["v"]))
@@ -1020,19 +1040,27 @@ def main():
     ge.sync()
     if dist is not None:
         dist.barrier()
+    n_log0 = len(ge.energy_log(log_cap))
     t0 = time.perf_counter()
     ge.upload(r0=host[0], v=host[1], a=host[2])
-    for k in range(a.steps):
-        ge.step(1)
-        ge.scalars()                         # the step's energies (fort.60 quantities) to the host
+    for ln in e2e_calls:
+        ge.step(ln)                          # mfa_step: `chunk` steps per call, as the timed loop
+        ge.scalars()                         # the call's last step: energies and error flags to the host
+    elog = ge.energy_log(log_cap)            # every step's energies to the host
     out = ge.download(_abi.R0 | _abi.V, out=dest)   # into pinned host buffers
     t_e2e = time.perf_counter() - t0
     ge.close()
+    assert len(elog) - n_log0 == a.steps, "energy log: one entry per timed step"
     t_e2e = max_over_ranks(t_e2e, dist, f"cuda:{dev}")
     e2e = world * n * a.steps / t_e2e
     scal_bytes = 16 * 8 + 8 * 4
     e2e_obj = {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": int(72 * n / a.steps),
-               "d2h_bytes_per_step": int(scal_bytes + 48 * n / a.steps)}
+               "d2h_bytes_per_step": int(32 * (len(elog)) / a.steps + scal_bytes * len(e2e_calls) / a.steps +
+                                         48 * n / a.steps),
+               "protocol": f"wall clock: state (r0, v, a) uploaded from pinned host memory, {len(e2e_calls)} "
+                           f"mfa_step calls of up to {a.chunk} steps with the call's scalars read back after "
+                           "each, every step's energies recorded on the device and read back, final r0 and v "
+                           "downloaded into pinned host memory"}
 
     line = None
     if rank == 0:
@@ -1071,7 +1099,8 @@ def main():
                          if "hbm_gbs" in peaks else "fallback 6650 GB/s",
                          "launch_ms": pair_ms, "algorithmic_bytes": pair_bytes,
                          "timing": f"CUDA events around {reps} launches on the context stream, L2 flushed before "
-                                   f"every {a.chunk}th as the timed loop flushes it before every call of {a.chunk} steps",
+                                   f"every {a.chunk}th as the timed loop flushes it before every call of {a.chunk} steps; "
+                                   "a device spin after each flush keeps the host's enqueue ahead of the device",
                          "launch_ms_l2_flushed_each": pair_ms_cold,
                          "launch_us_in_loop": pair_us_loop,
                          "fp32_tflops": pair_flops / (pair_ms * 1e-3) / 1e12, **work},

@@ -630,20 +630,16 @@ int mfa_zero_forces(mfa_ctx* c) {
 
 int mfa_fluid_fluid(mfa_ctx* c) {
     if (!c) return MFA_ERR_ARGS;
-    // fluid_fluid.f90:17 resets v_coul; the k-space part is added by ewald_k,
-    // the slab correction by dipolar_correction
-    MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VCK, 0, 8, c->st));
-    MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VDIP, 0, 8, c->st));
-    return launch_pair(c, 0);
+    // fluid_fluid.f90:17 resets v_coul (the kernel does); the k-space part is
+    // added by ewald_k, the slab correction by dipolar_correction
+    return launch_pair(c, 0, 1);
 }
 
 int mfa_pair_forces(mfa_ctx* c) {
     if (!c) return MFA_ERR_ARGS;
-    MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VCK, 0, 8, c->st));
-    MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VDIP, 0, 8, c->st));
-    if (c->p.symmetry != 0 || (c->p.wall != 2 && c->p.wall != 3 && c->p.wall != 4))
-        MFA_CUDA_TRY(cudaMemsetAsync(c->dscal + S_VFW, 0, 8, c->st));
-    TRY(launch_pair(c, c->p.symmetry == 0));
+    // v_coul reset as in fluid_fluid, and v_fluid_wall where no wall is fused
+    const bool wall_fused = c->p.symmetry == 0 && (c->p.wall == 2 || c->p.wall == 3 || c->p.wall == 4);
+    TRY(launch_pair(c, c->p.symmetry == 0, wall_fused ? 1 : 3));
     if (c->p.symmetry == 0 && (c->p.wall == 3 || c->p.wall == 4)) TRY(launch_wall(c, c->p.wall));
     return MFA_OK;
 }

@@ -475,7 +475,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, int32_t* flags) {
 }
 
 template <typename R4>
-__global__ void __launch_bounds__(COOP_T, 8) k_rebuild_coop(BinArgs a) {
+__global__ void __launch_bounds__(COOP_T, 10) k_rebuild_coop(BinArgs a) {
     // the flag is set before this launch and cleared only by the last stage,
     // after every CTA has passed the barriers: all CTAs read the same value
     if (*(volatile const int32_t*)&a.flags[F_SKIN] == 0) return;

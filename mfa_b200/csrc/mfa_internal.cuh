@@ -201,7 +201,9 @@ int launch_refresh_sorted(mfa_ctx* c);
 int launch_rebuild_coop(mfa_ctx* c, int rule);
 int rebuild_coop_setup(mfa_ctx* c);
 // pair.cu
-int launch_pair(mfa_ctx* c, int fuse_wall);   // adds to force
+// adds to force; zero_slots: energy slots the kernel resets (1: S_VCK and
+// S_VDIP, 2: S_VFW), for the subroutine entry points
+int launch_pair(mfa_ctx* c, int fuse_wall, int zero_slots = 0);
 size_t pair_args_bytes();
 int pair_stage_args(mfa_ctx* c, int fuse_wall, void* out, int* grid_out, size_t* smem_out, int* ft_out);
 int launch_pair_grouped(int prec, int k, int block, int ft, const void* dargs, const int* doff, int nsys, int grid,

@@ -58,6 +58,7 @@ struct PairArgs {
     unsigned long long* qctr;  // work-queue tickets (untiled launches with a queue), or null
     int qmod;                  // tickets per launch: pieces + warps of the grid
     int split;                 // pieces per chunk (untiled): warps that share one chunk's entries
+    int zero_slots;            // energy slots the launch resets: 1 v_coul k-space and slab parts, 2 v_fluid_wall
     int nb[3], rule, wy, nseg, tile_cap, rowmode;
     int half;                 // 1: half list (partner gets -f), 0: full list
     int symmetry, thermostat, dpd_weight, noise, charged, real_in_lj, fsw;
@@ -100,17 +101,10 @@ __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
 __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
 
 // erfc(x) and exp(-x^2) of the Ewald real-space term (x = sqrt(alpha) r,
-// x2 = alpha r^2).  FP64: the library functions.  FP32 (mixed): exp(-x^2)
-// once, and erfc(x) from it by the rational approximation of Abramowitz and
-// Stegun, Handbook of Mathematical Functions, eq. 7.1.26 (absolute error below
-// 1.5e-7 for x >= 0), so the pair costs one exponential instead of an erfc and
-// an exponential.
+// x2 = alpha r^2), the library functions in the kernel's precision
 __device__ __forceinline__ void ewald_erfc_exp(float x, float x2, float& ec, float& ex) {
+    ec = erfcf(x);
     ex = expf(-x2);
-    const float t = __frcp_rn(fmaf(0.3275911f, x, 1.0f));
-    const float poly = fmaf(fmaf(fmaf(fmaf(1.061405429f, t, -1.453152027f), t, 1.421413741f), t, -0.284496736f), t,
-                            0.254829592f);
-    ec = t * poly * ex;
 }
 __device__ __forceinline__ void ewald_erfc_exp(double x, double x2, double& ec, double& ex) {
     ec = erfc(x);
@@ -281,6 +275,12 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
     const bool QSEP = has<FT>(a, FT_QSEP), FSW = has<FT>(a, FT_FSW), WALL = has<FT>(a, FT_WALL);
     const bool need_v = DPD || QLJ || QSEP;
     const int nx = a.nb[0], ny = a.nb[1], nz = a.nb[2];
+    if (a.zero_slots && blk.id == 0 && threadIdx.x == 0) {
+        // the subroutine entry points' resets (fluid_fluid.f90:17: v_coul),
+        // here rather than as copies of their own on the stream
+        if (a.zero_slots & 1) { a.dscal[S_VCK] = 0.0; a.dscal[S_VDIP] = 0.0; }
+        if (a.zero_slots & 2) a.dscal[S_VFW] = 0.0;
+    }
     int p0, p1;
     if (a.rowmode) {
         const int row = blk.id;
@@ -786,6 +786,7 @@ int pair_stage_args(mfa_ctx* c, int fuse_wall, void* out, int* grid_out, size_t*
     // untiled: one warp per piece (a chunk's entries cut into `split` pieces),
     // at most max_blocks CTAs (the warps then take several pieces each)
     a.split = c->pair_tiled ? 1 : c->pair_split;
+    a.zero_slots = 0;
     const long long npiece = (long long)((c->n + 31) / 32) * a.split;
     const int nwarp = c->pair_block / 32;
     int grid = c->pair_tiled ? c->nb[1] * c->nb[2] : (int)((npiece + nwarp - 1) / nwarp);
@@ -829,11 +830,12 @@ int launch_pair_grouped(int prec, int k, int block, int ft, const void* dargs, c
     return MFA_OK;
 }
 
-int launch_pair(mfa_ctx* c, int fuse_wall) {
+int launch_pair(mfa_ctx* c, int fuse_wall, int zero_slots) {
     PairArgs a;
     int grid, ft;
     size_t smem;
     TRY_(pair_stage_args(c, fuse_wall, &a, &grid, &smem, &ft));
+    a.zero_slots = zero_slots;
     const int rc = c->prec == MFA_MIXED ? launch_r<float>(c->pair_tpp, ft, a, nullptr, grid, c->pair_block, smem, c->st)
                                         : launch_r<double>(c->pair_tpp, ft, a, nullptr, grid, c->pair_block, smem, c->st);
     if (rc != MFA_OK) return rc;
