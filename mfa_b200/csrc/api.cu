@@ -98,7 +98,8 @@ void free_all(mfa_ctx* c) {
     void* ptrs[] = {c->rx, c->mx, c->type, c->mass, c->force, c->pos_s, c->vel_s, c->pos64, c->pos32,
                     c->ids, c->cell_count, c->nbr, c->nnb, c->partials, c->counters, c->dscal,
                     c->dstep, c->kvec, c->rho, c->rho_part, c->qidx, c->elog, c->elog_n, c->tabs,
-                    c->obs_buf, c->hist, c->fd, c->term_buf, c->d_stage, c->f_heads, c->pair_qctr};
+                    c->obs_buf, c->hist, c->fd, c->term_buf, c->d_stage, c->f_heads, c->pair_qctr,
+                    c->grid_bar};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->h_scal) cudaFreeHost(c->h_scal);

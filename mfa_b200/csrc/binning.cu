@@ -428,11 +428,11 @@ __global__ void k_bin_grouped(const BinArgs* __restrict__ as, const int* __restr
 // graphs: the six stages above, each a grid-stride loop over the blocks it
 // would have as a launch of its own, with a grid-wide barrier between stages.
 // When no rebuild is due every CTA returns after one flag read -- a launch of
-// a few microseconds in place of a conditional graph node, whose evaluation
-// costs the step more.  The grid is co-resident (cooperative launch), so the
-// barrier's waits end; each is bounded all the same (2 s), after which the
-// CTA reports MFA_ERR_TIMEOUT and returns.
-constexpr int COOP_T = 128;
+// one to three microseconds in place of a conditional graph node, whose
+// evaluation held the device idle for about seven.  The grid is co-resident
+// (cooperative launch), so the barrier's waits end; each is bounded all the
+// same (2 s), after which the CTA reports MFA_ERR_TIMEOUT and returns.
+constexpr int COOP_T = 256;
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -440,31 +440,55 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
-// arrivals in bar[0], generation in bar[1]; the last CTA to arrive resets the
-// count and advances the generation.  Every CTA's writes before the barrier
-// are visible to every CTA after it (fences on both sides, as a cooperative
-// group's grid sync does).
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Two-level arrival: CTA b counts into group b % GB_SUB, the last of a group
+// into the root, the last group resets the root and advances the generation
+// (bar[0]); the CTAs of the other groups poll the generation with a growing
+// pause.  Spreading the arrivals over GB_SUB + 1 lines keeps any one line's
+// atomics to a few dozen.  Every CTA's writes before the barrier are visible
+// to every CTA after it (fences on both sides, as a cooperative group's grid
+// sync does).
 __device__ __forceinline__ bool grid_barrier(unsigned* bar, int32_t* flags) {
     __shared__ int ok_s;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned* vgen = bar + 1;
-        const unsigned g = *vgen;
+        const unsigned nb = gridDim.x;
+        const unsigned grp = blockIdx.x % GB_SUB;
+        const unsigned ngrp = nb < (unsigned)GB_SUB ? nb : (unsigned)GB_SUB;
+        const unsigned in_grp = (nb - grp + GB_SUB - 1) / GB_SUB;
+        unsigned* gen = bar;
+        unsigned* root = bar + 32;
+        unsigned* sub = bar + 64 + 32 * grp;
+        const unsigned g = ld_acquire(gen);
         int ok = 1;
         __threadfence();
-        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
-            bar[0] = 0u;
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
+        bool released = false;
+        if (atomicAdd(sub, 1u) == in_grp - 1) {
+            *sub = 0u;
+            __threadfence();   // the reset lands before the release that lets the group count again
+            if (atomicAdd(root, 1u) == ngrp - 1) {
+                *root = 0u;
+                __threadfence();
+                atomicAdd(gen, 1u);
+                released = true;
+            }
+        }
+        if (!released) {
             const unsigned long long t0 = global_ns();
-            while (*vgen == g) {
+            unsigned pause = 32;
+            while (ld_acquire(gen) == g) {
                 if (global_ns() - t0 > 2000000000ull) {
                     set_err(flags, MFA_ERR_TIMEOUT);
                     ok = 0;
                     break;
                 }
-                __nanosleep(64);
+                __nanosleep(pause);
+                if (pause < 512) pause *= 2;
             }
         }
         __threadfence();
@@ -474,8 +498,11 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, int32_t* flags) {
     return ok_s != 0;
 }
 
+// 48 registers: five 256-thread CTAs per SM, 740 on 148 SMs, so every stage of
+// a 189k-particle system takes one round (a few bytes of the list builder's
+// registers spill)
 template <typename R4>
-__global__ void __launch_bounds__(COOP_T, 10) k_rebuild_coop(BinArgs a) {
+__global__ void __launch_bounds__(COOP_T, 5) k_rebuild_coop(BinArgs a) {
     // the flag is set before this launch and cleared only by the last stage,
     // after every CTA has passed the barriers: all CTAs read the same value
     if (*(volatile const int32_t*)&a.flags[F_SKIN] == 0) return;
@@ -598,7 +625,7 @@ int launch_rebuild_coop(mfa_ctx* c, int rule) {
     a.vnb[3] = (c->ncell + COOP_T - 1) / COOP_T;
     a.vnb[4] = (c->n + COOP_T - 1) / COOP_T;
     a.vnb[5] = (c->n + COOP_T - 1) / COOP_T;
-    a.bar = c->counters + R_GRID;
+    a.bar = c->grid_bar;
     const void* fn = c->prec == MFA_MIXED ? (const void*)k_rebuild_coop<float4> : (const void*)k_rebuild_coop<double4>;
     if (c->coop_grid < 1) return MFA_ERR_STATE;
     int vmax = 1;
@@ -623,6 +650,11 @@ int launch_rebuild_coop(mfa_ctx* c, int rule) {
 // the cooperative rebuild's grid: the CTAs that fit the device at once
 int rebuild_coop_setup(mfa_ctx* c) {
     const void* fn = c->prec == MFA_MIXED ? (const void*)k_rebuild_coop<float4> : (const void*)k_rebuild_coop<double4>;
+    if (!c->grid_bar) {
+        MFA_CUDA_TRY(cudaMalloc((void**)&c->grid_bar, GB_WORDS * sizeof(unsigned)));
+        MFA_CUDA_TRY(cudaMemsetAsync(c->grid_bar, 0, GB_WORDS * sizeof(unsigned), c->st));
+        MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    }
     int per_sm = 0;
     MFA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, COOP_T, 0));
     c->coop_grid = per_sm * c->n_sm;

@@ -49,9 +49,12 @@ enum {
 };
 
 // reduction counters (last-block-done pattern), one per reducing kernel
-// reduction counters (and partial-sum regions); R_GRID: the two words (arrivals,
-// generation) of the cooperative rebuild's grid barrier
-enum { R_PAIR = 0, R_BOND = 1, R_WALL = 2, R_VV = 3, R_EWALD = 4, R_OBS = 5, R_BIN = 7, R_GRID = 8, R_N = 10 };
+// reduction counters (and partial-sum regions)
+enum { R_PAIR = 0, R_BOND = 1, R_WALL = 2, R_VV = 3, R_EWALD = 4, R_OBS = 5, R_BIN = 7, R_N = 8 };
+// the cooperative rebuild's grid barrier: a generation word, a root count and
+// GB_SUB group counts, each on its own 128-byte line
+constexpr int GB_SUB = 16;
+constexpr int GB_WORDS = (GB_SUB + 2) * 32;
 // whole-run graphs kept per context (distinct step counts of mfa_step calls)
 constexpr int N_CALL_GRAPHS = 4;
 
@@ -127,7 +130,8 @@ struct mfa_ctx {
     const void* graph_key[4];           // what the captured arguments depend on
     int cond_rebuild;                   // rebuilds in conditional graph nodes (1) or early-exit kernels (0)
     int coop_rebuild;                   // captured steps rebuild in one cooperative kernel (1) or as above (0)
-    int coop_grid;                      // its grid (co-resident CTAs), 0 until first computed
+    int coop_grid;                      // its grid (co-resident CTAs)
+    unsigned* grid_bar;                 // its barrier words (GB_WORDS, zeroed)
     // kernel launch accounting
     long long launches;
     long long cap_count;
