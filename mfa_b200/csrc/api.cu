@@ -99,7 +99,7 @@ void free_all(mfa_ctx* c) {
                     c->ids, c->cell_count, c->nbr, c->nnb, c->partials, c->counters, c->dscal,
                     c->dstep, c->kvec, c->rho, c->rho_part, c->qidx, c->elog, c->elog_n, c->tabs,
                     c->obs_buf, c->hist, c->fd, c->term_buf, c->d_stage, c->f_heads, c->pair_qctr,
-                    c->grid_bar};
+                    c->grid_bar, c->coop_stage_ns};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->h_scal) cudaFreeHost(c->h_scal);
@@ -585,6 +585,7 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
 int mfa_finalize(mfa_ctx* c) {
     if (!c) return MFA_ERR_ARGS;
     cudaStreamSynchronize(c->st);
+    rebuild_coop_report(c);
     free_all(c);
     free(c);
     return MFA_OK;

@@ -23,6 +23,8 @@
 // entry is (partner slot << 5 | lane of the owning slot in the chunk).
 #include "mfa_internal.cuh"
 
+#include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 namespace {
@@ -56,7 +58,8 @@ struct BinArgs {
     int with_pos64;      // the gather also writes the list builder's FP64/FP32 copies
     const double* cut2;  // list criterion range_2 + skin_2 (T8 x T8)
     int vnb[N_BIN_STAGES];   // cooperative rebuild: blocks of each stage at COOP_T threads
-    unsigned* bar;           // cooperative rebuild: grid barrier (arrivals, generation)
+    unsigned* bar;           // cooperative rebuild: grid barrier words
+    unsigned long long* stage_ns;   // cooperative rebuild: CTA 0's stage times (MFA_DEBUG=1), or null
 };
 
 __device__ __forceinline__ bool skip(const BinArgs& a) {
@@ -506,6 +509,10 @@ __global__ void __launch_bounds__(COOP_T, 5) k_rebuild_coop(BinArgs a) {
     // the flag is set before this launch and cleared only by the last stage,
     // after every CTA has passed the barriers: all CTAs read the same value
     if (*(volatile const int32_t*)&a.flags[F_SKIN] == 0) return;
+    // with MFA_DEBUG=1, CTA 0 sums the time from each stage's start to the
+    // barrier after it (the stage's critical path; the last stage: its own part)
+    __shared__ unsigned long long t_prev;   // thread 0 of CTA 0 only (no register held across stages)
+    if (a.stage_ns && blockIdx.x == 0 && threadIdx.x == 0) t_prev = global_ns();
     for (int st = 0; st < N_BIN_STAGES; ++st) {
         const int nv = a.vnb[st];
         for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
@@ -521,7 +528,13 @@ __global__ void __launch_bounds__(COOP_T, 5) k_rebuild_coop(BinArgs a) {
             __syncthreads();
         }
         if (st + 1 < N_BIN_STAGES && !grid_barrier(a.bar, a.flags)) return;
+        if (a.stage_ns && blockIdx.x == 0 && threadIdx.x == 0) {
+            const unsigned long long t = global_ns();
+            atomicAdd(&a.stage_ns[st], t - t_prev);
+            t_prev = t;
+        }
     }
+    if (a.stage_ns && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.stage_ns[N_BIN_STAGES], 1ull);
 }
 
 // block size of each rebuild stage (assign, row scan, scatter, sort, gather, build)
@@ -569,6 +582,7 @@ int bin_stage_args(mfa_ctx* c, int rule, int conditional, int in_cond_body, void
     BinArgs a = make_args(c, rule, conditional);
     for (int s = 0; s < N_BIN_STAGES; ++s) a.vnb[s] = 0;
     a.bar = nullptr;
+    a.stage_ns = nullptr;
     a.in_cond_body = in_cond_body;
     a.with_pos64 = 1;
     a.cut2 = c->tabs;
@@ -626,6 +640,7 @@ int launch_rebuild_coop(mfa_ctx* c, int rule) {
     a.vnb[4] = (c->n + COOP_T - 1) / COOP_T;
     a.vnb[5] = (c->n + COOP_T - 1) / COOP_T;
     a.bar = c->grid_bar;
+    a.stage_ns = c->coop_stage_ns;
     const void* fn = c->prec == MFA_MIXED ? (const void*)k_rebuild_coop<float4> : (const void*)k_rebuild_coop<double4>;
     if (c->coop_grid < 1) return MFA_ERR_STATE;
     int vmax = 1;
@@ -655,10 +670,29 @@ int rebuild_coop_setup(mfa_ctx* c) {
         MFA_CUDA_TRY(cudaMemsetAsync(c->grid_bar, 0, GB_WORDS * sizeof(unsigned), c->st));
         MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
     }
+    const char* dbg = getenv("MFA_DEBUG");
+    if (dbg && dbg[0] == '1' && !c->coop_stage_ns) {
+        MFA_CUDA_TRY(cudaMalloc((void**)&c->coop_stage_ns, 8 * sizeof(unsigned long long)));
+        MFA_CUDA_TRY(cudaMemsetAsync(c->coop_stage_ns, 0, 8 * sizeof(unsigned long long), c->st));
+        MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    }
     int per_sm = 0;
     MFA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, COOP_T, 0));
     c->coop_grid = per_sm * c->n_sm;
     return per_sm >= 1 ? MFA_OK : MFA_ERR_UNSUPPORTED;
+}
+
+// MFA_DEBUG=1: the cooperative rebuild's stage times to stderr (at mfa_finalize)
+void rebuild_coop_report(mfa_ctx* c) {
+    if (!c->coop_stage_ns) return;
+    unsigned long long h[8] = {0};
+    if (cudaMemcpy(h, c->coop_stage_ns, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess || h[N_BIN_STAGES] == 0)
+        return;
+    const double k = 1e-3 / (double)h[N_BIN_STAGES];
+    fprintf(stderr,
+            "mfa: cooperative rebuild, %llu rebuilds, mean us per stage (CTA 0, to the barrier after it): "
+            "assign %.1f scan %.1f scatter %.1f sort %.1f gather %.1f build %.1f\n",
+            h[N_BIN_STAGES], h[0] * k, h[1] * k, h[2] * k, h[3] * k, h[4] * k, h[5] * k);
 }
 
 int launch_refresh_sorted(mfa_ctx* c) {

@@ -132,6 +132,7 @@ struct mfa_ctx {
     int coop_rebuild;                   // captured steps rebuild in one cooperative kernel (1) or as above (0)
     int coop_grid;                      // its grid (co-resident CTAs)
     unsigned* grid_bar;                 // its barrier words (GB_WORDS, zeroed)
+    unsigned long long* coop_stage_ns;  // its stage times under MFA_DEBUG=1, else null
     // kernel launch accounting
     long long launches;
     long long cap_count;
@@ -204,6 +205,7 @@ int launch_bin_grouped(int prec, int stage, const void* dargs, const int* doff, 
 int launch_refresh_sorted(mfa_ctx* c);
 int launch_rebuild_coop(mfa_ctx* c, int rule);
 int rebuild_coop_setup(mfa_ctx* c);
+void rebuild_coop_report(mfa_ctx* c);
 // pair.cu
 // adds to force; zero_slots: energy slots the kernel resets (1: S_VCK and
 // S_VDIP, 2: S_VFW), for the subroutine entry points
