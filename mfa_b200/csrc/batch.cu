@@ -1,14 +1,17 @@
 // Many independent systems advanced together (mfa_batch_*).
 //
 // Each system keeps its own context (its own buffers, cell grid, lists, energy
-// slots and error flags), exactly as mfa_init made it.  A batch launches every
-// kernel stage of the time step ONCE for all systems: the argument records of
-// the systems sit in device memory, and a table of block offsets maps each block
-// of the grid to its system and to its block index there (group_of).  A step of
-// 64 uneven systems is therefore the same handful of launches as a step of one,
-// captured as CUDA graphs; the rebuild sits in a conditional node that any
-// system whose skin check tripped opens, and inside it every block returns at
-// once unless its own system is due.
+// slots and error flags), exactly as mfa_init made it.  The argument records of
+// the systems sit in device memory, and a table of block offsets per kernel
+// stage maps each block of a stage to its system and to its block index there
+// (group_of).  A run of steps of all systems is ONE persistent cooperative
+// launch (persist.cu: every stage of every step as a grid-stride loop over
+// those blocks, grid barriers between stages).  Where that kernel is not
+// available (a feature set it is not built for, no cooperative launch, or
+// MFA_BATCH_PERSIST=0) every kernel stage of a step is one grouped launch for
+// all systems, captured as CUDA graphs, with the rebuild in a conditional node
+// that any system whose skin check tripped opens; inside it every block
+// returns at once unless its own system is due.
 #include "mfa_internal.cuh"
 
 #include <stdlib.h>
@@ -45,7 +48,24 @@ struct mfa_batch {
     long long cap_count;
     int capturing;
     int* dnodes;                  // conditional rebuild nodes that opened (device counter)
+    // the persistent launch: kernel (null: grouped launches), grid, dynamic
+    // shared memory, barrier words, block offsets of its rebuild stages
+    const void* persist_fn;
+    int persist_grid;
+    size_t persist_smem;
+    unsigned* grid_bar;
+    size_t f_binp;
 };
+
+// persist.cu
+const void* persist_kernel(int prec, int ft);
+size_t persist_args_bytes();
+size_t persist_smem(int prec);
+int persist_threads();
+void persist_bin_blocks(const mfa_ctx* c, int nb[N_BIN_STAGES]);
+void persist_args(const void* pair, const void* vvpos, const void* vvfused, const void* vvvel, const void* bin_first,
+                  const void* bin_body, const int* off_pair, const int* off_vv, const int* off_bin, int nsys,
+                  int nsteps, long long energy_span, unsigned* bar, int32_t* status, void* out);
 
 namespace {
 
@@ -117,13 +137,20 @@ int build_tables(mfa_batch* b) {
     b->f_pair = 0;
     b->f_vv = n + 1;
     b->f_bin = 2 * (n + 1);
-    b->hoff.assign((2 + N_BIN_STAGES) * (size_t)(n + 1), 0);
+    b->f_binp = (2 + N_BIN_STAGES) * (size_t)(n + 1);
+    b->hoff.assign((2 + 2 * N_BIN_STAGES) * (size_t)(n + 1), 0);
     // one pair-kernel shape for all systems (the batch's), set before the
-    // records are made; whole chunk lists (the systems together fill the GPU)
+    // records are made; whole chunk lists (the systems together fill the GPU);
+    // the persistent kernel's pair stage is untiled without a work queue
     for (mfa_ctx* c : b->ctx) {
+        if (b->persist_fn) {
+            c->pair_tiled = 0;
+            c->pair_queue = 0;
+        }
         TRY_(pair_set_shape(c, b->k, b->block, c->tile_cap));
         c->pair_split = 1;
     }
+    int nbp_total[N_BIN_STAGES] = {0, 0, 0, 0, 0, 0};
     b->pair_smem = 0;
     b->nb_pair = b->nb_vv = 0;
     for (int s = 0; s < N_BIN_STAGES; ++s) b->nb_bin[s] = 0;
@@ -150,10 +177,18 @@ int build_tables(mfa_batch* b) {
             b->hoff[b->f_bin + s * (n + 1) + i] = b->nb_bin[s];
             b->nb_bin[s] += nbs[s];
         }
+        // the persistent kernel's rebuild stages run with its own CTA size
+        int nbp[N_BIN_STAGES];
+        persist_bin_blocks(c, nbp);
+        for (int s = 0; s < N_BIN_STAGES; ++s) {
+            b->hoff[b->f_binp + s * (n + 1) + i] = nbp_total[s];
+            nbp_total[s] += nbp[s];
+        }
     }
     b->hoff[b->f_pair + n] = b->nb_pair;
     b->hoff[b->f_vv + n] = b->nb_vv;
     for (int s = 0; s < N_BIN_STAGES; ++s) b->hoff[b->f_bin + s * (n + 1) + n] = b->nb_bin[s];
+    for (int s = 0; s < N_BIN_STAGES; ++s) b->hoff[b->f_binp + s * (n + 1) + n] = nbp_total[s];
     b->next_fused_slot = 0;
     TRY_(upload(b));
     b->tables_ok = true;
@@ -249,6 +284,38 @@ int capture(mfa_batch* b, int kind) {
     return MFA_OK;
 }
 
+// A whole run of nsteps steps of every system as one cooperative launch.
+int run_persistent(mfa_batch* b, int nsteps) {
+    if (b->persist_grid == 0) {
+        int per_sm = 0, n_sm = 0;
+        MFA_CUDA_TRY(cudaFuncSetAttribute(b->persist_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)b->persist_smem));
+        MFA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b->persist_fn, persist_threads(),
+                                                                   b->persist_smem));
+        MFA_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, b->dev));
+        if (per_sm < 1) return MFA_ERR_UNSUPPORTED;
+        b->persist_grid = per_sm * n_sm;
+    }
+    std::vector<unsigned char> rec(persist_args_bytes());
+    persist_args(b->dargs + b->o_pair, b->dargs + b->o_vvpos, vvfused_slot(b, 0), b->dargs + b->o_vvvel,
+                 b->dargs + b->o_bin_first, b->dargs + b->o_bin_body, b->doff + b->f_pair, b->doff + b->f_vv,
+                 b->doff + b->f_binp, b->nsys, nsteps, nsteps, b->grid_bar, b->ctx[0]->dflags, rec.data());
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)b->persist_grid);
+    cfg.blockDim = dim3((unsigned)persist_threads());
+    cfg.dynamicSmemBytes = b->persist_smem;
+    cfg.stream = b->st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    void* argv[] = {rec.data()};
+    MFA_CUDA_TRY(cudaLaunchKernelExC(&cfg, b->persist_fn, argv));
+    note(b, 1);
+    return MFA_OK;
+}
+
 int replay(mfa_batch* b, int kind) {
     if (!b->gexec[kind]) TRY_(capture(b, kind));
     MFA_CUDA_TRY(cudaGraphLaunch(b->gexec[kind], b->st));
@@ -286,6 +353,10 @@ int mfa_batch_create(mfa_ctx* const* ctxs, int32_t n, mfa_batch** out) {
     b->fuse_wall = ctxs[0]->p.symmetry == 0;
     b->ft = -1;
     b->fused_handles.assign(BODY + 1, 0);
+    b->persist_fn = nullptr;
+    b->persist_grid = 0;
+    b->persist_smem = 0;
+    b->grid_bar = nullptr;
     if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&b->st_body, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc((void**)&b->dnodes, sizeof(int)) != cudaSuccess) {
@@ -314,6 +385,24 @@ int mfa_batch_create(mfa_ctx* const* ctxs, int32_t n, mfa_batch** out) {
             else if (ft != b->ft) { mfa_batch_destroy(b); return MFA_ERR_UNSUPPORTED; }
         }
     }
+    // the persistent launch, unless MFA_BATCH_PERSIST=0, the device has no
+    // cooperative launch or the feature set has no persistent kernel
+    {
+        const char* e = getenv("MFA_BATCH_PERSIST");
+        int coop = 0;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, b->dev);
+        const void* fn = persist_kernel(b->prec, b->ft);
+        if (!(e && e[0] == '0') && coop && fn &&
+            cudaMalloc((void**)&b->grid_bar, GB_WORDS * sizeof(unsigned)) == cudaSuccess &&
+            cudaMemsetAsync(b->grid_bar, 0, GB_WORDS * sizeof(unsigned), b->st) == cudaSuccess &&
+            cudaStreamSynchronize(b->st) == cudaSuccess) {
+            b->persist_fn = fn;
+            b->persist_smem = persist_smem(b->prec);
+            b->k = 2;
+            b->block = persist_threads();
+        }
+        cudaGetLastError();
+    }
     *out = b;
     return MFA_OK;
 }
@@ -325,6 +414,7 @@ int mfa_batch_destroy(mfa_batch* b) {
     if (b->dargs) cudaFree(b->dargs);
     if (b->doff) cudaFree(b->doff);
     if (b->dnodes) cudaFree(b->dnodes);
+    if (b->grid_bar) cudaFree(b->grid_bar);
     if (b->st) cudaStreamDestroy(b->st);
     if (b->st_body) cudaStreamDestroy(b->st_body);
     delete b;
@@ -344,6 +434,11 @@ int mfa_batch_step(mfa_batch* b, int32_t nsteps) {
         invalidate(b);
         TRY_(build_tables(b));
         b->key = current_key(b);
+    }
+    if (b->persist_fn) {
+        TRY_(run_persistent(b, nsteps));
+        for (mfa_ctx* c : b->ctx) c->i_time += nsteps;
+        return MFA_OK;
     }
     // first step: positions (+ skin check, force reset; every system reduces
     // its energies on the last step of the run only, and on the steps its

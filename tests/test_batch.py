@@ -39,7 +39,11 @@ def _systems(cfgs, prec):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("prec", [FP64, MIXED])
-def test_batch_equals_systems_stepped_alone(prec):
+@pytest.mark.parametrize("persist", ["1", "0"])
+def test_batch_equals_systems_stepped_alone(prec, persist, monkeypatch):
+    """One persistent cooperative launch per run (default), or grouped
+    launches per stage in captured graphs (MFA_BATCH_PERSIST=0)."""
+    monkeypatch.setenv("MFA_BATCH_PERSIST", persist)
     cfgs = configs.uneven_brushes(seed=7, n_sys=4, grids=(4, 7), lengths=(16, 32))
     alone = _systems(cfgs, prec)
     grouped = _systems(cfgs, prec)
@@ -56,8 +60,11 @@ def test_batch_equals_systems_stepped_alone(prec):
         tol = 1e-11 if prec == FP64 else 1e-4
         assert float(np.abs(r1 - r2).max()) < tol
         assert s2["e_total"] == pytest.approx(s1["e_total"], rel=1e-10 if prec == FP64 else 1e-5)
-    # one launch per stage for all four systems: two per step plus the rebuilds
-    assert b.launches() < 2 * 47 + 6 * 47
+    if persist == "1":
+        assert b.launches() == 1                  # the whole 47-step run
+    else:
+        # one launch per stage for all four systems: two per step plus the rebuilds
+        assert b.launches() < 2 * 47 + 6 * 47
     # further runs: the energies reduced are those of each run's last step
     for n in (10, 10, 3):
         for g in alone:
