@@ -466,10 +466,12 @@ def pair_work(g, cfg):
 
 def batch_bench(a):
     """Uneven implicit-solvent brushes (default 64 systems, ~0.95 M beads)
-    advanced together: each kernel stage of a step is one launch for all
-    systems (mfa_batch_step).  Beside it: the same systems stepped one after
-    another through mfa_step (one system per launch sequence), FP64, and the
-    serial CPU restatement on a sample of the systems."""
+    advanced together (mfa_batch_step): each kernel stage of a step is one
+    grouped launch for all systems, captured graphs (with MFA_BATCH_PERSIST=1:
+    each call of --chunk steps is one persistent cooperative launch).  Beside it: the
+    same systems stepped one after another through mfa_step (one system per
+    launch sequence), FP64, and the serial CPU restatement on a sample of the
+    systems."""
     import numpy as np
     import torch
     from mfa_b200 import _abi, configs
@@ -539,6 +541,7 @@ def batch_bench(a):
         clocks = sampler.stop()
         ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
         launches = b.launches() - l0
+        timed_batch.calls = len(chunks)
         sc = b.scalars()
         errs = sum(1 for x in sc if x["error_bits"])
         b.close()
@@ -607,6 +610,7 @@ def batch_bench(a):
             "one_system_at_a_time": {"value": n * seq_steps / t_seq,
                                      "note": "the same systems through mfa_step one after another (wall clock)"},
             "gpu_launches": int(launches),
+            "launches_per_call": launches / timed_batch.calls,
             "systems_with_errors": errs,
             "gathered": {"systems": int(table.shape[0]), "systems_with_errors": int(table[:, 2].sum()),
                          "kinetic_temperature_mean": float((2.0 * table[:, 1] / (3.0 * np.array(

@@ -99,7 +99,7 @@ void free_all(mfa_ctx* c) {
                     c->ids, c->cell_count, c->nbr, c->nnb, c->partials, c->counters, c->dscal,
                     c->dstep, c->kvec, c->rho, c->rho_part, c->qidx, c->elog, c->elog_n, c->tabs,
                     c->obs_buf, c->hist, c->fd, c->term_buf, c->d_stage, c->f_heads, c->pair_qctr,
-                    c->grid_bar, c->coop_stage_ns};
+                    c->grid_bar, c->coop_stage_ns, c->kruns};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->h_scal) cudaFreeHost(c->h_scal);

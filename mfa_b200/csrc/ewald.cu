@@ -3,21 +3,25 @@
 // mode 0 (host): the half-space set of k-vectors with |k| <= k_c, enumerated
 //   exactly as ewald_k.f90:47-124 does (same FP64 expressions, same int()
 //   truncations, so the same vectors are kept at the boundary of the sphere).
-// mode 1 (device):
-//   k_rho_partial  - structure factors rho(k) = sum_i q_i exp(i k.r_i).  Each
-//                    block takes a contiguous range of particles; for a batch of
-//                    particles it builds exp(i n dk_d r_d), n = 0..kmax_d, per
-//                    axis by a complex power recurrence from one sincos per axis,
-//                    and every thread accumulates a fixed set of k in registers
-//                    (12 FP64 flops per (particle, k)).  Partials per block.
+// mode 1 (device), over "runs": the k-vectors are enumerated x fastest
+// (ewald_k.f90:104-124), so those with the same (n_y, n_z) form runs of
+// consecutive n_x, and along a run exp(i k.r) advances by one complex product
+// with exp(i dk_x x).  Per particle, exp(i n dk_d r_d) for n = 0..kmax_d per
+// axis comes from one sincos and a complex power recurrence (tables in shared
+// memory, laid out so the 32 lanes of a warp read 32 particles' entries).
+//   k_rho_runs     - structure factors rho(k) = sum_i q_i exp(i k.r_i): a
+//                    lane holds RG particles, a warp walks runs, and per k
+//                    the warp sums its lanes' q exp(i k.r) with a fixed
+//                    shuffle tree (deterministic); partials per block row.
 //   k_rho_reduce   - a warp per k sums the block partials (each lane a fixed
 //                    stride of blocks, then a fixed shuffle tree: deterministic)
 //                    and the energy 4 pi / V sum_k inv_k2 exp(-k2/4a) |rho|^2.
-//   k_ewald_force  - 32 particles per block, 8 threads per particle, each over
-//                    every 8th k-vector (the particles' per-axis tables in
-//                    shared memory), the 8 partial forces summed by a fixed
-//                    shuffle tree: F_i = -8 pi q_i / V sum_k k inv_k2 exp(..)
-//                    (cos Im - sin Re).
+//   k_force_runs   - a lane per particle, the warps of a block over runs (the
+//                    k data of a run read by the whole warp at once), then the
+//                    warps' partial forces summed in a fixed order:
+//                    F_i = -8 pi q_i / V sum_k k inv_k2 exp(..) (cos Im - sin Re).
+// Per (particle, k) both passes take one complex product (the run step) and
+// three to five FP64 multiply-adds.
 // Both k-space passes visit the charged particles only (a list made once by
 // ewald_k(0)): the others contribute nothing to rho and feel no k-space force.
 // Slab correction (dipolar_correction.f90, SYMMETRY 0):
@@ -37,9 +41,6 @@ constexpr int KPT = 8;        // k per thread: a block row covers KPT * RHO_T ve
 constexpr int NK_MAX = 1 << 16;   // k-vectors of one context
 constexpr int CH = 32;        // particles per table batch
 constexpr int FT = 64;        // threads per block in k_ewald_adj
-constexpr int FP = 16;        // particles per block in k_ewald_force
-constexpr int FS = 16;        // threads per particle in k_ewald_force (k-vector stride)
-constexpr int TK = 256;       // k-vectors staged in shared memory at a time by k_ewald_force
 
 struct EwArgs {
     const double *rx, *ry, *rz, *q;
@@ -91,8 +92,10 @@ __device__ __forceinline__ double2 phase_from(const double2* t, int ts, int4 kn)
     return cmul(cmul(ex, ey), ez);
 }
 
-// blockIdx.x: a range of particles; blockIdx.y: a row of KPT * RHO_T k-vectors.
-// Dynamic shared memory: CH tables of 3 * ts phases, then CH charges.
+// Structure factors with a thread per k (the layout of the adjoint's
+// k_sig_partial, which runs beside it): blockIdx.x: a range of particles;
+// blockIdx.y: a row of KPT * RHO_T k-vectors.  Dynamic shared memory: CH
+// tables of 3 * ts phases, then CH charges.
 __global__ void __launch_bounds__(RHO_T) k_rho_partial(EwArgs a) {
     extern __shared__ double2 rtab[];
     double* sq = (double*)(rtab + CH * 3 * a.ts);
@@ -165,65 +168,142 @@ __global__ void k_rho_reduce(EwArgs a) {
         a.dscal[S_VCK] = ((a.dscal[S_TMP0 + 2] * 4.0) * a.pi) * a.inv_V;   // :159
 }
 
-template <typename R4>
-__global__ void __launch_bounds__(FP * FS) k_ewald_force(EwArgs a) {
-    extern __shared__ double2 ftab[];
-    // [FP x 3 x ts per-axis tables][TK k-vectors: index, rho, (k, A_k)]
-    int4* s_kn = (int4*)(ftab + FP * 3 * a.ts);
-    double2* s_rho = (double2*)(s_kn + TK);
-    double4* s_kv = (double4*)(s_rho + TK);
-    const int p = threadIdx.x / FS, sl = threadIdx.x % FS;
-    const int slot = blockIdx.x * FP + p;
-    const bool act = slot < a.nq;
-    const int i = act ? a.qidx[slot] : 0;
-    double2* t = ftab + p * 3 * a.ts;
-    // the particle's three per-axis tables, one axis per thread (sl < 3)
-    if (act && sl < 3) {
-        const double r = sl == 0 ? a.rx[i] : (sl == 1 ? a.ry[i] : a.rz[i]);
+constexpr int RP = 32;        // particles per block (a lane each) in k_force_runs
+constexpr int RW = 8;         // warps per block in the run kernels
+constexpr int RG = 2;         // particles per lane in k_rho_runs
+constexpr int RY = 2;         // block rows (run sets) of k_rho_runs
+
+// run r: (n_x of its first vector, n_y, n_z, index of its first vector); the
+// entry nrun holds nk in .w, so a run's length is runs[r+1].w - runs[r].w
+struct RunArgs {
+    const int4* runs;
+    int nrun;
+};
+
+// the per-axis tables of np particles (slots b0 ..), one (particle, axis) per
+// thread: t[(d * ts + n) * np + p] = exp(i n dk_d r_d)
+__device__ __forceinline__ void run_tables(double2* t, const EwArgs& a, int b0, int np) {
+    for (int w = threadIdx.x; w < 3 * np; w += blockDim.x) {
+        const int p = w % np, d = w / np;
+        const int slot = b0 + p;
+        double r = 0.0;
+        if (slot < a.nq) {
+            const int i = a.qidx[slot];
+            r = d == 0 ? a.rx[i] : (d == 1 ? a.ry[i] : a.rz[i]);
+        }
         double s, c;
-        sincos(a.dk[sl] * r, &s, &c);
+        sincos(a.dk[d] * r, &s, &c);
         const double2 e1 = make_double2(c, s);
         double2 e = make_double2(1.0, 0.0);
-        t[sl * a.ts] = e;
-        for (int n = 1; n <= a.kmax[sl]; ++n) {
+        t[(d * a.ts) * np + p] = e;
+        for (int n = 1; n <= a.kmax[d]; ++n) {
             e = cmul(e, e1);
-            t[sl * a.ts + n] = e;
+            t[(d * a.ts + n) * np + p] = e;
         }
     }
-    double fx = 0.0, fy = 0.0, fz = 0.0;
-    for (int k0 = 0; k0 < a.nk; k0 += TK) {
-        const int nt = min(TK, a.nk - k0);
-        __syncthreads();   // the tables are written / the previous tile is consumed
-        for (int j = threadIdx.x; j < nt; j += blockDim.x) {
-            s_kn[j] = a.kn[k0 + j];
-            s_rho[j] = a.rho[k0 + j];
-            s_kv[j] = a.kvec[k0 + j];
+}
+
+// exp(i n dk_d r_d) for a signed n (conjugate for n < 0)
+__device__ __forceinline__ double2 tab_at(const double2* t, int ts, int np, int d, int n, int p) {
+    double2 e = t[(d * ts + abs(n)) * np + p];
+    if (n < 0) e.y = -e.y;
+    return e;
+}
+
+// Dynamic shared memory: RG * 32 particles' tables, then their charges.
+// blockIdx.x: particles [blockIdx.x * 32 RG, +32 RG); blockIdx.y: runs
+// blockIdx.y * RW + warp, + RW * RY, ...
+__global__ void __launch_bounds__(RW * 32) k_rho_runs(EwArgs a, RunArgs ra) {
+    constexpr int NP = 32 * RG;
+    extern __shared__ double2 rt[];
+    double* sq = (double*)(rt + 3 * a.ts * NP);
+    const int b0 = blockIdx.x * NP;
+    run_tables(rt, a, b0, NP);
+    for (int p = threadIdx.x; p < NP; p += blockDim.x)
+        sq[p] = b0 + p < a.nq ? a.q[a.qidx[b0 + p]] : 0.0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double qg[RG];
+    double2 ex1[RG];
+#pragma unroll
+    for (int g = 0; g < RG; ++g) {
+        qg[g] = sq[lane + 32 * g];
+        ex1[g] = tab_at(rt, a.ts, NP, 0, 1, lane + 32 * g);
+    }
+    double2* part = a.rho_part + (size_t)blockIdx.x * a.nk;
+    for (int r = blockIdx.y * RW + warp; r < ra.nrun; r += RW * RY) {
+        const int4 run = __ldg(&ra.runs[r]);
+        const int k1 = __ldg(&ra.runs[r + 1].w);
+        double2 e[RG];
+#pragma unroll
+        for (int g = 0; g < RG; ++g) {
+            const int p = lane + 32 * g;
+            const double2 ezy = cmul(tab_at(rt, a.ts, NP, 2, run.z, p), tab_at(rt, a.ts, NP, 1, run.y, p));
+            e[g] = cmul(ezy, tab_at(rt, a.ts, NP, 0, run.x, p));
         }
-        __syncthreads();
-        if (act)
-            for (int j = sl; j < nt; j += FS) {
-                const double2 e = phase_from(t, a.ts, s_kn[j]);
-                const double2 r = s_rho[j];
-                const double4 kv = s_kv[j];
-                const double sc = (e.x * r.y - e.y * r.x) * kv.w;   // (cos Im - sin Re) inv_k2 exp()
-                fx += kv.x * sc;
-                fy += kv.y * sc;
-                fz += kv.z * sc;
+        for (int k = run.w; k < k1; ++k) {
+            double vx = 0.0, vy = 0.0;
+#pragma unroll
+            for (int g = 0; g < RG; ++g) {
+                vx += qg[g] * e[g].x;
+                vy += qg[g] * e[g].y;
+                e[g] = cmul(e[g], ex1[g]);
             }
+            for (int o = 16; o > 0; o >>= 1) {
+                vx += __shfl_down_sync(0xffffffffu, vx, o);
+                vy += __shfl_down_sync(0xffffffffu, vy, o);
+            }
+            if (lane == 0) part[k] = make_double2(vx, vy);
+        }
     }
-    // the FS partial sums of a particle: adjacent lanes, fixed tree
-    for (int o = FS / 2; o > 0; o >>= 1) {
-        fx += __shfl_down_sync(0xffffffffu, fx, o, FS);
-        fy += __shfl_down_sync(0xffffffffu, fy, o, FS);
-        fz += __shfl_down_sync(0xffffffffu, fz, o, FS);
+}
+
+// Dynamic shared memory: RP particles' tables, then RW x RP x 3 partial forces.
+template <typename R4>
+__global__ void __launch_bounds__(RW * 32) k_force_runs(EwArgs a, RunArgs ra) {
+    extern __shared__ double2 ft2[];
+    double* red = (double*)(ft2 + 3 * a.ts * RP);
+    const int b0 = blockIdx.x * RP;
+    run_tables(ft2, a, b0, RP);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double2 ex1 = tab_at(ft2, a.ts, RP, 0, 1, lane);
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    for (int r = warp; r < ra.nrun; r += RW) {
+        const int4 run = __ldg(&ra.runs[r]);
+        const int k1 = __ldg(&ra.runs[r + 1].w);
+        const double2 ezy = cmul(tab_at(ft2, a.ts, RP, 2, run.z, lane), tab_at(ft2, a.ts, RP, 1, run.y, lane));
+        double2 e = cmul(ezy, tab_at(ft2, a.ts, RP, 0, run.x, lane));
+        for (int k = run.w; k < k1; ++k) {
+            const double4 kv = a.kvec[k];
+            const double2 rk = __ldg(&a.rho[k]);
+            const double sc = (e.x * rk.y - e.y * rk.x) * kv.w;   // (cos Im - sin Re) inv_k2 exp()
+            fx += kv.x * sc;
+            fy += kv.y * sc;
+            fz += kv.z * sc;
+            e = cmul(e, ex1);
+        }
     }
-    if (!act || sl != 0) return;
+    red[(warp * RP + lane) * 3 + 0] = fx;
+    red[(warp * RP + lane) * 3 + 1] = fy;
+    red[(warp * RP + lane) * 3 + 2] = fz;
+    __syncthreads();
+    if (warp != 0) return;
+    const int slot = b0 + lane;
+    if (slot >= a.nq) return;
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int w = 0; w < RW; ++w) {
+        sx += red[(w * RP + lane) * 3 + 0];
+        sy += red[(w * RP + lane) * 3 + 1];
+        sz += red[(w * RP + lane) * 3 + 2];
+    }
+    const int i = a.qidx[slot];
     const double pre = ((-8.0 * a.pi) * a.q[i]) * a.inv_V;   // ewald_k.f90:194
     R4* f4 = (R4*)a.force;
     R4 o = f4[i];
-    o.x += pre * fx;
-    o.y += pre * fy;
-    o.z += pre * fz;
+    o.x += pre * sx;
+    o.y += pre * sy;
+    o.z += pre * sz;
     f4[i] = o;
 }
 
@@ -240,10 +320,14 @@ int reduce_grid(const mfa_ctx* c) {
     if (g > c->max_blocks) g = c->max_blocks;
     return g < 1 ? 1 : g;
 }
-size_t force_smem(const mfa_ctx* c) {
-    return (size_t)FP * 3 * table_stride(c) * sizeof(double2) + (size_t)TK * (sizeof(int4) + sizeof(double2) + sizeof(double4));
-}
 size_t adj_smem(const mfa_ctx* c) { return (size_t)FT * 3 * table_stride(c) * sizeof(double2); }
+size_t rho_runs_smem(const mfa_ctx* c) {
+    return (size_t)32 * RG * (3 * table_stride(c) * sizeof(double2) + sizeof(double));
+}
+size_t force_runs_smem(const mfa_ctx* c) {
+    return (size_t)RP * 3 * table_stride(c) * sizeof(double2) + (size_t)RW * RP * 3 * sizeof(double);
+}
+RunArgs run_args(const mfa_ctx* c) { return RunArgs{(const int4*)c->kruns, c->nrun}; }
 
 EwArgs make_args(mfa_ctx* c) {
     EwArgs a;
@@ -341,19 +425,36 @@ int ewald_setup(mfa_ctx* c) {
             MFA_CUDA_TRY(cudaMemcpyAsync(c->qidx, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice, c->st));
         MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
     }
-    int nblk = (c->nq + CH - 1) / CH;
-    if (nblk > 2 * 148) nblk = 2 * 148;
+    // runs of consecutive n_x at fixed (n_y, n_z); entry nrun closes the last
+    {
+        std::vector<int4> runs;
+        for (int k = 0; k < c->nk; ++k) {
+            const bool cont = k > 0 && kn[k].y == kn[k - 1].y && kn[k].z == kn[k - 1].z && kn[k].x == kn[k - 1].x + 1;
+            if (!cont) runs.push_back(make_int4(kn[k].x, kn[k].y, kn[k].z, k));
+        }
+        c->nrun = (int)runs.size();
+        runs.push_back(make_int4(0, 0, 0, c->nk));
+        if (c->kruns) cudaFree(c->kruns);
+        c->kruns = nullptr;
+        MFA_CUDA_TRY(cudaMalloc(&c->kruns, runs.size() * sizeof(int4)));
+        MFA_CUDA_TRY(cudaMemcpyAsync(c->kruns, runs.data(), runs.size() * sizeof(int4), cudaMemcpyHostToDevice, c->st));
+        MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
+    }
+    // block partials of rho: one per 32 RG charged particles
+    int nblk = (c->nq + 32 * RG - 1) / (32 * RG);
     if (nblk < 1) nblk = 1;
     c->nblk_rho = nblk;
     MFA_CUDA_TRY(cudaMalloc(&c->rho, (size_t)c->nk * sizeof(double2)));
     MFA_CUDA_TRY(cudaMalloc(&c->rho_part, (size_t)nblk * c->nk * sizeof(double2)));
     // the attribute is per function and shared by every context: admit the
     // largest tables any context can have (a launch passes its own size)
-    const int fsm = FP * 3 * (KM + 1) * (int)sizeof(double2) + TK * (int)(sizeof(int4) + sizeof(double2) + sizeof(double4));
     const int rsm = CH * (3 * (KM + 1) * (int)sizeof(double2) + (int)sizeof(double));
-    MFA_CUDA_TRY(cudaFuncSetAttribute(k_ewald_force<float4>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
-    MFA_CUDA_TRY(cudaFuncSetAttribute(k_ewald_force<double4>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
     MFA_CUDA_TRY(cudaFuncSetAttribute(k_rho_partial, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm));
+    const int rrs = 32 * RG * (3 * (KM + 1) * (int)sizeof(double2) + (int)sizeof(double));
+    const int frs = RP * 3 * (KM + 1) * (int)sizeof(double2) + RW * RP * 3 * (int)sizeof(double);
+    MFA_CUDA_TRY(cudaFuncSetAttribute(k_rho_runs, cudaFuncAttributeMaxDynamicSharedMemorySize, rrs));
+    MFA_CUDA_TRY(cudaFuncSetAttribute(k_force_runs<float4>, cudaFuncAttributeMaxDynamicSharedMemorySize, frs));
+    MFA_CUDA_TRY(cudaFuncSetAttribute(k_force_runs<double4>, cudaFuncAttributeMaxDynamicSharedMemorySize, frs));
     return MFA_OK;
 }
 
@@ -361,14 +462,13 @@ int launch_ewald(mfa_ctx* c) {
     if (!c->p.charged) return MFA_OK;
     if (c->nk == 0) return MFA_ERR_STATE;
     EwArgs a = make_args(c);
-    const dim3 rgrid(c->nblk_rho, (c->nk + KPT * RHO_T - 1) / (KPT * RHO_T));
-    k_rho_partial<<<rgrid, RHO_T, rho_smem(c), c->st>>>(a);
+    const RunArgs ra = run_args(c);
+    k_rho_runs<<<dim3(c->nblk_rho, RY), RW * 32, rho_runs_smem(c), c->st>>>(a, ra);
     k_rho_reduce<<<reduce_grid(c), 256, 0, c->st>>>(a);
-    const size_t fsm = force_smem(c);
-    const int fgrid = (c->nq + FP - 1) / FP;
+    const int fgrid = (c->nq + RP - 1) / RP;
     if (fgrid > 0) {
-        if (c->prec == MFA_MIXED) k_ewald_force<float4><<<fgrid, FP * FS, fsm, c->st>>>(a);
-        else k_ewald_force<double4><<<fgrid, FP * FS, fsm, c->st>>>(a);
+        if (c->prec == MFA_MIXED) k_force_runs<float4><<<fgrid, RW * 32, force_runs_smem(c), c->st>>>(a, ra);
+        else k_force_runs<double4><<<fgrid, RW * 32, force_runs_smem(c), c->st>>>(a, ra);
     }
     MFA_CUDA_TRY(cudaGetLastError());
     note_launch(c, 3);

@@ -108,6 +108,8 @@ struct mfa_ctx {
     double2* rho;                       // nk
     double2* rho_part;                  // nblk_rho x nk
     int nblk_rho;
+    void* kruns;                        // runs of the k-vectors (int4: n_x, n_y, n_z, first k), nrun + 1
+    int nrun;
     int* qidx;                          // ids of the charged particles (k-space sums skip the rest)
     int nq;
     int kmax[3];

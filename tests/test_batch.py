@@ -41,8 +41,8 @@ def _systems(cfgs, prec):
 @pytest.mark.parametrize("prec", [FP64, MIXED])
 @pytest.mark.parametrize("persist", ["1", "0"])
 def test_batch_equals_systems_stepped_alone(prec, persist, monkeypatch):
-    """One persistent cooperative launch per run (default), or grouped
-    launches per stage in captured graphs (MFA_BATCH_PERSIST=0)."""
+    """Grouped launches per stage in captured graphs (default), or one
+    persistent cooperative launch per run (MFA_BATCH_PERSIST=1)."""
     monkeypatch.setenv("MFA_BATCH_PERSIST", persist)
     cfgs = configs.uneven_brushes(seed=7, n_sys=4, grids=(4, 7), lengths=(16, 32))
     alone = _systems(cfgs, prec)
