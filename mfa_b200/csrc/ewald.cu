@@ -168,10 +168,15 @@ __global__ void k_rho_reduce(EwArgs a) {
         a.dscal[S_VCK] = ((a.dscal[S_TMP0 + 2] * 4.0) * a.pi) * a.inv_V;   // :159
 }
 
+// The run kernels take their warps per block from blockDim and k_rho_runs its
+// run sets from gridDim.y; ewald_setup chooses both from the occupancy
+// calculator so that the whole grid is resident at once (a second wave would
+// double the time: every block walks all of its runs).
 constexpr int RP = 32;        // particles per block (a lane each) in k_force_runs
-constexpr int RW = 8;         // warps per block in the run kernels
-constexpr int RG = 2;         // particles per lane in k_rho_runs
-constexpr int RY = 2;         // block rows (run sets) of k_rho_runs
+constexpr int RWMAX = 16;     // most warps per block in k_force_runs
+constexpr int RHW = 8;        // warps per block in k_rho_runs
+constexpr int RG = 4;         // particles per lane in k_rho_runs
+constexpr int RSEG = 8;       // longest run (longer ones are cut, for balance between warps)
 
 // run r: (n_x of its first vector, n_y, n_z, index of its first vector); the
 // entry nrun holds nk in .w, so a run's length is runs[r+1].w - runs[r].w
@@ -212,8 +217,8 @@ __device__ __forceinline__ double2 tab_at(const double2* t, int ts, int np, int 
 
 // Dynamic shared memory: RG * 32 particles' tables, then their charges.
 // blockIdx.x: particles [blockIdx.x * 32 RG, +32 RG); blockIdx.y: runs
-// blockIdx.y * RW + warp, + RW * RY, ...
-__global__ void __launch_bounds__(RW * 32) k_rho_runs(EwArgs a, RunArgs ra) {
+// blockIdx.y * RHW + warp, + RHW * gridDim.y, ...
+__global__ void __launch_bounds__(RHW * 32) k_rho_runs(EwArgs a, RunArgs ra) {
     constexpr int NP = 32 * RG;
     extern __shared__ double2 rt[];
     double* sq = (double*)(rt + 3 * a.ts * NP);
@@ -231,7 +236,7 @@ __global__ void __launch_bounds__(RW * 32) k_rho_runs(EwArgs a, RunArgs ra) {
         ex1[g] = tab_at(rt, a.ts, NP, 0, 1, lane + 32 * g);
     }
     double2* part = a.rho_part + (size_t)blockIdx.x * a.nk;
-    for (int r = blockIdx.y * RW + warp; r < ra.nrun; r += RW * RY) {
+    for (int r = blockIdx.y * RHW + warp; r < ra.nrun; r += RHW * gridDim.y) {
         const int4 run = __ldg(&ra.runs[r]);
         const int k1 = __ldg(&ra.runs[r + 1].w);
         double2 e[RG];
@@ -258,15 +263,15 @@ __global__ void __launch_bounds__(RW * 32) k_rho_runs(EwArgs a, RunArgs ra) {
     }
 }
 
-// Dynamic shared memory: RP particles' tables, then RW x RP x 3 partial forces.
+// Dynamic shared memory: RP particles' tables, then (warps) x RP x 3 partial forces.
 template <typename R4>
-__global__ void __launch_bounds__(RW * 32) k_force_runs(EwArgs a, RunArgs ra) {
+__global__ void __launch_bounds__(RWMAX * 32) k_force_runs(EwArgs a, RunArgs ra) {
     extern __shared__ double2 ft2[];
     double* red = (double*)(ft2 + 3 * a.ts * RP);
     const int b0 = blockIdx.x * RP;
     run_tables(ft2, a, b0, RP);
     __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, RW = blockDim.x >> 5;
     const double2 ex1 = tab_at(ft2, a.ts, RP, 0, 1, lane);
     double fx = 0.0, fy = 0.0, fz = 0.0;
     for (int r = warp; r < ra.nrun; r += RW) {
@@ -274,14 +279,29 @@ __global__ void __launch_bounds__(RW * 32) k_force_runs(EwArgs a, RunArgs ra) {
         const int k1 = __ldg(&ra.runs[r + 1].w);
         const double2 ezy = cmul(tab_at(ft2, a.ts, RP, 2, run.z, lane), tab_at(ft2, a.ts, RP, 1, run.y, lane));
         double2 e = cmul(ezy, tab_at(ft2, a.ts, RP, 0, run.x, lane));
-        for (int k = run.w; k < k1; ++k) {
+        // two vectors per iteration, each phase advanced by exp(2 i dk_x x):
+        // two independent recurrences in flight
+        double2 e2 = cmul(e, ex1);
+        const double2 ex2 = cmul(ex1, ex1);
+        int k = run.w;
+        for (; k + 1 < k1; k += 2) {
+            const double4 kv = a.kvec[k], kw = a.kvec[k + 1];
+            const double2 rk = __ldg(&a.rho[k]), rw = __ldg(&a.rho[k + 1]);
+            const double sc = (e.x * rk.y - e.y * rk.x) * kv.w;   // (cos Im - sin Re) inv_k2 exp()
+            const double sd = (e2.x * rw.y - e2.y * rw.x) * kw.w;
+            fx += kv.x * sc + kw.x * sd;
+            fy += kv.y * sc + kw.y * sd;
+            fz += kv.z * sc + kw.z * sd;
+            e = cmul(e, ex2);
+            e2 = cmul(e2, ex2);
+        }
+        if (k < k1) {
             const double4 kv = a.kvec[k];
             const double2 rk = __ldg(&a.rho[k]);
-            const double sc = (e.x * rk.y - e.y * rk.x) * kv.w;   // (cos Im - sin Re) inv_k2 exp()
+            const double sc = (e.x * rk.y - e.y * rk.x) * kv.w;
             fx += kv.x * sc;
             fy += kv.y * sc;
             fz += kv.z * sc;
-            e = cmul(e, ex1);
         }
     }
     red[(warp * RP + lane) * 3 + 0] = fx;
@@ -324,8 +344,8 @@ size_t adj_smem(const mfa_ctx* c) { return (size_t)FT * 3 * table_stride(c) * si
 size_t rho_runs_smem(const mfa_ctx* c) {
     return (size_t)32 * RG * (3 * table_stride(c) * sizeof(double2) + sizeof(double));
 }
-size_t force_runs_smem(const mfa_ctx* c) {
-    return (size_t)RP * 3 * table_stride(c) * sizeof(double2) + (size_t)RW * RP * 3 * sizeof(double);
+size_t force_runs_smem(const mfa_ctx* c, int warps) {
+    return (size_t)RP * 3 * table_stride(c) * sizeof(double2) + (size_t)warps * RP * 3 * sizeof(double);
 }
 RunArgs run_args(const mfa_ctx* c) { return RunArgs{(const int4*)c->kruns, c->nrun}; }
 
@@ -425,11 +445,12 @@ int ewald_setup(mfa_ctx* c) {
             MFA_CUDA_TRY(cudaMemcpyAsync(c->qidx, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice, c->st));
         MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
     }
-    // runs of consecutive n_x at fixed (n_y, n_z); entry nrun closes the last
+    // runs of consecutive n_x at fixed (n_y, n_z), at most RSEG long; entry nrun closes the last
     {
         std::vector<int4> runs;
         for (int k = 0; k < c->nk; ++k) {
-            const bool cont = k > 0 && kn[k].y == kn[k - 1].y && kn[k].z == kn[k - 1].z && kn[k].x == kn[k - 1].x + 1;
+            const bool cont = k > 0 && kn[k].y == kn[k - 1].y && kn[k].z == kn[k - 1].z &&
+                              kn[k].x == kn[k - 1].x + 1 && k - runs.back().w < RSEG;
             if (!cont) runs.push_back(make_int4(kn[k].x, kn[k].y, kn[k].z, k));
         }
         c->nrun = (int)runs.size();
@@ -451,10 +472,30 @@ int ewald_setup(mfa_ctx* c) {
     const int rsm = CH * (3 * (KM + 1) * (int)sizeof(double2) + (int)sizeof(double));
     MFA_CUDA_TRY(cudaFuncSetAttribute(k_rho_partial, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm));
     const int rrs = 32 * RG * (3 * (KM + 1) * (int)sizeof(double2) + (int)sizeof(double));
-    const int frs = RP * 3 * (KM + 1) * (int)sizeof(double2) + RW * RP * 3 * (int)sizeof(double);
+    const int frs = RP * 3 * (KM + 1) * (int)sizeof(double2) + RWMAX * RP * 3 * (int)sizeof(double);
     MFA_CUDA_TRY(cudaFuncSetAttribute(k_rho_runs, cudaFuncAttributeMaxDynamicSharedMemorySize, rrs));
     MFA_CUDA_TRY(cudaFuncSetAttribute(k_force_runs<float4>, cudaFuncAttributeMaxDynamicSharedMemorySize, frs));
     MFA_CUDA_TRY(cudaFuncSetAttribute(k_force_runs<double4>, cudaFuncAttributeMaxDynamicSharedMemorySize, frs));
+    // launch shapes that keep each grid resident at once: the structure-factor
+    // pass adds run sets (block rows) while they fit, the force pass takes the
+    // most warps per block that still fit every block
+    {
+        int occ = 0;
+        MFA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rho_runs, RHW * 32, rho_runs_smem(c)));
+        const int cap = (occ > 0 ? occ : 1) * c->n_sm;
+        int ry = cap / nblk;
+        c->ew_rho_rows = ry < 1 ? 1 : (ry > 16 ? 16 : ry);
+        const int fb = (c->nq + RP - 1) / RP;
+        const void* ff = c->prec == MFA_MIXED ? (const void*)k_force_runs<float4> : (const void*)k_force_runs<double4>;
+        c->ew_force_warps = 4;
+        for (int w = RWMAX; w > 4; --w) {
+            MFA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ff, w * 32, force_runs_smem(c, w)));
+            if ((long long)occ * c->n_sm >= fb) {
+                c->ew_force_warps = w;
+                break;
+            }
+        }
+    }
     return MFA_OK;
 }
 
@@ -463,12 +504,13 @@ int launch_ewald(mfa_ctx* c) {
     if (c->nk == 0) return MFA_ERR_STATE;
     EwArgs a = make_args(c);
     const RunArgs ra = run_args(c);
-    k_rho_runs<<<dim3(c->nblk_rho, RY), RW * 32, rho_runs_smem(c), c->st>>>(a, ra);
+    k_rho_runs<<<dim3(c->nblk_rho, c->ew_rho_rows), RHW * 32, rho_runs_smem(c), c->st>>>(a, ra);
     k_rho_reduce<<<reduce_grid(c), 256, 0, c->st>>>(a);
     const int fgrid = (c->nq + RP - 1) / RP;
+    const int fw = c->ew_force_warps;
     if (fgrid > 0) {
-        if (c->prec == MFA_MIXED) k_force_runs<float4><<<fgrid, RW * 32, force_runs_smem(c), c->st>>>(a, ra);
-        else k_force_runs<double4><<<fgrid, RW * 32, force_runs_smem(c), c->st>>>(a, ra);
+        if (c->prec == MFA_MIXED) k_force_runs<float4><<<fgrid, fw * 32, force_runs_smem(c, fw), c->st>>>(a, ra);
+        else k_force_runs<double4><<<fgrid, fw * 32, force_runs_smem(c, fw), c->st>>>(a, ra);
     }
     MFA_CUDA_TRY(cudaGetLastError());
     note_launch(c, 3);
