@@ -471,7 +471,12 @@ int ewald_setup(mfa_ctx* c) {
     // largest tables any context can have (a launch passes its own size)
     const int rsm = CH * (3 * (KM + 1) * (int)sizeof(double2) + (int)sizeof(double));
     MFA_CUDA_TRY(cudaFuncSetAttribute(k_rho_partial, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm));
-    const int rrs = 32 * RG * (3 * (KM + 1) * (int)sizeof(double2) + (int)sizeof(double));
+    // (k_rho_runs: as far as the device's shared memory per block goes; a
+    // context whose tables need more uses k_rho_partial)
+    int optin = 0;
+    MFA_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dev));
+    int rrs = 32 * RG * (3 * (KM + 1) * (int)sizeof(double2) + (int)sizeof(double));
+    if (rrs > optin) rrs = optin;
     const int frs = RP * 3 * (KM + 1) * (int)sizeof(double2) + RWMAX * RP * 3 * (int)sizeof(double);
     MFA_CUDA_TRY(cudaFuncSetAttribute(k_rho_runs, cudaFuncAttributeMaxDynamicSharedMemorySize, rrs));
     MFA_CUDA_TRY(cudaFuncSetAttribute(k_force_runs<float4>, cudaFuncAttributeMaxDynamicSharedMemorySize, frs));
@@ -481,10 +486,14 @@ int ewald_setup(mfa_ctx* c) {
     // most warps per block that still fit every block
     {
         int occ = 0;
-        MFA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rho_runs, RHW * 32, rho_runs_smem(c)));
-        const int cap = (occ > 0 ? occ : 1) * c->n_sm;
-        int ry = cap / nblk;
-        c->ew_rho_rows = ry < 1 ? 1 : (ry > 16 ? 16 : ry);
+        if (rho_runs_smem(c) <= (size_t)rrs) {
+            MFA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rho_runs, RHW * 32, rho_runs_smem(c)));
+            const int cap = (occ > 0 ? occ : 1) * c->n_sm;
+            const int ry = cap / nblk;
+            c->ew_rho_rows = ry < 1 ? 1 : (ry > 16 ? 16 : ry);
+        } else {
+            c->ew_rho_rows = 0;   // k_rho_partial
+        }
         const int fb = (c->nq + RP - 1) / RP;
         const void* ff = c->prec == MFA_MIXED ? (const void*)k_force_runs<float4> : (const void*)k_force_runs<double4>;
         c->ew_force_warps = 4;
@@ -504,7 +513,12 @@ int launch_ewald(mfa_ctx* c) {
     if (c->nk == 0) return MFA_ERR_STATE;
     EwArgs a = make_args(c);
     const RunArgs ra = run_args(c);
-    k_rho_runs<<<dim3(c->nblk_rho, c->ew_rho_rows), RHW * 32, rho_runs_smem(c), c->st>>>(a, ra);
+    if (c->ew_rho_rows > 0) {
+        k_rho_runs<<<dim3(c->nblk_rho, c->ew_rho_rows), RHW * 32, rho_runs_smem(c), c->st>>>(a, ra);
+    } else {
+        const dim3 rgrid(c->nblk_rho, (c->nk + KPT * RHO_T - 1) / (KPT * RHO_T));
+        k_rho_partial<<<rgrid, RHO_T, rho_smem(c), c->st>>>(a);
+    }
     k_rho_reduce<<<reduce_grid(c), 256, 0, c->st>>>(a);
     const int fgrid = (c->nq + RP - 1) / RP;
     const int fw = c->ew_force_warps;

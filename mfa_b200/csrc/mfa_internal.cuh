@@ -110,7 +110,7 @@ struct mfa_ctx {
     int nblk_rho;
     void* kruns;                        // runs of the k-vectors (int4: n_x, n_y, n_z, first k), nrun + 1
     int nrun;
-    int ew_rho_rows, ew_force_warps;    // launch shapes of the k-space passes (ewald_setup)
+    int ew_rho_rows, ew_force_warps;    // launch shapes of the k-space passes (ewald_setup; rows 0: k_rho_partial)
     int* qidx;                          // ids of the charged particles (k-space sums skip the rest)
     int nq;
     int kmax[3];

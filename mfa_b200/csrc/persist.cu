@@ -103,8 +103,8 @@ __device__ __noinline__ bool stage_rebuild(const PersistArgs& p, const BinArgs* 
     return true;
 }
 
-// 64 registers: four CTAs of 256 threads per SM (the integrator's bonded window
-// would spill at 48)
+// FP32: 64 registers, four CTAs of 256 threads per SM (the integrator's bonded
+// window would spill at 48); FP64: 128 registers, two CTAs (the FP64 pair body)
 template <typename R4, typename R, int K, int FT>
 __global__ void __launch_bounds__(PT, sizeof(R) == 4 ? 4 : 2) k_batch_run(PersistArgs p) {
     stage_vv<R4>(p, p.vvpos, VV_POSITIONS, 0);
