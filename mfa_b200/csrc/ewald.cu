@@ -279,29 +279,14 @@ __global__ void __launch_bounds__(RWMAX * 32) k_force_runs(EwArgs a, RunArgs ra)
         const int k1 = __ldg(&ra.runs[r + 1].w);
         const double2 ezy = cmul(tab_at(ft2, a.ts, RP, 2, run.z, lane), tab_at(ft2, a.ts, RP, 1, run.y, lane));
         double2 e = cmul(ezy, tab_at(ft2, a.ts, RP, 0, run.x, lane));
-        // two vectors per iteration, each phase advanced by exp(2 i dk_x x):
-        // two independent recurrences in flight
-        double2 e2 = cmul(e, ex1);
-        const double2 ex2 = cmul(ex1, ex1);
-        int k = run.w;
-        for (; k + 1 < k1; k += 2) {
-            const double4 kv = a.kvec[k], kw = a.kvec[k + 1];
-            const double2 rk = __ldg(&a.rho[k]), rw = __ldg(&a.rho[k + 1]);
-            const double sc = (e.x * rk.y - e.y * rk.x) * kv.w;   // (cos Im - sin Re) inv_k2 exp()
-            const double sd = (e2.x * rw.y - e2.y * rw.x) * kw.w;
-            fx += kv.x * sc + kw.x * sd;
-            fy += kv.y * sc + kw.y * sd;
-            fz += kv.z * sc + kw.z * sd;
-            e = cmul(e, ex2);
-            e2 = cmul(e2, ex2);
-        }
-        if (k < k1) {
+        for (int k = run.w; k < k1; ++k) {
             const double4 kv = a.kvec[k];
             const double2 rk = __ldg(&a.rho[k]);
-            const double sc = (e.x * rk.y - e.y * rk.x) * kv.w;
+            const double sc = (e.x * rk.y - e.y * rk.x) * kv.w;   // (cos Im - sin Re) inv_k2 exp()
             fx += kv.x * sc;
             fy += kv.y * sc;
             fz += kv.z * sc;
+            e = cmul(e, ex1);
         }
     }
     red[(warp * RP + lane) * 3 + 0] = fx;
