@@ -53,6 +53,7 @@ struct BinArgs {
     int conditional;
     int rule;            // 0: binning.f90, 1: my_binning.f90
     int prefilter;       // FP32 prefilter of list candidates (n_bin >= 3 on every axis)
+    int dense;           // crowded cells (prefilter grids only): a warp per cell sorts, 4 warps per chunk build
     float prefilter_margin;
     int in_cond_body;    // launched from a conditional graph node: count the rebuild there
     int with_pos64;      // the gather also writes the list builder's FP64/FP32 copies
@@ -180,20 +181,52 @@ __device__ __forceinline__ void cell_scatter_body(const BinArgs& a, Blk blk) {
     a.ids[p] = i;
 }
 
-// insertion sort of each cell's ids (cells hold a few to a few tens of
-// particles); the row histogram is cleared here for the next rebuild
+// each cell's ids in ascending order; the row histogram is cleared here for
+// the next rebuild.  Thread per cell: insertion sort (cells of a few to a few
+// tens of particles).  Crowded cells (dense): a warp per cell, each lane ranks
+// up to 4 ids against all of the cell's ids (ids are distinct) and writes them
+// to their places -- O(k) steps for the warp instead of O(k^2) for one thread;
+// a cell of more than 128 falls back to lane 0's insertion sort.
+__device__ __forceinline__ void insertion_sort_ids(int32_t* ids, int b, int e) {
+    for (int k = b + 1; k < e; ++k) {
+        const int v = ids[k];
+        int j = k - 1;
+        while (j >= b && ids[j] > v) { ids[j + 1] = ids[j]; --j; }
+        ids[j + 1] = v;
+    }
+}
+
 __device__ __forceinline__ void cell_sort_body(const BinArgs& a, Blk blk) {
     if (skip(a)) return;
-    const int c = blk.id * blockDim.x + threadIdx.x;
-    if (c < a.nrow) a.row_count[c] = 0;
-    if (c >= a.ncell) return;
-    const int b = a.cell_start[c], e = a.cell_start[c + 1];
-    for (int k = b + 1; k < e; ++k) {
-        const int v = a.ids[k];
-        int j = k - 1;
-        while (j >= b && a.ids[j] > v) { a.ids[j + 1] = a.ids[j]; --j; }
-        a.ids[j + 1] = v;
+    const int t = blk.id * blockDim.x + threadIdx.x;
+    if (t < a.nrow) a.row_count[t] = 0;
+    if (!a.dense) {
+        if (t >= a.ncell) return;
+        insertion_sort_ids(a.ids, a.cell_start[t], a.cell_start[t + 1]);
+        return;
     }
+    const int c = t >> 5, lane = t & 31;      // c is the same for the whole warp
+    if (c >= a.ncell) return;
+    const int b = a.cell_start[c], k = a.cell_start[c + 1] - b;
+    if (k > 128) {
+        if (lane == 0) insertion_sort_ids(a.ids, b, b + k);
+        return;
+    }
+    int v[4], rk[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        v[m] = lane + 32 * m < k ? a.ids[b + lane + 32 * m] : 0x7fffffff;
+        rk[m] = 0;
+    }
+    for (int j = 0; j < k; ++j) {
+        const int w = a.ids[b + j];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) rk[m] += w < v[m] ? 1 : 0;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+        if (lane + 32 * m < k) a.ids[b + rk[m]] = v[m];
 }
 
 template <typename R4>
@@ -270,23 +303,32 @@ __device__ __forceinline__ void build_nbr_body(const BinArgs& a, Blk blk) {
     if (skip(a)) return;
     __shared__ double sc[T8 * T8];
     __shared__ float scmax[T8];
+    // the list of a 32-slot chunk is one run of entries (partner slot << 5 |
+    // owner lane), appended through a shared cursor.  A chunk is one warp, or
+    // with crowded cells (dense) four warps that split the owners' nine
+    // neighbouring rows (3, 2, 2 and 2 of them), their counts summed in
+    // shared memory.
+    __shared__ int wcur[32];
+    __shared__ int ccnt[8 * 32];
+    const int R = a.dense ? 4 : 1;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int cib = wib / R, part = wib - cib * R;
+    const int chunk = blk.id * ((blockDim.x >> 5) / R) + cib;
+    const int t = (chunk << 5) + lane;
+    const long long capc = 32LL * a.maxnb;
+    int32_t* crow = a.nbr + (size_t)chunk * capc;
     for (int k = threadIdx.x; k < T8 * T8; k += blockDim.x) sc[k] = a.cut2[k];
     if (threadIdx.x < T8) {
         double m = 0.0;
         for (int k = 0; k < T8; ++k) m = fmax(m, a.cut2[threadIdx.x * T8 + k]);
         scmax[threadIdx.x] = (float)m + a.prefilter_margin;
     }
+    if (part == 0) {
+        if (lane == 0) wcur[cib] = 0;
+        if (R > 1) ccnt[cib * 32 + lane] = 0;
+    }
     __syncthreads();
-    // the list of a 32-slot chunk (this warp) is one run of entries
-    // (partner slot << 5 | owner lane), appended through a shared cursor
-    __shared__ int wcur[32];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int t = blk.id * blockDim.x + threadIdx.x;
-    const int chunk = t >> 5;
-    const long long capc = 32LL * a.maxnb;
-    int32_t* crow = a.nbr + (size_t)chunk * capc;
-    if (lane == 0) wcur[wib] = 0;
-    __syncwarp();
+    int cnt = 0;
     if (t < a.n) {
         const double4 pi = a.pos64[t];
         const int wi = wbits(pi.w);
@@ -297,7 +339,6 @@ __device__ __forceinline__ void build_nbr_body(const BinArgs& a, Blk blk) {
         const int cx = cell_coord(a, pi.x, 0, bad), cy = cell_coord(a, pi.y, 1, bad),
                   cz = cell_coord(a, pi.z, 2, bad);
         const int trow = (ti - 1) * T8 - 1;
-        int cnt = 0;
         // the reference's FP64 test of candidate slot s (binning.f90:89-104)
         auto exact = [&](int s) {
             const double4 pj = a.pos64[s];
@@ -308,7 +349,7 @@ __device__ __forceinline__ void build_nbr_body(const BinArgs& a, Blk blk) {
             if (a.symmetry == 1) d2 = mimage64(d2, a.L[2], a.invL[2]);
             const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
             if (r2 < sc[trow + tj]) {
-                const int q = atomicAdd(&wcur[wib], 1);
+                const int q = atomicAdd(&wcur[cib], 1);
                 if (q < capc) crow[q] = (s << 5) | lane;
                 ++cnt;
             }
@@ -327,6 +368,8 @@ __device__ __forceinline__ void build_nbr_body(const BinArgs& a, Blk blk) {
             const float sxb = cx == 0 ? 0.0f : -Lx;
             for (int iz = 0; iz < 3; ++iz)
             for (int iy = 0; iy < 3; ++iy) {
+                const int rr = 3 * iz + iy;
+                if (R > 1 && part != (rr < 3 ? 0 : (rr - 1) >> 1)) continue;
                 int ky, kz;
                 neighbour_row(a.rule, cy, cz, iy, iz, ny, nz, ky, kz);
                 const int uy = cy - 1 + iy, uz = cz - 1 + iz;
@@ -349,7 +392,7 @@ __device__ __forceinline__ void build_nbr_body(const BinArgs& a, Blk blk) {
                     }
                 }
             }
-        } else {
+        } else if (part == 0) {
             const int wx = a.rule == 0 ? a.dl[0] + 2 : 3;
             const int wy = a.rule == 0 ? a.dl[1] + 2 : 3;
             const int wz = a.rule == 0 ? a.dl[2] + 2 : 3;
@@ -369,21 +412,26 @@ __device__ __forceinline__ void build_nbr_body(const BinArgs& a, Blk blk) {
                 }
             }
         }
-        a.nnb[t] = cnt;
+        if (R > 1) atomicAdd(&ccnt[cib * 32 + lane], cnt);
     }
-    // the longest row: one atomic per warp (a per-thread atomic on this one
-    // address would serialise every thread of the grid at one L2 slice)
-    {
-        const int mx = __reduce_max_sync(0xffffffffu, t < a.n ? a.nnb[t] : 0);
+    __syncthreads();
+    if (part == 0) {
+        int mine = 0;
+        if (t < a.n) {
+            mine = R > 1 ? ccnt[cib * 32 + lane] : cnt;
+            a.nnb[t] = mine;
+        }
+        // the longest row: one atomic per warp (a per-thread atomic on this one
+        // address would serialise every thread of the grid at one L2 slice)
+        const int mx = __reduce_max_sync(0xffffffffu, mine);
         if (lane == 0 && mx > 0) atomicMax(&a.flags[F_MAXNB], mx);
-    }
-    __syncwarp();
-    if (lane == 0 && chunk * 32 < a.n) {
-        const int total = wcur[wib];
-        a.ccount[chunk] = (int)(total < capc ? total : capc);
-        if (total > capc) {
-            set_err(a.flags, MFA_ERR_NEIGH_OVERFLOW);
-            atomicMax(&a.flags[F_NEEDNB], (total + 31) / 32);
+        if (lane == 0 && chunk * 32 < a.n) {
+            const int total = wcur[cib];
+            a.ccount[chunk] = (int)(total < capc ? total : capc);
+            if (total > capc) {
+                set_err(a.flags, MFA_ERR_NEIGH_OVERFLOW);
+                atomicMax(&a.flags[F_NEEDNB], (total + 31) / 32);
+            }
         }
     }
     // the last block to finish closes the rebuild: f_skin = 0 (binning.f90:125)
@@ -540,6 +588,27 @@ __global__ void __launch_bounds__(COOP_T, 5) k_rebuild_coop(BinArgs a) {
 // block size of each rebuild stage (assign, row scan, scatter, sort, gather, build)
 constexpr int BIN_T[N_BIN_STAGES] = {256, 256, 256, 128, 256, 128};
 
+// crowded cells (8 or more particles on average, on a grid of at least 3
+// cells per axis): the sort and the list build take more threads per cell
+int bin_dense(const mfa_ctx* c) {
+    return c->nb[0] >= 3 && c->nb[1] >= 3 && c->nb[2] >= 3 && (long long)c->n >= 8LL * c->ncell;
+}
+
+// blocks of T threads of each rebuild stage (T a multiple of 128)
+int bin_stage_blocks(const mfa_ctx* c, int stage, int T) {
+    const int nrow = c->nb[1] * c->nb[2];
+    const bool dense = bin_dense(c) != 0;
+    switch (stage) {
+        case 1: return (nrow + T / 32 - 1) / (T / 32);
+        case 3: return dense ? (int)(((long long)c->ncell * 32 + T - 1) / T) : (c->ncell + T - 1) / T;
+        case 5: {
+            const int nchunk = (c->n + 31) / 32, per = dense ? T / 128 : T / 32;
+            return (nchunk + per - 1) / per;
+        }
+        default: return (c->n + T - 1) / T;
+    }
+}
+
 BinArgs make_args(mfa_ctx* c, int rule, int conditional) {
     BinArgs a;
     a.rx = c->rx; a.ry = c->ry; a.rz = c->rz; a.vx = c->vx; a.vy = c->vy; a.vz = c->vz;
@@ -567,6 +636,7 @@ BinArgs make_args(mfa_ctx* c, int rule, int conditional) {
     for (int d = 0; d < 3; ++d) lmax = fmax(lmax, c->p.boundary[d]);
     for (int k = 0; k < T8 * T8; ++k) c2max = fmax(c2max, c->p.range_2[k] + c->p.skin_2);
     a.prefilter = c->nb[0] >= 3 && c->nb[1] >= 3 && c->nb[2] >= 3;
+    a.dense = bin_dense(c);
     a.prefilter_margin = (float)(0.01 + 1e-4 * (lmax + 1.0) * sqrt(c2max));
     return a;
 }
@@ -586,13 +656,7 @@ int bin_stage_args(mfa_ctx* c, int rule, int conditional, int in_cond_body, void
     a.in_cond_body = in_cond_body;
     a.with_pos64 = 1;
     a.cut2 = c->tabs;
-    const int nrow = c->nb[1] * c->nb[2];
-    nblocks[0] = (c->n + BIN_T[0] - 1) / BIN_T[0];
-    nblocks[1] = (nrow + BIN_T[1] / 32 - 1) / (BIN_T[1] / 32);
-    nblocks[2] = (c->n + BIN_T[2] - 1) / BIN_T[2];
-    nblocks[3] = (c->ncell + BIN_T[3] - 1) / BIN_T[3];
-    nblocks[4] = (c->n + BIN_T[4] - 1) / BIN_T[4];
-    nblocks[5] = (c->n + BIN_T[5] - 1) / BIN_T[5];
+    for (int s = 0; s < N_BIN_STAGES; ++s) nblocks[s] = bin_stage_blocks(c, s, BIN_T[s]);
     memcpy(out, &a, sizeof(a));
     return MFA_OK;
 }
@@ -632,13 +696,7 @@ int launch_rebuild_coop(mfa_ctx* c, int rule) {
     BinArgs a;
     int nb[N_BIN_STAGES];
     TRY_(bin_stage_args(c, rule, 0, 0, &a, nb));
-    const int nrow = c->nb[1] * c->nb[2];
-    a.vnb[0] = (c->n + COOP_T - 1) / COOP_T;
-    a.vnb[1] = (nrow + COOP_T / 32 - 1) / (COOP_T / 32);
-    a.vnb[2] = (c->n + COOP_T - 1) / COOP_T;
-    a.vnb[3] = (c->ncell + COOP_T - 1) / COOP_T;
-    a.vnb[4] = (c->n + COOP_T - 1) / COOP_T;
-    a.vnb[5] = (c->n + COOP_T - 1) / COOP_T;
+    for (int s = 0; s < N_BIN_STAGES; ++s) a.vnb[s] = bin_stage_blocks(c, s, COOP_T);
     a.bar = c->grid_bar;
     a.stage_ns = c->coop_stage_ns;
     const void* fn = c->prec == MFA_MIXED ? (const void*)k_rebuild_coop<float4> : (const void*)k_rebuild_coop<double4>;

@@ -159,13 +159,7 @@ int persist_threads() { return PT; }
 // block counts of the rebuild stages for PT-thread CTAs (the stage bodies take
 // their geometry from blockDim)
 void persist_bin_blocks(const mfa_ctx* c, int nb[N_BIN_STAGES]) {
-    const int nrow = c->nb[1] * c->nb[2];
-    nb[0] = (c->n + PT - 1) / PT;
-    nb[1] = (nrow + PT / 32 - 1) / (PT / 32);
-    nb[2] = (c->n + PT - 1) / PT;
-    nb[3] = (c->ncell + PT - 1) / PT;
-    nb[4] = (c->n + PT - 1) / PT;
-    nb[5] = (c->n + PT - 1) / PT;
+    for (int s = 0; s < N_BIN_STAGES; ++s) nb[s] = bin_stage_blocks(c, s, PT);
 }
 
 // Writes the argument record of the persistent kernel (device table pointers,
