@@ -50,6 +50,7 @@ struct EwArgs {
     const int4* kn;           // nx, ny, nz
     double2* rho_part;
     double2* rho;
+    double2* rhow;            // rho(k) * inv_k2 exp(-k2/4a) (the force pass's weight per k)
     void* force;
     double* partials;
     unsigned* counter;
@@ -161,6 +162,8 @@ __global__ void k_rho_reduce(EwArgs a) {
         const double2 s = warp_sum_partials(a.rho_part, a.nblk, a.nk, k, lane);
         if (lane == 0) {
             a.rho[k] = s;
+            const double w = a.kvec[k].w;
+            a.rhow[k] = make_double2(s.x * w, s.y * w);
             acc[0] += a.kvec[k].w * (s.x * s.x + s.y * s.y);   // ewald_k.f90:155-156
         }
     }
@@ -279,15 +282,18 @@ __global__ void __launch_bounds__(RWMAX * 32) k_force_runs(EwArgs a, RunArgs ra)
         const int k1 = __ldg(&ra.runs[r + 1].w);
         const double2 ezy = cmul(tab_at(ft2, a.ts, RP, 2, run.z, lane), tab_at(ft2, a.ts, RP, 1, run.y, lane));
         double2 e = cmul(ezy, tab_at(ft2, a.ts, RP, 0, run.x, lane));
+        // along a run k_y and k_z are fixed and k_x = n_x dk_x (the product the
+        // k-set is built with); one 16-byte load per k: rho(k) A_k
+        double ssum = 0.0;
         for (int k = run.w; k < k1; ++k) {
-            const double4 kv = a.kvec[k];
-            const double2 rk = __ldg(&a.rho[k]);
-            const double sc = (e.x * rk.y - e.y * rk.x) * kv.w;   // (cos Im - sin Re) inv_k2 exp()
-            fx += kv.x * sc;
-            fy += kv.y * sc;
-            fz += kv.z * sc;
+            const double2 rw = __ldg(&a.rhow[k]);
+            const double sc = e.x * rw.y - e.y * rw.x;   // (cos Im - sin Re) inv_k2 exp()
+            fx += ((double)(run.x + (k - run.w)) * a.dk[0]) * sc;
+            ssum += sc;
             e = cmul(e, ex1);
         }
+        fy += ((double)run.y * a.dk[1]) * ssum;
+        fz += ((double)run.z * a.dk[2]) * ssum;
     }
     red[(warp * RP + lane) * 3 + 0] = fx;
     red[(warp * RP + lane) * 3 + 1] = fy;
@@ -338,7 +344,7 @@ EwArgs make_args(mfa_ctx* c) {
     EwArgs a;
     a.rx = c->rx; a.ry = c->ry; a.rz = c->rz; a.q = c->q;
     a.kvec = c->kvec; a.kn = (const int4*)(c->kvec + c->nk);
-    a.rho_part = c->rho_part; a.rho = c->rho; a.force = c->force;
+    a.rho_part = c->rho_part; a.rho = c->rho; a.rhow = c->rho + c->nk; a.force = c->force;
     a.qidx = c->qidx; a.nq = c->nq;
     a.partials = c->partials + (size_t)R_EWALD * 4 * c->max_blocks;
     a.counter = c->counters + R_EWALD;
@@ -450,7 +456,7 @@ int ewald_setup(mfa_ctx* c) {
     int nblk = (c->nq + 32 * RG - 1) / (32 * RG);
     if (nblk < 1) nblk = 1;
     c->nblk_rho = nblk;
-    MFA_CUDA_TRY(cudaMalloc(&c->rho, (size_t)c->nk * sizeof(double2)));
+    MFA_CUDA_TRY(cudaMalloc(&c->rho, (size_t)2 * c->nk * sizeof(double2)));   // rho, then rho * A_k
     MFA_CUDA_TRY(cudaMalloc(&c->rho_part, (size_t)nblk * c->nk * sizeof(double2)));
     // the attribute is per function and shared by every context: admit the
     // largest tables any context can have (a launch passes its own size)
