@@ -55,10 +55,6 @@ struct VVArgs {
     // launches pass both as kernel parameters instead)
     long long energy_span;
     int energy_reset;
-    // fused pass: beads [0, pair0) a thread each (the chains, with their bonded
-    // window), the rest two per thread, j and j + pair_half (no bonds: short
-    // work); pair0 = n, pair_half = 0 leaves one bead per thread everywhere
-    int pair0, pair_half;
 };
 
 // r += dt v + (0.5 dt^2) a ; v += (0.5 dt) a   (verlet_positions.f90:153,169)
@@ -254,29 +250,21 @@ __device__ __forceinline__ void vv_velocities_body(const VVArgs& a, Blk blk, int
 // COND: the kernel may open the rebuild's conditional graph node (a kernel
 // that can does not run under profilers that replay graph nodes one by one,
 // so the launches without a node use the variant that cannot)
-template <typename R4>
-__device__ __forceinline__ double fused_bead(const VVArgs& a, int i, double eb[2], int& clamped) {
-    decltype(R4::x) fb[3] = {0, 0, 0};
-    if (a.fuse_bonds) bonded_on_bead(a.bond, i, fb, eb[0], eb[1], clamped);
-    double vx = a.vx[i], vy = a.vy[i], vz = a.vz[i], ax, ay, az;
-    const double ke = velocity_half<R4>(a, i, vx, vy, vz, ax, ay, az, fb, false);
-    R4 z4; z4.x = 0; z4.y = 0; z4.z = 0; z4.w = 0;
-    ((R4*)a.force)[i] = z4;
-    // a = F/m is used at once by the position half; the stored copy of a
-    // is written by the velocity half that closes a run of steps
-    position_half<R4>(a, i, a.rx[i], a.ry[i], a.rz[i], vx, vy, vz, ax, ay, az, true);
-    return ke;
-}
-
 template <typename R4, bool COND>
 __device__ __forceinline__ void vv_fused_body(const VVArgs& a, Blk blk) {
-    const int j = blk.id * blockDim.x + threadIdx.x;
+    const int i = blk.id * blockDim.x + threadIdx.x;
     double ke = 0.0, eb[2] = {0.0, 0.0};
     int clamped = 0;
-    if (j < a.n && j < a.pair0 + a.pair_half) {
-        ke = fused_bead<R4>(a, j, eb, clamped);
-        const int j2 = j + a.pair_half;
-        if (j >= a.pair0 && j2 < a.n) ke += fused_bead<R4>(a, j2, eb, clamped);
+    decltype(R4::x) fb[3] = {0, 0, 0};
+    if (i < a.n && a.fuse_bonds) bonded_on_bead(a.bond, i, fb, eb[0], eb[1], clamped);
+    if (i < a.n) {
+        double vx = a.vx[i], vy = a.vy[i], vz = a.vz[i], ax, ay, az;
+        ke = velocity_half<R4>(a, i, vx, vy, vz, ax, ay, az, fb, false);
+        R4 z4; z4.x = 0; z4.y = 0; z4.z = 0; z4.w = 0;
+        ((R4*)a.force)[i] = z4;
+        // a = F/m is used at once by the position half; the stored copy of a
+        // is written by the velocity half that closes a run of steps
+        position_half<R4>(a, i, a.rx[i], a.ry[i], a.rz[i], vx, vy, vz, ax, ay, az, true);
     }
     // every block reads the step before the last block advances it
     const bool en = energy_needed(a.dstep, a.elog ? a.elog_every : 0);
@@ -322,8 +310,6 @@ __global__ void VV_BOUNDS
 
 VVArgs make_args(mfa_ctx* c) {
     VVArgs a;
-    a.pair0 = c->n;
-    a.pair_half = 0;
     a.rx = c->rx; a.ry = c->ry; a.rz = c->rz;
     a.vx = c->vx; a.vy = c->vy; a.vz = c->vz;
     a.ax = c->ax; a.ay = c->ay; a.az = c->az;
@@ -448,22 +434,6 @@ int launch_vv_fused(mfa_ctx* c, cudaGraphConditionalHandle rebuild_cond, int fus
     VVArgs a;
     int nb;
     TRY_(vv_stage_args(c, VV_FUSED, 1, 1, fuse_bonds, rebuild_cond, &a, &nb));
-    // the beads past the last chain (solvent, counterions) two per thread, so
-    // that the grid fits the device in one wave sooner
-    {
-        const mfa_params& p = c->p;
-        long long bonded = (long long)p.n_chain * p.n_mon;
-        if (p.n_mon_d >= 2) {
-            const long long e = (long long)p.n_mon * p.n_chain + (long long)p.n_chain_d * p.n_mon_d;
-            if (e > bonded) bonded = e;
-        }
-        const long long p0 = (bonded + TPB - 1) / TPB * TPB;
-        if (p0 < c->n) {
-            a.pair0 = (int)p0;
-            a.pair_half = (int)((c->n - p0 + 1) / 2);
-            nb = (a.pair0 + a.pair_half + TPB - 1) / TPB;
-        }
-    }
     void (*k)(VVArgs);
     if (rebuild_cond) k = c->prec == MFA_MIXED ? k_vv_fused_cond<float4> : k_vv_fused_cond<double4>;
     else k = c->prec == MFA_MIXED ? k_vv_fused<float4> : k_vv_fused<double4>;
