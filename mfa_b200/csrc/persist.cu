@@ -140,8 +140,8 @@ struct PersistDispatch<R4, R, -1> {
 
 }  // namespace
 
-// The persistent kernel of a batch's precision and feature set (list entries
-// per round 2), or null when there is none.
+// The persistent kernel of a batch's precision and feature set (its pair stage
+// tests two list entries per lane at a time), or null when there is none.
 const void* persist_kernel(int prec, int ft) {
     return prec == MFA_MIXED ? PersistDispatch<float4, float, N_PERSIST_FT - 1>::fn(ft)
                              : PersistDispatch<double4, double, N_PERSIST_FT - 1>::fn(ft);
