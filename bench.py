@@ -68,6 +68,9 @@ def args_():
     ap.add_argument("--fixed-skin", type=float, default=None,
                     help="--kernel-times: this skin (and the finest cells for it) after the autotuner, so that "
                          "two builds are compared at equal list lengths")
+    ap.add_argument("--energy-every", type=int, default=0,
+                    help="--kernel-times: record the energies every this many steps (the device energy log), "
+                         "as a driver that reads them would")
     ap.add_argument("--kernel-times", action="store_true",
                     help="device time of every kernel inside the time-step loop (CUPTI through the torch "
                          "profiler, no serialisation), per step; not a throughput run")
@@ -98,6 +101,8 @@ def kernel_times(a):
     if a.fixed_skin is not None:
         from mfa_b200.tune import cells_for
         g.set_cells(cells_for(g.params, a.fixed_skin), a.fixed_skin)
+    if a.energy_every:
+        g.set_energy_log(a.energy_every, (a.steps + a.warmup) // a.energy_every + 64)
     for _ in range(max(3, a.warmup // a.chunk)):
         g.step(a.chunk)
     g.sync()
@@ -1053,12 +1058,19 @@ def main():
     n_log0 = len(ge.energy_log(log_cap))
     t0 = time.perf_counter()
     ge.upload(r0=host[0], v=host[1], a=host[2])
+    t1 = time.perf_counter()
     for ln in e2e_calls:
         ge.step(ln)                          # mfa_step: `chunk` steps per call, as the timed loop
         ge.scalars()                         # the call's last step: energies and error flags to the host
+    t2 = time.perf_counter()
     elog = ge.energy_log(log_cap)            # every step's energies to the host
+    t3 = time.perf_counter()
     out = ge.download(_abi.R0 | _abi.V, out=dest)   # into pinned host buffers
     t_e2e = time.perf_counter() - t0
+    # wall time of each phase (each call returns once its work is done: the
+    # reads synchronise, the upload too)
+    e2e_phases = {"upload": round((t1 - t0) * 1e3, 3), "steps_and_scalars": round((t2 - t1) * 1e3, 3),
+                  "energy_log": round((t3 - t2) * 1e3, 3), "download": round((t0 + t_e2e - t3) * 1e3, 3)}
     ge.close()
     assert len(elog) - n_log0 == a.steps, "energy log: one entry per timed step"
     t_e2e = max_over_ranks(t_e2e, dist, f"cuda:{dev}")
@@ -1070,7 +1082,7 @@ def main():
                "protocol": f"wall clock: state (r0, v, a) uploaded from pinned host memory, {len(e2e_calls)} "
                            f"mfa_step calls of up to {a.chunk} steps with the call's scalars read back after "
                            "each, every step's energies recorded on the device and read back, final r0 and v "
-                           "downloaded into pinned host memory"}
+                           "downloaded into pinned host memory", "phases_ms": e2e_phases}
 
     line = None
     if rank == 0:
