@@ -278,6 +278,16 @@ int mfa_step(mfa_ctx* ctx, int32_t nsteps);
  * log of `capacity` entries (0 disables).  Read back with mfa_read_energy_log. */
 int mfa_set_energy_log(mfa_ctx* ctx, int32_t every, int32_t capacity);
 int mfa_read_energy_log(mfa_ctx* ctx, double* out3, int32_t max_entries, int32_t* n_out);
+/* No counterpart in the reference (its fort.60 is written by the time-step
+ * loop itself).  Enqueues, without waiting, the copy of log entries
+ * [first, first + count) (4 doubles each: step, e_total, v_total, t_fluid)
+ * into `out` on the context's stream, after every step enqueued before it, so
+ * a driver can collect each call's energies while the next call runs.  `out`
+ * should be pinned host memory; it is valid after the next synchronising call
+ * (mfa_sync, mfa_get_scalars, mfa_download).  With `every` = 1 the entry of
+ * the k-th step logged since mfa_set_energy_log is entry k - 1.
+ * MFA_ERR_STATE without a log, MFA_ERR_ARGS beyond its capacity. */
+int mfa_fetch_energy_log(mfa_ctx* ctx, double* out, int32_t first, int32_t count);
 
 /* Launch shape of the pair kernel: how many list entries a thread tests per
  * round before its warp evaluates the in-range pairs 32 at a time (2 or 4),

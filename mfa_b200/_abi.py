@@ -133,6 +133,7 @@ SIGNATURES = {
     "mfa_step": (C.c_int, [_P, C.c_int32]),
     "mfa_set_energy_log": (C.c_int, [_P, C.c_int32, C.c_int32]),
     "mfa_read_energy_log": (C.c_int, [_P, _DP, C.c_int32, _IP]),
+    "mfa_fetch_energy_log": (C.c_int, [_P, _DP, C.c_int32, C.c_int32]),
     "mfa_get_scalars": (C.c_int, [_P, C.POINTER(MfaScalars)]),
     "mfa_observe": (C.c_int, [_P, C.POINTER(MfaObservables)]),
     "mfa_observe_ends": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),

@@ -360,6 +360,15 @@ class System:
         check(self.lib.mfa_read_energy_log(self.ctx, _dp(out), max_entries, C.byref(n)), "mfa_read_energy_log")
         return out[: n.value].copy()
 
+    def fetch_energy_log(self, out: np.ndarray, first: int, count: int) -> None:
+        """mfa_fetch_energy_log: enqueue the copy of log entries
+        [first, first + count) into ``out`` (a C-contiguous float64 array of at
+        least count x 4, best in pinned memory) without waiting; ``out`` holds
+        them after the next synchronising call (sync, scalars, download)."""
+        if out.dtype != np.float64 or not out.flags.c_contiguous or out.size < 4 * count:
+            raise ValueError("out: C-contiguous float64 array of at least count x 4 entries")
+        check(self.lib.mfa_fetch_energy_log(self.ctx, _dp(out), first, count), "mfa_fetch_energy_log")
+
 
 def from_config(cfg, precision: int = _abi.MIXED, device: int = 0) -> System:
     """A System holding a generated configuration (mfa_b200.configs)."""

@@ -407,18 +407,17 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
     }
     int rc = MFA_OK;
 #define A(x) do { if (rc == MFA_OK) rc = (x); } while (0)
-    // FP64 state: r, v, a, r0_old (12 arrays)
+    // FP64 state: r, v, a, r0_old + mic_old * L (12 arrays)
     double* d12 = nullptr;
     A(dalloc(&d12, (size_t)12 * n));
     int32_t* i7 = nullptr;
-    A(dalloc(&i7, (size_t)6 * n));
+    A(dalloc(&i7, (size_t)3 * n));
     if (rc == MFA_OK) {
         c->rx = d12; c->ry = d12 + n; c->rz = d12 + 2 * n;
         c->vx = d12 + 3 * n; c->vy = d12 + 4 * n; c->vz = d12 + 5 * n;
         c->ax = d12 + 6 * n; c->ay = d12 + 7 * n; c->az = d12 + 8 * n;
         c->ox = d12 + 9 * n; c->oy = d12 + 10 * n; c->oz = d12 + 11 * n;
         c->mx = i7; c->my = i7 + n; c->mz = i7 + 2 * n;
-        c->omx = i7 + 3 * n; c->omy = i7 + 4 * n; c->omz = i7 + 5 * n;
     }
     A(dalloc(&c->type, n));
     double* d3 = nullptr;
@@ -504,7 +503,7 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
         if (rc == MFA_OK && dzero(c, c->f_heads, (size_t)3 * p->n_chain * sizeof(double)) != MFA_OK)
             rc = MFA_ERR_CUDA;
     }
-    A(dalloc(&c->d_stage, (size_t)3 * n));
+    A(dalloc(&c->d_stage, (size_t)9 * n));   // three 3 x n slots: r0, v, a move together
     if (rc == MFA_OK && cudaMallocHost((void**)&c->h_scal, (S_NSLOT + F_NFLAG / 2) * sizeof(double)) != cudaSuccess)
         rc = MFA_ERR_NOMEM;
     if (rc != MFA_OK) { free_all(c); free(c); return rc; }
@@ -515,12 +514,14 @@ int mfa_init(const mfa_params* p, int precision, int device, const double* r0, c
             soa[(size_t)d * n + i] = r0[3 * i + d];
             soa[(size_t)(3 + d) * n + i] = v ? v[3 * i + d] : 0.0;
             soa[(size_t)(6 + d) * n + i] = a ? a[3 * i + d] : 0.0;
-            soa[(size_t)(9 + d) * n + i] = r0[3 * i + d];
+            // the skin snapshot holds r0_old + mic_old * L (check_skin.f90:14-16)
+            const double m = mic_count ? (double)mic_count[3 * i + d] : 0.0;
+            soa[(size_t)(9 + d) * n + i] = r0[3 * i + d] + m * p->boundary[d];
         }
-    std::vector<int32_t> mic((size_t)6 * n, 0);
+    std::vector<int32_t> mic((size_t)3 * n, 0);
     if (mic_count)
         for (int i = 0; i < n; ++i)
-            for (int d = 0; d < 3; ++d) { mic[(size_t)d * n + i] = mic_count[3 * i + d]; mic[(size_t)(3 + d) * n + i] = mic_count[3 * i + d]; }
+            for (int d = 0; d < 3; ++d) mic[(size_t)d * n + i] = mic_count[3 * i + d];
     std::vector<double> m3((size_t)3 * n, 0.0);
     double vself = 0.0;
     for (int i = 0; i < n; ++i) {
@@ -766,6 +767,18 @@ int mfa_read_energy_log(mfa_ctx* c, double* out, int32_t max_entries, int32_t* n
     return MFA_OK;
 }
 
+int mfa_fetch_energy_log(mfa_ctx* c, double* out, int32_t first, int32_t count) {
+    if (!c || first < 0 || count < 0 || (count > 0 && !out)) return MFA_ERR_ARGS;
+    if (!c->elog) return MFA_ERR_STATE;
+    if ((long long)first + count > c->elog_cap) return MFA_ERR_ARGS;
+    if (count == 0) return MFA_OK;
+    // ordered after every step already enqueued on the context stream; the
+    // caller synchronises (mfa_sync, mfa_download, ...) before reading `out`
+    MFA_CUDA_TRY(cudaMemcpyAsync(out, c->elog + (size_t)4 * first, (size_t)count * 4 * sizeof(double),
+                                 cudaMemcpyDeviceToHost, c->st));
+    return MFA_OK;
+}
+
 int mfa_get_scalars(mfa_ctx* c, mfa_scalars* o) {
     if (!c || !o) return MFA_ERR_ARGS;
     // energies and flags are one device allocation: one copy into pinned memory
@@ -922,18 +935,19 @@ int mfa_sync(mfa_ctx* c) {
 int mfa_download(mfa_ctx* c, uint32_t mask, double* r0, double* v, double* a, double* force, int32_t* mic) {
     if (!c) return MFA_ERR_ARGS;
     const int n = c->n;
-    // x, y, z of one quantity are contiguous on the device: interleaved into the
-    // r0(3,n) layout by a kernel, then one copy per quantity (stream-ordered:
-    // the next interleave waits for the previous copy), one synchronisation
-    auto get3 = [&](double* dst, const double* x) -> int {
-        k_interleave3<<<(n + 255) / 256, 256, 0, c->st>>>(x, c->d_stage, n);
-        MFA_CUDA_TRY(cudaGetLastError());
-        MFA_CUDA_TRY(cudaMemcpyAsync(dst, c->d_stage, (size_t)3 * n * 8, cudaMemcpyDeviceToHost, c->st));
-        return MFA_OK;
-    };
-    if ((mask & MFA_R0) && r0) TRY(get3(r0, c->rx));
-    if ((mask & MFA_V) && v) TRY(get3(v, c->vx));
-    if ((mask & MFA_A) && a) TRY(get3(a, c->ax));
+    // x, y, z of one quantity are contiguous on the device: each quantity is
+    // interleaved into the r0(3,n) layout in a stage slot of its own, then the
+    // copies run back to back (one DMA stream from pinned memory), one
+    // synchronisation
+    double* dst3[3] = {(mask & MFA_R0) ? r0 : nullptr, (mask & MFA_V) ? v : nullptr, (mask & MFA_A) ? a : nullptr};
+    const double* src3[3] = {c->rx, c->vx, c->ax};
+    for (int k = 0; k < 3; ++k)
+        if (dst3[k]) k_interleave3<<<(n + 255) / 256, 256, 0, c->st>>>(src3[k], c->d_stage + (size_t)3 * n * k, n);
+    MFA_CUDA_TRY(cudaGetLastError());
+    for (int k = 0; k < 3; ++k)
+        if (dst3[k])
+            MFA_CUDA_TRY(cudaMemcpyAsync(dst3[k], c->d_stage + (size_t)3 * n * k, (size_t)3 * n * 8,
+                                         cudaMemcpyDeviceToHost, c->st));
     MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
     if ((mask & MFA_F) && force) {
         if (c->prec == MFA_MIXED) {
@@ -961,18 +975,19 @@ int mfa_upload(mfa_ctx* c, uint32_t mask, const double* r0, const double* v, con
                const double* force, const int32_t* mic) {
     if (!c) return MFA_ERR_ARGS;
     const int n = c->n;
-    // the r0(3,n) layout copied as it is, de-interleaved on the device; the
-    // copies and kernels are stream-ordered, and the call returns once they
-    // are done (the caller may reuse its buffers)
-    auto put3 = [&](const double* src, double* x) -> int {
-        MFA_CUDA_TRY(cudaMemcpyAsync(c->d_stage, src, (size_t)3 * n * 8, cudaMemcpyHostToDevice, c->st));
-        k_deinterleave3<<<(n + 255) / 256, 256, 0, c->st>>>(c->d_stage, x, n);
-        MFA_CUDA_TRY(cudaGetLastError());
-        return MFA_OK;
-    };
-    if ((mask & MFA_R0) && r0) TRY(put3(r0, c->rx));
-    if ((mask & MFA_V) && v) TRY(put3(v, c->vx));
-    if ((mask & MFA_A) && a) TRY(put3(a, c->ax));
+    // the r0(3,n) layout copied as it is into a stage slot per quantity (the
+    // copies back to back), then de-interleaved on the device; the copies and
+    // kernels are stream-ordered, and the call returns once they are done (the
+    // caller may reuse its buffers)
+    const double* src3[3] = {(mask & MFA_R0) ? r0 : nullptr, (mask & MFA_V) ? v : nullptr, (mask & MFA_A) ? a : nullptr};
+    double* dst3[3] = {c->rx, c->vx, c->ax};
+    for (int k = 0; k < 3; ++k)
+        if (src3[k])
+            MFA_CUDA_TRY(cudaMemcpyAsync(c->d_stage + (size_t)3 * n * k, src3[k], (size_t)3 * n * 8,
+                                         cudaMemcpyHostToDevice, c->st));
+    for (int k = 0; k < 3; ++k)
+        if (src3[k]) k_deinterleave3<<<(n + 255) / 256, 256, 0, c->st>>>(c->d_stage + (size_t)3 * n * k, dst3[k], n);
+    MFA_CUDA_TRY(cudaGetLastError());
     MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
     if ((mask & MFA_F) && force) {
         if (c->prec == MFA_MIXED) {

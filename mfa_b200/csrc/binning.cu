@@ -33,7 +33,6 @@ struct BinArgs {
     const double *rx, *ry, *rz, *vx, *vy, *vz;
     double *ox, *oy, *oz;
     const int32_t *mx, *my, *mz;
-    int32_t *omx, *omy, *omz;
     const int32_t* type;
     const double* q;
     int32_t *cell_count, *cell_start, *cell_cursor, *cell_of, *row_count;
@@ -106,9 +105,12 @@ __device__ __forceinline__ void cell_assign_body(const BinArgs& a, Blk blk) {
     a.cell_of[i] = c;
     atomicAdd(&a.cell_count[c], 1);
     atomicAdd(&a.row_count[r], 1);
-    // binning.f90:126-127 snapshot
-    a.ox[i] = x; a.oy[i] = y; a.oz[i] = z;
-    a.omx[i] = a.mx[i]; a.omy[i] = a.my[i]; a.omz[i] = a.mz[i];
+    // binning.f90:126-127 snapshot, kept unwrapped: r0_old + mic_old * L,
+    // rounded as the first operation of check_skin.f90:14-16 rounds it (the
+    // skin check then reads 24 bytes per particle instead of 36)
+    a.ox[i] = __dadd_rn(x, __dmul_rn((double)a.mx[i], a.L[0]));
+    a.oy[i] = __dadd_rn(y, __dmul_rn((double)a.my[i], a.L[1]));
+    a.oz[i] = __dadd_rn(z, __dmul_rn((double)a.mz[i], a.L[2]));
 }
 
 // Exclusive scan of the cell histogram into cell_start[0..ncell] (and the
@@ -614,7 +616,6 @@ BinArgs make_args(mfa_ctx* c, int rule, int conditional) {
     a.rx = c->rx; a.ry = c->ry; a.rz = c->rz; a.vx = c->vx; a.vy = c->vy; a.vz = c->vz;
     a.ox = c->ox; a.oy = c->oy; a.oz = c->oz;
     a.mx = c->mx; a.my = c->my; a.mz = c->mz;
-    a.omx = c->omx; a.omy = c->omy; a.omz = c->omz;
     a.type = c->type; a.q = c->p.charged ? c->q : nullptr;
     a.cell_count = c->cell_count; a.cell_start = c->cell_start; a.cell_cursor = c->cell_cursor;
     a.cell_of = c->cell_of; a.row_count = c->row_count; a.ids = c->ids; a.slot = c->slot;

@@ -14,7 +14,6 @@ struct VVArgs {
     double *rx, *ry, *rz, *vx, *vy, *vz, *ax, *ay, *az;
     const double *ox, *oy, *oz;
     int32_t *mx, *my, *mz;
-    const int32_t *omx, *omy, *omz;
     const int32_t* slot;
     const int32_t* type;
     const double* q;
@@ -84,12 +83,14 @@ __device__ __forceinline__ void store_sorted(const VVArgs& a, int i, double x, d
     vs[s] = vw;
 }
 
-// check_skin.f90:8-21 on one particle
+// check_skin.f90:8-21 on one particle; the snapshot (ox, oy, oz) holds
+// r0_old + mic_old * L, the first sum of the reference's expression, rounded
+// when the list was built
 __device__ __forceinline__ bool skin_tripped(const VVArgs& a, int i, double x, double y, double z,
                                              int mx, int my, int mz) {
-    double d0 = __dsub_rn(__dsub_rn(__dadd_rn(a.ox[i], __dmul_rn((double)a.omx[i], a.L[0])), x), __dmul_rn((double)mx, a.L[0]));
-    double d1 = __dsub_rn(__dsub_rn(__dadd_rn(a.oy[i], __dmul_rn((double)a.omy[i], a.L[1])), y), __dmul_rn((double)my, a.L[1]));
-    double d2 = __dsub_rn(__dsub_rn(__dadd_rn(a.oz[i], __dmul_rn((double)a.omz[i], a.L[2])), z), __dmul_rn((double)mz, a.L[2]));
+    double d0 = __dsub_rn(__dsub_rn(a.ox[i], x), __dmul_rn((double)mx, a.L[0]));
+    double d1 = __dsub_rn(__dsub_rn(a.oy[i], y), __dmul_rn((double)my, a.L[1]));
+    double d2 = __dsub_rn(__dsub_rn(a.oz[i], z), __dmul_rn((double)mz, a.L[2]));
     double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
     return r2 > a.skin_lim;
 }
@@ -315,7 +316,6 @@ VVArgs make_args(mfa_ctx* c) {
     a.ax = c->ax; a.ay = c->ay; a.az = c->az;
     a.ox = c->ox; a.oy = c->oy; a.oz = c->oz;
     a.mx = c->mx; a.my = c->my; a.mz = c->mz;
-    a.omx = c->omx; a.omy = c->omy; a.omz = c->omz;
     a.slot = c->slot; a.type = c->type; a.q = c->p.charged ? c->q : nullptr;
     a.mass = c->mass; a.inv_mass = c->inv_mass;
     a.uniform_mass = c->uniform_mass; a.umass = c->umass; a.uinv_mass = c->uinv_mass;

@@ -67,8 +67,8 @@ struct mfa_ctx {
     int n;
     // FP64 state
     double *rx, *ry, *rz, *vx, *vy, *vz, *ax, *ay, *az;
-    double *ox, *oy, *oz;               // r0_old
-    int32_t *mx, *my, *mz, *omx, *omy, *omz;
+    double *ox, *oy, *oz;               // r0_old + mic_old * L (the skin check's snapshot)
+    int32_t *mx, *my, *mz;
     int32_t* type;
     double *mass, *inv_mass, *q;
     // every particle has the same mass (then the integrator takes it from its

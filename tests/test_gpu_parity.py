@@ -398,6 +398,34 @@ def test_energy_log_of_the_fast_path(name, request):
     g2.close()
 
 
+def test_fetch_energy_log_while_stepping(melt_cfg):
+    """mfa_fetch_energy_log copies each call's entries behind the call without
+    waiting: after the next synchronising call the host buffer holds exactly
+    what mfa_read_energy_log returns; out-of-range and missing logs are
+    rejected."""
+    import torch
+    cfg = melt_cfg
+    g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, precision=MIXED)
+    g.init_forces()
+    with pytest.raises(MfaError):
+        g.fetch_energy_log(np.zeros((1, 4)), 0, 1)          # no log yet
+    g.set_energy_log(1, 64)
+    out = torch.zeros((40, 4), dtype=torch.float64, pin_memory=True).numpy()
+    done = 0
+    for ln in (10, 10, 7, 10, 3):
+        g.step(ln)
+        g.fetch_energy_log(out[done:], done, ln)
+        done += ln
+    g.sync()
+    log = g.energy_log()
+    assert log.shape == (40, 4)
+    assert np.array_equal(out, log)
+    assert [int(x) for x in out[:, 0]] == list(range(1, 41))
+    with pytest.raises(MfaError):
+        g.fetch_energy_log(np.zeros((8, 4)), 60, 8)         # past the capacity
+    g.close()
+
+
 @pytest.mark.parametrize("name", ["melt_cfg", "brush_small_cfg", "charged_small_cfg", "charged_slab_cfg"])
 @pytest.mark.parametrize("prec", [FP64, MIXED])
 def test_fused_forces_equal_the_subroutines(name, prec, request):
