@@ -6,7 +6,9 @@
 //   k_scan_rows     multi-block: each block gets its row offset from the row
 //                   histogram, then one warp per row scans that row's cells;
 //   k_cell_scatter  slot per particle (atomic cursor per cell);
-//   k_cell_sort     per-cell sort by particle id, so the order is deterministic;
+//   k_cell_sort     per-cell sort by particle id, so the order is deterministic
+//                   (the cooperative rebuild of the time-step graphs skips it
+//                   and writes the records as it scatters);
 //   k_gather_sorted the cell-sorted position/velocity records.
 // A "row" is the run of cells at fixed (y, z); cells are numbered x-fastest, so
 // a row is a contiguous range of slots.
@@ -231,12 +233,9 @@ __device__ __forceinline__ void cell_sort_body(const BinArgs& a, Blk blk) {
         if (lane + 32 * m < k) a.ids[b + rk[m]] = v[m];
 }
 
+// the records of slot t, which holds particle i
 template <typename R4>
-__device__ __forceinline__ void gather_sorted_body(const BinArgs& a, Blk blk) {
-    if (skip(a)) return;
-    const int t = blk.id * blockDim.x + threadIdx.x;
-    if (t >= a.n) return;
-    const int i = a.ids[t];
+__device__ __forceinline__ void write_slot(const BinArgs& a, int t, int i) {
     a.slot[i] = t;
     const int ty = a.type[i];
     const double x = a.rx[i], y = a.ry[i], z = a.rz[i];
@@ -263,6 +262,33 @@ __device__ __forceinline__ void gather_sorted_body(const BinArgs& a, Blk blk) {
         packw(f, i, ty);
         a.pos32[t] = f;
     }
+}
+
+template <typename R4>
+__device__ __forceinline__ void gather_sorted_body(const BinArgs& a, Blk blk) {
+    if (skip(a)) return;
+    const int t = blk.id * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
+    write_slot<R4>(a, t, a.ids[t]);
+}
+
+// The cooperative rebuild's scatter: each particle takes a slot of its cell
+// from the cell's cursor (order of arrival within a cell) and writes the
+// slot's records at once, in place of the plain launches' scatter, per-cell
+// id sort and gather (three stages and two grid barriers fewer).  The order
+// within a cell changes neither the listed pairs nor the forces beyond the
+// summation order, which the pair kernel's vector reductions leave unfixed
+// anyway.  The row histogram is cleared here for the next rebuild (the scan
+// was its last reader).
+template <typename R4>
+__device__ __forceinline__ void scatter_gather_body(const BinArgs& a, Blk blk) {
+    if (skip(a)) return;
+    const int i = blk.id * blockDim.x + threadIdx.x;
+    for (int r = i; r < a.nrow; r += blk.n * blockDim.x) a.row_count[r] = 0;
+    if (i >= a.n) return;
+    const int t = atomicAdd(&a.cell_cursor[a.cell_of[i]], 1);
+    a.ids[t] = i;
+    write_slot<R4>(a, t, i);
 }
 
 // The x neighbours of cell column cx, as runs of consecutive cells [x0, x1)
@@ -478,8 +504,10 @@ __global__ void k_bin_grouped(const BinArgs* __restrict__ as, const int* __restr
 }
 
 // One cooperative launch for the whole rebuild, used by the captured time-step
-// graphs: the six stages above, each a grid-stride loop over the blocks it
-// would have as a launch of its own, with a grid-wide barrier between stages.
+// graphs: cell assign, row scan, the scatter that writes the slots' records
+// (scatter_gather_body) and the list build, each a grid-stride loop over the
+// blocks it would have as a launch of its own, with a grid-wide barrier
+// between stages.
 // When no rebuild is due every CTA returns after one flag read -- a launch of
 // one to three microseconds in place of a conditional graph node, whose
 // evaluation held the device idle for about seven.  The grid is co-resident
@@ -563,21 +591,23 @@ __global__ void __launch_bounds__(COOP_T, 5) k_rebuild_coop(BinArgs a) {
     // barrier after it (the stage's critical path; the last stage: its own part)
     __shared__ unsigned long long t_prev;   // thread 0 of CTA 0 only (no register held across stages)
     if (a.stage_ns && blockIdx.x == 0 && threadIdx.x == 0) t_prev = global_ns();
-    for (int st = 0; st < N_BIN_STAGES; ++st) {
+    // four stages: cell assign, row scan, scatter with the records, list build
+    constexpr int NST = 4;
+    constexpr int STAGE[NST] = {0, 1, 2, 5};
+    for (int k = 0; k < NST; ++k) {
+        const int st = STAGE[k];
         const int nv = a.vnb[st];
         for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
             const Blk blk{vb, nv};
             switch (st) {
                 case 0: cell_assign_body(a, blk); break;
                 case 1: scan_rows_body(a, blk); break;
-                case 2: cell_scatter_body(a, blk); break;
-                case 3: cell_sort_body(a, blk); break;
-                case 4: gather_sorted_body<R4>(a, blk); break;
+                case 2: scatter_gather_body<R4>(a, blk); break;
                 default: build_nbr_body(a, blk); break;
             }
             __syncthreads();
         }
-        if (st + 1 < N_BIN_STAGES && !grid_barrier(a.bar, a.flags)) return;
+        if (k + 1 < NST && !grid_barrier(a.bar, a.flags)) return;
         if (a.stage_ns && blockIdx.x == 0 && threadIdx.x == 0) {
             const unsigned long long t = global_ns();
             atomicAdd(&a.stage_ns[st], t - t_prev);
@@ -750,8 +780,8 @@ void rebuild_coop_report(mfa_ctx* c) {
     const double k = 1e-3 / (double)h[N_BIN_STAGES];
     fprintf(stderr,
             "mfa: cooperative rebuild, %llu rebuilds, mean us per stage (CTA 0, to the barrier after it): "
-            "assign %.1f scan %.1f scatter %.1f sort %.1f gather %.1f build %.1f\n",
-            h[N_BIN_STAGES], h[0] * k, h[1] * k, h[2] * k, h[3] * k, h[4] * k, h[5] * k);
+            "assign %.1f scan %.1f scatter with records %.1f build %.1f\n",
+            h[N_BIN_STAGES], h[0] * k, h[1] * k, h[2] * k, h[5] * k);
 }
 
 int launch_refresh_sorted(mfa_ctx* c) {
