@@ -72,6 +72,11 @@ def args_():
     ap.add_argument("--energy-every", type=int, default=0,
                     help="--kernel-times: record the energies every this many steps (the device energy log), "
                          "as a driver that reads them would")
+    ap.add_argument("--shape", default=None,
+                    help="K,BLOCK,SPLIT: after the autotuner, run the pair kernel untiled with this shape (list "
+                         "entries per lane and round, threads per block, pieces per chunk), e.g. 2,128,1 -- so "
+                         "that a profiled run, whose timings the profiler perturbs, runs the shape an unprofiled "
+                         "run picks")
     ap.add_argument("--kernel-times", action="store_true",
                     help="device time of every kernel inside the time-step loop (CUPTI through the torch "
                          "profiler, no serialisation), per step; not a throughput run")
@@ -89,7 +94,7 @@ def kernel_times(a):
     from torch.profiler import ProfilerActivity, profile
     from mfa_b200 import _abi
     from mfa_b200.api import System
-    from mfa_b200.tune import autotune
+    from mfa_b200.tune import autotune, set_shape
     cfg, meta = make_config(a.workload, a.seed)
     prec = _abi.FP64 if a.precision == "fp64" else _abi.MIXED
     g = System(cfg.params, cfg.r0, cfg.v, cfg.a_type, cfg.mass, q=cfg.q, precision=prec, device=0)
@@ -99,6 +104,9 @@ def kernel_times(a):
     if a.equil:
         g.step(a.equil)
     autotune(g)
+    if a.shape:
+        k, b, sp = (int(x) for x in a.shape.split(","))
+        set_shape(g, k, b, False, 0, sp)
     if a.fixed_skin is not None:
         from mfa_b200.tune import cells_for
         g.set_cells(cells_for(g.params, a.fixed_skin), a.fixed_skin)
@@ -793,7 +801,7 @@ def main():
     import torch
     from mfa_b200 import _abi
     from mfa_b200.api import System
-    from mfa_b200.tune import autotune
+    from mfa_b200.tune import autotune, set_shape
 
     dist = None
     if world > 1:
@@ -818,6 +826,10 @@ def main():
         tuned = autotune(g)
         shapes = tuned["pair_shape"]
         g.tuned = min(shapes, key=shapes.get)
+        if a.shape:
+            k, b, sp = (int(x) for x in a.shape.split(","))
+            set_shape(g, k, b, False, 0, sp)
+            g.tuned = (k, b, False, 0, sp)
         g.tuning = {f"{k}x{b}{'-tiled' if t else ''}{f'-queue{q}' if q else ''}{f'-split{p}' if p > 1 else ''}":
                     round(1e3 * s / 300, 4) for (k, b, t, q, p), s in shapes.items()}
         g.skin_tuning = {f"{s:g}": round(1e3 * v / 300, 4) for s, v in tuned["skin_for_shape"].items()}

@@ -159,9 +159,11 @@ int rebuild_abi(mfa_ctx* c, int rule) {
 // epilogue, then hard walls (WALL 3/4) and Ewald k-space if used.  The chains'
 // FENE and bending forces (md_main.f90:106-111) are added bead by bead by the
 // integrator kernel that consumes the force (launch_vv_* with fuse_bonds).
-int forces_fused(mfa_ctx* c) {
+// defer_sum: the pair energies' grid sum is left to the integrator launch of
+// the same step (the time-step fast path, where one always follows)
+int forces_fused(mfa_ctx* c, int defer_sum = 0) {
     // fluid_wall is called for SYMMETRY 0 only (md_main.f90:97)
-    TRY(launch_pair(c, c->p.symmetry == 0));
+    TRY(launch_pair(c, c->p.symmetry == 0, 0, defer_sum));
     if (c->p.symmetry == 0 && (c->p.wall == 3 || c->p.wall == 4)) TRY(launch_wall(c, c->p.wall));
     if (c->p.charged) {
         TRY(launch_ewald(c));
@@ -210,7 +212,7 @@ int capture_conditional_rebuild(mfa_ctx* c, int opener) {
 // A body step of a run of steps: forces of step n, then velocities of n fused
 // with positions of n+1, then the rebuild of n+1 if due.
 int launch_body_step(mfa_ctx* c) {
-    TRY(forces_fused(c));
+    TRY(forces_fused(c, 1));
     if (c->coop_rebuild) {
         TRY(launch_vv_fused(c, 0, 1));
         return launch_rebuild_coop(c, c->bin_type);
@@ -234,7 +236,7 @@ int launch_head_step(mfa_ctx* c, int nsteps) {
 // The last step of a run: forces and the velocity half (energies reduced, and
 // every step's energies wanted again afterwards).
 int launch_tail_step(mfa_ctx* c) {
-    TRY(forces_fused(c));
+    TRY(forces_fused(c, 1));
     return launch_vv_velocities(c, 1, 1);
 }
 

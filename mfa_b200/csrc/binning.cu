@@ -579,23 +579,19 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, int32_t* flags) {
     return ok_s != 0;
 }
 
-// 48 registers: five 256-thread CTAs per SM, 740 on 148 SMs, so every stage of
-// a 189k-particle system takes one round (a few bytes of the list builder's
-// registers spill)
+// The stages of a cooperative rebuild on a co-resident grid: cell assign,
+// row scan, scatter with the records, list build, with a grid barrier between
+// stages.  False when a barrier wait timed out.  With MFA_DEBUG=1 (stage_ns
+// set), CTA 0 sums the time from each stage's start to the barrier after it
+// (the stage's critical path; the last stage: its own part).
 template <typename R4>
-__global__ void __launch_bounds__(COOP_T, 5) k_rebuild_coop(BinArgs a) {
-    // the flag is set before this launch and cleared only by the last stage,
-    // after every CTA has passed the barriers: all CTAs read the same value
-    if (*(volatile const int32_t*)&a.flags[F_SKIN] == 0) return;
-    // with MFA_DEBUG=1, CTA 0 sums the time from each stage's start to the
-    // barrier after it (the stage's critical path; the last stage: its own part)
+__device__ __forceinline__ bool rebuild_stages(const BinArgs& a) {
     __shared__ unsigned long long t_prev;   // thread 0 of CTA 0 only (no register held across stages)
     if (a.stage_ns && blockIdx.x == 0 && threadIdx.x == 0) t_prev = global_ns();
-    // four stages: cell assign, row scan, scatter with the records, list build
     constexpr int NST = 4;
-    constexpr int STAGE[NST] = {0, 1, 2, 5};
+#pragma unroll
     for (int k = 0; k < NST; ++k) {
-        const int st = STAGE[k];
+        const int st = k < 3 ? k : 5;
         const int nv = a.vnb[st];
         for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
             const Blk blk{vb, nv};
@@ -607,7 +603,7 @@ __global__ void __launch_bounds__(COOP_T, 5) k_rebuild_coop(BinArgs a) {
             }
             __syncthreads();
         }
-        if (k + 1 < NST && !grid_barrier(a.bar, a.flags)) return;
+        if (k + 1 < NST && !grid_barrier(a.bar, a.flags)) return false;
         if (a.stage_ns && blockIdx.x == 0 && threadIdx.x == 0) {
             const unsigned long long t = global_ns();
             atomicAdd(&a.stage_ns[st], t - t_prev);
@@ -615,6 +611,18 @@ __global__ void __launch_bounds__(COOP_T, 5) k_rebuild_coop(BinArgs a) {
         }
     }
     if (a.stage_ns && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.stage_ns[N_BIN_STAGES], 1ull);
+    return true;
+}
+
+// 48 registers: five 256-thread CTAs per SM, 740 on 148 SMs, so every stage of
+// a 189k-particle system takes one round (a few bytes of the list builder's
+// registers spill)
+template <typename R4>
+__global__ void __launch_bounds__(COOP_T, 5) k_rebuild_coop(BinArgs a) {
+    // the flag is set before this launch and cleared only by the last stage,
+    // after every CTA has passed the barriers: all CTAs read the same value
+    if (*(volatile const int32_t*)&a.flags[F_SKIN] == 0) return;
+    rebuild_stages<R4>(a);
 }
 
 // block size of each rebuild stage (assign, row scan, scatter, sort, gather, build)

@@ -54,7 +54,20 @@ struct VVArgs {
     // launches pass both as kernel parameters instead)
     long long energy_span;
     int energy_reset;
+    // the energies of the pair launch before this one, left as block partials
+    // (pair_nblk blocks, pair_nq quantities; 0: none): block 0 adds them up
+    // into the pair's energy slots before it arrives at the grid reduction
+    const double* pair_partials;
+    int pair_nblk, pair_nq, pair_max_blocks;
 };
+
+// the pair kernel's deferred grid sum (see VVArgs), by block 0, uniform over
+// the block; before the block's own arrival, so the last block sees it
+__device__ __forceinline__ void reduce_pair_partials(const VVArgs& a, Blk blk, bool en) {
+    if (!en || a.pair_nblk <= 0 || blk.id != 0) return;
+    if (a.pair_nq == 4) reduce_partials<4>(a.pair_partials, a.pair_max_blocks, a.pair_nblk, a.dscal + S_VFF);
+    else reduce_partials<3>(a.pair_partials, a.pair_max_blocks, a.pair_nblk, a.dscal + S_VFF);
+}
 
 // r += dt v + (0.5 dt^2) a ; v += (0.5 dt) a   (verlet_positions.f90:153,169)
 __device__ __forceinline__ void drift_kick(double& r, double& v, double a, double dt, double hdt2, double hdt) {
@@ -224,6 +237,7 @@ __device__ __forceinline__ bool vv_commit(const VVArgs& a, double ke, const doub
 template <typename R4>
 __device__ __forceinline__ void vv_velocities_body(const VVArgs& a, Blk blk, int energy_reset) {
     const int i = blk.id * blockDim.x + threadIdx.x;
+    reduce_pair_partials(a, blk, energy_needed(a.dstep, a.elog ? a.elog_every : 0));
     double ke = 0.0, eb[2] = {0.0, 0.0};
     int clamped = 0;
     // the bonded force first: its chain-window loads are in flight before the
@@ -254,6 +268,7 @@ __device__ __forceinline__ void vv_velocities_body(const VVArgs& a, Blk blk, int
 template <typename R4, bool COND>
 __device__ __forceinline__ void vv_fused_body(const VVArgs& a, Blk blk) {
     const int i = blk.id * blockDim.x + threadIdx.x;
+    reduce_pair_partials(a, blk, energy_needed(a.dstep, a.elog ? a.elog_every : 0));
     double ke = 0.0, eb[2] = {0.0, 0.0};
     int clamped = 0;
     decltype(R4::x) fb[3] = {0, 0, 0};
@@ -341,7 +356,18 @@ VVArgs make_args(mfa_ctx* c) {
     a.zero_force = 0;
     a.energy_span = 0;
     a.energy_reset = 0;
+    a.pair_partials = c->partials + (size_t)R_PAIR * 4 * c->max_blocks;
+    a.pair_nblk = 0;
+    a.pair_nq = 3;
+    a.pair_max_blocks = c->max_blocks;
     return a;
+}
+
+// the pair launch just before left its energy sum to this launch
+void take_pair_sum(mfa_ctx* c, VVArgs& a) {
+    a.pair_nblk = c->pair_sum_nblk;
+    a.pair_nq = c->pair_sum_nq;
+    c->pair_sum_nblk = 0;
 }
 
 constexpr int TPB = 256;
@@ -427,6 +453,7 @@ int launch_vv_velocities(mfa_ctx* c, int fuse_bonds, int energy_reset) {
     int nb;
     TRY_(vv_stage_args(c, VV_VELOCITIES, 0, 0, fuse_bonds, 0, &a, &nb));
     a.energy_reset = energy_reset;
+    take_pair_sum(c, a);
     return launch_vv_kernel(c, c->prec == MFA_MIXED ? k_vv_velocities<float4> : k_vv_velocities<double4>, nb, a);
 }
 
@@ -434,6 +461,7 @@ int launch_vv_fused(mfa_ctx* c, cudaGraphConditionalHandle rebuild_cond, int fus
     VVArgs a;
     int nb;
     TRY_(vv_stage_args(c, VV_FUSED, 1, 1, fuse_bonds, rebuild_cond, &a, &nb));
+    take_pair_sum(c, a);
     void (*k)(VVArgs);
     if (rebuild_cond) k = c->prec == MFA_MIXED ? k_vv_fused_cond<float4> : k_vv_fused_cond<double4>;
     else k = c->prec == MFA_MIXED ? k_vv_fused<float4> : k_vv_fused<double4>;

@@ -133,6 +133,7 @@ struct mfa_ctx {
     const void* graph_key[4];           // what the captured arguments depend on
     int cond_rebuild;                   // rebuilds in conditional graph nodes (1) or early-exit kernels (0)
     int coop_rebuild;                   // captured steps rebuild in one cooperative kernel (1) or as above (0)
+    int pair_sum_nblk, pair_sum_nq;     // block partials of the last pair launch left to the next integrator launch
     int coop_grid;                      // its grid (co-resident CTAs)
     unsigned* grid_bar;                 // its barrier words (GB_WORDS, zeroed)
     unsigned long long* coop_stage_ns;  // its stage times under MFA_DEBUG=1, else null
@@ -212,7 +213,9 @@ void rebuild_coop_report(mfa_ctx* c);
 // pair.cu
 // adds to force; zero_slots: energy slots the kernel resets (1: S_VCK and
 // S_VDIP, 2: S_VFW), for the subroutine entry points
-int launch_pair(mfa_ctx* c, int fuse_wall, int zero_slots = 0);
+// defer_sum: the energies' grid-wide sum is left to the integrator launch
+// that follows (launch_vv_fused / launch_vv_velocities), off the pair kernel's tail
+int launch_pair(mfa_ctx* c, int fuse_wall, int zero_slots = 0, int defer_sum = 0);
 size_t pair_args_bytes();
 int pair_stage_args(mfa_ctx* c, int fuse_wall, void* out, int* grid_out, size_t* smem_out, int* ft_out);
 int launch_pair_grouped(int prec, int k, int block, int ft, const void* dargs, const int* doff, int nsys, int grid,
@@ -376,14 +379,12 @@ __device__ __forceinline__ Blk group_blk(const int* __restrict__ off, int s) {
     return Blk{(int)blockIdx.x - o, __ldg(&off[s + 1]) - o};
 }
 
-// Block-wide FP64 sums of NQ values, committed deterministically: each block
-// writes its partials, the last block to finish adds them in block order and
-// stores the result in out[0..NQ).  Requires blockDim.x a multiple of 32, <= 1024.
+// Block-wide FP64 sums of NQ values: the block's partials into
+// partials[q * max_blocks + blk.id].  Requires blockDim.x a multiple of 32,
+// <= 1024.
 template <int NQ>
-__device__ __forceinline__ bool block_sum_commit(double (&v)[NQ], double* partials, int max_blocks,
-                                                 unsigned* counter, double* out, Blk blk = plain_blk()) {
+__device__ __forceinline__ void block_partials(double (&v)[NQ], double* partials, int max_blocks, Blk blk) {
     __shared__ double sm[NQ][32];
-    __shared__ bool am_last;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
     for (int q = 0; q < NQ; ++q) {
@@ -400,25 +401,29 @@ __device__ __forceinline__ bool block_sum_commit(double (&v)[NQ], double* partia
             if (lane == 0) partials[q * max_blocks + blk.id] = x;
         }
     }
-    __threadfence();
-    if (threadIdx.x == 0) am_last = (atomicAdd(counter, 1u) == (unsigned)blk.n - 1);
-    __syncthreads();
-    if (!am_last) return false;
-    __threadfence();
-    // every thread sums a fixed stripe of blocks (deterministic order); the
-    // loads of U blocks x NQ quantities are issued before any of them is used,
-    // so the last block waits for ~n/(U blockDim) L2 round trips, not n/blockDim
+}
+
+// The sums of the nblk partials of each of NQ quantities, added in a fixed
+// order (deterministic) by the whole block and stored in out[0..NQ).  Every
+// thread of the block calls it.
+template <int NQ>
+__device__ __forceinline__ void reduce_partials(const double* partials, int max_blocks, int nblk, double* out) {
+    __shared__ double sm[NQ][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    // every thread sums a fixed stripe of blocks; the loads of U blocks x NQ
+    // quantities are issued before any of them is used, so the block waits for
+    // ~n/(U blockDim) L2 round trips, not n/blockDim
     double xs[NQ];
 #pragma unroll
     for (int q = 0; q < NQ; ++q) xs[q] = 0.0;
     constexpr int U = NQ <= 2 ? 8 : 4;
-    for (int b0 = threadIdx.x; b0 < blk.n; b0 += U * blockDim.x) {
+    for (int b0 = threadIdx.x; b0 < nblk; b0 += U * blockDim.x) {
         double v[U][NQ];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const int b = b0 + u * blockDim.x;
 #pragma unroll
-            for (int q = 0; q < NQ; ++q) v[u][q] = b < blk.n ? __ldcg(&partials[q * max_blocks + b]) : 0.0;
+            for (int q = 0; q < NQ; ++q) v[u][q] = b < nblk ? __ldcg(&partials[q * max_blocks + b]) : 0.0;
         }
 #pragma unroll
         for (int u = 0; u < U; ++u)
@@ -438,6 +443,22 @@ __device__ __forceinline__ bool block_sum_commit(double (&v)[NQ], double* partia
             if (lane == 0) out[q] = y;
         }
     }
+}
+
+// Block-wide FP64 sums of NQ values, committed deterministically: each block
+// writes its partials, the last block to finish adds them in block order and
+// stores the result in out[0..NQ) (true in that block).
+template <int NQ>
+__device__ __forceinline__ bool block_sum_commit(double (&v)[NQ], double* partials, int max_blocks,
+                                                 unsigned* counter, double* out, Blk blk = plain_blk()) {
+    __shared__ bool am_last;
+    block_partials<NQ>(v, partials, max_blocks, blk);
+    __threadfence();
+    if (threadIdx.x == 0) am_last = (atomicAdd(counter, 1u) == (unsigned)blk.n - 1);
+    __syncthreads();
+    if (!am_last) return false;
+    __threadfence();
+    reduce_partials<NQ>(partials, max_blocks, blk.n, out);
     if (threadIdx.x == 0) *counter = 0u;
     return true;
 }

@@ -59,6 +59,7 @@ struct PairArgs {
     int qmod;                  // tickets per launch: pieces + warps of the grid
     int split;                 // pieces per chunk (untiled): warps that share one chunk's entries
     int zero_slots;            // energy slots the launch resets: 1 v_coul k-space and slab parts, 2 v_fluid_wall
+    int defer_sum;             // energies: block partials only; the integrator launch after it adds them up
     int nb[3], rule, wy, nseg, tile_cap, rowmode;
     int half;                 // 1: half list (partner gets -f), 0: full list
     int symmetry, thermostat, dpd_weight, noise, charged, real_in_lj, fsw;
@@ -596,13 +597,17 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
         }
     }
     if (!EN) return;   // no energies this step: nothing to reduce
+    // with defer_sum the grid-wide sum is left to the next kernel (the time
+    // step's integrator, reduce_pair_partials), off this kernel's tail
     if (WALL) {
         double acc[4] = {a.lj_energy_factor * (double)e_lj, a.lj_energy_factor * (double)vir, (double)e_c,
                          (double)e_w};
-        block_sum_commit<4>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_VFF, blk);
+        if (a.defer_sum) block_partials<4>(acc, a.partials, a.max_blocks, blk);
+        else block_sum_commit<4>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_VFF, blk);
     } else {
         double acc[3] = {a.lj_energy_factor * (double)e_lj, a.lj_energy_factor * (double)vir, (double)e_c};
-        block_sum_commit<3>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_VFF, blk);
+        if (a.defer_sum) block_partials<3>(acc, a.partials, a.max_blocks, blk);
+        else block_sum_commit<3>(acc, a.partials, a.max_blocks, a.counter, a.dscal + S_VFF, blk);
     }
 }
 #undef Lx
@@ -787,6 +792,7 @@ int pair_stage_args(mfa_ctx* c, int fuse_wall, void* out, int* grid_out, size_t*
     // at most max_blocks CTAs (the warps then take several pieces each)
     a.split = c->pair_tiled ? 1 : c->pair_split;
     a.zero_slots = 0;
+    a.defer_sum = 0;
     const long long npiece = (long long)((c->n + 31) / 32) * a.split;
     const int nwarp = c->pair_block / 32;
     int grid = c->pair_tiled ? c->nb[1] * c->nb[2] : (int)((npiece + nwarp - 1) / nwarp);
@@ -830,12 +836,16 @@ int launch_pair_grouped(int prec, int k, int block, int ft, const void* dargs, c
     return MFA_OK;
 }
 
-int launch_pair(mfa_ctx* c, int fuse_wall, int zero_slots) {
+int launch_pair(mfa_ctx* c, int fuse_wall, int zero_slots, int defer_sum) {
     PairArgs a;
     int grid, ft;
     size_t smem;
     TRY_(pair_stage_args(c, fuse_wall, &a, &grid, &smem, &ft));
     a.zero_slots = zero_slots;
+    a.defer_sum = defer_sum;
+    // the integrator launch that follows adds up the block partials
+    c->pair_sum_nblk = defer_sum ? grid : 0;
+    c->pair_sum_nq = (ft & FT_WALL) ? 4 : 3;
     const int rc = c->prec == MFA_MIXED ? launch_r<float>(c->pair_tpp, ft, a, nullptr, grid, c->pair_block, smem, c->st)
                                         : launch_r<double>(c->pair_tpp, ft, a, nullptr, grid, c->pair_block, smem, c->st);
     if (rc != MFA_OK) return rc;

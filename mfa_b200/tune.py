@@ -74,7 +74,10 @@ def autotune(system, steps: int = 300) -> dict:
     return {"skin": cells, "pair_shape": shape, "skin_for_shape": cells2}
 
 
-def _set_shape(system, k, block, tiled, queue, split):
+def set_shape(system, k, block, tiled, queue, split):
+    """The pair kernel's launch shape on `system`: list entries per lane and
+    round, threads per block, tiled or not, work-queue CTAs per SM (untiled;
+    0: static) and pieces per chunk (untiled)."""
     system.set_pair_shape(k, block, tiled)
     system.set_pair_queue(0 if tiled else queue)
     system.set_pair_split(1 if tiled else split)
@@ -88,14 +91,14 @@ def tune_pair_shape(system, steps: int = 300, candidates=CANDIDATES, splits=SPLI
     split0 = system.pair_split()
     timings = {}
     for k, block, tiled, queue in candidates:
-        _set_shape(system, k, block, tiled, queue, split0)
+        set_shape(system, k, block, tiled, queue, split0)
         timings[(k, block, tiled, queue, 1 if tiled else split0)] = _time(system, steps, repeats)
     untiled = [c for c in timings if not c[2]]
     if untiled:
         k, block, _, queue, _ = min(untiled, key=timings.get)
         for split in splits:
             if (k, block, False, queue, split) not in timings:
-                _set_shape(system, k, block, False, queue, split)
+                set_shape(system, k, block, False, queue, split)
                 timings[(k, block, False, queue, split)] = _time(system, steps, repeats)
-    _set_shape(system, *min(timings, key=timings.get))
+    set_shape(system, *min(timings, key=timings.get))
     return timings

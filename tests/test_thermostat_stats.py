@@ -17,7 +17,12 @@ to decorrelate and 20,000 sampled steps):
     within 3.5 % (the scheme's own bias at dt = 0.005 is about +2 %);
   * the radial distribution function g(r) on 0.7 <= r < 2.5 (36 bins) from 100
     snapshots: block errors from 4 blocks, every bin within 5 combined errors
-    and chi^2 per bin below 2.5;
+    and chi^2 per bin below 3.5.  With 4 blocks a side each bin's combined
+    error has about 6 degrees of freedom, so z is close to Student's t(6):
+    E[z^2] = 1.5, and the mean over ~30 bins (correlated within a snapshot)
+    spreads by 0.6 or more; 3.5 is over three such spreads above 1.5 (values
+    seen: 0.7 to 2.8 over repeated runs, the GPU trajectory differing from run
+    to run with the order of its force reductions);
   * the radius of gyration (observation.f90:248-258) of each of the 100
     chains, averaged over the 100 snapshots: the chain-by-chain differences
     average to zero within 4 standard errors (paired test; both runs start
@@ -120,7 +125,7 @@ def test_temperature_rdf_and_rg_agree_with_the_reference_noise_within_statistica
     ok = (go > 0.05) | (gg > 0.05)
     z = (go - gg)[ok] / np.maximum(np.hypot(sgo, sgg)[ok], 1e-3)
     assert np.abs(z).max() < 5.0, z
-    assert (z ** 2).mean() < 2.5, (z ** 2).mean()
+    assert (z ** 2).mean() < 3.5, (z ** 2).mean()
     assert go.max() > 1.5 and gg.max() > 1.5        # the first shell is resolved
 
     d = RGo.mean(axis=0) - RGg.mean(axis=0)          # per chain
