@@ -517,7 +517,9 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
             }
 #pragma unroll
             for (int u = 0; u < K; ++u) {
-                if (jx[u] >= 0 && own_w[ol[u]] == 0) jx[u] = -1;   // owner outside this CTA's row
+                // owner outside this CTA's row (tiled: a chunk may straddle two
+                // rows; untiled, every listed owner is one of the piece's lanes)
+                if (tile && jx[u] >= 0 && own_w[ol[u]] == 0) jx[u] = -1;
                 if (jx[u] >= 0) {
                     if (tile) {
                         // list entries are slots; find the staged run holding the slot
@@ -545,7 +547,7 @@ __device__ __forceinline__ void pair_body(const PairArgs& a, Blk blk) {
                     if (a.symmetry == 1) dz = mimg(dz, Lz, iLz);
                     r2 = dx * dx + dy * dy + dz * dz;
                     wj = wbits(pj[u].w);
-                    const int rowo = ((own_w[ol[u]] & 0xff) - 1) * T8 - 1;
+                    const int rowo = ((wbits(po.w) & 0xff) - 1) * T8 - 1;   // the owner's type
                     keep = r2 < s_rc2[rowo + (wj & 0xff)] || (QSEP && r2 < ewrc2);
                 }
                 const unsigned mask = __ballot_sync(0xffffffffu, keep);
