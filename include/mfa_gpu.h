@@ -444,7 +444,11 @@ int mfa_trajectory_observable(mfa_ctx* ctx, int32_t nsteps, double* J);
  * need ewald_k(0) first, else MFA_ERR_STATE), FENE, bending and the 9-3 walls;
  * the Ewald parameters and k_bend are not among the parameters.  Systems with
  * the force switch-on, WALL 3/4, melt chains or DPD_VV return
- * MFA_ERR_UNSUPPORTED.  The state advances by nsteps. */
+ * MFA_ERR_UNSUPPORTED.  The state advances by nsteps.  The call's device
+ * workspace (checkpoints, one segment's states, adjoint vectors) and its
+ * captured sequences stay with the context for the next call of the same
+ * nsteps and every (freed by mfa_finalize, or rebuilt when the context's
+ * cells, list capacity, launch shapes or energy log change). */
 int mfa_adjoint(mfa_ctx* ctx, int32_t nsteps, int32_t every, double* out7);
 
 /* ---------------- binning without device allocation ---------------- */

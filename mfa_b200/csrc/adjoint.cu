@@ -607,6 +607,36 @@ int mfa_trajectory_observable(mfa_ctx* c, int32_t nsteps, double* J) {
     return mfa_sync(c);
 }
 
+}  // extern "C"
+
+// mfa_adjoint's device workspace and its four captured sequences, kept on the
+// context for the next call with the same length and checkpoint interval: a
+// repeated call (optimisation loops call it with the same S and K) then
+// allocates and captures nothing.  Dropped when the context's graphs are (list
+// capacity, cells, launch shapes, energy log), when what the sequences point
+// to moves, after a failed call, and at mfa_finalize.
+struct AdjCache {
+    int S, K;
+    unsigned long long gen;
+    const void* key[4];
+    size_t sizes[10];
+    void* bufs[10];
+    cudaGraphExec_t gx[4];
+    bool captured;
+};
+
+void adj_cache_free(mfa_ctx* c) {
+    AdjCache* ac = (AdjCache*)c->adj_cache;
+    if (!ac) return;
+    cudaStreamSynchronize(c->st);
+    for (cudaGraphExec_t g : ac->gx) if (g) cudaGraphExecDestroy(g);
+    for (void* b : ac->bufs) if (b) cudaFree(b);
+    delete ac;
+    c->adj_cache = nullptr;
+}
+
+extern "C" {
+
 int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
     if (!c || nsteps < 1 || every < 1 || !out) return MFA_ERR_ARGS;
     const mfa_params& p = c->p;
@@ -623,17 +653,30 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
     Work w;
     w.n = n; w.S = nsteps; w.K = every < nsteps ? every : nsteps;
     w.nseg = (nsteps + w.K - 1) / w.K;
-    void* bufs[10] = {nullptr};
     size_t sizes[10] = {(size_t)w.nseg * 3 * n3 * 8, (size_t)w.nseg * n3 * 4, (size_t)(w.K + 1) * n3 * 8,
                         (size_t)w.K * n3 * 8, (size_t)(w.K + 1) * n3 * 4, 6 * n3 * 8, (G_N + 1) * 8,
                         p.charged ? ewald_adj_bytes(c) : 0, (size_t)w.nseg * 8, (size_t)w.K * 8};
+    const void* key[4] = {c->nbr, c->kvec, c->elog, (const void*)(intptr_t)(c->bin_type + 1)};
+    AdjCache* ac = (AdjCache*)c->adj_cache;
+    if (ac && (ac->S != nsteps || ac->K != w.K || ac->gen != c->graph_gen || memcmp(ac->key, key, sizeof(key)) ||
+               memcmp(ac->sizes, sizes, sizeof(sizes))))
+        adj_cache_free(c);
+    ac = (AdjCache*)c->adj_cache;
     int rc = MFA_OK;
-    for (int k = 0; k < 10 && rc == MFA_OK; ++k)
-        if (sizes[k] && cudaMalloc(&bufs[k], sizes[k]) != cudaSuccess) rc = MFA_ERR_NOMEM;
-    if (rc != MFA_OK) {
-        for (void* b : bufs) if (b) cudaFree(b);
-        return rc;
+    if (!ac) {
+        ac = new AdjCache();
+        ac->S = nsteps; ac->K = w.K; ac->gen = c->graph_gen;
+        memcpy(ac->key, key, sizeof(key));
+        memcpy(ac->sizes, sizes, sizeof(sizes));
+        c->adj_cache = ac;
+        for (int k = 0; k < 10 && rc == MFA_OK; ++k)
+            if (sizes[k] && cudaMalloc(&ac->bufs[k], sizes[k]) != cudaSuccess) rc = MFA_ERR_NOMEM;
+        if (rc != MFA_OK) {
+            adj_cache_free(c);
+            return rc;
+        }
     }
+    void** bufs = ac->bufs;
     w.ck = (double*)bufs[0]; w.ckm = (int32_t*)bufs[1];
     w.seg_r = (double*)bufs[2]; w.seg_u = (double*)bufs[3]; w.seg_m = (int32_t*)bufs[4];
     w.ckstep = (int64_t*)bufs[8]; w.seg_step = (int64_t*)bufs[9];
@@ -720,9 +763,10 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
         }
         return MFA_OK;
     };
-    // Full segments replay captured graphs (one per sequence); a partial last
-    // segment, and any sequence whose capture fails, runs as plain launches.
-    cudaGraphExec_t gx[4] = {nullptr, nullptr, nullptr, nullptr};
+    // Full segments replay captured graphs (one per sequence, kept in the
+    // cache for the next call); a partial last segment, and any sequence whose
+    // capture fails, runs as plain launches.
+    cudaGraphExec_t* gx = ac->gx;
     // MFA_DEBUG=1 in the environment reports a sequence that could not be
     // captured (it then runs as plain launches)
     const bool dbg = getenv("MFA_DEBUG") && getenv("MFA_DEBUG")[0] == '1';
@@ -755,12 +799,13 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
         return fn();
     };
     const bool full_last = nsteps % w.K == 0;
-    if (w.nseg > 1 || full_last) {
+    if (!ac->captured && (w.nseg > 1 || full_last)) {
         capture(0, [&] { return fwd(w.K); });
         capture(1, [&] { return rec(w.K); });
         capture(2, [&] { return bwd(w.K, false); });
         capture(3, [&] { return bwd(w.K, true); });
     }
+    ac->captured = true;
     auto run = [&]() -> int {
         TRY_(mfa_sync(c));
         MFA_CUDA_TRY(cudaMemsetAsync(w.dg, 0, (G_N + 1) * 8, c->st));
@@ -816,8 +861,9 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
     };
     rc = run();
     cudaStreamSynchronize(c->st);
-    for (cudaGraphExec_t g : gx) if (g) cudaGraphExecDestroy(g);
-    for (void* b : bufs) if (b) cudaFree(b);
+    // the run may have grown the list or moved what the sequences point to
+    // (the closing mfa_binning); a failed run leaves nothing for the next call
+    if (rc != MFA_OK) adj_cache_free(c);
     return rc;
 }
 

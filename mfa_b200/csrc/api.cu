@@ -75,6 +75,7 @@ void invalidate_graph(mfa_ctx* c) {
         c->graph_kernels[k] = 0;
     }
     for (int k = 0; k < N_CALL_GRAPHS; ++k) c->call_n[k] = 0;
+    c->graph_gen += 1;   // mfa_adjoint's cached sequences are stale too
 }
 
 // r0(3,n) <-> three contiguous arrays (x[0..n), y[n..2n), z[2n..3n))
@@ -95,6 +96,7 @@ __global__ void k_deinterleave3(const double* __restrict__ aos, double* __restri
 
 void free_all(mfa_ctx* c) {
     invalidate_graph(c);
+    adj_cache_free(c);
     void* ptrs[] = {c->rx, c->mx, c->type, c->mass, c->force, c->pos_s, c->vel_s, c->pos64, c->pos32,
                     c->ids, c->cell_count, c->nbr, c->nnb, c->partials, c->counters, c->dscal,
                     c->dstep, c->kvec, c->rho, c->rho_part, c->qidx, c->elog, c->elog_n, c->tabs,

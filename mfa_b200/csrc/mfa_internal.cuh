@@ -131,6 +131,8 @@ struct mfa_ctx {
     long long call_clock;
     int last_call_n;                      // steps of the previous mfa_step call
     const void* graph_key[4];           // what the captured arguments depend on
+    unsigned long long graph_gen;       // advanced whenever the captured graphs are dropped
+    void* adj_cache;                    // mfa_adjoint's workspace and captured sequences (adjoint.cu)
     int cond_rebuild;                   // rebuilds in conditional graph nodes (1) or early-exit kernels (0)
     int coop_rebuild;                   // captured steps rebuild in one cooperative kernel (1) or as above (0)
     int pair_sum_nblk, pair_sum_nq;     // block partials of the last pair launch left to the next integrator launch
@@ -208,6 +210,7 @@ int launch_bin_grouped(int prec, int stage, const void* dargs, const int* doff, 
                        cudaStream_t st, int* node_count);
 int launch_refresh_sorted(mfa_ctx* c);
 int launch_rebuild_coop(mfa_ctx* c, int rule);
+void adj_cache_free(mfa_ctx* c);
 int rebuild_coop_setup(mfa_ctx* c);
 void rebuild_coop_report(mfa_ctx* c);
 // pair.cu

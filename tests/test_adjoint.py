@@ -93,6 +93,35 @@ def test_adjoint_checkpoint_interval_does_not_change_the_gradient(small_brush):
         assert g2[name] == pytest.approx(g1[name], rel=1e-9, abs=1e-12)
 
 
+def test_repeated_adjoint_calls_reuse_the_cached_sequences(small_brush):
+    """A second mfa_adjoint call of the same length and checkpoint interval on
+    the same context reuses the cached workspace and captured sequences; it
+    equals the first call of a fresh context brought to the same state and
+    step (the DPD noise is keyed by the step) by the forward run, and so does
+    a third call after a new cell grid dropped the context's graphs and the
+    cache with them."""
+    cfg, st = small_brush
+
+    def fresh():
+        g = System(cfg.params, st["r0"], st["v"], cfg.a_type, cfg.mass, a=st["a"], mic=st["mic"], precision=FP64)
+        g.binning()
+        return g
+
+    g = fresh()
+    g.adjoint(40, 10)                      # allocates its workspace, captures its sequences
+    for k in range(2):
+        J2, grad2 = g.adjoint(40, 10)      # steps 40k+40 .. 40k+80
+        f = fresh()
+        f.trajectory_observable(40 * (k + 1))
+        J1, grad1 = f.adjoint(40, 10)
+        f.close()
+        assert J2 == pytest.approx(J1, rel=1e-9), k
+        for name in NAMES:
+            assert grad2[name] == pytest.approx(grad1[name], rel=1e-7, abs=1e-12), (k, name)
+        g.set_cells(list(g.params.n_bin), g.params.skin)
+    g.close()
+
+
 def test_mixed_adjoint_close_to_fp64(small_brush):
     cfg, st = small_brush
     _, g64 = run(cfg, st, cfg.params, FP64, lambda g: g.adjoint(40, 10))
