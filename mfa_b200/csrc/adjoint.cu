@@ -484,16 +484,57 @@ struct Work {
     double* dg;          // G_N + 1 (J)
 };
 
+// One launch for the copies of a state (the time step's sequences would
+// otherwise hold a copy node per array): up to three FP64 blocks of n3
+// values, one int32 block of n3 and one step number; null pointers are
+// skipped.
+struct StateCopy {
+    double* d[3];
+    const double* s[3];
+    int32_t* dm;
+    const int32_t* sm;
+    int64_t* dstep;
+    const int64_t* sstep;
+    size_t n3;
+};
+
+__global__ void k_copy_state(StateCopy a) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n3; i += stride) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            if (a.d[k]) a.d[k][i] = a.s[k][i];
+        if (a.dm) a.dm[i] = a.sm[i];
+    }
+    if (a.dstep && blockIdx.x == 0 && threadIdx.x == 0) *a.dstep = *a.sstep;
+}
+
+int copy_state(mfa_ctx* c, double* d0, const double* s0, double* d1, const double* s1, double* d2,
+               const double* s2, int32_t* dm, const int32_t* sm, int64_t* dstep, const int64_t* sstep) {
+    StateCopy a;
+    a.d[0] = d0; a.s[0] = s0; a.d[1] = d1; a.s[1] = s1; a.d[2] = d2; a.s[2] = s2;
+    a.dm = dm; a.sm = sm; a.dstep = dstep; a.sstep = sstep;
+    a.n3 = (size_t)3 * c->n;
+    const int nb = (int)((a.n3 + T - 1) / T);
+    k_copy_state<<<nb, T, 0, c->st>>>(a);
+    MFA_CUDA_TRY(cudaGetLastError());
+    return MFA_OK;
+}
+
+// The step whose energies the forward steps reduce: dstep[1] = dstep[0] + span
+// (the last step of a run of span steps; the energies of the other steps are
+// not wanted there), or -1 (span < 0: every step, as the subroutine entry
+// points expect).
+__global__ void k_energy_want(int64_t* dstep, long long span) {
+    dstep[1] = span < 0 ? -1 : dstep[0] + span;
+}
+
 int adj_forward_step(mfa_ctx* c, double* sr, double* su, int32_t* sm, double w, double* dJ,
                      int64_t* sstep = nullptr) {
     const int n = c->n;
     TRY_(launch_vv_positions(c, 1, 1));
-    if (sstep) MFA_CUDA_TRY(cudaMemcpyAsync(sstep, c->dstep, 8, cudaMemcpyDeviceToDevice, c->st));
-    if (sr) {
-        MFA_CUDA_TRY(cudaMemcpyAsync(sr, c->rx, (size_t)3 * n * 8, cudaMemcpyDeviceToDevice, c->st));
-        MFA_CUDA_TRY(cudaMemcpyAsync(su, c->vx, (size_t)3 * n * 8, cudaMemcpyDeviceToDevice, c->st));
-        MFA_CUDA_TRY(cudaMemcpyAsync(sm, c->mx, (size_t)3 * n * 4, cudaMemcpyDeviceToDevice, c->st));
-    }
+    if (sr) TRY_(copy_state(c, sr, c->rx, su, c->vx, nullptr, nullptr, sm, c->mx, sstep, c->dstep));
+    else if (sstep) MFA_CUDA_TRY(cudaMemcpyAsync(sstep, c->dstep, 8, cudaMemcpyDeviceToDevice, c->st));
     TRY_(c->coop_rebuild ? launch_rebuild_coop(c, c->bin_type) : launch_rebuild(c, c->bin_type, 1));
     TRY_(launch_pair(c, c->p.symmetry == 0));
     if (c->p.charged) {
@@ -513,12 +554,9 @@ int adj_forward_step(mfa_ctx* c, double* sr, double* su, int32_t* sm, double w, 
 
 int checkpoint_save(mfa_ctx* c, Work& w, int k) {
     const size_t n3 = (size_t)3 * c->n;
-    MFA_CUDA_TRY(cudaMemcpyAsync(w.ck + k * 3 * n3, c->rx, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
-    MFA_CUDA_TRY(cudaMemcpyAsync(w.ck + k * 3 * n3 + n3, c->vx, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
-    MFA_CUDA_TRY(cudaMemcpyAsync(w.ck + k * 3 * n3 + 2 * n3, c->ax, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
-    MFA_CUDA_TRY(cudaMemcpyAsync(w.ckm + k * n3, c->mx, n3 * 4, cudaMemcpyDeviceToDevice, c->st));
-    MFA_CUDA_TRY(cudaMemcpyAsync(w.ckstep + k, c->dstep, 8, cudaMemcpyDeviceToDevice, c->st));
-    return MFA_OK;
+    double* ck = w.ck + k * 3 * n3;
+    return copy_state(c, ck, c->rx, ck + n3, c->vx, ck + 2 * n3, c->ax, w.ckm + k * n3, c->mx, w.ckstep + k,
+                      c->dstep);
 }
 
 // The state of checkpoint k back in the context, and its r and mic in the
@@ -527,16 +565,11 @@ int checkpoint_save(mfa_ctx* c, Work& w, int k) {
 // checks the skin against the last rebuild's positions and rebuilds when due.
 int checkpoint_restore(mfa_ctx* c, Work& w, int k) {
     const size_t n3 = (size_t)3 * c->n;
-    MFA_CUDA_TRY(cudaMemcpyAsync(c->rx, w.ck + k * 3 * n3, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
-    MFA_CUDA_TRY(cudaMemcpyAsync(c->vx, w.ck + k * 3 * n3 + n3, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
-    MFA_CUDA_TRY(cudaMemcpyAsync(c->ax, w.ck + k * 3 * n3 + 2 * n3, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
-    MFA_CUDA_TRY(cudaMemcpyAsync(c->mx, w.ckm + k * n3, n3 * 4, cudaMemcpyDeviceToDevice, c->st));
-    MFA_CUDA_TRY(cudaMemcpyAsync(c->dstep, w.ckstep + k, 8, cudaMemcpyDeviceToDevice, c->st));
-    MFA_CUDA_TRY(cudaMemcpyAsync(w.seg_r + (size_t)w.K * n3, w.ck + k * 3 * n3, n3 * 8, cudaMemcpyDeviceToDevice,
-                                 c->st));
-    MFA_CUDA_TRY(cudaMemcpyAsync(w.seg_m + (size_t)w.K * n3, w.ckm + k * n3, n3 * 4, cudaMemcpyDeviceToDevice,
-                                 c->st));
-    return MFA_OK;
+    const double* ck = w.ck + k * 3 * n3;
+    TRY_(copy_state(c, c->rx, ck, c->vx, ck + n3, c->ax, ck + 2 * n3, c->mx, w.ckm + k * n3, c->dstep,
+                    w.ckstep + k));
+    return copy_state(c, w.seg_r + (size_t)w.K * n3, ck, nullptr, nullptr, nullptr, nullptr, w.seg_m + (size_t)w.K * n3,
+                      w.ckm + k * n3, nullptr, nullptr);
 }
 
 AdjArgs pair_adj_args(mfa_ctx* c, Work& w, const int64_t* step_ptr) {
@@ -597,7 +630,10 @@ int mfa_trajectory_observable(mfa_ctx* c, int32_t nsteps, double* J) {
     if (cudaMalloc((void**)&dJ, 8) != cudaSuccess) return MFA_ERR_NOMEM;
     int rc = MFA_OK;
     if (cudaMemsetAsync(dJ, 0, 8, c->st) != cudaSuccess) rc = MFA_ERR_CUDA;
+    // energies for the run's last step only
+    k_energy_want<<<1, 1, 0, c->st>>>(c->dstep, nsteps);
     for (int s = 0; s < nsteps && rc == MFA_OK; ++s) rc = adj_forward_step(c, nullptr, nullptr, nullptr, 1.0 / nsteps, dJ);
+    k_energy_want<<<1, 1, 0, c->st>>>(c->dstep, -1);
     if (rc == MFA_OK && (cudaMemcpyAsync(J, dJ, 8, cudaMemcpyDeviceToHost, c->st) != cudaSuccess ||
                          cudaStreamSynchronize(c->st) != cudaSuccess))
         rc = MFA_ERR_CUDA;
@@ -706,9 +742,8 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
     auto bwd = [&](int len, bool first_seg) -> int {
         for (int j = len - 1; j >= 0; --j) {
             const double* r1 = w.seg_r + j * n3;
-            MFA_CUDA_TRY(cudaMemcpyAsync(c->rx, r1, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
-            MFA_CUDA_TRY(cudaMemcpyAsync(c->vx, w.seg_u + j * n3, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
-            MFA_CUDA_TRY(cudaMemcpyAsync(c->mx, w.seg_m + j * n3, n3 * 4, cudaMemcpyDeviceToDevice, c->st));
+            TRY_(copy_state(c, c->rx, r1, c->vx, w.seg_u + j * n3, nullptr, nullptr, c->mx, w.seg_m + j * n3,
+                            nullptr, nullptr));
             TRY_(launch_check_skin(c));
             TRY_(c->coop_rebuild ? launch_rebuild_coop(c, c->bin_type) : launch_rebuild(c, c->bin_type, 1));
             TRY_(launch_refresh_sorted(c));
@@ -810,6 +845,9 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
         TRY_(mfa_sync(c));
         MFA_CUDA_TRY(cudaMemsetAsync(w.dg, 0, (G_N + 1) * 8, c->st));
         MFA_CUDA_TRY(cudaMemsetAsync(adj, 0, 6 * n3 * 8, c->st));
+        // the forward and recomputed steps reduce energies for the
+        // trajectory's last step only (the adjoint needs none)
+        k_energy_want<<<1, 1, 0, c->st>>>(c->dstep, nsteps);
         // forward pass with checkpoints and the observable
         for (int seg = 0; seg < w.nseg; ++seg) {
             const int len = seg * w.K + w.K <= nsteps ? w.K : nsteps - seg * w.K;
@@ -849,6 +887,7 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
         MFA_CUDA_TRY(cudaMemcpyAsync(c->ax, fin_rva.data() + 2 * n3, n3 * 8, cudaMemcpyHostToDevice, c->st));
         MFA_CUDA_TRY(cudaMemcpyAsync(c->mx, fin_m.data(), n3 * 4, cudaMemcpyHostToDevice, c->st));
         MFA_CUDA_TRY(cudaMemcpyAsync(c->dstep, &fin_step, 8, cudaMemcpyHostToDevice, c->st));
+        k_energy_want<<<1, 1, 0, c->st>>>(c->dstep, -1);
         MFA_CUDA_TRY(cudaStreamSynchronize(c->st));
         TRY_(mfa_binning(c));
         double h[G_N + 1];
@@ -863,7 +902,10 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
     cudaStreamSynchronize(c->st);
     // the run may have grown the list or moved what the sequences point to
     // (the closing mfa_binning); a failed run leaves nothing for the next call
-    if (rc != MFA_OK) adj_cache_free(c);
+    if (rc != MFA_OK) {
+        k_energy_want<<<1, 1, 0, c->st>>>(c->dstep, -1);   // every step's energies again
+        adj_cache_free(c);
+    }
     return rc;
 }
 

@@ -149,7 +149,8 @@ int rebuild_abi(mfa_ctx* c, int rule) {
             long long cap = want + want / 8 + 32;
             if (cap > pair_tile_limit(c)) cap = pair_tile_limit(c);
             TRY(pair_set_shape(c, c->pair_tpp, c->pair_block, (int)cap));
-            invalidate_graph(c);
+            // only tiled launches size their shared memory by the tile
+            if (c->pair_tiled) invalidate_graph(c);
         }
         return first_error(bits);
     }
