@@ -521,6 +521,77 @@ int copy_state(mfa_ctx* c, double* d0, const double* s0, double* d1, const doubl
     return MFA_OK;
 }
 
+// The backward step's state in one pass: r', u and mic of a segment slot back
+// in the context, the skin check against the list's snapshot
+// (check_skin.f90:8-21, with the integrator's rounding) and the cell-sorted
+// records the pair kernels read (a rebuild, when the check trips, rewrites
+// them after this).
+struct RestoreArgs {
+    const double *sr, *su;
+    const int32_t* sm;
+    double *rx, *vx;
+    int32_t* mx;
+    const double *ox, *oy, *oz;
+    const int32_t* slot;
+    const int32_t* type;
+    const double* q;
+    void* pos_s;
+    void* vel_s;
+    int32_t* flags;
+    double L[3], skin_lim;
+    int n;
+};
+
+template <typename R4>
+__global__ void k_adj_restore(RestoreArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const size_t n = (size_t)a.n;
+    double r[3], u[3];
+    int m[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        r[d] = a.sr[d * n + i];
+        u[d] = a.su[d * n + i];
+        m[d] = a.sm[d * n + i];
+        a.rx[d * n + i] = r[d];
+        a.vx[d * n + i] = u[d];
+        a.mx[d * n + i] = m[d];
+    }
+    // the snapshot holds r0_old + mic_old * L
+    const double o[3] = {a.ox[i], a.oy[i], a.oz[i]};
+    double dd[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) dd[d] = __dsub_rn(__dsub_rn(o[d], r[d]), __dmul_rn((double)m[d], a.L[d]));
+    const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dd[0], dd[0]), __dmul_rn(dd[1], dd[1])), __dmul_rn(dd[2], dd[2]));
+    if (r2 > a.skin_lim) a.flags[F_SKIN] = 1;
+    const int s = a.slot[i];
+    R4 p;
+    p.x = r[0]; p.y = r[1]; p.z = r[2];
+    packw(p, i, a.type[i]);
+    ((R4*)a.pos_s)[s] = p;
+    R4 v;
+    v.x = u[0]; v.y = u[1]; v.z = u[2]; v.w = a.q ? a.q[i] : 0.0;
+    ((R4*)a.vel_s)[s] = v;
+}
+
+int launch_adj_restore(mfa_ctx* c, const double* sr, const double* su, const int32_t* sm) {
+    RestoreArgs a;
+    a.sr = sr; a.su = su; a.sm = sm;
+    a.rx = c->rx; a.vx = c->vx; a.mx = c->mx;
+    a.ox = c->ox; a.oy = c->oy; a.oz = c->oz;
+    a.slot = c->slot; a.type = c->type; a.q = c->p.charged ? c->q : nullptr;
+    a.pos_s = c->pos_s; a.vel_s = c->vel_s; a.flags = c->dflags;
+    for (int d = 0; d < 3; ++d) a.L[d] = c->p.boundary[d];
+    a.skin_lim = (c->p.skin / 2.0) * (c->p.skin / 2.0);
+    a.n = c->n;
+    const int nb = (c->n + T - 1) / T;
+    if (c->prec == MFA_MIXED) k_adj_restore<float4><<<nb, T, 0, c->st>>>(a);
+    else k_adj_restore<double4><<<nb, T, 0, c->st>>>(a);
+    MFA_CUDA_TRY(cudaGetLastError());
+    return MFA_OK;
+}
+
 // The step whose energies the forward steps reduce: dstep[1] = dstep[0] + span
 // (the last step of a run of span steps; the energies of the other steps are
 // not wanted there), or -1 (span < 0: every step, as the subroutine entry
@@ -742,11 +813,10 @@ int mfa_adjoint(mfa_ctx* c, int32_t nsteps, int32_t every, double* out) {
     auto bwd = [&](int len, bool first_seg) -> int {
         for (int j = len - 1; j >= 0; --j) {
             const double* r1 = w.seg_r + j * n3;
-            TRY_(copy_state(c, c->rx, r1, c->vx, w.seg_u + j * n3, nullptr, nullptr, c->mx, w.seg_m + j * n3,
-                            nullptr, nullptr));
-            TRY_(launch_check_skin(c));
+            // state, skin check and sorted records in one pass; then the
+            // rebuild when due
+            TRY_(launch_adj_restore(c, r1, w.seg_u + j * n3, w.seg_m + j * n3));
             TRY_(c->coop_rebuild ? launch_rebuild_coop(c, c->bin_type) : launch_rebuild(c, c->bin_type, 1));
-            TRY_(launch_refresh_sorted(c));
             k_adj_prep<<<nb, T, 0, c->st>>>(n, w.rho, w.nu, w.alpha, c->inv_mass, 0.5 * dt, p.pin_heads,
                                             p.n_chain * p.n_mon, p.n_mon > 0 ? p.n_mon : 1, w.lamF, w.lamU,
                                             w.lamR);
